@@ -1,0 +1,209 @@
+/*
+ * mh_darcy.h -- C ABI of the B200 mixed-hybrid (MH) Darcy flow library.
+ *
+ * The library replaces the MH Darcy hot path of Flow123d 1.7:
+ *   assembly of the saddle-point system  (src/flow/darcy_flow_mh.cc:525-694,
+ *                                          src/flow/mh_fe_values.cc:34-514)
+ *   first Schur complement (face fluxes)  (darcy_flow_mh.cc:1009-1090, src/la/schur.cc:566-611)
+ *   second Schur complement (pressures)   (darcy_flow_mh.cc:1095-1131)
+ *   iterative solve of the edge system    (src/la/solve.cc:316-466)
+ *   back-substitution                     (src/la/schur.cc:714-773, darcy_flow_mh.cc:414-415)
+ *   unsteady time term                    (darcy_flow_mh.cc:1614-1827)
+ * on one GPU.  All entry points are plain C: pointers, sizes and int status codes.
+ * Caller-owned host arrays are copied in and never retained; device memory is owned
+ * by the opaque handle.  Every function returns MH_OK (0), a positive "solved with a
+ * caveat" code, or a negative error code; nothing aborts.
+ *
+ * Numbering conventions follow the reference exactly:
+ *   - elements in input order; element sides numbered element-major
+ *     (MH_DofHandler::reinit, src/flow/mh_dofhandler.cc:12-24);
+ *   - side i of a simplex is the face opposite node i for tetrahedra and
+ *     {0,1},{1,2},{0,2} for triangles (src/mesh/ref_element.cc:51-76);
+ *   - edges (groups of coincident sides) and boundary objects in the creation order of
+ *     Mesh::make_neighbours_and_edges (src/mesh/mesh.cc:343-500);
+ *   - the solution vector is [side fluxes | element pressures | edge pressures]
+ *     (darcy_flow_mh.cc:337-355, mh_dofhandler.cc:37-50).
+ */
+#ifndef MH_DARCY_H
+#define MH_DARCY_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define MH_OK               0
+#define MH_NOT_CONVERGED    1   /* max_it reached; the result is the last iterate        */
+#define MH_FELL_BACK        2   /* converged, but only after falling back to plain PCG   */
+#define MH_ERR_INVALID     -1   /* bad argument, inconsistent mesh                        */
+#define MH_ERR_SINGULAR    -2   /* singular local MH block (|det| < DBL_MIN/DBL_EPSILON)  */
+#define MH_ERR_CUDA        -3   /* CUDA runtime error or no device                        */
+#define MH_ERR_STATE       -4   /* call out of order (e.g. solve before set_coeffs)       */
+#define MH_ERR_NOMEM       -5
+#define MH_ERR_NONFINITE   -6   /* NaN/Inf in coefficients or in the iteration            */
+#define MH_ERR_TOPOLOGY    -7   /* the mesh violates a rule of the reference topology     */
+#define MH_ERR_BREAKDOWN   -8   /* CG breakdown (p'Sp <= 0): system not SPD               */
+
+/* ---- boundary condition types (DarcyFlowMH::EqData::BC_Type, darcy_flow_mh.cc:81-87) --- */
+#define MH_BC_NONE       0
+#define MH_BC_DIRICHLET  1
+#define MH_BC_NEUMANN    2
+#define MH_BC_ROBIN      3
+
+/* ---- solver methods ------------------------------------------------------------------ */
+#define MH_SOLVER_PCG64     0   /* Jacobi-preconditioned CG, all FP64                     */
+#define MH_SOLVER_IR32      1   /* FP32 inner CG inside FP64 iterative refinement         */
+#define MH_SOLVER_CHEB64    2   /* Chebyshev-Jacobi preconditioned CG, FP64                */
+#define MH_SOLVER_FCG_LEARNED 3 /* learned preconditioner inside flexible CG (IR outer)   */
+
+typedef struct mh_handle mh_handle;
+typedef struct mh_mesh mh_mesh;
+
+/* Flat description of a mixed 1D/2D/3D simplicial mesh.  Element and boundary-element
+ * node lists have 4 slots per element; unused slots are -1.  Boundary elements are the
+ * explicit ones of a gmsh file (regions whose name starts with '.'); implicit boundary
+ * objects are created for every outer side without one, as in mesh.cc:445-472. */
+typedef struct mh_mesh_desc {
+    int64_t        n_nodes;
+    const double  *node_xyz;     /* [n_nodes*3]                                   */
+    int64_t        n_elements;
+    const int32_t *el_dim;       /* [n_elements], 1..3                            */
+    const int32_t *el_nodes;     /* [n_elements*4]                                */
+    int64_t        n_bc_elements;
+    const int32_t *bc_dim;       /* [n_bc_elements], 0..2 (may be NULL if 0)      */
+    const int32_t *bc_nodes;     /* [n_bc_elements*4]                             */
+} mh_mesh_desc;
+
+typedef struct mh_sizes {
+    int64_t n_nodes, n_elements, n_sides, n_edges, n_boundaries, n_neighbours;
+    int64_t n_el_dim[4];         /* elements per dimension                       */
+    int64_t mh_size;             /* n_sides + n_elements + n_edges               */
+    int64_t schur_nnz;           /* nonzeros of the edge (second Schur) system   */
+    int64_t sell_slots;          /* stored SELL-C-sigma slots incl. padding       */
+    int64_t n_rows_padded;       /* solver rows incl. per-instance padding        */
+    int64_t n_instances;
+} mh_sizes;
+
+/* Element-wise coefficient fields (EqData, darcy_flow_mh.cc:154-183).  NULL selects the
+ * reference default: anisotropy = I, cross_section = 1, conductivity = 1, sigma = 1,
+ * water_source_density = 0, storativity = 1. */
+typedef struct mh_coeffs {
+    const double *conductivity;          /* [n_elements]                          */
+    const double *anisotropy;            /* [n_elements*9] row-major 3x3 tensor   */
+    const double *cross_section;         /* [n_elements]                          */
+    const double *sigma;                 /* [n_elements] (used on lower-dim elem) */
+    const double *water_source_density;  /* [n_elements]                          */
+    const double *storativity;           /* [n_elements] (unsteady only)          */
+} mh_coeffs;
+
+/* Boundary data per boundary object (assembly_steady_mh_matrix, darcy_flow_mh.cc:570-596).
+ * Arrays may be NULL when no boundary uses them. */
+typedef struct mh_bc {
+    const int32_t *type;          /* [n_boundaries] MH_BC_*                        */
+    const double  *pressure;      /* Dirichlet / Robin pressure                    */
+    const double  *flux;          /* Neumann flux                                  */
+    const double  *robin_sigma;   /* Robin transfer coefficient                    */
+} mh_bc;
+
+typedef struct mh_solve_opts {
+    int32_t method;         /* MH_SOLVER_*                                          */
+    int32_t max_it;         /* cap on (inner) iterations, default 20000              */
+    double  r_tol;          /* stop when ||b - S x||_2 <= max(r_tol*||b||_2, a_tol)  */
+    double  a_tol;
+    int32_t use_initial_guess;  /* start from the current edge pressures             */
+    int32_t cheb_degree;    /* MH_SOLVER_CHEB64: polynomial degree (default 4)       */
+    double  inner_rtol;     /* MH_SOLVER_IR32/FCG: inner relative tolerance (1e-5)   */
+    int32_t inner_max_it;   /* inner iteration cap per refinement step (2000)        */
+    int32_t iters_per_graph;/* CG iterations per captured CUDA graph launch (16)     */
+    int32_t reserved[7];
+} mh_solve_opts;
+
+typedef struct mh_solve_stats {
+    int32_t status;
+    int32_t iterations;         /* total Krylov iterations (inner ones for IR)       */
+    int32_t outer_iterations;   /* refinement steps (IR/FCG), restarts (PCG)          */
+    int32_t fell_back;          /* 1 if the flexible iteration stalled -> plain PCG   */
+    double  rel_residual;       /* final FP64 true residual ||b-Sx||/||b||            */
+    double  ms_assembly;        /* device time of assembly + Schur elimination        */
+    double  ms_solve;           /* device time of the Krylov solve                    */
+    double  ms_backsub;         /* device time of back-substitution                   */
+    double  reserved[4];
+} mh_solve_stats;
+
+/* ---- library ---------------------------------------------------------------------- */
+const char *mh_version(void);
+const char *mh_status_string(int status);
+/* 1 if a CUDA device usable by the library is present, else 0. */
+int mh_device_available(void);
+/* Message of the last error recorded on a handle (empty if none). */
+const char *mh_last_error(const mh_handle *h);
+
+/* ---- synthetic meshes: unit cube of n^3 cubes, 6 Kuhn tetrahedra each -------------- */
+/* Fracture planes: axis (0=x,1=y,2=z) at grid index; each adds the 2n^2 coincident face
+ * triangles.  Channels: 1D segments along axis `line_axis` through grid indices
+ * (line_a, line_b) of the two other axes in increasing axis order.  Element order:
+ * tetrahedra (cube-major, x fastest), then triangles plane by plane, then segments. */
+int mh_cube_mesh_create(int32_t n, int32_t n_planes, const int32_t *plane_axis,
+                        const int32_t *plane_index, int32_t n_lines, const int32_t *line_axis,
+                        const int32_t *line_a, const int32_t *line_b, mh_mesh **out);
+int mh_mesh_describe(const mh_mesh *m, mh_mesh_desc *desc);
+void mh_mesh_destroy(mh_mesh *m);
+
+/* ---- the MH system (DarcyFlowMH_Steady, darcy_flow_mh.cc:249-433) ------------------- */
+/* Builds edges, boundaries and VB neighbours on the host (Mesh::setup_topology,
+ * mesh.cc:227-245, 343-500, 660-685) and uploads mesh, connectivity and the Schur
+ * pattern to the current CUDA device.  With no device the handle still builds the
+ * topology (mh_get_sizes/mh_get_topology work) and compute calls return MH_ERR_CUDA. */
+int mh_create(const mh_mesh_desc *mesh, mh_handle **out);
+void mh_destroy(mh_handle *h);
+int mh_get_sizes(const mh_handle *h, mh_sizes *out);
+/* Topology export (any pointer may be NULL):
+ *   el_side_start [n_elements+1]  first global side of each element
+ *   side_edge     [n_sides]       edge of each side
+ *   side_bdr      [n_sides]       boundary object of each side or -1
+ *   bdr_bc_element[n_boundaries]  explicit boundary element or -1 (implicit)
+ *   bdr_edge      [n_boundaries]
+ *   ngh_element   [n_neighbours]  lower-dimensional element of a VB neighbour
+ *   ngh_edge      [n_neighbours]  edge holding the single higher-dimensional side
+ *   ngh_side      [n_neighbours]  that side                                         */
+int mh_get_topology(const mh_handle *h, int32_t *el_side_start, int32_t *side_edge,
+                    int32_t *side_bdr, int32_t *bdr_bc_element, int32_t *bdr_edge,
+                    int32_t *ngh_element, int32_t *ngh_edge, int32_t *ngh_side);
+
+int mh_set_coeffs(mh_handle *h, const mh_coeffs *c);
+int mh_set_bc(mh_handle *h, const mh_bc *bc);
+
+/* K1: local RT0 matrices, FP64 inversion, both Schur eliminations and the SELL scatter
+ * (assembly_steady_mh_matrix + make_schur1 + make_schur2). */
+int mh_assemble(mh_handle *h);
+/* Krylov solve of the edge system followed by back-substitution (K2-K5 + K4). */
+int mh_solve(mh_handle *h, const mh_solve_opts *opts, mh_solve_stats *stats);
+/* Copies the MH solution [sides | elements | edges] (length mh_size) to the host. */
+int mh_get_solution(const mh_handle *h, double *out, int64_t len);
+/* Same, into a device buffer (a plain device pointer). */
+int mh_get_solution_device(const mh_handle *h, double *dev_out, int64_t len);
+
+/* Export of the assembled edge system in CSR form (rows = edges), for checking.  The
+ * values are the reference's schur2 matrix after scale(-1) (darcy_flow_mh.cc:1128-1130),
+ * rhs likewise.  row_ptr [n_edges+1], col/val [schur_nnz], rhs [n_edges]. */
+int mh_get_schur_system(const mh_handle *h, int32_t *row_ptr, int32_t *col, double *val,
+                        double *rhs);
+
+/* Fills opts with defaults. */
+void mh_solve_opts_default(mh_solve_opts *opts);
+
+/* ---- unsteady MH (DarcyFlowMH_Unsteady, darcy_flow_mh.cc:1601-1675) ----------------- */
+/* lumped = 0: MH time term on element rows (setup_time_term :1614-1658);
+ * lumped = 1: LMH time term on edge rows (DarcyFlowLMH_Unsteady :1695-1827).
+ * init_pressure [n_elements] may be NULL (zero). */
+int mh_unsteady_init(mh_handle *h, int32_t lumped, double dt, const double *init_pressure);
+/* One implicit-Euler step of length dt with the boundary data currently set. */
+int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts,
+                     mh_solve_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MH_DARCY_H */

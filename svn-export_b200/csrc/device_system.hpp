@@ -1,0 +1,111 @@
+// Device-side data structures shared by the host runtime (mh_handle.cpp) and the CUDA
+// translation units.  Plain structs of device pointers; no ownership here.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mh_types.hpp"
+
+namespace mh {
+
+constexpr int kSliceRows = 32;       // SELL-C-sigma chunk height C (one warp, one row per lane)
+constexpr int kWarpsPerBlock = 8;    // 256-thread blocks
+constexpr int kBlockThreads = kSliceRows * kWarpsPerBlock;
+
+// Per-instance Krylov control block.  One per independent system (one for a single
+// mesh, one per realisation in a batch).  Written only by the last block of each kernel
+// for that instance (ticket pattern), read by all blocks at kernel entry.
+struct InstCtl {
+    double rho;        // r.r of the current residual (scaled space)
+    double alpha, beta;
+    double rr0;        // r.r at (re)start
+    double tol2;       // stop when r.r <= tol2
+    double rr;         // last r.r
+    double scale;      // IR: norm of the outer residual the inner solve was started from
+    double aux[3];
+    int32_t iter;      // iterations of the current Krylov run
+    int32_t max_it;
+    int32_t done;      // 1 once converged, stopped or broken down
+    int32_t status;    // 0 converged, 1 max_it, -8 breakdown, -6 non-finite
+    int32_t tile_begin, tile_end;
+    uint32_t ticket;
+    int32_t pad;
+};
+
+// SELL-C-sigma matrix view in solver-row space (rows padded per instance to whole tiles).
+template <typename T> struct SellView {
+    int64_t n_rows;
+    const int64_t *slice_off;  // [n_slices+1] first slot of each 32-row slice
+    const int32_t *col;        // [slots]
+    const T *val;              // [slots]
+};
+
+// Handle-owned device buffers of the edge system and the Krylov work vectors.
+struct DevSystem {
+    int64_t n_rows = 0, n_slices = 0, n_tiles = 0, n_slots = 0;
+    int32_t rows_per_thread = 1;     // R: slices per warp per tile
+    int32_t n_inst = 0;
+    int64_t *slice_off = nullptr;
+    int32_t *col = nullptr;
+    double *val_raw = nullptr;       // S  (reference schur2 after scale(-1))
+    double *val64 = nullptr;         // D^-1/2 S D^-1/2
+    float *val32 = nullptr;          // same in FP32
+    int32_t *diag_slot = nullptr;    // [n_rows]
+    int32_t *row_edge = nullptr;     // [n_rows] edge of each solver row or -1 (padding)
+    int32_t *edge_row = nullptr;     // [n_edges]
+    int32_t *tile_inst = nullptr;    // [n_tiles]
+    double *dsq = nullptr;           // sqrt(diag S) per row
+    double *b = nullptr;             // rhs (original scaling)
+    double *bh = nullptr;            // D^-1/2 b
+    // FP64 Krylov vectors (scaled space)
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *w = nullptr;
+    // FP32 inner vectors
+    float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
+    double *partial = nullptr;       // [n_tiles * 4]
+    InstCtl *ctl = nullptr;          // [n_inst]
+    int32_t *n_done = nullptr;       // instances finished in the current Krylov run
+    double *inst_sums = nullptr;     // [n_inst * 4] results of the residual kernel
+    uint32_t *sum_ticket = nullptr;  // [n_inst]
+};
+
+// Contribution maps from element-local blocks to SELL slots / solver rows.
+struct DevAssembly {
+    int64_t n_blk = 0, n_rhs_loc = 0;
+    int64_t *blk_off = nullptr;      // [n_el]
+    int64_t *rhs_off = nullptr;      // [n_el]
+    double *blk = nullptr;           // element-local S2 blocks, m x m row-major
+    double *rhs_loc = nullptr;       // element-local r2 entries
+    int32_t *slot_cstart = nullptr;  // [n_slots+1]
+    int32_t *slot_cidx = nullptr;    // [n_blk]
+    int32_t *row_cstart = nullptr;   // [n_rows+1]
+    int32_t *row_cidx = nullptr;     // [n_rhs_loc]
+    int32_t *dim_list[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t dim_count[4] = {0, 0, 0, 0};
+    int32_t *status = nullptr;       // bit 0: singular local matrix, bit 1: non-finite value
+};
+
+// ---- launchers (assembly.cu) ----
+cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mode, cudaStream_t s);
+cudaError_t launch_gather(const DevAssembly &a, const DevSystem &sys, int mode, cudaStream_t s);
+cudaError_t launch_scale(const DevSystem &sys, int matrix, cudaStream_t s);
+cudaError_t launch_backsub(const ElemData &d, const DevAssembly &a, const DevSystem &sys, double *sol,
+                           int64_t n_sides, int64_t n_el, int64_t n_edges, cudaStream_t s);
+
+// x = lambda * dsq (initial guess in scaled space; padding rows 0).
+cudaError_t launch_scale_in(const DevSystem &sys, const double *lambda, cudaStream_t s);
+
+// ---- launchers (solver.cu) ----
+// Krylov kernels on the scaled system; `prec` = 64 or 32.
+// FP64 CG start from sys.x: tol2 = max(rtol2 * |bh|^2, atol2); with use_active only the
+// instances flagged in inst_sums[4i+3] run.
+cudaError_t launch_cg_init(const DevSystem &sys, double rtol2, double atol2, int max_it, int use_active,
+                           cudaStream_t s);
+cudaError_t launch_cg_iteration(const DevSystem &sys, int prec, cudaStream_t s);
+// r = bh - S64 x (FP64) and per-instance sums {sum r^2, sum d r^2, sum d bh^2}.
+cudaError_t launch_residual64(const DevSystem &sys, cudaStream_t s);
+// IR helpers: start an FP32 inner solve from r; fold its correction back into x.
+cudaError_t launch_ir_start(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
+cudaError_t launch_ir_correct(const DevSystem &sys, cudaStream_t s);
+cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s);
+
+}  // namespace mh

@@ -1,0 +1,886 @@
+// Host runtime behind the C ABI of mh_darcy.h: owns the mesh topology, the device buffers,
+// the CUDA stream and the captured Krylov graphs, and drives the kernels of assembly.cu and
+// solver.cu.  It plays the role of DarcyFlowMH_Steady::update_solution with n_schurs = 2
+// (src/flow/darcy_flow_mh.cc:375-433) and of make_schur0/1/2 + solve_system + resolve.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device_system.hpp"
+#include "mh_darcy.h"
+#include "system_build.hpp"
+#include "topology.hpp"
+
+struct mh_mesh {
+    mh::MeshData m;
+};
+
+struct mh_handle {
+    mh::MeshData mesh;
+    mh::Topology topo;
+    mh::HostSystem hs;
+    std::vector<int32_t> ngh_hi_el;
+    std::vector<double> ngh_meas;
+    bool device = false;
+    int device_id = -1;
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocs;
+    mh::ElemData ed{};
+    mh::DevSystem sys{};
+    mh::DevAssembly as{};
+    double *sol = nullptr, *sol_prev = nullptr;
+    double *d_aniso = nullptr;
+    bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
+    int time_mode = 0;
+    double dt = 0.0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_iters[2] = {0, 0};
+    int32_t *h_done = nullptr;
+    cudaEvent_t ev[6] = {};
+    float ms_assembly = 0.f;
+    std::string err;
+};
+
+namespace {
+
+using mh::HostSystem;
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            return MH_ERR_CUDA;                                                         \
+        }                                                                               \
+    } while (0)
+
+template <class T> T *dalloc(mh_handle *h, size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    h->allocs.push_back(p);
+    return (T *)p;
+}
+
+template <class T> int upload(mh_handle *h, T *&dst, const std::vector<T> &src) {
+    dst = dalloc<T>(h, src.size());
+    if (!dst) {
+        h->err = "cudaMalloc failed";
+        return MH_ERR_NOMEM;
+    }
+    if (!src.empty()) CK(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MH_OK;
+}
+
+double side_measure_host(const mh::MeshData &m, int64_t e, int s) {
+    int d = m.dim[e];
+    if (d == 1) return 1.0;
+    const double *X[3];
+    for (int k = 0; k < d; ++k) X[k] = &m.xyz[3 * m.nodes[4 * e + mh::side_node(d, s, k)]];
+    if (d == 2) {
+        double dx = X[1][0] - X[0][0], dy = X[1][1] - X[0][1], dz = X[1][2] - X[0][2];
+        return std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    double u[3] = {X[1][0] - X[0][0], X[1][1] - X[0][1], X[1][2] - X[0][2]};
+    double v[3] = {X[2][0] - X[0][0], X[2][1] - X[0][1], X[2][2] - X[0][2]};
+    double c[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+    return 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+}
+
+int device_setup(mh_handle *h) {
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+        cudaGetLastError();
+        h->device = false;
+        return MH_OK;
+    }
+    CK(cudaGetDevice(&h->device_id));
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    for (auto &e : h->ev) CK(cudaEventCreate(&e));
+    CK(cudaHostAlloc((void **)&h->h_done, sizeof(int32_t) * 4, cudaHostAllocDefault));
+    const mh::MeshData &m = h->mesh;
+    const mh::Topology &t = h->topo;
+    const HostSystem &hs = h->hs;
+    int rc;
+    double *xyz;
+    int32_t *el_nodes, *el_side_start, *side_edge, *side_bdr, *el_ngh_start, *el_ngh, *ngh_edge, *ngh_hi;
+    double *ngh_meas;
+    if ((rc = upload(h, xyz, m.xyz)) || (rc = upload(h, el_nodes, m.nodes)) ||
+        (rc = upload(h, el_side_start, t.el_side_start)) || (rc = upload(h, side_edge, t.side_edge)) ||
+        (rc = upload(h, side_bdr, t.side_bdr)) || (rc = upload(h, el_ngh_start, t.el_ngh_start)) ||
+        (rc = upload(h, el_ngh, t.el_ngh)) || (rc = upload(h, ngh_edge, t.ngh_edge)) ||
+        (rc = upload(h, ngh_hi, h->ngh_hi_el)) || (rc = upload(h, ngh_meas, h->ngh_meas)))
+        return rc;
+    mh::ElemData &d = h->ed;
+    d.xyz = xyz;
+    d.el_nodes = el_nodes;
+    d.el_side_start = el_side_start;
+    d.side_edge = side_edge;
+    d.side_bdr = side_bdr;
+    d.el_ngh_start = el_ngh_start;
+    d.el_ngh = el_ngh;
+    d.ngh_edge = ngh_edge;
+    d.ngh_hi_el = ngh_hi;
+    d.ngh_side_measure = ngh_meas;
+    const int64_t n_el = m.n_el, n_bdr = t.n_bdr();
+    double *cond = dalloc<double>(h, n_el), *cs = dalloc<double>(h, n_el), *sg = dalloc<double>(h, n_el);
+    double *src = dalloc<double>(h, n_el), *sto = dalloc<double>(h, n_el);
+    int32_t *bct = dalloc<int32_t>(h, n_bdr);
+    double *bcp = dalloc<double>(h, n_bdr), *bcf = dalloc<double>(h, n_bdr), *bcs = dalloc<double>(h, n_bdr);
+    if (!cond || !cs || !sg || !src || !sto || !bct || !bcp || !bcf || !bcs) return MH_ERR_NOMEM;
+    d.conductivity = cond;
+    d.cross_section = cs;
+    d.sigma = sg;
+    d.source = src;
+    d.storativity = sto;
+    d.anisotropy = nullptr;
+    d.bc_type = bct;
+    d.bc_pressure = bcp;
+    d.bc_flux = bcf;
+    d.bc_sigma = bcs;
+    d.time_mode = 0;
+    d.inv_dt = 0.0;
+
+    mh::DevAssembly &a = h->as;
+    a.n_blk = hs.n_blk;
+    a.n_rhs_loc = hs.n_rhs_loc;
+    if ((rc = upload(h, a.blk_off, hs.blk_off)) || (rc = upload(h, a.rhs_off, hs.rhs_off)) ||
+        (rc = upload(h, a.slot_cstart, hs.slot_cstart)) || (rc = upload(h, a.slot_cidx, hs.slot_cidx)) ||
+        (rc = upload(h, a.row_cstart, hs.row_cstart)) || (rc = upload(h, a.row_cidx, hs.row_cidx)))
+        return rc;
+    for (int dd = 1; dd <= 3; ++dd) {
+        a.dim_count[dd] = (int64_t)hs.dim_list[dd].size();
+        if ((rc = upload(h, a.dim_list[dd], hs.dim_list[dd]))) return rc;
+    }
+    a.blk = dalloc<double>(h, hs.n_blk);
+    a.rhs_loc = dalloc<double>(h, hs.n_rhs_loc);
+    a.status = dalloc<int32_t>(h, 1);
+    if (!a.blk || !a.rhs_loc || !a.status) return MH_ERR_NOMEM;
+
+    mh::DevSystem &s = h->sys;
+    s.n_rows = hs.n_rows;
+    s.n_slices = hs.n_slices;
+    s.n_tiles = hs.n_tiles;
+    s.n_slots = hs.n_slots;
+    s.rows_per_thread = hs.rows_per_thread;
+    s.n_inst = (int32_t)hs.inst_el.size() - 1;
+    if ((rc = upload(h, s.slice_off, hs.slice_off)) || (rc = upload(h, s.col, hs.sell_col)) ||
+        (rc = upload(h, s.diag_slot, hs.diag_slot)) || (rc = upload(h, s.row_edge, hs.row_edge)) ||
+        (rc = upload(h, s.edge_row, hs.edge_row)) || (rc = upload(h, s.tile_inst, hs.tile_inst)))
+        return rc;
+    const int64_t nr = hs.n_rows;
+    s.val_raw = dalloc<double>(h, hs.n_slots);
+    s.val64 = dalloc<double>(h, hs.n_slots);
+    s.val32 = dalloc<float>(h, hs.n_slots);
+    s.dsq = dalloc<double>(h, nr);
+    s.b = dalloc<double>(h, nr);
+    s.bh = dalloc<double>(h, nr);
+    s.x = dalloc<double>(h, nr);
+    s.r = dalloc<double>(h, nr);
+    s.p = dalloc<double>(h, nr);
+    s.q = dalloc<double>(h, nr);
+    s.w = dalloc<double>(h, nr);
+    s.x32 = dalloc<float>(h, nr);
+    s.r32 = dalloc<float>(h, nr);
+    s.p32 = dalloc<float>(h, nr);
+    s.q32 = dalloc<float>(h, nr);
+    s.z32 = dalloc<float>(h, nr);
+    s.partial = dalloc<double>(h, hs.n_tiles * 4);
+    s.ctl = dalloc<mh::InstCtl>(h, s.n_inst);
+    s.n_done = dalloc<int32_t>(h, 1);
+    s.inst_sums = dalloc<double>(h, 4 * (size_t)s.n_inst);
+    s.sum_ticket = dalloc<uint32_t>(h, s.n_inst);
+    if (!s.val_raw || !s.val64 || !s.val32 || !s.dsq || !s.b || !s.bh || !s.x || !s.r || !s.p || !s.q || !s.w ||
+        !s.x32 || !s.r32 || !s.p32 || !s.q32 || !s.z32 || !s.partial || !s.ctl || !s.n_done || !s.inst_sums ||
+        !s.sum_ticket)
+        return MH_ERR_NOMEM;
+    std::vector<mh::InstCtl> ctl(s.n_inst);
+    const int64_t tr = hs.tile_rows;
+    for (int i = 0; i < s.n_inst; ++i) {
+        std::memset(&ctl[i], 0, sizeof(mh::InstCtl));
+        ctl[i].tile_begin = (int32_t)(hs.inst_row[i] / tr);
+        ctl[i].tile_end = (int32_t)(hs.inst_row[i + 1] / tr);
+        ctl[i].done = 1;
+    }
+    CK(cudaMemcpy(s.ctl, ctl.data(), sizeof(mh::InstCtl) * ctl.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemset(s.x, 0, nr * sizeof(double)));
+    CK(cudaMemset(s.x32, 0, nr * sizeof(float)));
+    CK(cudaMemset(s.sum_ticket, 0, s.n_inst * sizeof(uint32_t)));
+    const int64_t msize = t.n_sides() + m.n_el + t.n_edges();
+    h->sol = dalloc<double>(h, msize);
+    h->sol_prev = dalloc<double>(h, msize);
+    if (!h->sol || !h->sol_prev) return MH_ERR_NOMEM;
+    CK(cudaMemset(h->sol, 0, msize * sizeof(double)));
+    CK(cudaMemset(h->sol_prev, 0, msize * sizeof(double)));
+    h->device = true;
+    return MH_OK;
+}
+
+int need_device(mh_handle *h) {
+    if (!h) return MH_ERR_INVALID;
+    if (!h->device) {
+        h->err = "no CUDA device";
+        return MH_ERR_CUDA;
+    }
+    return MH_OK;
+}
+
+int check_finite(const double *a, int64_t n) {
+    if (!a) return 1;
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return 0;
+    return 1;
+}
+
+int fill_or_default(mh_handle *h, double *dst, const double *src, int64_t n, double dflt) {
+    if (src) {
+        CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    } else {
+        std::vector<double> v(n, dflt);
+        CK(cudaMemcpyAsync(dst, v.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return MH_OK;
+}
+
+// Assembly on the device: K1 local blocks -> gather -> scaling.  mode 3 = matrix + rhs, 2 = rhs.
+int assemble_impl(mh_handle *h, int mode) {
+    h->ed.prev_pressure = h->sol_prev + h->topo.n_sides();
+    h->ed.prev_edge = h->sol_prev + h->topo.n_sides() + h->mesh.n_el;
+    CK(cudaMemsetAsync(h->as.status, 0, sizeof(int32_t), h->stream));
+    CK(cudaEventRecord(h->ev[0], h->stream));
+    CK(mh::launch_local_blocks(h->ed, h->as, mode, h->stream));
+    CK(mh::launch_gather(h->as, h->sys, mode, h->stream));
+    CK(mh::launch_scale(h->sys, (mode & 1) ? 1 : 0, h->stream));
+    CK(cudaEventRecord(h->ev[1], h->stream));
+    int32_t st = 0;
+    CK(cudaMemcpyAsync(&st, h->as.status, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaEventElapsedTime(&h->ms_assembly, h->ev[0], h->ev[1]));
+    if (st & 1) {
+        h->err = "singular local MH matrix (|det| < DBL_MIN/DBL_EPSILON)";
+        return MH_ERR_SINGULAR;
+    }
+    if (st & 2) {
+        h->err = "non-finite value in the assembled system";
+        return MH_ERR_NONFINITE;
+    }
+    if (mode & 1) h->assembled = true;
+    return MH_OK;
+}
+
+// Runs captured Krylov iterations until every instance reports done.
+int run_krylov(mh_handle *h, int prec, int iters_per_graph, int max_it) {
+    const int gi = prec == 64 ? 0 : 1;
+    if (!h->graph[gi] || h->graph_iters[gi] != iters_per_graph) {
+        if (h->graph[gi]) cudaGraphExecDestroy(h->graph[gi]);
+        h->graph[gi] = nullptr;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < iters_per_graph; ++k) {
+            cudaError_t e = mh::launch_cg_iteration(h->sys, prec, h->stream);
+            if (e != cudaSuccess) {
+                cudaStreamEndCapture(h->stream, &g);
+                h->err = cudaGetErrorString(e);
+                return MH_ERR_CUDA;
+            }
+        }
+        CK(cudaStreamEndCapture(h->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&h->graph[gi], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->err = cudaGetErrorString(e);
+            return MH_ERR_CUDA;
+        }
+        h->graph_iters[gi] = iters_per_graph;
+    }
+    const int n_inst = h->sys.n_inst;
+    int64_t launched = 0;
+    while (true) {
+        CK(cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (*h->h_done >= n_inst) break;
+        if (launched > (int64_t)max_it + 2 * iters_per_graph) break;  // device caps iterations itself
+        CK(cudaGraphLaunch(h->graph[gi], h->stream));
+        launched += iters_per_graph;
+    }
+    return MH_OK;
+}
+
+int read_ctl(mh_handle *h, std::vector<mh::InstCtl> &ctl) {
+    ctl.resize(h->sys.n_inst);
+    CK(cudaMemcpyAsync(ctl.data(), h->sys.ctl, sizeof(mh::InstCtl) * ctl.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+// FP64 true residual per instance: rel = |b - S x| / |b| and abs = |b - S x| (unscaled).
+int true_residual(mh_handle *h, std::vector<double> &sums) {
+    CK(mh::launch_residual64(h->sys, h->stream));
+    sums.resize(4 * (size_t)h->sys.n_inst);
+    CK(cudaMemcpyAsync(sums.data(), h->sys.inst_sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+struct SolveResult {
+    int status = MH_OK;
+    int iterations = 0, outer = 0, fell_back = 0;
+    double rel = 0.0;
+};
+
+int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
+    const int n_inst = h->sys.n_inst;
+    std::vector<double> sums;
+    std::vector<mh::InstCtl> ctl;
+    double tau = o.r_tol;
+    int total = 0;
+    for (int run = 0; run < 12; ++run) {
+        CK(mh::launch_reset_ctl(h->sys, h->stream));
+        CK(mh::launch_cg_init(h->sys, tau * tau, 0.0, std::max(1, o.max_it - total), run > 0, h->stream));
+        int rc = run_krylov(h, 64, o.iters_per_graph, o.max_it - total);
+        if (rc) return rc;
+        if ((rc = read_ctl(h, ctl))) return rc;
+        int worst = 0, maxit = 0;
+        for (auto &c : ctl) {
+            maxit = std::max(maxit, c.iter);
+            if (c.status < 0) worst = c.status;
+        }
+        total += maxit;
+        if ((rc = true_residual(h, sums))) return rc;
+        bool all_ok = true;
+        double worst_ratio = 1.0;
+        res.rel = 0.0;
+        for (int i = 0; i < n_inst; ++i) {
+            double rn = std::sqrt(sums[4 * i + 1]), bn = std::sqrt(sums[4 * i + 2]);
+            double rel = bn > 0.0 ? rn / bn : 0.0;
+            res.rel = std::max(res.rel, rel);
+            bool ok = (rel <= o.r_tol) || (rn <= o.a_tol);
+            sums[4 * i + 3] = ok ? 0.0 : 1.0;
+            if (!ok) {
+                all_ok = false;
+                worst_ratio = std::max(worst_ratio, rel / o.r_tol);
+            }
+        }
+        res.outer = run + 1;
+        res.iterations = total;
+        if (all_ok) return MH_OK;
+        if (worst < 0) {
+            res.status = worst;
+            return MH_OK;
+        }
+        if (total >= o.max_it) {
+            res.status = MH_NOT_CONVERGED;
+            return MH_OK;
+        }
+        CK(cudaMemcpyAsync(h->sys.inst_sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice,
+                           h->stream));
+        tau = tau / (2.0 * worst_ratio);
+        if (tau < 1e-300) tau = 1e-300;
+    }
+    res.status = MH_NOT_CONVERGED;
+    return MH_OK;
+}
+
+int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
+    const int n_inst = h->sys.n_inst;
+    std::vector<double> sums;
+    std::vector<mh::InstCtl> ctl;
+    int total = 0;
+    double best = 1e300;
+    int stall = 0;
+    for (int outer = 0; outer < 200; ++outer) {
+        int rc = true_residual(h, sums);
+        if (rc) return rc;
+        bool any = false;
+        res.rel = 0.0;
+        for (int i = 0; i < n_inst; ++i) {
+            double rn = std::sqrt(sums[4 * i + 1]), bn = std::sqrt(sums[4 * i + 2]);
+            double rel = bn > 0.0 ? rn / bn : 0.0;
+            if (!std::isfinite(rel)) {
+                res.status = MH_ERR_NONFINITE;
+                return MH_OK;
+            }
+            res.rel = std::max(res.rel, rel);
+            bool ok = (rel <= o.r_tol) || (rn <= o.a_tol);
+            sums[4 * i + 3] = ok ? 0.0 : 1.0;
+            any |= !ok;
+        }
+        res.outer = outer;
+        res.iterations = total;
+        if (!any) return MH_OK;
+        if (total >= o.max_it) {
+            res.status = MH_NOT_CONVERGED;
+            return MH_OK;
+        }
+        if (res.rel < 0.5 * best) {
+            best = res.rel;
+            stall = 0;
+        } else if (++stall >= 4) {
+            res.status = MH_NOT_CONVERGED;
+            return MH_OK;
+        }
+        CK(cudaMemcpyAsync(h->sys.inst_sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(mh::launch_reset_ctl(h->sys, h->stream));
+        CK(mh::launch_ir_start(h->sys, o.inner_rtol * o.inner_rtol, std::min(o.inner_max_it, o.max_it - total),
+                               h->stream));
+        if ((rc = run_krylov(h, 32, o.iters_per_graph, o.inner_max_it))) return rc;
+        CK(mh::launch_ir_correct(h->sys, h->stream));
+        if ((rc = read_ctl(h, ctl))) return rc;
+        int maxit = 0;
+        for (auto &c : ctl) maxit = std::max(maxit, c.iter);
+        total += maxit;
+    }
+    res.status = MH_NOT_CONVERGED;
+    return MH_OK;
+}
+
+int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats, bool have_guess_default) {
+    mh_solve_opts o;
+    mh_solve_opts_default(&o);
+    if (opts_in) o = *opts_in;
+    if (o.max_it <= 0) o.max_it = 20000;
+    if (o.iters_per_graph <= 0) o.iters_per_graph = 16;
+    if (o.inner_max_it <= 0) o.inner_max_it = 2000;
+    if (!(o.inner_rtol > 0.0)) o.inner_rtol = 1e-5;
+    if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
+    if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
+    const bool guess = o.use_initial_guess || have_guess_default;
+    CK(cudaEventRecord(h->ev[2], h->stream));
+    if (guess) {
+        CK(mh::launch_scale_in(h->sys, h->sol + h->topo.n_sides() + h->mesh.n_el, h->stream));
+    } else {
+        CK(cudaMemsetAsync(h->sys.x, 0, h->sys.n_rows * sizeof(double), h->stream));
+    }
+    SolveResult res;
+    int rc = MH_OK;
+    switch (o.method) {
+        case MH_SOLVER_PCG64: rc = solve_pcg64(h, o, res); break;
+        case MH_SOLVER_IR32: rc = solve_ir32(h, o, res); break;
+        default:
+            h->err = "solver method not available";
+            return MH_ERR_INVALID;
+    }
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev[3], h->stream));
+    CK(mh::launch_backsub(h->ed, h->as, h->sys, h->sol, h->topo.n_sides(), h->mesh.n_el, h->topo.n_edges(),
+                          h->stream));
+    CK(cudaEventRecord(h->ev[4], h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->solved = true;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->status = res.status;
+        stats->iterations = res.iterations;
+        stats->outer_iterations = res.outer;
+        stats->fell_back = res.fell_back;
+        stats->rel_residual = res.rel;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+        stats->ms_solve = ms;
+        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+        stats->ms_backsub = ms;
+        stats->ms_assembly = h->ms_assembly;
+    }
+    return res.status;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mh_version(void) { return "mh-darcy-b200 0.1 (sm_100a)"; }
+
+const char *mh_status_string(int s) {
+    switch (s) {
+        case MH_OK: return "ok";
+        case MH_NOT_CONVERGED: return "not converged";
+        case MH_FELL_BACK: return "converged after fallback";
+        case MH_ERR_INVALID: return "invalid argument";
+        case MH_ERR_SINGULAR: return "singular local matrix";
+        case MH_ERR_CUDA: return "CUDA error";
+        case MH_ERR_STATE: return "call out of order";
+        case MH_ERR_NOMEM: return "out of memory";
+        case MH_ERR_NONFINITE: return "non-finite value";
+        case MH_ERR_TOPOLOGY: return "invalid mesh topology";
+        case MH_ERR_BREAKDOWN: return "CG breakdown";
+        default: return "unknown status";
+    }
+}
+
+int mh_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0 ? 1 : 0;
+}
+
+int mh_cube_mesh_create(int32_t n, int32_t n_planes, const int32_t *plane_axis, const int32_t *plane_index,
+                        int32_t n_lines, const int32_t *line_axis, const int32_t *line_a, const int32_t *line_b,
+                        mh_mesh **out) {
+    if (!out || n_planes < 0 || n_lines < 0) return MH_ERR_INVALID;
+    *out = nullptr;
+    std::vector<int> pa, pi, la, l1, l2;
+    for (int i = 0; i < n_planes; ++i) {
+        pa.push_back(plane_axis[i]);
+        pi.push_back(plane_index[i]);
+    }
+    for (int i = 0; i < n_lines; ++i) {
+        la.push_back(line_axis[i]);
+        l1.push_back(line_a[i]);
+        l2.push_back(line_b[i]);
+    }
+    auto *m = new (std::nothrow) mh_mesh();
+    if (!m) return MH_ERR_NOMEM;
+    std::string err;
+    int rc = mh::build_cube_mesh(n, pa, pi, la, l1, l2, m->m, &err);
+    if (rc) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return MH_OK;
+}
+
+int mh_mesh_describe(const mh_mesh *m, mh_mesh_desc *d) {
+    if (!m || !d) return MH_ERR_INVALID;
+    d->n_nodes = m->m.n_nodes;
+    d->node_xyz = m->m.xyz.data();
+    d->n_elements = m->m.n_el;
+    d->el_dim = m->m.dim.data();
+    d->el_nodes = m->m.nodes.data();
+    d->n_bc_elements = m->m.n_bc;
+    d->bc_dim = m->m.bc_dim.data();
+    d->bc_nodes = m->m.bc_nodes.data();
+    return MH_OK;
+}
+
+void mh_mesh_destroy(mh_mesh *m) { delete m; }
+
+void mh_solve_opts_default(mh_solve_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->method = MH_SOLVER_PCG64;
+    o->max_it = 20000;
+    o->r_tol = 1e-10;
+    o->a_tol = 0.0;
+    o->use_initial_guess = 0;
+    o->cheb_degree = 4;
+    o->inner_rtol = 1e-5;
+    o->inner_max_it = 2000;
+    o->iters_per_graph = 16;
+}
+
+int mh_create(const mh_mesh_desc *md, mh_handle **out) {
+    if (!md || !out || md->n_nodes <= 0 || md->n_elements <= 0 || !md->node_xyz || !md->el_dim || !md->el_nodes)
+        return MH_ERR_INVALID;
+    if (md->n_bc_elements < 0 || (md->n_bc_elements > 0 && (!md->bc_dim || !md->bc_nodes))) return MH_ERR_INVALID;
+    *out = nullptr;
+    auto *h = new (std::nothrow) mh_handle();
+    if (!h) return MH_ERR_NOMEM;
+    mh::MeshData &m = h->mesh;
+    m.n_nodes = md->n_nodes;
+    m.xyz.assign(md->node_xyz, md->node_xyz + 3 * md->n_nodes);
+    m.n_el = md->n_elements;
+    m.dim.assign(md->el_dim, md->el_dim + md->n_elements);
+    m.nodes.assign(md->el_nodes, md->el_nodes + 4 * md->n_elements);
+    m.n_bc = md->n_bc_elements;
+    if (m.n_bc > 0) {
+        m.bc_dim.assign(md->bc_dim, md->bc_dim + m.n_bc);
+        m.bc_nodes.assign(md->bc_nodes, md->bc_nodes + 4 * m.n_bc);
+    }
+    if (!check_finite(m.xyz.data(), (int64_t)m.xyz.size())) {
+        delete h;
+        return MH_ERR_NONFINITE;
+    }
+    int rc = mh::build_topology(m, h->topo, &h->err);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    const mh::Topology &t = h->topo;
+    h->ngh_hi_el.resize(t.n_ngh());
+    h->ngh_meas.resize(t.n_ngh());
+    for (int64_t i = 0; i < t.n_ngh(); ++i) {
+        int32_t side = t.ngh_side[i];
+        int64_t e = std::upper_bound(t.el_side_start.begin(), t.el_side_start.end(), side) - t.el_side_start.begin() - 1;
+        h->ngh_hi_el[i] = (int32_t)e;
+        h->ngh_meas[i] = side_measure_host(m, e, side - t.el_side_start[e]);
+    }
+    int rpt = 2;
+    if (const char *env = getenv("MH_ROWS_PER_THREAD")) {
+        int v = atoi(env);
+        if (v == 1 || v == 2 || v == 4) rpt = v;
+    }
+    std::vector<int64_t> inst = {0, m.n_el};
+    rc = mh::build_host_system(m, h->topo, inst, rpt, h->hs, &h->err);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    rc = device_setup(h);
+    if (rc) {
+        mh_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return MH_OK;
+}
+
+void mh_destroy(mh_handle *h) {
+    if (!h) return;
+    if (h->device) cudaDeviceSynchronize();
+    for (auto &g : h->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (void *p : h->allocs) cudaFree(p);
+    for (auto &e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->h_done) cudaFreeHost(h->h_done);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int mh_get_sizes(const mh_handle *h, mh_sizes *o) {
+    if (!h || !o) return MH_ERR_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->n_nodes = h->mesh.n_nodes;
+    o->n_elements = h->mesh.n_el;
+    o->n_sides = h->topo.n_sides();
+    o->n_edges = h->topo.n_edges();
+    o->n_boundaries = h->topo.n_bdr();
+    o->n_neighbours = h->topo.n_ngh();
+    for (int d = 1; d <= 3; ++d) o->n_el_dim[d] = (int64_t)h->hs.dim_list[d].size();
+    o->mh_size = o->n_sides + o->n_elements + o->n_edges;
+    o->schur_nnz = h->hs.nnz;
+    o->sell_slots = h->hs.n_slots;
+    o->n_rows_padded = h->hs.n_rows;
+    o->n_instances = (int64_t)h->hs.inst_el.size() - 1;
+    return MH_OK;
+}
+
+int mh_get_topology(const mh_handle *h, int32_t *el_side_start, int32_t *side_edge, int32_t *side_bdr,
+                    int32_t *bdr_bc_element, int32_t *bdr_edge, int32_t *ngh_element, int32_t *ngh_edge,
+                    int32_t *ngh_side) {
+    if (!h) return MH_ERR_INVALID;
+    const mh::Topology &t = h->topo;
+    auto cp = [](int32_t *dst, const std::vector<int32_t> &v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int32_t));
+    };
+    cp(el_side_start, t.el_side_start);
+    cp(side_edge, t.side_edge);
+    cp(side_bdr, t.side_bdr);
+    cp(bdr_bc_element, t.bdr_bc_el);
+    cp(bdr_edge, t.bdr_edge);
+    cp(ngh_element, t.ngh_el);
+    cp(ngh_edge, t.ngh_edge);
+    cp(ngh_side, t.ngh_side);
+    return MH_OK;
+}
+
+int mh_set_coeffs(mh_handle *h, const mh_coeffs *c) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!c) return MH_ERR_INVALID;
+    const int64_t n = h->mesh.n_el;
+    const double *arrs[6] = {c->conductivity, c->cross_section, c->sigma, c->water_source_density, c->storativity,
+                             nullptr};
+    for (int i = 0; i < 5; ++i)
+        if (!check_finite(arrs[i], n)) return MH_ERR_NONFINITE;
+    if (c->anisotropy && !check_finite(c->anisotropy, 9 * n)) return MH_ERR_NONFINITE;
+    for (int64_t e = 0; e < n; ++e) {
+        if (c->conductivity && !(c->conductivity[e] > 0.0)) {
+            h->err = "conductivity must be positive";
+            return MH_ERR_INVALID;
+        }
+        if (c->cross_section && !(c->cross_section[e] > 0.0)) {
+            h->err = "cross_section must be positive";
+            return MH_ERR_INVALID;
+        }
+    }
+    mh::ElemData &d = h->ed;
+    if ((rc = fill_or_default(h, (double *)d.conductivity, c->conductivity, n, 1.0)) ||
+        (rc = fill_or_default(h, (double *)d.cross_section, c->cross_section, n, 1.0)) ||
+        (rc = fill_or_default(h, (double *)d.sigma, c->sigma, n, 1.0)) ||
+        (rc = fill_or_default(h, (double *)d.source, c->water_source_density, n, 0.0)) ||
+        (rc = fill_or_default(h, (double *)d.storativity, c->storativity, n, 1.0)))
+        return rc;
+    if (c->anisotropy) {
+        if (!h->d_aniso) {
+            h->d_aniso = dalloc<double>(h, 9 * n);
+            if (!h->d_aniso) return MH_ERR_NOMEM;
+        }
+        CK(cudaMemcpyAsync(h->d_aniso, c->anisotropy, 9 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        d.anisotropy = h->d_aniso;
+    } else {
+        d.anisotropy = nullptr;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->coeffs_set = true;
+    h->assembled = false;
+    return MH_OK;
+}
+
+int mh_set_bc(mh_handle *h, const mh_bc *bc) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!bc) return MH_ERR_INVALID;
+    const int64_t n = h->topo.n_bdr();
+    if (bc->type)
+        for (int64_t i = 0; i < n; ++i)
+            if (bc->type[i] < MH_BC_NONE || bc->type[i] > MH_BC_ROBIN) {
+                h->err = "unknown boundary condition type";
+                return MH_ERR_INVALID;
+            }
+    if (!check_finite(bc->pressure, n) || !check_finite(bc->flux, n) || !check_finite(bc->robin_sigma, n))
+        return MH_ERR_NONFINITE;
+    mh::ElemData &d = h->ed;
+    if (bc->type) {
+        CK(cudaMemcpyAsync((void *)d.bc_type, bc->type, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    } else {
+        CK(cudaMemsetAsync((void *)d.bc_type, 0, n * sizeof(int32_t), h->stream));
+    }
+    if ((rc = fill_or_default(h, (double *)d.bc_pressure, bc->pressure, n, 0.0)) ||
+        (rc = fill_or_default(h, (double *)d.bc_flux, bc->flux, n, 0.0)) ||
+        (rc = fill_or_default(h, (double *)d.bc_sigma, bc->robin_sigma, n, 0.0)))
+        return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    h->bc_set = true;
+    h->assembled = false;
+    return MH_OK;
+}
+
+int mh_assemble(mh_handle *h) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->coeffs_set || !h->bc_set) {
+        h->err = "mh_set_coeffs and mh_set_bc must come before mh_assemble";
+        return MH_ERR_STATE;
+    }
+    return assemble_impl(h, 3);
+}
+
+int mh_solve(mh_handle *h, const mh_solve_opts *opts, mh_solve_stats *stats) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) {
+        h->err = "mh_assemble must come before mh_solve";
+        return MH_ERR_STATE;
+    }
+    return solve_impl(h, opts, stats, false);
+}
+
+int mh_get_solution(const mh_handle *hc, double *out, int64_t len) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t msize = h->topo.n_sides() + h->mesh.n_el + h->topo.n_edges();
+    if (!out || len < msize) return MH_ERR_INVALID;
+    CK(cudaMemcpyAsync(out, h->sol, msize * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_get_solution_device(const mh_handle *hc, double *dev_out, int64_t len) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t msize = h->topo.n_sides() + h->mesh.n_el + h->topo.n_edges();
+    if (!dev_out || len < msize) return MH_ERR_INVALID;
+    CK(cudaMemcpyAsync(dev_out, h->sol, msize * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_get_schur_system(const mh_handle *hc, int32_t *row_ptr, int32_t *col, double *val, double *rhs) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    const HostSystem &hs = h->hs;
+    std::vector<double> v(hs.n_slots), b(hs.n_rows);
+    CK(cudaMemcpyAsync(v.data(), h->sys.val_raw, hs.n_slots * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(b.data(), h->sys.b, hs.n_rows * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int64_t ne = h->topo.n_edges();
+    int64_t k = 0;
+    if (row_ptr) row_ptr[0] = 0;
+    for (int64_t e = 0; e < ne; ++e) {
+        const int64_t r = hs.edge_row[e];
+        const int64_t sl = r / mh::kSliceRowsHost, lane = r % mh::kSliceRowsHost;
+        const int64_t off = hs.slice_off[sl];
+        for (int64_t j = 0; j < hs.row_ptr[r + 1] - hs.row_ptr[r]; ++j) {
+            if (col) col[k] = hs.row_edge[hs.row_col[hs.row_ptr[r] + j]];
+            if (val) val[k] = v[off + j * mh::kSliceRowsHost + lane];
+            ++k;
+        }
+        if (row_ptr) row_ptr[e + 1] = (int32_t)k;
+        if (rhs) rhs[e] = b[r];
+    }
+    return MH_OK;
+}
+
+int mh_unsteady_init(mh_handle *h, int32_t lumped, double dt, const double *init_pressure) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return MH_ERR_INVALID;
+    if (!h->coeffs_set || !h->bc_set) return MH_ERR_STATE;
+    const int64_t n_el = h->mesh.n_el, ns = h->topo.n_sides(), ne = h->topo.n_edges();
+    if (init_pressure && !check_finite(init_pressure, n_el)) return MH_ERR_NONFINITE;
+    std::vector<double> s0(ns + n_el + ne, 0.0);
+    if (init_pressure) {
+        if (!lumped) {
+            for (int64_t e = 0; e < n_el; ++e) s0[ns + e] = init_pressure[e];
+        } else {
+            // DarcyFlowLMH_Unsteady::setup_time_term: edge value += init / n_sides per side
+            for (int64_t e = 0; e < n_el; ++e) {
+                const int n = h->mesh.dim[e] + 1;
+                for (int i = 0; i < n; ++i)
+                    s0[ns + n_el + h->topo.side_edge[h->topo.el_side_start[e] + i]] += init_pressure[e] / n;
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(h->sol_prev, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->sol, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->time_mode = lumped ? 2 : 1;
+    h->ed.time_mode = h->time_mode;
+    h->dt = dt;
+    h->ed.inv_dt = 1.0 / dt;
+    return assemble_impl(h, 3);
+}
+
+int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts, mh_solve_stats *stats) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (h->time_mode == 0) return MH_ERR_STATE;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return MH_ERR_INVALID;
+    if (dt != h->dt || !h->assembled) {
+        h->dt = dt;
+        h->ed.inv_dt = 1.0 / dt;
+        rc = assemble_impl(h, 3);
+    } else {
+        rc = assemble_impl(h, 2);  // matrix unchanged: only the time-term rhs moves
+    }
+    if (rc) return rc;
+    int st = solve_impl(h, opts, stats, true);
+    if (st < 0) return st;
+    const int64_t msize = h->topo.n_sides() + h->mesh.n_el + h->topo.n_edges();
+    CK(cudaMemcpyAsync(h->sol_prev, h->sol, msize * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return st;
+}
+
+const char *mh_last_error(const mh_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+}  // extern "C"

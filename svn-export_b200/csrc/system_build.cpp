@@ -1,0 +1,222 @@
+// See system_build.hpp.
+#include "system_build.hpp"
+
+#include <algorithm>
+#include <cstdio>
+
+#include "mh_darcy.h"
+#include "mh_types.hpp"
+
+namespace mh {
+
+int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out) {
+    int n = m.dim[e] + 1;
+    int c = 0;
+    for (int i = 0; i < n; ++i) out[c++] = t.side_edge[t.el_side_start[e] + i];
+    for (int j = t.el_ngh_start[e]; j < t.el_ngh_start[e + 1]; ++j) out[c++] = t.ngh_edge[t.el_ngh[j]];
+    return c;
+}
+
+int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
+                      int rows_per_thread, HostSystem &hs, std::string *err) {
+    char msg[256];
+    hs = HostSystem();
+    hs.inst_el = inst_el;
+    hs.rows_per_thread = rows_per_thread;
+    hs.tile_rows = (int64_t)kTileRowsBase * rows_per_thread;
+    const int64_t n_el = m.n_el, n_edges = t.n_edges();
+    const int n_inst = (int)inst_el.size() - 1;
+
+    // local block sizes and offsets
+    hs.el_m.resize(n_el);
+    hs.blk_off.resize(n_el);
+    hs.rhs_off.resize(n_el);
+    int64_t nb = 0, nr = 0;
+    for (int64_t e = 0; e < n_el; ++e) {
+        int d = m.dim[e];
+        int k = t.el_ngh_start[e + 1] - t.el_ngh_start[e];
+        int kmax = (d == 1) ? kMaxNgh1 : (d == 2 ? kMaxNgh2 : 0);
+        if (k > kmax) {
+            snprintf(msg, sizeof msg, "element %lld has %d VB neighbours (limit %d for dimension %d)",
+                     (long long)e, k, kmax, d);
+            if (err) *err = msg;
+            return MH_ERR_TOPOLOGY;
+        }
+        int mm = d + 1 + k;
+        hs.el_m[e] = mm;
+        hs.blk_off[e] = nb;
+        hs.rhs_off[e] = nr;
+        nb += (int64_t)mm * mm;
+        nr += mm;
+        hs.dim_list[d].push_back((int32_t)e);
+    }
+    hs.n_blk = nb;
+    hs.n_rhs_loc = nr;
+    if (nb > INT32_MAX || nr > INT32_MAX) {
+        if (err) *err = "mesh too large for 32-bit contribution indices";
+        return MH_ERR_INVALID;
+    }
+
+    // instance edge ranges: edges are created while the instance's elements are visited,
+    // so each instance owns a contiguous edge range
+    hs.inst_edge.assign(n_inst + 1, 0);
+    {
+        std::vector<int32_t> owner(n_edges, -1);
+        int32_t loc[16];
+        for (int i = 0; i < n_inst; ++i)
+            for (int64_t e = inst_el[i]; e < inst_el[i + 1]; ++e) {
+                int c = local_edges(m, t, e, loc);
+                for (int l = 0; l < c; ++l) {
+                    if (owner[loc[l]] >= 0 && owner[loc[l]] != i) {
+                        if (err) *err = "instances share an edge";
+                        return MH_ERR_INVALID;
+                    }
+                    owner[loc[l]] = i;
+                }
+            }
+        for (int64_t g = 0; g < n_edges; ++g) {
+            if (owner[g] < 0) {
+                if (err) *err = "edge without an element";
+                return MH_ERR_TOPOLOGY;
+            }
+            if (g > 0 && owner[g] < owner[g - 1]) {
+                if (err) *err = "instance edge ranges are not contiguous";
+                return MH_ERR_INVALID;
+            }
+        }
+        int64_t g = 0;
+        for (int i = 0; i < n_inst; ++i) {
+            hs.inst_edge[i] = g;
+            while (g < n_edges && owner[g] == i) ++g;
+        }
+        hs.inst_edge[n_inst] = g;
+    }
+
+    // padded solver rows per instance (whole tiles)
+    hs.inst_row.assign(n_inst + 1, 0);
+    for (int i = 0; i < n_inst; ++i) {
+        int64_t ne = hs.inst_edge[i + 1] - hs.inst_edge[i];
+        int64_t pad = ((ne + hs.tile_rows - 1) / hs.tile_rows) * hs.tile_rows;
+        if (pad == 0) pad = hs.tile_rows;
+        hs.inst_row[i + 1] = hs.inst_row[i] + pad;
+    }
+    hs.n_rows = hs.inst_row[n_inst];
+    hs.n_slices = hs.n_rows / kSliceRowsHost;
+    hs.n_tiles = hs.n_rows / hs.tile_rows;
+    hs.edge_row.resize(n_edges);
+    hs.row_edge.assign(hs.n_rows, -1);
+    for (int i = 0; i < n_inst; ++i)
+        for (int64_t g = hs.inst_edge[i]; g < hs.inst_edge[i + 1]; ++g) {
+            int64_t r = hs.inst_row[i] + (g - hs.inst_edge[i]);
+            hs.edge_row[g] = (int32_t)r;
+            hs.row_edge[r] = (int32_t)g;
+        }
+    hs.tile_inst.resize(hs.n_tiles);
+    for (int i = 0; i < n_inst; ++i)
+        for (int64_t tl = hs.inst_row[i] / hs.tile_rows; tl < hs.inst_row[i + 1] / hs.tile_rows; ++tl)
+            hs.tile_inst[tl] = i;
+
+    // symmetric pattern: every pair of an element's local edges
+    std::vector<int64_t> cnt(hs.n_rows + 1, 0);
+    int32_t loc[16];
+    for (int64_t e = 0; e < n_el; ++e) {
+        int c = local_edges(m, t, e, loc);
+        for (int a = 0; a < c; ++a) cnt[hs.edge_row[loc[a]] + 1] += c;
+    }
+    for (int64_t r = 0; r < hs.n_rows; ++r)
+        if (hs.row_edge[r] < 0) cnt[r + 1] += 1;
+    for (int64_t r = 0; r < hs.n_rows; ++r) cnt[r + 1] += cnt[r];
+    std::vector<int32_t> raw(cnt[hs.n_rows]);
+    {
+        std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+        for (int64_t e = 0; e < n_el; ++e) {
+            int c = local_edges(m, t, e, loc);
+            for (int a = 0; a < c; ++a) {
+                int64_t ra = hs.edge_row[loc[a]];
+                for (int b = 0; b < c; ++b) raw[fill[ra]++] = hs.edge_row[loc[b]];
+            }
+        }
+        for (int64_t r = 0; r < hs.n_rows; ++r)
+            if (hs.row_edge[r] < 0) raw[fill[r]++] = (int32_t)r;
+    }
+    hs.row_ptr.assign(hs.n_rows + 1, 0);
+    std::vector<int64_t> len(hs.n_rows);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t r = 0; r < hs.n_rows; ++r) {
+        auto b = raw.begin() + cnt[r], e = raw.begin() + cnt[r + 1];
+        std::sort(b, e);
+        len[r] = std::unique(b, e) - b;
+    }
+    for (int64_t r = 0; r < hs.n_rows; ++r) hs.row_ptr[r + 1] = hs.row_ptr[r] + len[r];
+    hs.row_col.resize(hs.row_ptr[hs.n_rows]);
+    for (int64_t r = 0; r < hs.n_rows; ++r)
+        std::copy(raw.begin() + cnt[r], raw.begin() + cnt[r] + len[r], hs.row_col.begin() + hs.row_ptr[r]);
+    hs.nnz = 0;
+    for (int64_t r = 0; r < hs.n_rows; ++r)
+        if (hs.row_edge[r] >= 0) hs.nnz += len[r];
+    raw.clear();
+    raw.shrink_to_fit();
+
+    // SELL-C-sigma with C = 32 (sigma = 1: the mesh ordering already keeps row lengths even)
+    hs.slice_off.assign(hs.n_slices + 1, 0);
+    for (int64_t s = 0; s < hs.n_slices; ++s) {
+        int64_t w = 0;
+        for (int l = 0; l < kSliceRowsHost; ++l) w = std::max(w, len[s * kSliceRowsHost + l]);
+        hs.slice_off[s + 1] = hs.slice_off[s] + w * kSliceRowsHost;
+    }
+    hs.n_slots = hs.slice_off[hs.n_slices];
+    if (hs.n_slots > INT32_MAX) {
+        if (err) *err = "system too large for 32-bit slot indices";
+        return MH_ERR_INVALID;
+    }
+    hs.sell_col.resize(hs.n_slots);
+    hs.diag_slot.resize(hs.n_rows);
+    for (int64_t r = 0; r < hs.n_rows; ++r) {
+        int64_t s = r / kSliceRowsHost, lane = r % kSliceRowsHost;
+        int64_t off = hs.slice_off[s], w = (hs.slice_off[s + 1] - off) / kSliceRowsHost;
+        for (int64_t j = 0; j < w; ++j) {
+            int32_t c = (j < len[r]) ? hs.row_col[hs.row_ptr[r] + j] : (int32_t)r;
+            hs.sell_col[off + j * kSliceRowsHost + lane] = c;
+            if (j < len[r] && c == r) hs.diag_slot[r] = (int32_t)(off + j * kSliceRowsHost + lane);
+        }
+    }
+    auto slot_of = [&](int64_t r, int32_t c) -> int64_t {
+        auto b = hs.row_col.begin() + hs.row_ptr[r], e = hs.row_col.begin() + hs.row_ptr[r + 1];
+        int64_t j = std::lower_bound(b, e, c) - b;
+        return hs.slice_off[r / kSliceRowsHost] + j * kSliceRowsHost + r % kSliceRowsHost;
+    };
+
+    // contributions: element blocks -> slots, element rhs -> rows (element order)
+    hs.slot_cstart.assign(hs.n_slots + 1, 0);
+    hs.row_cstart.assign(hs.n_rows + 1, 0);
+    for (int64_t e = 0; e < n_el; ++e) {
+        int c = local_edges(m, t, e, loc);
+        for (int a = 0; a < c; ++a) {
+            int64_t ra = hs.edge_row[loc[a]];
+            hs.row_cstart[ra + 1]++;
+            for (int b = 0; b < c; ++b) hs.slot_cstart[slot_of(ra, hs.edge_row[loc[b]]) + 1]++;
+        }
+    }
+    for (int64_t s = 0; s < hs.n_slots; ++s) hs.slot_cstart[s + 1] += hs.slot_cstart[s];
+    for (int64_t r = 0; r < hs.n_rows; ++r) hs.row_cstart[r + 1] += hs.row_cstart[r];
+    hs.slot_cidx.resize(hs.slot_cstart[hs.n_slots]);
+    hs.row_cidx.resize(hs.row_cstart[hs.n_rows]);
+    {
+        std::vector<int32_t> sf(hs.slot_cstart.begin(), hs.slot_cstart.end() - 1);
+        std::vector<int32_t> rf(hs.row_cstart.begin(), hs.row_cstart.end() - 1);
+        for (int64_t e = 0; e < n_el; ++e) {
+            int c = local_edges(m, t, e, loc);
+            for (int a = 0; a < c; ++a) {
+                int64_t ra = hs.edge_row[loc[a]];
+                hs.row_cidx[rf[ra]++] = (int32_t)(hs.rhs_off[e] + a);
+                for (int b = 0; b < c; ++b) {
+                    int64_t sl = slot_of(ra, hs.edge_row[loc[b]]);
+                    hs.slot_cidx[sf[sl]++] = (int32_t)(hs.blk_off[e] + (int64_t)a * c + b);
+                }
+            }
+        }
+    }
+    return MH_OK;
+}
+
+}  // namespace mh

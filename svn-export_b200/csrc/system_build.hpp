@@ -1,0 +1,42 @@
+// Host construction of the edge-system layout: local edge lists, the symmetric Schur
+// pattern, the SELL-C-sigma slot layout, and the element-block -> slot contribution maps.
+// Pure integer bookkeeping, done once per mesh.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "topology.hpp"
+
+namespace mh {
+
+struct HostSystem {
+    // instances: element ranges [inst_el[i], inst_el[i+1])
+    std::vector<int64_t> inst_el;
+    std::vector<int64_t> inst_edge;      // [n_inst+1] edge ranges
+    std::vector<int64_t> inst_row;       // [n_inst+1] padded solver-row ranges
+    int32_t rows_per_thread = 1;
+    int64_t tile_rows = 0;
+    int64_t n_rows = 0, n_slices = 0, n_tiles = 0, n_slots = 0, nnz = 0;
+    std::vector<int32_t> el_m;           // local block size per element
+    std::vector<int64_t> blk_off, rhs_off;
+    int64_t n_blk = 0, n_rhs_loc = 0;
+    std::vector<int32_t> edge_row, row_edge;
+    std::vector<int64_t> row_ptr;        // sorted pattern per solver row (solver-row columns)
+    std::vector<int32_t> row_col;
+    std::vector<int64_t> slice_off;
+    std::vector<int32_t> sell_col;
+    std::vector<int32_t> diag_slot;
+    std::vector<int32_t> tile_inst;
+    std::vector<int32_t> slot_cstart, slot_cidx;
+    std::vector<int32_t> row_cstart, row_cidx;
+    std::vector<int32_t> dim_list[4];
+};
+
+// Local edge list of element e: own side edges then VB-neighbour edges.
+int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out);
+
+int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
+                      int rows_per_thread, HostSystem &hs, std::string *err);
+
+}  // namespace mh

@@ -1,0 +1,153 @@
+"""ctypes binding of libmhdarcy.so (the C ABI declared in include/mh_darcy.h).
+
+The shared library is built in-tree by ``make -C svn-export_b200/csrc`` and loaded from this
+directory.  There is no Python or CPU fallback for any compute entry point: if the library
+is missing the import fails, and compute calls on a machine without a CUDA device return
+MH_ERR_CUDA, which is raised as :class:`MHError`.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmhdarcy.so")
+
+MH_OK = 0
+MH_NOT_CONVERGED = 1
+MH_FELL_BACK = 2
+MH_ERR_INVALID = -1
+MH_ERR_SINGULAR = -2
+MH_ERR_CUDA = -3
+MH_ERR_STATE = -4
+MH_ERR_NOMEM = -5
+MH_ERR_NONFINITE = -6
+MH_ERR_TOPOLOGY = -7
+MH_ERR_BREAKDOWN = -8
+
+MH_BC_NONE, MH_BC_DIRICHLET, MH_BC_NEUMANN, MH_BC_ROBIN = 0, 1, 2, 3
+
+MH_SOLVER_PCG64 = 0
+MH_SOLVER_IR32 = 1
+MH_SOLVER_CHEB64 = 2
+MH_SOLVER_FCG_LEARNED = 3
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("node_xyz", _f64p), ("n_elements", C.c_int64),
+                ("el_dim", _i32p), ("el_nodes", _i32p), ("n_bc_elements", C.c_int64),
+                ("bc_dim", _i32p), ("bc_nodes", _i32p)]
+
+
+class Sizes(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("n_elements", C.c_int64), ("n_sides", C.c_int64),
+                ("n_edges", C.c_int64), ("n_boundaries", C.c_int64), ("n_neighbours", C.c_int64),
+                ("n_el_dim", C.c_int64 * 4), ("mh_size", C.c_int64), ("schur_nnz", C.c_int64),
+                ("sell_slots", C.c_int64), ("n_rows_padded", C.c_int64), ("n_instances", C.c_int64)]
+
+
+class Coeffs(C.Structure):
+    _fields_ = [("conductivity", _f64p), ("anisotropy", _f64p), ("cross_section", _f64p),
+                ("sigma", _f64p), ("water_source_density", _f64p), ("storativity", _f64p)]
+
+
+class BC(C.Structure):
+    _fields_ = [("type", _i32p), ("pressure", _f64p), ("flux", _f64p), ("robin_sigma", _f64p)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("method", C.c_int32), ("max_it", C.c_int32), ("r_tol", C.c_double),
+                ("a_tol", C.c_double), ("use_initial_guess", C.c_int32), ("cheb_degree", C.c_int32),
+                ("inner_rtol", C.c_double), ("inner_max_it", C.c_int32),
+                ("iters_per_graph", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("outer_iterations", C.c_int32),
+                ("fell_back", C.c_int32), ("rel_residual", C.c_double), ("ms_assembly", C.c_double),
+                ("ms_solve", C.c_double), ("ms_backsub", C.c_double), ("reserved", C.c_double * 4)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class MHError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{lib.mh_status_string(status).decode()} ({status}): {msg}")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C svn-export_b200/csrc` "
+                          "(there is no fallback implementation)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "mh_version": (C.c_char_p, []),
+        "mh_status_string": (C.c_char_p, [C.c_int]),
+        "mh_device_available": (C.c_int, []),
+        "mh_last_error": (C.c_char_p, [vp]),
+        "mh_cube_mesh_create": (C.c_int, [C.c_int32, C.c_int32, _i32p, _i32p, C.c_int32, _i32p, _i32p,
+                                          _i32p, C.POINTER(vp)]),
+        "mh_mesh_describe": (C.c_int, [vp, C.POINTER(MeshDesc)]),
+        "mh_mesh_destroy": (None, [vp]),
+        "mh_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(vp)]),
+        "mh_destroy": (None, [vp]),
+        "mh_get_sizes": (C.c_int, [vp, C.POINTER(Sizes)]),
+        "mh_get_topology": (C.c_int, [vp] + [_i32p] * 8),
+        "mh_set_coeffs": (C.c_int, [vp, C.POINTER(Coeffs)]),
+        "mh_set_bc": (C.c_int, [vp, C.POINTER(BC)]),
+        "mh_assemble": (C.c_int, [vp]),
+        "mh_solve": (C.c_int, [vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+        "mh_get_solution": (C.c_int, [vp, _f64p, C.c_int64]),
+        "mh_get_solution_device": (C.c_int, [vp, vp, C.c_int64]),
+        "mh_get_schur_system": (C.c_int, [vp, _i32p, _i32p, _f64p, _f64p]),
+        "mh_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
+        "mh_unsteady_init": (C.c_int, [vp, C.c_int32, C.c_double, _f64p]),
+        "mh_unsteady_step": (C.c_int, [vp, C.c_double, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+# every symbol the header declares, for the load/export check
+EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_error",
+            "mh_cube_mesh_create", "mh_mesh_describe", "mh_mesh_destroy", "mh_create", "mh_destroy",
+            "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
+            "mh_solve", "mh_get_solution", "mh_get_solution_device", "mh_get_schur_system",
+            "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step")
+
+
+def ptr(a, ctype):
+    """Pointer to a C-contiguous numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def check(status, handle=None):
+    if status < 0:
+        msg = lib.mh_last_error(handle).decode() if handle else ""
+        raise MHError(status, msg)
+    return status
+
+
+def device_available():
+    return bool(lib.mh_device_available())

@@ -1,0 +1,248 @@
+"""Host-side mirror of the reference's DarcyFlowMH interface over the C ABI.
+
+Names follow the reference: DarcyFlowMH_Steady.update_solution / get_solution_vector
+(src/flow/darcy_flow_mh.cc:375-433, 485-500), DarcyFlowMH_Unsteady and
+DarcyFlowLMH_Unsteady (:1601-1827), and the MH_DofHandler accessors side_flux / side_scalar
+/ element_scalar (src/flow/mh_dofhandler.cc:37-50).  All compute runs in libmhdarcy.so on
+the GPU; every error is raised, nothing falls back to the CPU.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib, check, f64, i32, ptr
+
+
+def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000,
+               use_initial_guess=False, inner_rtol=1e-5, inner_max_it=2000, iters_per_graph=16,
+               cheb_degree=4):
+    o = _lib.SolveOpts()
+    lib.mh_solve_opts_default(C.byref(o))
+    o.method = method
+    o.r_tol = r_tol
+    o.a_tol = a_tol
+    o.max_it = max_it
+    o.use_initial_guess = int(bool(use_initial_guess))
+    o.inner_rtol = inner_rtol
+    o.inner_max_it = inner_max_it
+    o.iters_per_graph = iters_per_graph
+    o.cheb_degree = cheb_degree
+    return o
+
+
+class MHSystem:
+    """One mixed-hybrid Darcy system on the GPU (an mh_handle)."""
+
+    def __init__(self, mesh):
+        self.mesh = mesh
+        h = C.c_void_p()
+        d = mesh.desc()
+        check(lib.mh_create(C.byref(d), C.byref(h)))
+        self.h = h
+        s = _lib.Sizes()
+        check(lib.mh_get_sizes(h, C.byref(s)))
+        self.sizes = s
+        self._topo = None
+
+    def close(self):
+        if self.h:
+            lib.mh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def n_sides(self):
+        return self.sizes.n_sides
+
+    @property
+    def n_elements(self):
+        return self.sizes.n_elements
+
+    @property
+    def n_edges(self):
+        return self.sizes.n_edges
+
+    @property
+    def n_boundaries(self):
+        return self.sizes.n_boundaries
+
+    def topology(self):
+        if self._topo is None:
+            s = self.sizes
+            t = {
+                "el_side_start": np.zeros(s.n_elements + 1, np.int32),
+                "side_edge": np.zeros(s.n_sides, np.int32),
+                "side_bdr": np.zeros(s.n_sides, np.int32),
+                "bdr_bc_element": np.zeros(max(s.n_boundaries, 1), np.int32),
+                "bdr_edge": np.zeros(max(s.n_boundaries, 1), np.int32),
+                "ngh_element": np.zeros(max(s.n_neighbours, 1), np.int32),
+                "ngh_edge": np.zeros(max(s.n_neighbours, 1), np.int32),
+                "ngh_side": np.zeros(max(s.n_neighbours, 1), np.int32),
+            }
+            check(lib.mh_get_topology(self.h, *[ptr(t[k], C.c_int32) for k in
+                                                ("el_side_start", "side_edge", "side_bdr",
+                                                 "bdr_bc_element", "bdr_edge", "ngh_element",
+                                                 "ngh_edge", "ngh_side")]), self.h)
+            for k, n in (("bdr_bc_element", s.n_boundaries), ("bdr_edge", s.n_boundaries),
+                         ("ngh_element", s.n_neighbours), ("ngh_edge", s.n_neighbours),
+                         ("ngh_side", s.n_neighbours)):
+                t[k] = t[k][:n]
+            self._topo = t
+        return self._topo
+
+    def set_coeffs(self, conductivity=None, anisotropy=None, cross_section=None, sigma=None,
+                   water_source_density=None, storativity=None):
+        n = self.n_elements
+
+        def arr(a, shape):
+            if a is None:
+                return None
+            a = np.asarray(a, np.float64)
+            if a.ndim == 0:
+                a = np.full(shape, float(a))
+            return np.ascontiguousarray(a.reshape(shape))
+
+        keep = [arr(conductivity, n), arr(anisotropy, (n, 9)) if anisotropy is not None else None,
+                arr(cross_section, n), arr(sigma, n), arr(water_source_density, n),
+                arr(storativity, n)]
+        c = _lib.Coeffs(*[ptr(a, C.c_double) for a in keep])
+        check(lib.mh_set_coeffs(self.h, C.byref(c)), self.h)
+        self._coeffs = keep
+
+    def set_bc(self, bc_type, pressure=None, flux=None, robin_sigma=None):
+        nb = self.n_boundaries
+        keep = [i32(np.broadcast_to(np.asarray(bc_type, np.int32), (nb,)).copy())]
+        for a in (pressure, flux, robin_sigma):
+            keep.append(None if a is None else f64(np.broadcast_to(np.asarray(a, np.float64), (nb,)).copy()))
+        b = _lib.BC(ptr(keep[0], C.c_int32), ptr(keep[1], C.c_double), ptr(keep[2], C.c_double),
+                    ptr(keep[3], C.c_double))
+        check(lib.mh_set_bc(self.h, C.byref(b)), self.h)
+        self._bc = keep
+
+    def assemble(self):
+        check(lib.mh_assemble(self.h), self.h)
+
+    def solve(self, **kw):
+        o = solve_opts(**kw)
+        st = _lib.SolveStats()
+        rc = check(lib.mh_solve(self.h, C.byref(o), C.byref(st)), self.h)
+        d = st.as_dict()
+        d["status"] = rc
+        return d
+
+    def solution(self):
+        out = np.zeros(self.sizes.mh_size)
+        check(lib.mh_get_solution(self.h, ptr(out, C.c_double), len(out)), self.h)
+        return out
+
+    def schur_system(self):
+        """The assembled edge system (reference schur2 after scale(-1)) as CSR + rhs."""
+        s = self.sizes
+        rp = np.zeros(s.n_edges + 1, np.int32)
+        col = np.zeros(s.schur_nnz, np.int32)
+        val = np.zeros(s.schur_nnz)
+        rhs = np.zeros(s.n_edges)
+        check(lib.mh_get_schur_system(self.h, ptr(rp, C.c_int32), ptr(col, C.c_int32),
+                                      ptr(val, C.c_double), ptr(rhs, C.c_double)), self.h)
+        return rp, col, val, rhs
+
+    def unsteady_init(self, dt, init_pressure=None, lumped=False):
+        ip = None if init_pressure is None else f64(np.broadcast_to(init_pressure, (self.n_elements,)).copy())
+        check(lib.mh_unsteady_init(self.h, int(bool(lumped)), float(dt), ptr(ip, C.c_double)), self.h)
+
+    def unsteady_step(self, dt, **kw):
+        o = solve_opts(**kw)
+        st = _lib.SolveStats()
+        rc = check(lib.mh_unsteady_step(self.h, float(dt), C.byref(o), C.byref(st)), self.h)
+        d = st.as_dict()
+        d["status"] = rc
+        return d
+
+    # ---- MH_DofHandler accessors on a solution vector ----
+    def split(self, sol):
+        ns, ne = self.n_sides, self.n_elements
+        return sol[:ns], sol[ns:ns + ne], sol[ns + ne:]
+
+
+class MH_DofHandler:
+    """Accessors of the MH solution layout [side fluxes | element pressures | edge pressures]."""
+
+    def __init__(self, system, solution):
+        self.sys = system
+        self.sol = solution
+        t = system.topology()
+        self.el_side_start = t["el_side_start"]
+        self.side_edge = t["side_edge"]
+
+    def side_flux(self, element, local_side):
+        return self.sol[self.el_side_start[element] + local_side]
+
+    def side_scalar(self, element, local_side):
+        e = self.side_edge[self.el_side_start[element] + local_side]
+        return self.sol[self.sys.n_sides + self.sys.n_elements + e]
+
+    def element_scalar(self, element):
+        return self.sol[self.sys.n_sides + element]
+
+
+class DarcyFlowMH_Steady:
+    """Steady MH Darcy flow with n_schurs = 2, solved on the GPU."""
+
+    def __init__(self, mesh, coeffs, bc, solver=None):
+        self.system = MHSystem(mesh)
+        self.system.set_coeffs(**coeffs)
+        self.system.set_bc(**bc)
+        self.solver = dict(solver or {})
+        self.stats = None
+        self._solution = None
+
+    def update_solution(self):
+        self.system.assemble()
+        self.stats = self.system.solve(**self.solver)
+        self._solution = None
+        return self.stats
+
+    def get_solution_vector(self):
+        if self._solution is None:
+            self._solution = self.system.solution()
+        return self._solution
+
+    def get_mh_dofhandler(self):
+        return MH_DofHandler(self.system, self.get_solution_vector())
+
+
+class DarcyFlowMH_Unsteady(DarcyFlowMH_Steady):
+    """Implicit Euler; time term -S|E|/dt on the element diagonal (darcy_flow_mh.cc:1614-1675)."""
+
+    lumped = False
+
+    def __init__(self, mesh, coeffs, bc, dt, init_pressure=None, solver=None):
+        super().__init__(mesh, coeffs, bc, solver)
+        self.dt = dt
+        self.time = 0.0
+        self.system.unsteady_init(dt, init_pressure, lumped=self.lumped)
+
+    def update_solution(self, dt=None):
+        dt = self.dt if dt is None else dt
+        self.stats = self.system.unsteady_step(dt, **self.solver)
+        self.time += dt
+        self._solution = None
+        return self.stats
+
+
+class DarcyFlowLMH_Unsteady(DarcyFlowMH_Unsteady):
+    """Lumped variant: time term on the edge rows (darcy_flow_mh.cc:1695-1827)."""
+
+    lumped = True

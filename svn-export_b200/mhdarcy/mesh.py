@@ -1,0 +1,159 @@
+"""Meshes as flat arrays: the synthetic Kuhn cube meshes and a gmsh 2.2 ASCII reader.
+
+The gmsh reader follows GmshMeshReader (src/mesh/msh_gmshreader.cc:125-260): elements keep
+file order; an element whose physical region name starts with '.' is a boundary element
+(read_physical_names, msh_gmshreader.cc:242-262); element types 1/2/4/15 are lines,
+triangles, tetrahedra and points.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib, check
+
+
+@dataclass
+class Mesh:
+    nodes: np.ndarray                      # (n_nodes, 3) float64
+    el_dim: np.ndarray                     # (n_el,) int32
+    el_nodes: np.ndarray                   # (n_el, 4) int32, -1 padded
+    bc_dim: np.ndarray = None              # (n_bc,) int32
+    bc_nodes: np.ndarray = None            # (n_bc, 4) int32
+    el_region: np.ndarray = None           # physical region id per bulk element
+    bc_region: np.ndarray = None           # physical region id per boundary element
+    el_id: np.ndarray = None               # gmsh element ids
+    region_names: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        self.nodes = np.ascontiguousarray(self.nodes, dtype=np.float64).reshape(-1, 3)
+        self.el_dim = np.ascontiguousarray(self.el_dim, dtype=np.int32)
+        self.el_nodes = np.ascontiguousarray(self.el_nodes, dtype=np.int32).reshape(-1, 4)
+        if self.bc_dim is None:
+            self.bc_dim = np.zeros(0, np.int32)
+            self.bc_nodes = np.zeros((0, 4), np.int32)
+        self.bc_dim = np.ascontiguousarray(self.bc_dim, dtype=np.int32)
+        self.bc_nodes = np.ascontiguousarray(self.bc_nodes, dtype=np.int32).reshape(-1, 4)
+
+    @property
+    def n_elements(self):
+        return len(self.el_dim)
+
+    def desc(self):
+        """mh_mesh_desc pointing into this mesh's arrays (keep the mesh alive while used)."""
+        d = _lib.MeshDesc()
+        d.n_nodes = len(self.nodes)
+        d.node_xyz = _lib.ptr(self.nodes, C.c_double)
+        d.n_elements = len(self.el_dim)
+        d.el_dim = _lib.ptr(self.el_dim, C.c_int32)
+        d.el_nodes = _lib.ptr(self.el_nodes, C.c_int32)
+        d.n_bc_elements = len(self.bc_dim)
+        d.bc_dim = _lib.ptr(self.bc_dim, C.c_int32) if len(self.bc_dim) else None
+        d.bc_nodes = _lib.ptr(self.bc_nodes, C.c_int32) if len(self.bc_dim) else None
+        return d
+
+    def centres(self):
+        """Element barycentres (Element::centre, src/mesh/elements.cc:139-150)."""
+        n = self.el_dim + 1
+        idx = np.where(self.el_nodes >= 0, self.el_nodes, 0)
+        pts = self.nodes[idx]                                  # (n_el, 4, 3)
+        mask = (np.arange(4)[None, :] < n[:, None])[..., None]
+        return (pts * mask).sum(axis=1) / n[:, None]
+
+    def bc_centres(self):
+        if len(self.bc_dim) == 0:
+            return np.zeros((0, 3))
+        n = self.bc_dim + 1
+        idx = np.where(self.bc_nodes >= 0, self.bc_nodes, 0)
+        pts = self.nodes[idx]
+        mask = (np.arange(4)[None, :] < n[:, None])[..., None]
+        return (pts * mask).sum(axis=1) / n[:, None]
+
+
+def cube_mesh(n, planes=(), lines=()):
+    """Kuhn mesh of the unit cube (6 tetrahedra per cube of an n^3 grid).
+
+    planes: iterable of (axis, grid_index) fracture planes (2n^2 triangles each).
+    lines:  iterable of (axis, a, b) 1D channels along `axis` through grid indices (a, b) of the
+            two other axes in increasing axis order (n segments each).
+    """
+    planes = list(planes)
+    lines = list(lines)
+    pa = np.array([p[0] for p in planes] or [0], np.int32)
+    pi = np.array([p[1] for p in planes] or [0], np.int32)
+    la = np.array([l[0] for l in lines] or [0], np.int32)
+    l1 = np.array([l[1] for l in lines] or [0], np.int32)
+    l2 = np.array([l[2] for l in lines] or [0], np.int32)
+    h = C.c_void_p()
+    check(lib.mh_cube_mesh_create(n, len(planes), _lib.ptr(pa, C.c_int32), _lib.ptr(pi, C.c_int32),
+                                  len(lines), _lib.ptr(la, C.c_int32), _lib.ptr(l1, C.c_int32),
+                                  _lib.ptr(l2, C.c_int32), C.byref(h)))
+    try:
+        d = _lib.MeshDesc()
+        check(lib.mh_mesh_describe(h, C.byref(d)))
+        nodes = np.ctypeslib.as_array(d.node_xyz, shape=(d.n_nodes * 3,)).reshape(-1, 3).copy()
+        dim = np.ctypeslib.as_array(d.el_dim, shape=(d.n_elements,)).copy()
+        eln = np.ctypeslib.as_array(d.el_nodes, shape=(d.n_elements * 4,)).reshape(-1, 4).copy()
+    finally:
+        lib.mh_mesh_destroy(h)
+    return Mesh(nodes, dim, eln)
+
+
+def read_gmsh(path):
+    """Reads a gmsh 2.2 ASCII mesh (nodes, elements, physical names)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    i = 0
+    names = {}
+    node_ids = []
+    coords = []
+    bulk = []
+    bnd = []
+    boundary_regions = set()
+    while i < len(lines):
+        s = lines[i].strip()
+        if s == "$PhysicalNames":
+            n = int(lines[i + 1])
+            for k in range(n):
+                parts = lines[i + 2 + k].split(None, 2)
+                dim, rid, name = int(parts[0]), int(parts[1]), parts[2].strip().strip('"')
+                names[rid] = name
+                if name.startswith("."):
+                    boundary_regions.add(rid)
+            i += n + 2
+        elif s == "$Nodes":
+            n = int(lines[i + 1])
+            for k in range(n):
+                p = lines[i + 2 + k].split()
+                node_ids.append(int(p[0]))
+                coords.append([float(p[1]), float(p[2]), float(p[3])])
+            i += n + 2
+        elif s == "$Elements":
+            n = int(lines[i + 1])
+            nmap = {nid: k for k, nid in enumerate(node_ids)}
+            tdim = {1: 1, 2: 2, 4: 3, 15: 0}
+            for k in range(n):
+                p = [int(v) for v in lines[i + 2 + k].split()]
+                eid, etype, ntags = p[0], p[1], p[2]
+                dim = tdim[etype]
+                region = p[3]
+                nd = [nmap[v] for v in p[3 + ntags:3 + ntags + dim + 1]]
+                nd = nd + [-1] * (4 - len(nd))
+                rec = (eid, dim, nd, region)
+                if region in boundary_regions:
+                    bnd.append(rec)
+                elif dim > 0:
+                    bulk.append(rec)
+            i += n + 2
+        else:
+            i += 1
+    m = Mesh(np.array(coords), np.array([r[1] for r in bulk], np.int32),
+             np.array([r[2] for r in bulk], np.int32),
+             np.array([r[1] for r in bnd], np.int32) if bnd else None,
+             np.array([r[2] for r in bnd], np.int32).reshape(-1, 4) if bnd else None)
+    m.el_region = np.array([r[3] for r in bulk], np.int32)
+    m.bc_region = np.array([r[3] for r in bnd], np.int32)
+    m.el_id = np.array([r[0] for r in bulk], np.int64)
+    m.region_names = names
+    return m

@@ -1,0 +1,196 @@
+"""Generates the golden fixtures under tests/golden/ from the Flow123d reference tree.
+
+Run once in a checkout that has the reference sources (default /root/reference):
+    python tests/golden/make_fixtures.py [REFERENCE_ROOT]
+Each case is written as <case>.npz holding the mesh (nodes, bulk and boundary elements with
+their physical regions), the coefficient and boundary data of the case's .con file (evaluated
+the way the reference evaluates them: element fields per region, boundary fields at the
+boundary element's barycentre, bc_piezo_head converted to pressure by adding the potential
+(0,0,-1).x as FieldAddPotential does), and the reference's own results:
+  * t01            tests/01_steady_flow_123d (flow_gmsh.con): ref_output raw_output.txt, i.e.
+                   per element pressure, barycentric flux, side (edge) pressures, side fluxes;
+  * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output;
+  * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
+  * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5.
+The parsers here are self-contained (independent of the package under test).
+"""
+import os
+import re
+import sys
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.dirname(os.path.abspath(__file__))
+TDIM = {1: 1, 2: 2, 4: 3, 15: 0}
+
+
+def parse_gmsh(path):
+    txt = open(path).read().split("\n")
+    names, node_ids, xyz, elems = {}, [], [], []
+    i = 0
+    while i < len(txt):
+        t = txt[i].strip()
+        if t == "$PhysicalNames":
+            n = int(txt[i + 1])
+            for k in range(n):
+                d, rid, nm = txt[i + 2 + k].split(None, 2)
+                names[int(rid)] = nm.strip().strip('"')
+            i += n + 2
+        elif t == "$Nodes":
+            n = int(txt[i + 1])
+            for k in range(n):
+                p = txt[i + 2 + k].split()
+                node_ids.append(int(p[0]))
+                xyz.append([float(v) for v in p[1:4]])
+            i += n + 2
+        elif t == "$Elements":
+            n = int(txt[i + 1])
+            for k in range(n):
+                p = [int(v) for v in txt[i + 2 + k].split()]
+                elems.append(p)
+            i += n + 2
+        else:
+            i += 1
+    nmap = {nid: k for k, nid in enumerate(node_ids)}
+    bulk, bnd = [], []
+    for p in elems:
+        eid, et, nt = p[0], p[1], p[2]
+        d = TDIM[et]
+        reg = p[3]
+        nd = [nmap[v] for v in p[3 + nt:3 + nt + d + 1]] + [-1] * (3 - d)
+        if names.get(reg, "").startswith("."):
+            bnd.append((eid, d, nd, reg))
+        elif d > 0:
+            bulk.append((eid, d, nd, reg))
+    return dict(
+        nodes=np.array(xyz), el_id=np.array([b[0] for b in bulk]), el_dim=np.array([b[1] for b in bulk], np.int32),
+        el_nodes=np.array([b[2] for b in bulk], np.int32), el_region=np.array([b[3] for b in bulk], np.int32),
+        bc_id=np.array([b[0] for b in bnd]), bc_dim=np.array([b[1] for b in bnd], np.int32),
+        bc_nodes=np.array([b[2] for b in bnd], np.int32).reshape(-1, 4),
+        bc_region=np.array([b[3] for b in bnd], np.int32)), names
+
+
+def centres(nodes, dims, conn):
+    out = np.zeros((len(dims), 3))
+    for k, (d, c) in enumerate(zip(dims, conn)):
+        out[k] = nodes[c[:d + 1]].mean(axis=0)
+    return out
+
+
+def vtu_cell_array(path, name):
+    txt = open(path).read()
+    m = re.search(r'<DataArray[^>]*Name="' + re.escape(name) + r'"[^>]*>(.*?)</DataArray>', txt, re.S)
+    return np.array([float(v) for v in m.group(1).split()])
+
+
+def raw_output(path):
+    lines = open(path).read().split("\n")
+    k = next(i for i, l in enumerate(lines) if l.startswith("$FlowField"))
+    n = int(lines[k + 2])
+    ids, p, flux, ns, sp, sf = [], [], [], [], np.zeros((n, 4)), np.zeros((n, 4))
+    for j in range(n):
+        v = lines[k + 3 + j].split()
+        ids.append(int(v[0]))
+        p.append(float(v[1]))
+        flux.append([float(x) for x in v[2:5]])
+        m = int(v[5])
+        ns.append(m)
+        sp[j, :m] = [float(x) for x in v[6:6 + m]]
+        sf[j, :m] = [float(x) for x in v[6 + m:6 + 2 * m]]
+    return dict(ref_el_id=np.array(ids), ref_pressure=np.array(p), ref_flux=np.array(flux),
+                ref_n_sides=np.array(ns, np.int32), ref_side_pressure=sp, ref_side_flux=sf)
+
+
+def case(mesh_path, bulk, bcs, extra, out_name, meta):
+    m, names = parse_gmsh(mesh_path)
+    rid = {v: k for k, v in names.items()}
+    ne, nb = len(m["el_dim"]), len(m["bc_dim"])
+    f = dict(conductivity=np.ones(ne), anisotropy=np.ones(ne), cross_section=np.ones(ne), sigma=np.ones(ne),
+             water_source_density=np.zeros(ne), storativity=np.ones(ne), init_pressure=np.zeros(ne))
+    for reg, vals in bulk.items():
+        sel = m["el_region"] == rid[reg]
+        assert sel.any(), reg
+        for k, v in vals.items():
+            f[k][sel] = v
+    bc_c = centres(m["nodes"], m["bc_dim"], m["bc_nodes"])
+    b = dict(bc_type=np.zeros(nb, np.int32), bc_pressure=np.zeros(nb), bc_flux=np.zeros(nb),
+             bc_robin_sigma=np.zeros(nb))
+    types = {"none": 0, "dirichlet": 1, "neumann": 2, "robin": 3}
+    for reg, spec in bcs.items():
+        sel = np.where(m["bc_region"] == rid[reg])[0]
+        assert len(sel), reg
+        b["bc_type"][sel] = types[spec["type"]]
+        for key in ("pressure", "flux", "robin_sigma"):
+            if key in spec:
+                b["bc_" + key][sel] = [spec[key](*bc_c[i]) for i in sel]
+        if "piezo_head" in spec:  # FieldAddPotential with gravity (0,0,-1,0): p = h - z
+            b["bc_pressure"][sel] = [spec["piezo_head"](*bc_c[i]) - bc_c[i][2] for i in sel]
+    np.savez_compressed(os.path.join(OUT, out_name + ".npz"), **m, **f, **b, **extra,
+                        meta=np.array(meta))
+    print(out_name, ne, "elements", nb, "boundary elements", list(extra))
+
+
+def main():
+    t = lambda *p: os.path.join(REF, "tests", *p)
+    # test 01: 1D-2D-3D steady flow, n_schurs = 2
+    case(t("01_steady_flow_123d", "input", "test1_new.msh"),
+         {"1d_channel": {"anisotropy": 10.0}, "2d_fraction_1": {"anisotropy": 1.0},
+          "2d_fraction_2": {"anisotropy": 1.0}, "3d_cube": {"anisotropy": 0.1}},
+         {r: {"type": "dirichlet", "pressure": lambda x, y, z: x - z}
+          for r in (".1d_channel", ".2d_fraction_1", ".2d_fraction_2", ".3d_cube")},
+         raw_output(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "raw_output.txt")),
+         "t01", "tests/01_steady_flow_123d flow_gmsh.con; raw_output %.8g; solver -ksp_rtol 1e-10")
+    # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
+    vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
+                                      "test05-000000.vtu"), "pressure_elements_[L]")
+    case(t("05_flow_boundary_conditions", "input", "test05.msh"), {"plane": {"anisotropy": 1.0}},
+         {".bc_south": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0},
+          ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
+          ".bc_north": {"type": "dirichlet", "pressure": lambda x, y, z: x},
+          ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure": vtu5("flow_dirichlet.con")}, "t05_dirichlet", "tests/05 flow_dirichlet.con VTK")
+    case(t("05_flow_boundary_conditions", "input", "test05.msh"), {"plane": {"anisotropy": 1.0}},
+         {".bc_south": {"type": "neumann", "flux": lambda x, y, z: x},
+          ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
+          ".bc_north": {"type": "neumann", "flux": lambda x, y, z: -x},
+          ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure": vtu5("flow_neumann.con")}, "t05_neumann", "tests/05 flow_neumann.con VTK")
+    case(t("05_flow_boundary_conditions", "input", "test05.msh"), {"plane": {"anisotropy": 1.0}},
+         {".bc_south": {"type": "robin", "pressure": lambda x, y, z: -2 * x, "robin_sigma": lambda x, y, z: 0.5},
+          ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
+          ".bc_north": {"type": "robin", "pressure": lambda x, y, z: 3 * x, "robin_sigma": lambda x, y, z: 0.5},
+          ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure": vtu5("flow_robin.con")}, "t05_robin", "tests/05 flow_robin.con VTK")
+    # test 06: dimension coupling, known answers p2 = -3 (head), p1 = -2.5
+    case(t("06_flow_coupling", "input", "test6_32d.msh"),
+         {"2d_fraction": {"conductivity": 16.0, "sigma": 1.0, "cross_section": 10.0,
+                          "water_source_density": -2.0 / 10.0},
+          "3d_cube": {"conductivity": 2.0}},
+         {".2d_fraction": {"type": "neumann", "flux": lambda x, y, z: 0.0},
+          ".3d_cube": {"type": "dirichlet", "piezo_head": lambda x, y, z: z}},
+         {"ref_pressure": vtu_cell_array(t("06_flow_coupling", "ref_output", "flow_32d.con", "test6_32d",
+                                           "test6_32d-000000.vtu"), "pressure_elements_[L]")},
+         "t06_32", "tests/06 flow_32d.con VTK; analytic 2D piezometric head -3")
+    case(t("06_flow_coupling", "input", "test6_21d.msh"),
+         {"plane": {"conductivity": 5.0, "cross_section": 10.0},
+          "channel": {"conductivity": 50.0, "cross_section": 20.0, "sigma": 2.0,
+                      "water_source_density": -1.0 / 20.0 * (10.0 * 5.0)}},
+         {".plane": {"type": "dirichlet", "piezo_head": lambda x, y, z: x},
+          ".channel": {"type": "neumann", "flux": lambda x, y, z: 0.0}},
+         {"ref_pressure": vtu_cell_array(t("06_flow_coupling", "ref_output", "flow_21d.con", "test6_21d",
+                                           "test6_21d-000000.vtu"), "pressure_elements_[L]")},
+         "t06_21", "tests/06 flow_21d.con VTK; analytic 1D pressure -2.5")
+    # test 10: unsteady MH, dt = 0.01, outputs every 0.1 up to 0.5
+    steps = [vtu_cell_array(t("10_unsteady_2d", "ref_output", "flow_MH.con", "test10", "test10-%06d.vtu" % k),
+                            "pressure_elements_[L]") for k in range(6)]
+    case(t("10_unsteady_2d", "input", "test10.msh"),
+         {"plane": {"anisotropy": 0.02, "storativity": 1.0, "init_pressure": 0.0}},
+         {".bc_inflow": {"type": "dirichlet", "pressure": lambda x, y, z: 100.0},
+          ".bc_outflow": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure_steps": np.array(steps), "ref_times": np.arange(6) * 0.1, "dt": np.array(0.01)},
+         "t10_mh", "tests/10_unsteady_2d flow_MH.con VTK every 0.1")
+
+
+if __name__ == "__main__":
+    main()
