@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark: steady MH Darcy solves/s to relative residual 1e-10 on one B200.
+
+Workload (default): the n=64 fractured Kuhn cube — 1,572,864 tetrahedra, the 8,192 fracture
+triangles of the z=0.5 plane (delta=1e-3, K=1e-3), a 64-segment 1D channel along x at
+y=z=0.5 (delta=1e-4, K=1e-2), log10 K ~ N(-6, 1.5) Gaussian-correlated with correlation
+length 0.1, Dirichlet p=1 at x=0 / p=0 at x=1.  Synthetic, seeded (no public dataset).
+
+A step is one full solve: local MH assembly + both Schur eliminations (K1), the Krylov solve
+of the edge system to FP64 true relative residual <= 1e-10 (Jacobi-scaled and unscaled), and
+back-substitution of element pressures and side fluxes (K4), with mesh, coefficients and
+boundary data resident in HBM.  `e2e` times the same step through the public API with host
+buffers: coefficients and boundary data copied in from pinned memory every step and the full
+MH solution copied back.
+
+--impl reference times the CPU path (the FP64 C restatement of the reference in oracle/,
+OpenMP over all host threads) on a bounded sample of the same workload.
+Multi-GPU (torchrun): independent replicas, one per GPU, no data-path collective.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "svn-export_b200"))
+
+METRIC = "MH Darcy solves/s to 1e-10 residual: learned+FP32 vs plain FP64 PCG, 1 B200"
+WORKLOADS = {
+    1: "n=16 fractured Kuhn cube: 24,576 tets + 512 fracture triangles + 16 channel segments, log10 K ~ N(-6,1)",
+    2: "n=64 fractured Kuhn cube: 1,572,864 tets + 8,192 fracture triangles + 64 channel segments, "
+       "log10 K ~ N(-6,1.5) correlated (length 0.1)",
+    4: "n=48 fractured Kuhn cube: 663,552 tets + 4,608 fracture triangles, log10 K ~ N(-6,1)",
+    5: "n=96 cube: 5,308,416 tets, 6 fracture planes, 4 channels, log10 K ~ N(-7,2) correlated (0.05)",
+}
+# Jacobi-PCG iterations to 1e-10 (same algorithm and stopping rule on CPU and GPU), measured on
+# the GPU FP64 path; used to scale the CPU per-iteration sample to a full solve.
+JACOBI_PCG_ITERS = {}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2, choices=sorted(WORKLOADS))
+    ap.add_argument("--methods", default="pcg64,ir32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-iters", type=int, default=200)
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+def load_json(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- clocks ----------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- roofline -----------------
+def algorithmic_bytes(kernel, N, Z):
+    """Bytes each launch must move at minimum (every array once; no padding, no re-reads).
+    spmv:   values + column indices of the Z nonzeros, p (gathered, counted once), r read, q written.
+    update: x, r, p read and written, q read."""
+    s = 8 if kernel.endswith("64") else 4
+    if kernel.startswith("spmv"):
+        return Z * (s + 4) + 3 * s * N
+    return 7 * s * N
+
+
+def roofline(stats_list, N, Z, peaks):
+    names = ["spmv64", "update64", "spmv32", "update32"]
+    tot = [0.0] * 4
+    cnt = [0] * 4
+    for st in stats_list:
+        for k in range(4):
+            tot[k] += st["kernel_ms"][k]
+            cnt[k] += st["kernel_count"][k]
+    k = max(range(4), key=lambda i: tot[i])
+    if cnt[k] == 0:
+        return None
+    per_launch_s = tot[k] / cnt[k] / 1e3
+    bytes_ = algorithmic_bytes(names[k], N, Z)
+    achieved = bytes_ / per_launch_s / 1e9
+    peak = peaks.get("hbm_gbs") if peaks else None
+    peak_note = "measured"
+    if not peak:
+        peak, peak_note = 6650.0, "fallback"
+    traffic = None
+    tj = load_json(os.path.join(ROOT, "profiles", "traffic.json"))
+    if tj and names[k] in tj.get("bytes_per_unit", {}):
+        traffic = tj["bytes_per_unit"][names[k]] * (N if tj.get("unit") == "row" else 1)
+    share = {names[i]: round(tot[i] / max(sum(tot), 1e-30), 4) for i in range(4) if cnt[i]}
+    return {"bound": "hbm", "kernel": "k_cg_" + names[k][:-2] + "<" + ("double" if names[k].endswith("64") else "float") + ">",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_note, "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_),
+            "avg_launch_us": round(per_launch_s * 1e6, 3), "launches": cnt[k], "time_share": share}
+
+
+# ---------------------------------------------------------------- ours ------------------
+def run_ours(a, rank, world):
+    import numpy as np
+    import torch
+
+    import mhdarcy
+    from mhdarcy.cases import dirichlet_x_bc, make_case
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    stream = torch.cuda.Stream()
+    mesh, coeffs = make_case(a.config, seed=1234 + a.config + 1000 * rank)
+    system = mhdarcy.MHSystem(mesh)
+    system.set_stream(stream.cuda_stream)
+    topo = system.topology()
+    bc, _ = dirichlet_x_bc(topo, mesh)
+    system.set_coeffs(**coeffs)
+    system.set_bc(bc["bc_type"], bc["pressure"])
+    sz = system.sizes
+    N, Z = sz.n_edges, sz.schur_nnz
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32}
+    results = {}
+    clocks = ClockSampler(local) if not a.no_clocks else None
+    for name in a.methods.split(","):
+        m = methods[name]
+        for _ in range(a.warmup):
+            system.assemble()
+            st = system.solve(method=m, r_tol=1e-10)
+        barrier()
+        if clocks and not results:
+            clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        l0 = system.kernel_launches()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+        for _ in range(a.steps):
+            system.assemble()
+            stats.append(system.solve(method=m, r_tol=1e-10, profile_kernels=True))
+        with torch.cuda.stream(stream):
+            ev1.record(stream)
+        barrier()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        launches = system.kernel_launches() - l0
+        ok = all(s["status"] == 0 for s in stats)
+        results[name] = {"ms_per_solve": ms / a.steps, "solves_per_s": world * a.steps / (ms / 1e3),
+                         "iterations": stats[-1]["iterations"], "outer": stats[-1]["outer_iterations"],
+                         "rel_residual": stats[-1]["rel_residual"],
+                         "rel_residual_unscaled": stats[-1]["rel_residual_unscaled"], "converged": ok,
+                         "ms_assembly": stats[-1]["ms_assembly"], "ms_backsub": stats[-1]["ms_backsub"],
+                         "stats": stats, "launches": launches}
+    clock_info = clocks.stop() if clocks else None
+    best = max((r for r in results if results[r]["converged"]), key=lambda r: results[r]["solves_per_s"])
+    rb = results[best]
+
+    # end to end through the public API with host buffers
+    ne, nb = sz.n_elements, sz.n_boundaries
+    pin = lambda arr, dt: torch.from_numpy(np.ascontiguousarray(arr, dtype=dt)).pin_memory().numpy()
+    hc = {k: pin(v, np.float64) for k, v in coeffs.items()}
+    hbt, hbp = pin(bc["bc_type"], np.int32), pin(bc["pressure"], np.float64)
+    hsol = torch.empty(sz.mh_size, dtype=torch.float64).pin_memory().numpy()
+    import ctypes as C
+
+    from mhdarcy import _lib
+    for _ in range(max(1, a.warmup - 1)):
+        system.set_coeffs(**hc)
+        system.set_bc(hbt, hbp)
+        system.assemble()
+        system.solve(method=methods[best], r_tol=1e-10)
+        _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
+    barrier()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(a.steps):
+        system.set_coeffs(**hc)
+        system.set_bc(hbt, hbp)
+        system.assemble()
+        system.solve(method=methods[best], r_tol=1e-10)
+        _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
+    # set_coeffs uploads all six element fields (absent ones as defaults), set_bc four arrays
+    h2d = 8 * ne * 5 + nb * (4 + 8 * 3)
+    d2h = 8 * sz.mh_size
+    peaks = load_json(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+    roof = roofline(rb["stats"], N, Z, peaks)
+    out = {
+        "metric": METRIC, "value": round(rb["solves_per_s"], 4), "unit": "solves/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(rb["ms_per_solve"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if best == "pcg64" else "f32+f64",
+        "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
+        "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": best,
+                   "n_edges": N, "schur_nnz": Z, "mh_size": sz.mh_size, "elements": ne,
+                   "r_tol": 1e-10, "l2": "inputs larger than L2 (edge matrix %.0f MB)" % (sz.sell_slots * 24 / 1e6),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "e2e": {"value": round(world * a.steps / (ms_e2e / 1e3), 4), "unit": "solves/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roof,
+        "gpu_launches": int(rb["launches"]),
+        "methods": {k: {kk: vv for kk, vv in v.items() if kk != "stats"} for k, v in results.items()},
+        "dofs_per_s": round(rb["solves_per_s"] * sz.mh_size, 1),
+        "clocks": clock_info,
+    }
+    if "pcg64" in results:
+        JACOBI_PCG_ITERS[a.config] = results["pcg64"]["iterations"]
+    system.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out, (mesh, coeffs, bc, topo, N)
+
+
+# ------------------------------------------------------------ CPU path ------------------
+def cpu_sample(a, mesh=None, coeffs=None, bc=None, topo=None, n_edges=None, pcg_iters=None):
+    """Times the CPU restatement (oracle/, all host threads) on a bounded sample of the workload:
+    the threaded element-local double-Schur assembly, `cpu_sample_iters` Jacobi-PCG iterations and
+    the threaded back-substitution, projected to a full solve with the Jacobi-PCG iteration count
+    of this system (same algorithm and stopping rule as the GPU FP64 path)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+    if mesh is None:
+        import mhdarcy
+        from mhdarcy.cases import dirichlet_x_bc, make_case
+        mesh, coeffs = make_case(a.config)
+        with mhdarcy.MHSystem(mesh) as s:
+            topo = s.topology()
+            n_edges = s.n_edges
+        bc, _ = dirichlet_x_bc(topo, mesh)
+    P = O.Problem(mesh, topo, n_edges, conductivity=coeffs["conductivity"], cross_section=coeffs["cross_section"],
+                  storativity=coeffs.get("storativity", 1.0), bc_type=bc["bc_type"], bc_pressure=bc["pressure"])
+    S, r = O.schur2(P)                      # pattern (setup, untimed)
+    rp = np.ascontiguousarray(S.indptr, np.int32)
+    col = np.ascontiguousarray(S.indices, np.int32)
+    val = np.zeros(len(col))
+    rhs = np.zeros(n_edges)
+    t0 = time.perf_counter()
+    O.schur2_csr_into(P, rp, col, val, rhs)
+    t_asm = time.perf_counter() - t0
+    S.data[:] = val
+    k = a.cpu_sample_iters
+    t0 = time.perf_counter()
+    x, it, res = O.pcg_jacobi(S, rhs, rtol=1e-30, max_it=k)
+    t_iter = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    O.resolve(P, x)
+    t_res = time.perf_counter() - t0
+    iters = pcg_iters or JACOBI_PCG_ITERS.get(a.config)
+    t_solve = t_asm + t_iter * iters + t_res if iters else None
+    return {"t_asm": t_asm, "t_iter": t_iter, "t_res": t_res, "iters": iters, "t_solve": t_solve,
+            "cores": O.num_threads(),
+            "sample": "cfg%d full mesh: threaded double-Schur assembly + %d Jacobi-PCG iterations + "
+                      "back-substitution, projected to %s iterations" % (a.config, k, iters)}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return None
+    samples = []
+    for _ in range(a.warmup):
+        cpu_sample(a)
+    for _ in range(a.steps):
+        samples.append(cpu_sample(a))
+    t = statistics.median(s["t_solve"] for s in samples) if samples[0]["t_solve"] else None
+    v = round(1.0 / t, 6) if t else None
+    s0 = samples[0]
+    return {"metric": METRIC, "impl": "reference", "value": v, "unit": "solves/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(t * 1e3, 3) if t else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
+            "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": "jacobi-pcg64 (CPU)",
+                       "r_tol": 1e-10},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": s0["cores"], "kind": "port",
+                             "sample": s0["sample"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", a.gpus))
+    if a.impl == "reference":
+        out = run_reference(a)
+        if out:
+            print(json.dumps(out))
+        return
+    out, ctx = run_ours(a, rank, world)
+    if rank == 0:
+        if not a.no_cpu_baseline and world == 1:
+            mesh, coeffs, bc, topo, N = ctx
+            cb = cpu_sample(a, mesh, coeffs, bc, topo, N, out["methods"].get("pcg64", {}).get("iterations"))
+            out["cpu_baseline"] = {"value": round(1.0 / cb["t_solve"], 6) if cb["t_solve"] else None,
+                                   "unit": "solves/s", "cores": cb["cores"], "kind": "port", "sample": cb["sample"],
+                                   "detail": {k: cb[k] for k in ("t_asm", "t_iter", "t_res")}}
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -107,28 +107,43 @@ typedef struct mh_bc {
     const double  *robin_sigma;   /* Robin transfer coefficient                    */
 } mh_bc;
 
+/* Convergence is judged on the FP64 true residual r = b - S x of the edge system S x = b:
+ * both the Jacobi-scaled relative residual |D^-1/2 r|/|D^-1/2 b| (D = diag S; the norm
+ * PETSc's preconditioned CG monitors) and the unscaled |r|/|b| must be <= r_tol, or
+ * |r| <= a_tol. */
 typedef struct mh_solve_opts {
     int32_t method;         /* MH_SOLVER_*                                          */
     int32_t max_it;         /* cap on (inner) iterations, default 20000              */
-    double  r_tol;          /* stop when ||b - S x||_2 <= max(r_tol*||b||_2, a_tol)  */
-    double  a_tol;
+    double  r_tol;          /* relative tolerance (default 1e-10)                    */
+    double  a_tol;          /* absolute tolerance on |b - S x| (default 0)           */
     int32_t use_initial_guess;  /* start from the current edge pressures             */
     int32_t cheb_degree;    /* MH_SOLVER_CHEB64: polynomial degree (default 4)       */
     double  inner_rtol;     /* MH_SOLVER_IR32/FCG: inner relative tolerance (1e-5)   */
     int32_t inner_max_it;   /* inner iteration cap per refinement step (2000)        */
     int32_t iters_per_graph;/* CG iterations per captured CUDA graph launch (16)     */
-    int32_t reserved[7];
+    int32_t profile_kernels;/* 1: time every Krylov kernel with CUDA events in-graph */
+    int32_t reserved[6];
 } mh_solve_opts;
+
+/* kernel classes of mh_solve_stats.kernel_ms / kernel_count */
+#define MH_KERNEL_SPMV64   0
+#define MH_KERNEL_UPDATE64 1
+#define MH_KERNEL_SPMV32   2
+#define MH_KERNEL_UPDATE32 3
 
 typedef struct mh_solve_stats {
     int32_t status;
     int32_t iterations;         /* total Krylov iterations (inner ones for IR)       */
     int32_t outer_iterations;   /* refinement steps (IR/FCG), restarts (PCG)          */
     int32_t fell_back;          /* 1 if the flexible iteration stalled -> plain PCG   */
-    double  rel_residual;       /* final FP64 true residual ||b-Sx||/||b||            */
-    double  ms_assembly;        /* device time of assembly + Schur elimination        */
+    double  rel_residual;       /* final Jacobi-scaled relative FP64 true residual    */
+    double  ms_assembly;        /* device time of the last assembly                   */
     double  ms_solve;           /* device time of the Krylov solve                    */
     double  ms_backsub;         /* device time of back-substitution                   */
+    double  rel_residual_unscaled; /* final |b - S x| / |b|                           */
+    int64_t kernel_launches;    /* kernels launched by this call (graph nodes too)    */
+    double  kernel_ms[4];       /* with profile_kernels: summed device time of the    */
+    int32_t kernel_count[4];    /*   launches that did work, per MH_KERNEL_* class    */
     double  reserved[4];
 } mh_solve_stats;
 
@@ -158,6 +173,11 @@ void mh_mesh_destroy(mh_mesh *m);
  * topology (mh_get_sizes/mh_get_topology work) and compute calls return MH_ERR_CUDA. */
 int mh_create(const mh_mesh_desc *mesh, mh_handle **out);
 void mh_destroy(mh_handle *h);
+/* Runs all further work of the handle on the caller's cudaStream_t (NULL: the handle's own
+ * stream).  Every call still returns only after its work on that stream is complete. */
+int mh_set_stream(mh_handle *h, void *cuda_stream);
+/* Kernels launched by the handle so far (the graph nodes of captured iterations included). */
+int64_t mh_kernel_launches(const mh_handle *h);
 int mh_get_sizes(const mh_handle *h, mh_sizes *out);
 /* Topology export (any pointer may be NULL):
  *   el_side_start [n_elements+1]  first global side of each element

@@ -670,8 +670,9 @@ int orc_resolve(const orc_problem *P, double *sol) {
 
 /* ------------------------------------------------------------ Jacobi PCG -------------- */
 /* CG with diagonal preconditioning on a CSR SPD matrix, FP64, threaded with OpenMP.  Stops
- * when the recursively updated residual satisfies |r| <= rtol |b|; returns iterations, or -1
- * if max_it was reached.  res_out gets the true relative residual |b - A x| / |b|. */
+ * when the recursively updated residual satisfies both |D^-1/2 r| <= rtol |D^-1/2 b| (for
+ * Jacobi, r.z is that squared norm) and |r| <= rtol |b|; returns iterations, or -1 if max_it
+ * was reached.  res_out gets the true Jacobi-scaled relative residual. */
 static void csr_mv(int64_t n, const int32_t *rp, const int32_t *col, const double *val, const double *x, double *y) {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
@@ -694,21 +695,22 @@ int orc_pcg_jacobi(int64_t n, const int32_t *rp, const int32_t *col, const doubl
         dinv[i] = 1.0 / d;
     }
     csr_mv(n, rp, col, val, x, q);
-    double bb = 0.0, rz = 0.0;
-#pragma omp parallel for schedule(static) reduction(+ : bb, rz)
+    double bb = 0.0, bdb = 0.0, rz = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : bb, bdb, rz)
     for (int64_t i = 0; i < n; ++i) {
         r[i] = b[i] - q[i];
         z[i] = dinv[i] * r[i];
         p[i] = z[i];
         bb += b[i] * b[i];
+        bdb += b[i] * dinv[i] * b[i];
         rz += r[i] * z[i];
     }
-    const double tol2 = rtol * rtol * bb;
+    const double tol2 = rtol * rtol * bb, tol2s = rtol * rtol * bdb;
     int it = 0;
     double rr = 0.0;
 #pragma omp parallel for schedule(static) reduction(+ : rr)
     for (int64_t i = 0; i < n; ++i) rr += r[i] * r[i];
-    while (rr > tol2 && it < max_it) {
+    while ((rr > tol2 || rz > tol2s) && it < max_it) {
         csr_mv(n, rp, col, val, p, q);
         double pq = 0.0;
 #pragma omp parallel for schedule(static) reduction(+ : pq)
@@ -733,10 +735,10 @@ int orc_pcg_jacobi(int64_t n, const int32_t *rp, const int32_t *col, const doubl
     csr_mv(n, rp, col, val, x, q);
     double res = 0.0;
 #pragma omp parallel for schedule(static) reduction(+ : res)
-    for (int64_t i = 0; i < n; ++i) res += (b[i] - q[i]) * (b[i] - q[i]);
-    if (res_out) *res_out = bb > 0.0 ? sqrt(res / bb) : 0.0;
+    for (int64_t i = 0; i < n; ++i) res += (b[i] - q[i]) * dinv[i] * (b[i] - q[i]);
+    if (res_out) *res_out = bdb > 0.0 ? sqrt(res / bdb) : 0.0;
     free(r); free(z); free(p); free(q); free(dinv);
-    return (rr > tol2) ? -1 : it;
+    return (rr > tol2 || rz > tol2s) ? -1 : it;
 }
 
 int orc_num_threads(void) {

@@ -11,6 +11,10 @@ namespace mh {
 constexpr int kSliceRows = 32;       // SELL-C-sigma chunk height C (one warp, one row per lane)
 constexpr int kWarpsPerBlock = 8;    // 256-thread blocks
 constexpr int kBlockThreads = kSliceRows * kWarpsPerBlock;
+// Per-instance results of the FP64 residual kernel: {r^.r^, sum d r^2, sum d b^2, b^.b^,
+// active flag, unused...} (r^ = D^-1/2 r is the Jacobi-scaled residual, d = diag S).
+constexpr int kSumStride = 8;
+constexpr int kSumActive = 4;
 
 // Per-instance Krylov control block.  One per independent system (one for a single
 // mesh, one per realisation in a batch).  Written only by the last block of each kernel
@@ -101,6 +105,8 @@ cudaError_t launch_scale_in(const DevSystem &sys, const double *lambda, cudaStre
 cudaError_t launch_cg_init(const DevSystem &sys, double rtol2, double atol2, int max_it, int use_active,
                            cudaStream_t s);
 cudaError_t launch_cg_iteration(const DevSystem &sys, int prec, cudaStream_t s);
+cudaError_t launch_cg_spmv(const DevSystem &sys, int prec, cudaStream_t s);
+cudaError_t launch_cg_update(const DevSystem &sys, int prec, cudaStream_t s);
 // r = bh - S64 x (FP64) and per-instance sums {sum r^2, sum d r^2, sum d bh^2}.
 cudaError_t launch_residual64(const DevSystem &sys, cudaStream_t s);
 // IR helpers: start an FP32 inner solve from r; fold its correction back into x.

@@ -30,7 +30,8 @@ struct mh_handle {
     std::vector<double> ngh_meas;
     bool device = false;
     int device_id = -1;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream all work is issued on (own or caller's)
+    cudaStream_t own_stream = nullptr;  // the handle's stream; CUDA graphs are captured on it
     std::vector<void *> allocs;
     mh::ElemData ed{};
     mh::DevSystem sys{};
@@ -40,11 +41,16 @@ struct mh_handle {
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
     int time_mode = 0;
     double dt = 0.0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int graph_iters[2] = {0, 0};
+    // captured Krylov iterations: [precision 64/32][plain / with per-kernel timing events]
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_iters[2][2] = {{0, 0}, {0, 0}};
+    std::vector<cudaEvent_t> prof_ev[2];
     int32_t *h_done = nullptr;
     cudaEvent_t ev[6] = {};
     float ms_assembly = 0.f;
+    int64_t n_launch = 0;               // kernels launched so far
+    double kernel_ms[4] = {0, 0, 0, 0};
+    int32_t kernel_count[4] = {0, 0, 0, 0};
     std::string err;
 };
 
@@ -102,7 +108,8 @@ int device_setup(mh_handle *h) {
         return MH_OK;
     }
     CK(cudaGetDevice(&h->device_id));
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
     for (auto &e : h->ev) CK(cudaEventCreate(&e));
     CK(cudaHostAlloc((void **)&h->h_done, sizeof(int32_t) * 4, cudaHostAllocDefault));
     const mh::MeshData &m = h->mesh;
@@ -260,6 +267,8 @@ int assemble_impl(mh_handle *h, int mode) {
     CK(mh::launch_gather(h->as, h->sys, mode, h->stream));
     CK(mh::launch_scale(h->sys, (mode & 1) ? 1 : 0, h->stream));
     CK(cudaEventRecord(h->ev[1], h->stream));
+    for (int d = 1; d <= 3; ++d) h->n_launch += h->as.dim_count[d] > 0;
+    h->n_launch += 1 + ((mode & 1) ? 3 : 1);
     int32_t st = 0;
     CK(cudaMemcpyAsync(&st, h->as.status, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -276,44 +285,6 @@ int assemble_impl(mh_handle *h, int mode) {
     return MH_OK;
 }
 
-// Runs captured Krylov iterations until every instance reports done.
-int run_krylov(mh_handle *h, int prec, int iters_per_graph, int max_it) {
-    const int gi = prec == 64 ? 0 : 1;
-    if (!h->graph[gi] || h->graph_iters[gi] != iters_per_graph) {
-        if (h->graph[gi]) cudaGraphExecDestroy(h->graph[gi]);
-        h->graph[gi] = nullptr;
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < iters_per_graph; ++k) {
-            cudaError_t e = mh::launch_cg_iteration(h->sys, prec, h->stream);
-            if (e != cudaSuccess) {
-                cudaStreamEndCapture(h->stream, &g);
-                h->err = cudaGetErrorString(e);
-                return MH_ERR_CUDA;
-            }
-        }
-        CK(cudaStreamEndCapture(h->stream, &g));
-        cudaError_t e = cudaGraphInstantiate(&h->graph[gi], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            h->err = cudaGetErrorString(e);
-            return MH_ERR_CUDA;
-        }
-        h->graph_iters[gi] = iters_per_graph;
-    }
-    const int n_inst = h->sys.n_inst;
-    int64_t launched = 0;
-    while (true) {
-        CK(cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        if (*h->h_done >= n_inst) break;
-        if (launched > (int64_t)max_it + 2 * iters_per_graph) break;  // device caps iterations itself
-        CK(cudaGraphLaunch(h->graph[gi], h->stream));
-        launched += iters_per_graph;
-    }
-    return MH_OK;
-}
-
 int read_ctl(mh_handle *h, std::vector<mh::InstCtl> &ctl) {
     ctl.resize(h->sys.n_inst);
     CK(cudaMemcpyAsync(ctl.data(), h->sys.ctl, sizeof(mh::InstCtl) * ctl.size(), cudaMemcpyDeviceToHost, h->stream));
@@ -321,10 +292,101 @@ int read_ctl(mh_handle *h, std::vector<mh::InstCtl> &ctl) {
     return MH_OK;
 }
 
+// Captures `ipg` CG iterations (two kernels each) into a graph on the handle's own stream;
+// with `prof`, an event is recorded after every kernel so each launch can be timed.
+int capture_iterations(mh_handle *h, int prec, int ipg, bool prof) {
+    const int gi = prec == 64 ? 0 : 1, pi = prof ? 1 : 0;
+    if (h->graph[gi][pi] && h->graph_iters[gi][pi] == ipg) return MH_OK;
+    if (h->graph[gi][pi]) cudaGraphExecDestroy(h->graph[gi][pi]);
+    h->graph[gi][pi] = nullptr;
+    if (prof) {
+        auto &ev = h->prof_ev[gi];
+        while ((int)ev.size() < 2 * ipg + 1) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+    }
+    cudaStream_t cs = h->own_stream;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    if (prof) e = cudaEventRecord(h->prof_ev[gi][0], cs);
+    for (int k = 0; k < ipg && e == cudaSuccess; ++k) {
+        if (prof) {
+            e = mh::launch_cg_spmv(h->sys, prec, cs);
+            if (e == cudaSuccess) e = cudaEventRecord(h->prof_ev[gi][2 * k + 1], cs);
+            if (e == cudaSuccess) e = mh::launch_cg_update(h->sys, prec, cs);
+            if (e == cudaSuccess) e = cudaEventRecord(h->prof_ev[gi][2 * k + 2], cs);
+        } else {
+            e = mh::launch_cg_iteration(h->sys, prec, cs);
+        }
+    }
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (e2 == cudaSuccess) cudaGraphDestroy(g);
+        h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
+        return MH_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&h->graph[gi][pi], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->graph[gi][pi] = nullptr;
+        h->err = cudaGetErrorString(e);
+        return MH_ERR_CUDA;
+    }
+    h->graph_iters[gi][pi] = ipg;
+    return MH_OK;
+}
+
+// Runs captured Krylov iterations until every instance reports done.  With `prof`, the
+// kernels of the iterations that still did work are timed from the in-graph events.
+int run_krylov(mh_handle *h, int prec, int ipg, int max_it, bool prof) {
+    const int gi = prec == 64 ? 0 : 1, pi = prof ? 1 : 0;
+    int rc = capture_iterations(h, prec, ipg, prof);
+    if (rc) return rc;
+    const int n_inst = h->sys.n_inst;
+    int64_t launched = 0;
+    std::vector<mh::InstCtl> ctl;
+    int it_before = 0;
+    if (prof) {
+        if ((rc = read_ctl(h, ctl))) return rc;
+        for (auto &c : ctl) it_before = std::max(it_before, c.iter);
+    }
+    while (true) {
+        CK(cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (*h->h_done >= n_inst) break;
+        if (launched > (int64_t)max_it + 2 * ipg) break;  // the device caps iterations itself
+        CK(cudaGraphLaunch(h->graph[gi][pi], h->stream));
+        launched += ipg;
+        h->n_launch += 2 * ipg;
+        if (prof) {
+            if ((rc = read_ctl(h, ctl))) return rc;
+            int it_now = 0;
+            for (auto &c : ctl) it_now = std::max(it_now, c.iter);
+            const int active = std::min(ipg, it_now - it_before);
+            it_before = it_now;
+            const int ks = prec == 64 ? MH_KERNEL_SPMV64 : MH_KERNEL_SPMV32;
+            for (int k = 0; k < active; ++k) {
+                float a = 0.f, b = 0.f;
+                CK(cudaEventElapsedTime(&a, h->prof_ev[gi][2 * k], h->prof_ev[gi][2 * k + 1]));
+                CK(cudaEventElapsedTime(&b, h->prof_ev[gi][2 * k + 1], h->prof_ev[gi][2 * k + 2]));
+                h->kernel_ms[ks] += a;
+                h->kernel_ms[ks + 1] += b;
+                h->kernel_count[ks] += 1;
+                h->kernel_count[ks + 1] += 1;
+            }
+        }
+    }
+    return MH_OK;
+}
+
 // FP64 true residual per instance: rel = |b - S x| / |b| and abs = |b - S x| (unscaled).
 int true_residual(mh_handle *h, std::vector<double> &sums) {
     CK(mh::launch_residual64(h->sys, h->stream));
-    sums.resize(4 * (size_t)h->sys.n_inst);
+    h->n_launch += 1;
+    sums.resize(mh::kSumStride * (size_t)h->sys.n_inst);
     CK(cudaMemcpyAsync(sums.data(), h->sys.inst_sums, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -334,8 +396,32 @@ int true_residual(mh_handle *h, std::vector<double> &sums) {
 struct SolveResult {
     int status = MH_OK;
     int iterations = 0, outer = 0, fell_back = 0;
-    double rel = 0.0;
+    double rel = 0.0;       // worst Jacobi-scaled relative true residual
+    double rel_orig = 0.0;  // worst unscaled relative true residual
 };
+
+// Convergence test on the FP64 true residual of every instance: the Jacobi-scaled relative
+// residual |D^-1/2 (b - S x)| / |D^-1/2 b| and the unscaled |b - S x| / |b| must both be
+// <= r_tol (or the unscaled absolute residual <= a_tol).  Marks unconverged instances
+// active in `sums`; returns the worst ratio achieved/target (<= 1 when all converged).
+double evaluate(const mh_solve_opts &o, int n_inst, std::vector<double> &sums, SolveResult &res, bool &finite) {
+    double worst = 0.0;
+    res.rel = res.rel_orig = 0.0;
+    finite = true;
+    for (int i = 0; i < n_inst; ++i) {
+        double *s = &sums[mh::kSumStride * i];
+        double rs = std::sqrt(s[0]), bs = std::sqrt(s[3]), ro = std::sqrt(s[1]), bo = std::sqrt(s[2]);
+        double rel_s = bs > 0.0 ? rs / bs : 0.0, rel_o = bo > 0.0 ? ro / bo : 0.0;
+        if (!std::isfinite(rel_s) || !std::isfinite(rel_o)) finite = false;
+        res.rel = std::max(res.rel, rel_s);
+        res.rel_orig = std::max(res.rel_orig, rel_o);
+        double ratio = (o.r_tol > 0.0) ? std::max(rel_s, rel_o) / o.r_tol : (ro > 0.0 ? 1e300 : 0.0);
+        if (ro <= o.a_tol) ratio = 0.0;
+        s[mh::kSumActive] = ratio > 1.0 ? 1.0 : 0.0;
+        worst = std::max(worst, ratio);
+    }
+    return worst;
+}
 
 int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
     const int n_inst = h->sys.n_inst;
@@ -346,7 +432,8 @@ int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
     for (int run = 0; run < 12; ++run) {
         CK(mh::launch_reset_ctl(h->sys, h->stream));
         CK(mh::launch_cg_init(h->sys, tau * tau, 0.0, std::max(1, o.max_it - total), run > 0, h->stream));
-        int rc = run_krylov(h, 64, o.iters_per_graph, o.max_it - total);
+        h->n_launch += 1;
+        int rc = run_krylov(h, 64, o.iters_per_graph, o.max_it - total, o.profile_kernels != 0);
         if (rc) return rc;
         if ((rc = read_ctl(h, ctl))) return rc;
         int worst = 0, maxit = 0;
@@ -356,23 +443,15 @@ int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         }
         total += maxit;
         if ((rc = true_residual(h, sums))) return rc;
-        bool all_ok = true;
-        double worst_ratio = 1.0;
-        res.rel = 0.0;
-        for (int i = 0; i < n_inst; ++i) {
-            double rn = std::sqrt(sums[4 * i + 1]), bn = std::sqrt(sums[4 * i + 2]);
-            double rel = bn > 0.0 ? rn / bn : 0.0;
-            res.rel = std::max(res.rel, rel);
-            bool ok = (rel <= o.r_tol) || (rn <= o.a_tol);
-            sums[4 * i + 3] = ok ? 0.0 : 1.0;
-            if (!ok) {
-                all_ok = false;
-                worst_ratio = std::max(worst_ratio, rel / o.r_tol);
-            }
-        }
+        bool finite;
+        double worst_ratio = evaluate(o, n_inst, sums, res, finite);
         res.outer = run + 1;
         res.iterations = total;
-        if (all_ok) return MH_OK;
+        if (!finite) {
+            res.status = MH_ERR_NONFINITE;
+            return MH_OK;
+        }
+        if (worst_ratio <= 1.0) return MH_OK;
         if (worst < 0) {
             res.status = worst;
             return MH_OK;
@@ -400,29 +479,21 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
     for (int outer = 0; outer < 200; ++outer) {
         int rc = true_residual(h, sums);
         if (rc) return rc;
-        bool any = false;
-        res.rel = 0.0;
-        for (int i = 0; i < n_inst; ++i) {
-            double rn = std::sqrt(sums[4 * i + 1]), bn = std::sqrt(sums[4 * i + 2]);
-            double rel = bn > 0.0 ? rn / bn : 0.0;
-            if (!std::isfinite(rel)) {
-                res.status = MH_ERR_NONFINITE;
-                return MH_OK;
-            }
-            res.rel = std::max(res.rel, rel);
-            bool ok = (rel <= o.r_tol) || (rn <= o.a_tol);
-            sums[4 * i + 3] = ok ? 0.0 : 1.0;
-            any |= !ok;
+        bool finite;
+        double worst_ratio = evaluate(o, n_inst, sums, res, finite);
+        if (!finite) {
+            res.status = MH_ERR_NONFINITE;
+            return MH_OK;
         }
         res.outer = outer;
         res.iterations = total;
-        if (!any) return MH_OK;
+        if (worst_ratio <= 1.0) return MH_OK;
         if (total >= o.max_it) {
             res.status = MH_NOT_CONVERGED;
             return MH_OK;
         }
-        if (res.rel < 0.5 * best) {
-            best = res.rel;
+        if (worst_ratio < 0.5 * best) {
+            best = worst_ratio;
             stall = 0;
         } else if (++stall >= 4) {
             res.status = MH_NOT_CONVERGED;
@@ -433,8 +504,9 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         CK(mh::launch_reset_ctl(h->sys, h->stream));
         CK(mh::launch_ir_start(h->sys, o.inner_rtol * o.inner_rtol, std::min(o.inner_max_it, o.max_it - total),
                                h->stream));
-        if ((rc = run_krylov(h, 32, o.iters_per_graph, o.inner_max_it))) return rc;
+        if ((rc = run_krylov(h, 32, o.iters_per_graph, o.inner_max_it, o.profile_kernels != 0))) return rc;
         CK(mh::launch_ir_correct(h->sys, h->stream));
+        h->n_launch += 2;
         if ((rc = read_ctl(h, ctl))) return rc;
         int maxit = 0;
         for (auto &c : ctl) maxit = std::max(maxit, c.iter);
@@ -455,9 +527,15 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
     if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
     const bool guess = o.use_initial_guess || have_guess_default;
+    const int64_t launches0 = h->n_launch;
+    for (int k = 0; k < 4; ++k) {
+        h->kernel_ms[k] = 0.0;
+        h->kernel_count[k] = 0;
+    }
     CK(cudaEventRecord(h->ev[2], h->stream));
     if (guess) {
         CK(mh::launch_scale_in(h->sys, h->sol + h->topo.n_sides() + h->mesh.n_el, h->stream));
+        h->n_launch += 1;
     } else {
         CK(cudaMemsetAsync(h->sys.x, 0, h->sys.n_rows * sizeof(double), h->stream));
     }
@@ -476,6 +554,8 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
                           h->stream));
     CK(cudaEventRecord(h->ev[4], h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->n_launch += 1;
+    for (int d = 1; d <= 3; ++d) h->n_launch += h->as.dim_count[d] > 0;
     h->solved = true;
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -484,6 +564,12 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
         stats->outer_iterations = res.outer;
         stats->fell_back = res.fell_back;
         stats->rel_residual = res.rel;
+        stats->rel_residual_unscaled = res.rel_orig;
+        stats->kernel_launches = h->n_launch - launches0;
+        for (int k = 0; k < 4; ++k) {
+            stats->kernel_ms[k] = h->kernel_ms[k];
+            stats->kernel_count[k] = h->kernel_count[k];
+        }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
         stats->ms_solve = ms;
@@ -641,13 +727,16 @@ int mh_create(const mh_mesh_desc *md, mh_handle **out) {
 void mh_destroy(mh_handle *h) {
     if (!h) return;
     if (h->device) cudaDeviceSynchronize();
-    for (auto &g : h->graph)
-        if (g) cudaGraphExecDestroy(g);
+    for (auto &gp : h->graph)
+        for (auto &g : gp)
+            if (g) cudaGraphExecDestroy(g);
+    for (auto &evs : h->prof_ev)
+        for (auto e : evs) cudaEventDestroy(e);
     for (void *p : h->allocs) cudaFree(p);
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->h_done) cudaFreeHost(h->h_done);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
 
@@ -882,5 +971,15 @@ int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts, mh_solv
 }
 
 const char *mh_last_error(const mh_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int mh_set_stream(mh_handle *h, void *cuda_stream) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    return MH_OK;
+}
+
+int64_t mh_kernel_launches(const mh_handle *h) { return h ? h->n_launch : 0; }
 
 }  // extern "C"

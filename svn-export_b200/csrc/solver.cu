@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, 
 }
 
 // r = b - S^ x; p = r; start a CG run.  tol2 = max(rtol2 * (use_b ? b.b : r.r), atol2).
-// With use_active, instances whose flag inst_sums[4i+3] is 0 are marked done at once.
+// With use_active, instances whose flag inst_sums[kSumStride*i + kSumActive] is 0 are marked done at once.
 template <typename T, int R>
 __global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<T> A, const T *__restrict__ b, const T *__restrict__ x,
                                                            T *__restrict__ r, T *__restrict__ p,
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<T> A, const 
     const int tile = blockIdx.x;
     const int inst = tile_inst[tile];
     InstCtl *c = ctl + inst;
-    const bool active = !use_active || inst_sums[4 * inst + 3] != 0.0;
+    const bool active = !use_active || inst_sums[kSumStride * inst + kSumActive] != 0.0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sums<2> s = {{0.0, 0.0}};
 #pragma unroll
@@ -220,8 +220,10 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<T> A, const 
     }
 }
 
-// FP64 true residual r = bh - S^ x, with per-instance sums {r.r, sum d r^2, sum d bh^2}
-// (d = diag S, so the last two are the squared norms of the unscaled residual and rhs).
+// FP64 true residual r = bh - S^ x, with per-instance sums
+//   {r.r, sum d r^2, sum d bh^2, bh.bh}
+// (d = diag S: the middle two are the squared norms of the unscaled residual and rhs, the
+// outer two those of the Jacobi-scaled ones).
 template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A, const double *__restrict__ bh,
                                                               const double *__restrict__ x, const double *__restrict__ dsq,
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A
     const int inst = tile_inst[tile];
     InstCtl *c = ctl + inst;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Sums<3> s = {{0.0, 0.0, 0.0}};
+    Sums<4> s = {{0.0, 0.0, 0.0, 0.0}};
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int64_t sl = ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
@@ -252,17 +254,17 @@ __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A
         s.v[0] += rr * rr;
         s.v[1] += d * rr * rr;
         s.v[2] += d * b * b;
+        s.v[3] += b * b;
     }
-    Sums<3> tot;
-    if (tile_finish<3>(s, partial, c, tile, tot) && threadIdx.x == 0) {
-        inst_sums[4 * inst + 0] = tot.v[0];
-        inst_sums[4 * inst + 1] = tot.v[1];
-        inst_sums[4 * inst + 2] = tot.v[2];
+    Sums<4> tot;
+    if (tile_finish<4>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) inst_sums[kSumStride * inst + k] = tot.v[k];
     }
 }
 
 // Start an FP32 inner solve of S^ d = r / |r| for every instance whose outer residual is
-// above its target (inst_sums[4i+3] = 1 marks an instance as still active).
+// above its target (inst_sums[kSumStride*i + kSumActive] = 1 marks an active instance).
 template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__restrict__ r64, float *__restrict__ x32,
                                                             float *__restrict__ r32, float *__restrict__ p32,
@@ -273,8 +275,8 @@ __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__rest
     const int tile = blockIdx.x;
     const int inst = tile_inst[tile];
     InstCtl *c = ctl + inst;
-    const bool active = inst_sums[4 * inst + 3] != 0.0;
-    const double nrm = sqrt(inst_sums[4 * inst + 0]);
+    const bool active = inst_sums[kSumStride * inst + kSumActive] != 0.0;
+    const double nrm = sqrt(inst_sums[kSumStride * inst + 0]);
     const double inv = (active && nrm > 0.0) ? 1.0 / nrm : 0.0;
     Sums<1> s = {{0.0}};
 #pragma unroll
@@ -328,20 +330,31 @@ template <int R> cudaError_t cg_init_r(const DevSystem &sys, double rtol2, doubl
     return cudaGetLastError();
 }
 
-template <int R> cudaError_t cg_iter_r(const DevSystem &sys, int prec, cudaStream_t st) {
+template <int R> cudaError_t cg_spmv_r(const DevSystem &sys, int prec, cudaStream_t st) {
     const unsigned g = (unsigned)sys.n_tiles;
-    if (prec == 64) {
+    if (prec == 64)
         k_cg_spmv<double, R><<<g, kBlockThreads, 0, st>>>(view<double>(sys), sys.p, sys.q, sys.r, sys.partial, sys.ctl,
                                                           sys.tile_inst, sys.n_done);
-        k_cg_update<double, R><<<g, kBlockThreads, 0, st>>>(sys.x, sys.r, sys.p, sys.q, sys.partial, sys.ctl,
-                                                            sys.tile_inst, sys.n_done);
-    } else {
+    else
         k_cg_spmv<float, R><<<g, kBlockThreads, 0, st>>>(view<float>(sys), sys.p32, sys.q32, sys.r32, sys.partial,
                                                          sys.ctl, sys.tile_inst, sys.n_done);
+    return cudaGetLastError();
+}
+
+template <int R> cudaError_t cg_update_r(const DevSystem &sys, int prec, cudaStream_t st) {
+    const unsigned g = (unsigned)sys.n_tiles;
+    if (prec == 64)
+        k_cg_update<double, R><<<g, kBlockThreads, 0, st>>>(sys.x, sys.r, sys.p, sys.q, sys.partial, sys.ctl,
+                                                            sys.tile_inst, sys.n_done);
+    else
         k_cg_update<float, R><<<g, kBlockThreads, 0, st>>>(sys.x32, sys.r32, sys.p32, sys.q32, sys.partial, sys.ctl,
                                                            sys.tile_inst, sys.n_done);
-    }
     return cudaGetLastError();
+}
+
+template <int R> cudaError_t cg_iter_r(const DevSystem &sys, int prec, cudaStream_t st) {
+    cudaError_t e = cg_spmv_r<R>(sys, prec, st);
+    return e == cudaSuccess ? cg_update_r<R>(sys, prec, st) : e;
 }
 
 }  // namespace
@@ -352,6 +365,24 @@ cudaError_t launch_cg_init(const DevSystem &sys, double rtol2, double atol2, int
         case 1: return cg_init_r<1>(sys, rtol2, atol2, max_it, use_active, s);
         case 2: return cg_init_r<2>(sys, rtol2, atol2, max_it, use_active, s);
         case 4: return cg_init_r<4>(sys, rtol2, atol2, max_it, use_active, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_cg_spmv(const DevSystem &sys, int prec, cudaStream_t s) {
+    switch (sys.rows_per_thread) {
+        case 1: return cg_spmv_r<1>(sys, prec, s);
+        case 2: return cg_spmv_r<2>(sys, prec, s);
+        case 4: return cg_spmv_r<4>(sys, prec, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_cg_update(const DevSystem &sys, int prec, cudaStream_t s) {
+    switch (sys.rows_per_thread) {
+        case 1: return cg_update_r<1>(sys, prec, s);
+        case 2: return cg_update_r<2>(sys, prec, s);
+        case 4: return cg_update_r<4>(sys, prec, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -62,16 +62,21 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int32), ("max_it", C.c_int32), ("r_tol", C.c_double),
                 ("a_tol", C.c_double), ("use_initial_guess", C.c_int32), ("cheb_degree", C.c_int32),
                 ("inner_rtol", C.c_double), ("inner_max_it", C.c_int32),
-                ("iters_per_graph", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("iters_per_graph", C.c_int32), ("profile_kernels", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class SolveStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("outer_iterations", C.c_int32),
                 ("fell_back", C.c_int32), ("rel_residual", C.c_double), ("ms_assembly", C.c_double),
-                ("ms_solve", C.c_double), ("ms_backsub", C.c_double), ("reserved", C.c_double * 4)]
+                ("ms_solve", C.c_double), ("ms_backsub", C.c_double),
+                ("rel_residual_unscaled", C.c_double), ("kernel_launches", C.c_int64),
+                ("kernel_ms", C.c_double * 4), ("kernel_count", C.c_int32 * 4), ("reserved", C.c_double * 4)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["kernel_ms"] = list(self.kernel_ms)
+        d["kernel_count"] = list(self.kernel_count)
+        return d
 
 
 class MHError(RuntimeError):
@@ -97,6 +102,8 @@ def _load():
         "mh_mesh_destroy": (None, [vp]),
         "mh_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(vp)]),
         "mh_destroy": (None, [vp]),
+        "mh_set_stream": (C.c_int, [vp, vp]),
+        "mh_kernel_launches": (C.c_int64, [vp]),
         "mh_get_sizes": (C.c_int, [vp, C.POINTER(Sizes)]),
         "mh_get_topology": (C.c_int, [vp] + [_i32p] * 8),
         "mh_set_coeffs": (C.c_int, [vp, C.POINTER(Coeffs)]),
@@ -122,6 +129,7 @@ lib = _load()
 # every symbol the header declares, for the load/export check
 EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_error",
             "mh_cube_mesh_create", "mh_mesh_describe", "mh_mesh_destroy", "mh_create", "mh_destroy",
+            "mh_set_stream", "mh_kernel_launches",
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device", "mh_get_schur_system",
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step")

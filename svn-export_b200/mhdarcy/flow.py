@@ -16,7 +16,7 @@ from ._lib import lib, check, f64, i32, ptr
 
 def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000,
                use_initial_guess=False, inner_rtol=1e-5, inner_max_it=2000, iters_per_graph=16,
-               cheb_degree=4):
+               cheb_degree=4, profile_kernels=False):
     o = _lib.SolveOpts()
     lib.mh_solve_opts_default(C.byref(o))
     o.method = method
@@ -28,6 +28,7 @@ def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000
     o.inner_max_it = inner_max_it
     o.iters_per_graph = iters_per_graph
     o.cheb_degree = cheb_degree
+    o.profile_kernels = int(bool(profile_kernels))
     return o
 
 
@@ -44,6 +45,14 @@ class MHSystem:
         check(lib.mh_get_sizes(h, C.byref(s)))
         self.sizes = s
         self._topo = None
+
+    def set_stream(self, cuda_stream):
+        """Issue all work on the caller's cudaStream_t (an int handle, e.g. torch's
+        Stream.cuda_stream); None returns to the handle's own stream."""
+        check(lib.mh_set_stream(self.h, C.c_void_p(cuda_stream) if cuda_stream else None), self.h)
+
+    def kernel_launches(self):
+        return lib.mh_kernel_launches(self.h)
 
     def close(self):
         if self.h:

@@ -1,0 +1,259 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the reference's golden
+outputs.
+
+Tolerances:
+  * assembled edge system (K1) vs the oracle's element-local double Schur: normwise
+    |S_gpu - S_orc|_ij <= 1e-12 sqrt(S_ii S_jj), rhs likewise (pure FP64 algebra, only the
+    rounding order differs);
+  * back-substitution (K4) given the same edge pressures: 1e-12 relative;
+  * solves: the FP64 true residual recomputed by the oracle on its own S2 satisfies the
+    criterion (Jacobi-scaled and unscaled relative residual <= 1e-10, with 10% slack for the
+    different summation order), and the solution agrees with the FP64 direct solve within
+    what that residual allows (checked against the oracle's own Jacobi-PCG at the same
+    tolerance); golden fixtures agree with the reference's outputs at the reference's accuracy.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+import mhdarcy
+import oracle as O
+from helpers import cube_bc, fixture_bc, fixture_coeffs, load_fixture, oracle_problem
+from mhdarcy import _lib
+from mhdarcy.cases import make_case
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["t01", "t05_dirichlet", "t05_neumann", "t05_robin", "t06_32", "t06_21"]
+
+
+def gpu_system(mesh, coeffs, bc):
+    s = mhdarcy.MHSystem(mesh)
+    s.set_coeffs(**coeffs)
+    s.set_bc(bc["bc_type"], bc.get("pressure"), bc.get("flux"), bc.get("robin_sigma"))
+    s.assemble()
+    return s
+
+
+def fixture_case(name):
+    z, mesh = load_fixture(name)
+    s = mhdarcy.MHSystem(mesh)
+    topo = s.topology()
+    coeffs = fixture_coeffs(z)
+    bc = fixture_bc(z, topo)
+    s.close()
+    return z, mesh, coeffs, bc
+
+
+def scaled_residuals(S, r, lam):
+    d = S.diagonal()
+    res = r - S @ lam
+    rel_s = np.sqrt(np.sum(res ** 2 / d) / np.sum(r ** 2 / d))
+    rel_o = np.linalg.norm(res) / np.linalg.norm(r)
+    return rel_s, rel_o
+
+
+def assert_schur_parity(s, P):
+    rp, col, val, rhs = s.schur_system()
+    S, r = O.schur2(P)
+    import scipy.sparse as sp
+    G = sp.csr_matrix((val, col, rp), shape=S.shape)
+    d = np.sqrt(np.abs(S.diagonal()))
+    D = sp.diags(1.0 / d)
+    diff = D @ (G - S) @ D
+    assert abs(diff).max() <= 1e-12, abs(diff).max()
+    # rhs in the same (Jacobi-scaled) units
+    assert np.abs((rhs - r) / d).max() <= 1e-12 * np.abs(r / d).max(), np.abs((rhs - r) / d).max()
+    return S, r
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_fixture_schur_system(gpu, name):
+    z, mesh, coeffs, bc = fixture_case(name)
+    with gpu_system(mesh, coeffs, bc) as s:
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        assert_schur_parity(s, P)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("method", [_lib.MH_SOLVER_PCG64, _lib.MH_SOLVER_IR32])
+def test_fixture_solution(gpu, name, method):
+    z, mesh, coeffs, bc = fixture_case(name)
+    with gpu_system(mesh, coeffs, bc) as s:
+        st = s.solve(method=method, r_tol=1e-10)
+        assert st["status"] == 0 and st["rel_residual"] <= 1e-10
+        sol = s.solution()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        ref = O.solve_mh_direct(P)
+        ns, ne = s.n_sides, s.n_elements
+        scale = np.abs(ref).max()
+        assert np.abs(sol - ref).max() <= 1e-8 * scale
+        # the reference's own outputs
+        p = sol[ns:ns + ne]
+        if "ref_pressure" in z and name == "t01":
+            assert np.abs(p - z["ref_pressure"]).max() < 1e-8
+        elif "ref_pressure" in z:
+            assert np.abs(p - z["ref_pressure"]).max() < 1e-6
+
+
+def test_t01_side_values_match_raw_output(gpu):
+    z, mesh, coeffs, bc = fixture_case("t01")
+    with gpu_system(mesh, coeffs, bc) as s:
+        s.solve()
+        dh = mhdarcy.MH_DofHandler(s, s.solution())
+        for e in range(0, s.n_elements, 7):
+            n = z["el_dim"][e] + 1
+            for i in range(n):
+                assert abs(dh.side_scalar(e, i) - z["ref_side_pressure"][e, i]) < 1e-8 + 5e-9 * abs(z["ref_side_pressure"][e, i])
+                assert abs(dh.side_flux(e, i) - z["ref_side_flux"][e, i]) < 1e-8 + 5e-9 * abs(z["ref_side_flux"][e, i])
+            assert abs(dh.element_scalar(e) - z["ref_pressure"][e]) < 1e-8 + 5e-9 * abs(z["ref_pressure"][e])
+
+
+def cube(n=8, seed=7, aniso=False, lines=True):
+    mesh, coeffs = make_case(1, seed=seed, n=n)
+    if not lines:
+        mesh, coeffs = make_case(3, seed=seed, n=n)
+    if aniso:
+        rng = np.random.default_rng(seed)
+        ne = mesh.n_elements
+        Q = rng.normal(size=(ne, 3, 3))
+        A = Q @ np.transpose(Q, (0, 2, 1)) + 3 * np.eye(3)
+        coeffs["anisotropy"] = A.reshape(ne, 9)
+    s = mhdarcy.MHSystem(mesh)
+    bc = cube_bc(s, mesh)
+    s.close()
+    return mesh, coeffs, bc
+
+
+@pytest.mark.parametrize("aniso", [False, True])
+def test_cube_schur_system(gpu, aniso):
+    mesh, coeffs, bc = cube(8, aniso=aniso)
+    with gpu_system(mesh, coeffs, bc) as s:
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        assert_schur_parity(s, P)
+
+
+def test_cube_solve_and_backsub(gpu):
+    """cfg1 shape (n=16, fracture + channel, log10 K ~ N(-6,1))."""
+    mesh, coeffs = make_case(1)
+    with mhdarcy.MHSystem(mesh) as s:
+        bc = cube_bc(s, mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        S, r = assert_schur_parity(s, P)
+        lam_direct = spla.spsolve(S.tocsc(), r)
+        x_cpu, it_cpu, res_cpu = O.pcg_jacobi(S, r, rtol=1e-10)
+        err_cpu = np.abs(x_cpu - lam_direct).max()
+        for method in (_lib.MH_SOLVER_PCG64, _lib.MH_SOLVER_IR32):
+            st = s.solve(method=method, r_tol=1e-10)
+            assert st["status"] == 0, st
+            sol = s.solution()
+            ns, ne = s.n_sides, s.n_elements
+            lam = sol[ns + ne:]
+            rel_s, rel_o = scaled_residuals(S, r, lam)
+            assert rel_s <= 1.1e-10 and rel_o <= 1.1e-10, (rel_s, rel_o)
+            assert np.abs(lam - lam_direct).max() <= max(20 * err_cpu, 1e-12), (np.abs(lam - lam_direct).max(), err_cpu)
+            # back-substitution parity for the same edge pressures
+            ref = O.resolve(P, lam)
+            assert np.abs(sol[:ns] - ref[:ns]).max() <= 1e-12 * np.abs(ref[:ns]).max() + 1e-300
+            assert np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max() <= 1e-12 * np.abs(ref[ns:ns + ne]).max()
+
+
+def test_tight_tolerance_matches_direct(gpu):
+    mesh, coeffs, bc = cube(8)
+    with gpu_system(mesh, coeffs, bc) as s:
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        ref, S, r = O.solve_schur_direct(P)
+        st = s.solve(r_tol=1e-14)
+        assert st["status"] == 0
+        sol = s.solution()
+        assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+def test_unsteady_mh_matches_reference(gpu):
+    z, mesh, coeffs, bc = fixture_case("t10_mh")
+    dt = float(z["dt"])
+    with mhdarcy.MHSystem(mesh) as s:
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.unsteady_init(dt, z["init_pressure"])
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc, time_mode=1, dt=dt)
+        prev = np.zeros(s.sizes.mh_size)
+        prev[s.n_sides:s.n_sides + s.n_elements] = z["init_pressure"]
+        for step in range(1, 51):
+            st = s.unsteady_step(dt, r_tol=1e-12)
+            assert st["status"] == 0
+            sol = s.solution()
+            P.set_prev(prev)
+            ref = O.solve_mh_direct(P)
+            assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
+            prev = ref
+            if step % 10 == 0:
+                p = sol[s.n_sides:s.n_sides + s.n_elements]
+                r = z["ref_pressure_steps"][step // 10]
+                assert np.abs(p - r).max() < 1e-5 * np.abs(r).max()
+
+
+def test_unsteady_lmh_matches_oracle(gpu):
+    z, mesh, coeffs, bc = fixture_case("t10_mh")
+    dt = float(z["dt"])
+    with mhdarcy.MHSystem(mesh) as s:
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        init = np.linspace(0.0, 1.0, s.n_elements)
+        s.unsteady_init(dt, init, lumped=True)
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc, time_mode=2, dt=dt)
+        prev = np.zeros(s.sizes.mh_size)
+        ss, se = s.topology()["el_side_start"], s.topology()["side_edge"]
+        for e in range(s.n_elements):
+            n = mesh.el_dim[e] + 1
+            for i in range(n):
+                prev[s.n_sides + s.n_elements + se[ss[e] + i]] += init[e] / n
+        for step in range(5):
+            st = s.unsteady_step(dt, r_tol=1e-12)
+            assert st["status"] == 0
+            sol = s.solution()
+            P.set_prev(prev)
+            S, r = O.schur2(P)
+            lam = spla.spsolve(S.tocsc(), r)
+            ref = O.resolve(P, lam)
+            assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
+            prev = ref
+
+
+def test_errors_are_reported(gpu):
+    mesh, coeffs, bc = cube(4)
+    with mhdarcy.MHSystem(mesh) as s:
+        with pytest.raises(mhdarcy.MHError) as ei:
+            s.assemble()
+        assert ei.value.status == _lib.MH_ERR_STATE
+        bad = dict(coeffs)
+        bad["conductivity"] = coeffs["conductivity"].copy()
+        bad["conductivity"][3] = np.nan
+        with pytest.raises(mhdarcy.MHError) as ei:
+            s.set_coeffs(**bad)
+        assert ei.value.status == _lib.MH_ERR_NONFINITE
+        bad["conductivity"][3] = -1.0
+        with pytest.raises(mhdarcy.MHError) as ei:
+            s.set_coeffs(**bad)
+        assert ei.value.status == _lib.MH_ERR_INVALID
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        st = s.solve(max_it=3)
+        assert st["status"] == _lib.MH_NOT_CONVERGED
+        st = s.solve()
+        assert st["status"] == 0
+
+
+def test_degenerate_element_is_singular(gpu):
+    mesh = mhdarcy.cube_mesh(2)
+    mesh.nodes[mesh.el_nodes[0, 3]] = mesh.nodes[mesh.el_nodes[0, 0]]  # collapse a tetrahedron
+    with mhdarcy.MHSystem(mesh) as s:
+        s.set_coeffs(conductivity=np.ones(s.n_elements))
+        s.set_bc(np.ones(s.n_boundaries, np.int32), np.zeros(s.n_boundaries))
+        with pytest.raises(mhdarcy.MHError) as ei:
+            s.assemble()
+        assert ei.value.status in (_lib.MH_ERR_SINGULAR, _lib.MH_ERR_NONFINITE)

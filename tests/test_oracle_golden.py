@@ -1,0 +1,114 @@
+"""Pins the CPU oracle to the reference's own golden outputs (no GPU).
+
+t01: raw_output.txt of tests/01_steady_flow_123d, printed with %.8g after a PETSc CG solve to
+rtol 1e-10, so agreement is expected at the printing precision.  t05/t06/t10: element
+pressures of the reference's VTK outputs, solved with the reference's default tolerances
+(r_tol 1e-7), so agreement is expected at that level.  t06 also has analytic answers."""
+import numpy as np
+import pytest
+
+import oracle as O
+import topology as T
+from helpers import fixture_bc, fixture_coeffs, load_fixture, oracle_problem
+
+
+def problem(name, **kw):
+    z, mesh = load_fixture(name)
+    topo = T.build(mesh)
+    P = oracle_problem(mesh, topo, topo["n_edges"], fixture_coeffs(z), fixture_bc(z, topo), **kw)
+    return z, mesh, topo, P
+
+
+def test_t01_raw_output():
+    z, mesh, topo, P = problem("t01")
+    sol = O.solve_mh_direct(P)
+    ns, ne = P.n_sides, P.n_el
+    assert np.array_equal(z["ref_el_id"], z["el_id"])
+    p = sol[ns:ns + ne]
+    # the reference solved to PETSc rtol 1e-10 and printed %.8g: agreement to ~5e-9 absolute
+    tol = lambda ref: 1e-8 + 5e-9 * np.abs(ref)
+    assert np.all(np.abs(p - z["ref_pressure"]) <= tol(z["ref_pressure"]))
+    ss, se = topo["el_side_start"], topo["side_edge"]
+    lam = sol[ns + ne:]
+    for e in range(ne):
+        n = z["el_dim"][e] + 1
+        assert z["ref_n_sides"][e] == n
+        sp = lam[se[ss[e]:ss[e] + n]]
+        sf = sol[ss[e]:ss[e] + n]
+        np.testing.assert_array_less(np.abs(sp - z["ref_side_pressure"][e, :n]), tol(z["ref_side_pressure"][e, :n]))
+        np.testing.assert_array_less(np.abs(sf - z["ref_side_flux"][e, :n]), tol(z["ref_side_flux"][e, :n]))
+
+
+def test_t01_schur_path_equals_direct():
+    z, mesh, topo, P = problem("t01")
+    full = O.solve_mh_direct(P)
+    via_schur, S, r = O.solve_schur_direct(P)
+    assert np.abs(full - via_schur).max() <= 1e-12 * np.abs(full).max()
+    # S2 is symmetric positive definite
+    assert abs(S - S.T).max() <= 1e-14 * abs(S).max()
+    assert np.all(S.diagonal() > 0)
+
+
+@pytest.mark.parametrize("name", ["t05_dirichlet", "t05_neumann", "t05_robin"])
+def test_t05_boundary_conditions(name):
+    z, mesh, topo, P = problem(name)
+    sol = O.solve_mh_direct(P)
+    p = sol[P.n_sides:P.n_sides + P.n_el]
+    assert np.abs(p - z["ref_pressure"]).max() < 1e-6
+    # the exact solution u = xy is approximated
+    c = mesh.centres()
+    assert np.abs(p - c[:, 0] * c[:, 1]).max() < 2e-2
+
+
+def test_t06_coupling_known_answers():
+    z, mesh, topo, P = problem("t06_32")
+    sol = O.solve_mh_direct(P)
+    p = sol[P.n_sides:P.n_sides + P.n_el]
+    assert np.abs(p - z["ref_pressure"]).max() < 1e-7
+    d2 = mesh.el_dim == 2
+    head = p[d2] + mesh.centres()[d2, 2]
+    assert np.abs(head + 3.0).max() < 1e-12                        # p2 = -3 (piezometric head)
+    z, mesh, topo, P = problem("t06_21")
+    sol = O.solve_mh_direct(P)
+    p = sol[P.n_sides:P.n_sides + P.n_el]
+    assert np.abs(p - z["ref_pressure"]).max() < 1e-6
+    assert np.abs(p[mesh.el_dim == 1] + 2.5).max() < 1e-12         # p1 = -2.5
+
+
+def test_t10_unsteady_mh():
+    z, mesh, topo, P = problem("t10_mh", time_mode=1, dt=float(z_dt()))
+    prev = np.zeros(P.mh_size)
+    prev[P.n_sides:P.n_sides + P.n_el] = z["init_pressure"]
+    for step in range(1, 51):
+        P.set_prev(prev)
+        prev = O.solve_mh_direct(P)
+        if step % 10 == 0:
+            ref = z["ref_pressure_steps"][step // 10]
+            p = prev[P.n_sides:P.n_sides + P.n_el]
+            assert np.abs(p - ref).max() < 1e-7 * np.abs(ref).max() * 100
+
+
+def z_dt():
+    z, _ = load_fixture("t10_mh")
+    return z["dt"]
+
+
+def test_local_matrix_inverse_and_symmetry():
+    z, mesh = load_fixture("t01")
+    for e in (0, 10, 100, 500, 830):
+        A, Ai, det, rc = O.local_matrix(mesh, e, conductivity=2.0, cross_section=0.5)
+        assert rc == 0
+        n = A.shape[0]
+        assert np.allclose(A, A.T, rtol=1e-14, atol=0)
+        assert np.allclose(A @ Ai, np.eye(n), atol=1e-12)
+        assert np.all(np.linalg.eigvalsh(A) > 0)
+
+
+def test_cpu_pcg_matches_direct():
+    z, mesh, topo, P = problem("t01")
+    S, r = O.schur2(P)
+    x, it, res = O.pcg_jacobi(S, r, rtol=1e-12)
+    assert it > 0 and res <= 1e-12 * 1.01
+    import scipy.sparse.linalg as spla
+    lam = spla.spsolve(S.tocsc(), r)
+    assert np.abs(x - lam).max() < 1e-9
