@@ -63,6 +63,7 @@ using mh::HostSystem;
         cudaError_t e_ = (call);                                                        \
         if (e_ != cudaSuccess) {                                                        \
             h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            cudaGetLastError(); /* clear a non-sticky error so later checks see fresh state */ \
             return MH_ERR_CUDA;                                                         \
         }                                                                               \
     } while (0)
@@ -153,7 +154,7 @@ int device_setup(mh_handle *h) {
     d.bc_flux = bcf;
     d.bc_sigma = bcs;
     d.time_mode = 0;
-    d.inv_dt = 0.0;
+    d.dt = 1.0;
 
     mh::DevAssembly &a = h->as;
     a.n_blk = hs.n_blk;
@@ -202,7 +203,7 @@ int device_setup(mh_handle *h) {
     s.partial = dalloc<double>(h, hs.n_tiles * 4);
     s.ctl = dalloc<mh::InstCtl>(h, s.n_inst);
     s.n_done = dalloc<int32_t>(h, 1);
-    s.inst_sums = dalloc<double>(h, 4 * (size_t)s.n_inst);
+    s.inst_sums = dalloc<double>(h, mh::kSumStride * (size_t)s.n_inst);
     s.sum_ticket = dalloc<uint32_t>(h, s.n_inst);
     if (!s.val_raw || !s.val64 || !s.val32 || !s.dsq || !s.b || !s.bh || !s.x || !s.r || !s.p || !s.q || !s.w ||
         !s.x32 || !s.r32 || !s.p32 || !s.q32 || !s.z32 || !s.partial || !s.ctl || !s.n_done || !s.inst_sums ||
@@ -220,6 +221,7 @@ int device_setup(mh_handle *h) {
     CK(cudaMemset(s.x, 0, nr * sizeof(double)));
     CK(cudaMemset(s.x32, 0, nr * sizeof(float)));
     CK(cudaMemset(s.sum_ticket, 0, s.n_inst * sizeof(uint32_t)));
+    CK(cudaMemset(s.inst_sums, 0, mh::kSumStride * s.n_inst * sizeof(double)));
     const int64_t msize = t.n_sides() + m.n_el + t.n_edges();
     h->sol = dalloc<double>(h, msize);
     h->sol_prev = dalloc<double>(h, msize);
@@ -311,13 +313,15 @@ int capture_iterations(mh_handle *h, int prec, int ipg, bool prof) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
-    if (prof) e = cudaEventRecord(h->prof_ev[gi][0], cs);
+    // inside a capture only cudaEventRecordExternal turns a record into a graph node
+    auto rec = [&](cudaEvent_t ev) { return cudaEventRecordWithFlags(ev, cs, cudaEventRecordExternal); };
+    if (prof) e = rec(h->prof_ev[gi][0]);
     for (int k = 0; k < ipg && e == cudaSuccess; ++k) {
         if (prof) {
             e = mh::launch_cg_spmv(h->sys, prec, cs);
-            if (e == cudaSuccess) e = cudaEventRecord(h->prof_ev[gi][2 * k + 1], cs);
+            if (e == cudaSuccess) e = rec(h->prof_ev[gi][2 * k + 1]);
             if (e == cudaSuccess) e = mh::launch_cg_update(h->sys, prec, cs);
-            if (e == cudaSuccess) e = cudaEventRecord(h->prof_ev[gi][2 * k + 2], cs);
+            if (e == cudaSuccess) e = rec(h->prof_ev[gi][2 * k + 2]);
         } else {
             e = mh::launch_cg_iteration(h->sys, prec, cs);
         }
@@ -945,7 +949,7 @@ int mh_unsteady_init(mh_handle *h, int32_t lumped, double dt, const double *init
     h->time_mode = lumped ? 2 : 1;
     h->ed.time_mode = h->time_mode;
     h->dt = dt;
-    h->ed.inv_dt = 1.0 / dt;
+    h->ed.dt = dt;
     return assemble_impl(h, 3);
 }
 
@@ -956,7 +960,7 @@ int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts, mh_solv
     if (!(dt > 0.0) || !std::isfinite(dt)) return MH_ERR_INVALID;
     if (dt != h->dt || !h->assembled) {
         h->dt = dt;
-        h->ed.inv_dt = 1.0 / dt;
+        h->ed.dt = dt;
         rc = assemble_impl(h, 3);
     } else {
         rc = assemble_impl(h, 2);  // matrix unchanged: only the time-term rhs moves

@@ -37,32 +37,16 @@ __device__ __forceinline__ double v3norm(V3 a) { return sqrt(v3dot(a, a)); }
 __device__ __forceinline__ V3 v3scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
 __device__ __forceinline__ V3 v3div(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
 
-// 3x3 inverse by cofactors; a diagonal tensor is inverted entry-wise.
-__device__ __forceinline__ void inv3(const double *a, double *r) {
-    if (a[1] == 0.0 && a[2] == 0.0 && a[3] == 0.0 && a[5] == 0.0 && a[6] == 0.0 && a[7] == 0.0) {
-        for (int i = 0; i < 9; ++i) r[i] = 0.0;
-        r[0] = 1.0 / a[0];
-        r[4] = 1.0 / a[4];
-        r[8] = 1.0 / a[8];
-        return;
-    }
-    double c00 = a[4] * a[8] - a[5] * a[7];
-    double c01 = a[5] * a[6] - a[3] * a[8];
-    double c02 = a[3] * a[7] - a[4] * a[6];
-    double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
-    r[0] = c00 / det;
-    r[3] = c01 / det;
-    r[6] = c02 / det;
-    r[1] = (a[2] * a[7] - a[1] * a[8]) / det;
-    r[4] = (a[0] * a[8] - a[2] * a[6]) / det;
-    r[7] = (a[1] * a[6] - a[0] * a[7]) / det;
-    r[2] = (a[1] * a[5] - a[2] * a[4]) / det;
-    r[5] = (a[2] * a[3] - a[0] * a[5]) / det;
-    r[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+// Small-matrix inverses by the adjugate (cofactor matrix transposed over the determinant),
+// MatrixInverse of src/system/math_fce.cc:124-229; the caller applies the NUM_ZERO test.
+// The operation order is fixed (cofactors from cyclic 2x2 minors for n = 3, from 3x3 minor
+// determinants for n = 4) and the file is compiled without FMA contraction, so the element
+// arithmetic is reproducible bit for bit on any IEEE-754 FP64 unit.
+__device__ __forceinline__ double det3(double a00, double a01, double a02, double a10, double a11, double a12,
+                                       double a20, double a21, double a22) {
+    return a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) + a02 * (a10 * a21 - a11 * a20);
 }
 
-// Inverse of a small symmetric-or-not n x n matrix (n = 2,3,4) by the adjugate; returns
-// the determinant (the caller applies the NUM_ZERO singularity test).
 template <int N> __device__ __forceinline__ double inv_small(const double (&a)[N][N], double (&b)[N][N]);
 
 template <> __device__ __forceinline__ double inv_small<2>(const double (&a)[2][2], double (&b)[2][2]) {
@@ -75,54 +59,67 @@ template <> __device__ __forceinline__ double inv_small<2>(const double (&a)[2][
 }
 
 template <> __device__ __forceinline__ double inv_small<3>(const double (&a)[3][3], double (&b)[3][3]) {
-    double m00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
-    double m01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
-    double m02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
-    double det = a[0][0] * m00 + a[0][1] * m01 + a[0][2] * m02;
-    b[0][0] = m00 / det;
-    b[1][0] = m01 / det;
-    b[2][0] = m02 / det;
-    b[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
-    b[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
-    b[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
-    b[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
-    b[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
-    b[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    double cof[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int r0 = (i + 1) % 3, r1 = (i + 2) % 3, c0 = (j + 1) % 3, c1 = (j + 2) % 3;
+            cof[i][j] = a[r0][c0] * a[r1][c1] - a[r0][c1] * a[r1][c0];
+        }
+    double det = a[0][0] * cof[0][0] + a[0][1] * cof[0][1] + a[0][2] * cof[0][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) b[i][j] = cof[j][i] / det;
     return det;
 }
 
-// 4x4: Laplace expansion along the complementary 2x2 minors of rows {0,1} and {2,3}.
 template <> __device__ __forceinline__ double inv_small<4>(const double (&a)[4][4], double (&b)[4][4]) {
-    double s0 = a[0][0] * a[1][1] - a[1][0] * a[0][1];
-    double s1 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
-    double s2 = a[0][0] * a[1][3] - a[1][0] * a[0][3];
-    double s3 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
-    double s4 = a[0][1] * a[1][3] - a[1][1] * a[0][3];
-    double s5 = a[0][2] * a[1][3] - a[1][2] * a[0][3];
-    double c5 = a[2][2] * a[3][3] - a[3][2] * a[2][3];
-    double c4 = a[2][1] * a[3][3] - a[3][1] * a[2][3];
-    double c3 = a[2][1] * a[3][2] - a[3][1] * a[2][2];
-    double c2 = a[2][0] * a[3][3] - a[3][0] * a[2][3];
-    double c1 = a[2][0] * a[3][2] - a[3][0] * a[2][2];
-    double c0 = a[2][0] * a[3][1] - a[3][0] * a[2][1];
-    double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
-    b[0][0] = (a[1][1] * c5 - a[1][2] * c4 + a[1][3] * c3) / det;
-    b[0][1] = (-a[0][1] * c5 + a[0][2] * c4 - a[0][3] * c3) / det;
-    b[0][2] = (a[3][1] * s5 - a[3][2] * s4 + a[3][3] * s3) / det;
-    b[0][3] = (-a[2][1] * s5 + a[2][2] * s4 - a[2][3] * s3) / det;
-    b[1][0] = (-a[1][0] * c5 + a[1][2] * c2 - a[1][3] * c1) / det;
-    b[1][1] = (a[0][0] * c5 - a[0][2] * c2 + a[0][3] * c1) / det;
-    b[1][2] = (-a[3][0] * s5 + a[3][2] * s2 - a[3][3] * s1) / det;
-    b[1][3] = (a[2][0] * s5 - a[2][2] * s2 + a[2][3] * s1) / det;
-    b[2][0] = (a[1][0] * c4 - a[1][1] * c2 + a[1][3] * c0) / det;
-    b[2][1] = (-a[0][0] * c4 + a[0][1] * c2 - a[0][3] * c0) / det;
-    b[2][2] = (a[3][0] * s4 - a[3][1] * s2 + a[3][3] * s0) / det;
-    b[2][3] = (-a[2][0] * s4 + a[2][1] * s2 - a[2][3] * s0) / det;
-    b[3][0] = (-a[1][0] * c3 + a[1][1] * c1 - a[1][2] * c0) / det;
-    b[3][1] = (a[0][0] * c3 - a[0][1] * c1 + a[0][2] * c0) / det;
-    b[3][2] = (-a[3][0] * s3 + a[3][1] * s1 - a[3][2] * s0) / det;
-    b[3][3] = (a[2][0] * s3 - a[2][1] * s1 + a[2][2] * s0) / det;
+    double cof[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double m[9];
+            int k = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (r == i) continue;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (c == j) continue;
+                    m[k++] = a[r][c];
+                }
+            }
+            const double d = det3(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]);
+            cof[i][j] = ((i + j) % 2) ? -d : d;
+        }
+    double det = a[0][0] * cof[0][0] + a[0][1] * cof[0][1] + a[0][2] * cof[0][2] + a[0][3] * cof[0][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[i][j] = cof[j][i] / det;
     return det;
+}
+
+// Inverse of the anisotropy tensor; a diagonal tensor is inverted entry-wise.
+__device__ __forceinline__ void inv3(const double *a, double *r) {
+    if (a[1] == 0.0 && a[2] == 0.0 && a[3] == 0.0 && a[5] == 0.0 && a[6] == 0.0 && a[7] == 0.0) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) r[i] = 0.0;
+        r[0] = 1.0 / a[0];
+        r[4] = 1.0 / a[4];
+        r[8] = 1.0 / a[8];
+        return;
+    }
+    const double m[3][3] = {{a[0], a[1], a[2]}, {a[3], a[4], a[5]}, {a[6], a[7], a[8]}};
+    double inv[3][3];
+    inv_small<3>(m, inv);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r[3 * i + j] = inv[i][j];
 }
 
 // Side node tables (src/mesh/ref_element.cc:51-76).
@@ -228,32 +225,57 @@ template <> __device__ __forceinline__ double local_matrix<3>(const V3 (&X)[4], 
         V3 sc = {(a.x + b.x + d.x) / 3.0, (a.y + b.y + d.y) / 3.0, (a.z + b.z + d.z) / 3.0};
         delta[i] = 1.0 / (meas * (n.x * sc.x + n.y * sc.y + n.z * sc.z - n.x * X[i].x - n.y * X[i].y - n.z * X[i].z));
     }
-    // second moments about the centroid (exact quadratic integration over a tetrahedron)
-    double mxx = 0, myy = 0, mzz = 0, mxy = 0, mxz = 0, myz = 0;
+    // second moments about the centroid: the quadratic monomials integrate exactly to
+    // |E| (t_r t_c + M_rc / 20) (polynom_integral_tetrahedron)
+    double M[3][3];
+    const double t[3] = {c.x, c.y, c.z};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) M[r][q] = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        double dx = X[k].x - c.x, dy = X[k].y - c.y, dz = X[k].z - c.z;
-        mxx += dx * dx; myy += dy * dy; mzz += dz * dz;
-        mxy += dx * dy; mxz += dx * dz; myz += dy * dz;
+        const double d[3] = {X[k].x - t[0], X[k].y - t[1], X[k].z - t[2]};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) M[r][q] += d[r] * d[q];
     }
-    double Ixx = c.x * c.x + mxx / 20.0, Iyy = c.y * c.y + myy / 20.0, Izz = c.z * c.z + mzz / 20.0;
-    double Ixy = c.x * c.y + mxy / 20.0, Ixz = c.x * c.z + mxz / 20.0, Iyz = c.y * c.z + myz / 20.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = i; j < 4; ++j) {
-            // polynomial (x - X_j)^T R (x - X_i), integrated over the tetrahedron
-            V3 Xi = X[i], Xj = X[j];
-            double p0 = R[0] * Xi.x * Xj.x + R[1] * Xi.y * Xj.x + R[2] * Xi.z * Xj.x + R[3] * Xi.x * Xj.y +
-                        R[4] * Xi.y * Xj.y + R[5] * Xi.z * Xj.y + R[6] * Xi.x * Xj.z + R[7] * Xi.y * Xj.z +
-                        R[8] * Xi.z * Xj.z;
-            double px = -(R[0] * Xi.x + R[1] * Xi.y + R[2] * Xi.z + R[0] * Xj.x + R[3] * Xj.y + R[6] * Xj.z);
-            double py = -(R[3] * Xi.x + R[4] * Xi.y + R[5] * Xi.z + R[1] * Xj.x + R[4] * Xj.y + R[7] * Xj.z);
-            double pz = -(R[6] * Xi.x + R[7] * Xi.y + R[8] * Xi.z + R[2] * Xj.x + R[5] * Xj.y + R[8] * Xj.z);
-            double integral = vol * (p0 + px * c.x + py * c.y + pz * c.z + (R[1] + R[3]) * Ixy +
-                                     (R[2] + R[6]) * Ixz + (R[5] + R[7]) * Iyz + R[0] * Ixx + R[4] * Iyy +
-                                     R[8] * Izz);
-            A[i][j] = scale * delta[i] * delta[j] * integral;
+            // coefficients of (x - X_j)^T R (x - X_i) in the monomial basis
+            // {1, x, y, z, xy, xz, yz, x^2, y^2, z^2} (calc_polynom_tetrahedron)
+            const double Xi[3] = {X[i].x, X[i].y, X[i].z}, Xj[3] = {X[j].x, X[j].y, X[j].z};
+            double poly[10];
+            poly[0] = 0.0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) poly[0] += R[3 * r + q] * Xi[q] * Xj[r];
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                poly[1 + q] = -(R[3 * q] * Xi[0] + R[3 * q + 1] * Xi[1] + R[3 * q + 2] * Xi[2] + R[q] * Xj[0] +
+                                R[3 + q] * Xj[1] + R[6 + q] * Xj[2]);
+            poly[4] = R[1] + R[3];
+            poly[5] = R[2] + R[6];
+            poly[6] = R[5] + R[7];
+            poly[7] = R[0];
+            poly[8] = R[4];
+            poly[9] = R[8];
+            double rc = 0.0;
+            rc += poly[0] * vol;
+            rc += poly[1] * vol * t[0];
+            rc += poly[2] * vol * t[1];
+            rc += poly[3] * vol * t[2];
+            rc += poly[4] * vol * (t[0] * t[1] + 1.0 / 20.0 * M[0][1]);
+            rc += poly[5] * vol * (t[0] * t[2] + 1.0 / 20.0 * M[0][2]);
+            rc += poly[6] * vol * (t[1] * t[2] + 1.0 / 20.0 * M[1][2]);
+            rc += poly[7] * vol * (t[0] * t[0] + 1.0 / 20.0 * M[0][0]);
+            rc += poly[8] * vol * (t[1] * t[1] + 1.0 / 20.0 * M[1][1]);
+            rc += poly[9] * vol * (t[2] * t[2] + 1.0 / 20.0 * M[2][2]);
+            A[i][j] = scale * delta[i] * delta[j] * rc;
             A[j][i] = A[i][j];
         }
     return vol;
@@ -317,11 +339,11 @@ template <int DIM> __device__ __forceinline__ void build_local(const ElemData &d
     double dEE = 0.0;
     L.lmh_coef = 0.0;
     if (d.time_mode == 1) {
-        double tt = -d.storativity[e] * meas * d.inv_dt;
+        double tt = -d.storativity[e] * meas / d.dt;
         dEE += tt;
         bE += tt * d.prev_pressure[e];
     } else if (d.time_mode == 2) {
-        L.lmh_coef = meas * d.storativity[e] * delta * d.inv_dt / (double)N;
+        L.lmh_coef = meas * d.storativity[e] * delta / d.dt / (double)N;
     }
     L.src_side = -1.0 * meas * delta * d.source[e] / (double)N;
 

@@ -34,7 +34,7 @@ struct ElemData {
     const double *bc_pressure, *bc_flux, *bc_sigma;
     // unsteady time term
     int32_t time_mode;            // 0 steady, 1 MH (element diagonal), 2 LMH (edge diagonal)
-    double inv_dt;
+    double dt;
     const double *prev_pressure;  // MH: element pressures of the previous step [n_el]
     const double *prev_edge;      // LMH: edge pressures of the previous step  [n_edges]
 };
