@@ -223,6 +223,29 @@ int mh_unsteady_init(mh_handle *h, int32_t lumped, double dt, const double *init
 int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts,
                      mh_solve_stats *stats);
 
+/* ---- residual check without device allocation --------------------------------------- */
+/* No counterpart in the reference: Flow123d leaves this check to PETSc's KSP monitor.
+ * For callers that cannot call cudaMalloc at the point where they need to check a solution:
+ * code that runs after a device allocation has already failed and must decide whether the
+ * last iterate is usable, or a host framework that reserves the whole device for its own
+ * memory pool (PyTorch's caching allocator, a PETSc/MPI pool) and forbids raw allocations.
+ *
+ * Computes r = b - S x for an n x n CSR matrix (row_ptr [n+1], col/val [nnz]) and writes
+ *   out[0] = |D^-1/2 r| / |D^-1/2 b|   (D = diag S; the norm mh_solve judges convergence by)
+ *   out[1] = |r| / |b|,  out[2] = |r|,  out[3] = |b|
+ * and, if r is not NULL, the residual vector.  Every pointer is a device pointer owned by
+ * the caller; work runs on cuda_stream (NULL: the legacy default stream) and is complete
+ * when the call returns.  The call allocates nothing and calls no allocating routine: its
+ * scratch is a fixed array inside the library (about 512 KiB, held on every GPU that loads
+ * the library until the process exits), so n is limited to MH_NOALLOC_MAX_ROWS and larger n
+ * is rejected with MH_ERR_INVALID.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be serialised by
+ * the caller. */
+#define MH_NOALLOC_MAX_ROWS (16384 * 256)
+int mh_csr_residual_noalloc(int64_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
+                            const double *b, const double *x, double *r, double *out, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

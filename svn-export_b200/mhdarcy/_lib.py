@@ -116,6 +116,7 @@ def _load():
         "mh_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "mh_unsteady_init": (C.c_int, [vp, C.c_int32, C.c_double, _f64p]),
         "mh_unsteady_step": (C.c_int, [vp, C.c_double, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+        "mh_csr_residual_noalloc": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -132,7 +133,9 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_set_stream", "mh_kernel_launches",
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device", "mh_get_schur_system",
-            "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step")
+            "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc")
+
+MH_NOALLOC_MAX_ROWS = 16384 * 256
 
 
 def ptr(a, ctype):
