@@ -118,8 +118,9 @@ typedef struct mh_solve_opts {
     double  a_tol;          /* absolute tolerance on |b - S x| (default 0)           */
     int32_t use_initial_guess;  /* start from the current edge pressures             */
     int32_t cheb_degree;    /* MH_SOLVER_CHEB64: polynomial degree (default 4)       */
-    double  inner_rtol;     /* MH_SOLVER_IR32/FCG: inner relative tolerance (1e-5)   */
-    int32_t inner_max_it;   /* inner iteration cap per refinement step (2000)        */
+    double  inner_rtol;     /* MH_SOLVER_IR32: FP32 residual reduction between two FP64
+                               residual replacements (reliable updates), default 0.1 */
+    int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000) */
     int32_t iters_per_graph;/* CG iterations per captured CUDA graph launch (16)     */
     int32_t profile_kernels;/* 1: time every Krylov kernel with CUDA events in-graph */
     int32_t reserved[6];

@@ -8,10 +8,14 @@
 //           alpha = rho/(p.q) and beta from rho_new = rho - 2 alpha r.q + alpha^2 q.q;
 //   update: x += alpha p, r -= alpha q, p = r + beta p, partial r.r; the last block stores the
 //           exact rho for the next alpha and applies the stopping test.
-// Reductions are deterministic: each tile writes a partial, the last-arriving block of an
-// instance (atomic ticket, no spin-waits) sums that instance's partials in a fixed order.
-// Tiles never straddle instances, so a batch of independent systems shares every launch and
-// each keeps its own alpha/beta/convergence (per-instance masks).
+// Work distribution: rows are grouped into tiles of 256*R rows (a 256-thread block runs R
+// 32-row slices per warp), tiles never straddle instances, and a host-built block plan gives
+// every block a contiguous run of one instance's tiles (about as many blocks as fit on the GPU
+// at once).  A block accumulates over its tiles and publishes one partial sum; the last block of
+// an instance to arrive (atomic ticket, no spin-wait) sums that instance's partials in a fixed
+// order.  The reductions are therefore deterministic, each block pays for one fence and one
+// atomic per kernel, and a batch of independent systems shares every launch while each keeps
+// its own alpha/beta/convergence (per-instance masks).
 #include <cuda_runtime.h>
 
 #include "device_system.hpp"
@@ -22,7 +26,7 @@ namespace {
 
 template <int NV> struct Sums { double v[NV]; };
 
-// Block-wide sum of NV doubles; result valid in thread 0.
+// Block-wide sum of NV doubles; result valid in thread 0.  Fixed order.
 template <int NV> __device__ __forceinline__ Sums<NV> block_sum(Sums<NV> s) {
     __shared__ double sh[kWarpsPerBlock][NV];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -46,30 +50,49 @@ template <int NV> __device__ __forceinline__ Sums<NV> block_sum(Sums<NV> s) {
     return out;
 }
 
-// Writes this tile's partial sums and returns true in every thread of the block that
+// Publishes this block's partial sums and returns true in every thread of the block that
 // arrived last for its instance; that block then holds the instance totals in `tot`
 // (thread 0 only).
 template <int NV>
-__device__ __forceinline__ bool tile_finish(Sums<NV> s, double *partial, InstCtl *c, int tile, Sums<NV> &tot) {
+__device__ __forceinline__ bool block_finish(Sums<NV> s, double *partial, InstCtl *c, Sums<NV> &tot) {
     __shared__ bool am_last;
     Sums<NV> b = block_sum<NV>(s);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) partial[(int64_t)tile * 4 + k] = b.v[k];
+        for (int k = 0; k < NV; ++k) partial[(int64_t)blockIdx.x * 4 + k] = b.v[k];
         __threadfence();
-        const unsigned n_tiles = (unsigned)(c->tile_end - c->tile_begin);
+        const unsigned n_blk = (unsigned)(c->blk_end - c->blk_begin);
         const unsigned t = atomicAdd(&c->ticket, 1u);
-        am_last = (t == n_tiles - 1);
+        am_last = (t == n_blk - 1);
     }
     __syncthreads();
     if (!am_last) return false;
     __threadfence();
+    // eight independent accumulators per thread keep eight loads in flight
+    constexpr int U = 8;
+    double acc[U][NV];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[u][k] = 0.0;
+    const int pb = c->blk_begin, pe = c->blk_end;
+    for (int t0 = pb + threadIdx.x; t0 < pe; t0 += U * blockDim.x) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < pe) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) acc[u][k] += __ldcg(&partial[(int64_t)t * 4 + k]);
+            }
+        }
+    }
     Sums<NV> a;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) a.v[k] = 0.0;
-    for (int t = c->tile_begin + threadIdx.x; t < c->tile_end; t += blockDim.x)
+    for (int k = 0; k < NV; ++k) {
+        a.v[k] = 0.0;
 #pragma unroll
-        for (int k = 0; k < NV; ++k) a.v[k] += __ldcg(&partial[(int64_t)t * 4 + k]);
+        for (int u = 0; u < U; ++u) a.v[k] += acc[u][k];
+    }
     tot = block_sum<NV>(a);
     if (threadIdx.x == 0) c->ticket = 0u;
     return true;
@@ -83,35 +106,84 @@ __device__ __forceinline__ void finish_inst(InstCtl *c, int status, int32_t *n_d
 
 template <typename T> __device__ __forceinline__ T ldg_stream(const T *p) { return __ldcs(p); }
 
+struct Plan {
+    const int32_t *inst, *tile_begin, *tile_end;
+};
+
+__device__ __forceinline__ int64_t slice_of(int tile, int warp, int R, int k) {
+    return ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
+}
+
+// y = (S^ v)[row] for the R rows this thread owns in `tile`; all loads of the first kJ slots
+// of the R slices are issued before any use (2*kJ*R streaming loads and kJ*R gathers in flight).
+template <typename T, typename V, int R>
+__device__ __forceinline__ void sell_rows(const SellView<T> &A, const V *__restrict__ v, int tile, double (&y)[R]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kJ = 8;
+    int64_t off[R];
+    int w[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int64_t sl = slice_of(tile, warp, R, k);
+        off[k] = A.slice_off[sl];
+        w[k] = (int)((A.slice_off[sl + 1] - off[k]) / kSliceRows);
+    }
+    int32_t cj[R][kJ];
+    T vj[R][kJ];
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) {
+            const bool in = j < w[k];
+            const int64_t slot = off[k] + (int64_t)j * kSliceRows + lane;
+            cj[k][j] = in ? ldg_stream(A.col + slot) : 0;
+            vj[k][j] = in ? ldg_stream(A.val + slot) : (T)0;
+        }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < kJ; ++j) acc += (double)vj[k][j] * (double)v[cj[k][j]];
+        for (int j = kJ; j < w[k]; ++j) {
+            const int64_t slot = off[k] + (int64_t)j * kSliceRows + lane;
+            acc += (double)ldg_stream(A.val + slot) * (double)v[ldg_stream(A.col + slot)];
+        }
+        y[k] = acc;
+    }
+}
+
+template <int R> __device__ __forceinline__ int64_t sell_row(int tile, int k) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    return slice_of(tile, warp, R, k) * kSliceRows + lane;
+}
+
+template <int R> __device__ __forceinline__ int64_t flat_row(int tile, int k) {
+    return ((int64_t)tile * R + k) * kBlockThreads + threadIdx.x;
+}
+
 // q = S^ p and the three dot products.
 template <typename T, int R>
 __global__ void __launch_bounds__(kBlockThreads) k_cg_spmv(SellView<T> A, const T *__restrict__ p, T *__restrict__ q,
                                                            const T *__restrict__ r, double *__restrict__ partial,
-                                                           InstCtl *__restrict__ ctl, const int32_t *__restrict__ tile_inst,
-                                                           int32_t *n_done) {
-    const int tile = blockIdx.x;
-    InstCtl *c = ctl + tile_inst[tile];
+                                                           InstCtl *__restrict__ ctl, Plan plan, int32_t *n_done) {
+    InstCtl *c = ctl + plan.inst[blockIdx.x];
     if (c->done) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sums<3> s = {{0.0, 0.0, 0.0}};
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
+        double y[R];
+        sell_rows<T, T, R>(A, p, tile, y);
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t sl = ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
-        const int64_t off = A.slice_off[sl];
-        const int w = (int)((A.slice_off[sl + 1] - off) / kSliceRows);
-        const int64_t row = sl * kSliceRows + lane;
-        double y = 0.0;
-        const T *vv = A.val + off + lane;
-        const int32_t *cc = A.col + off + lane;
-        for (int j = 0; j < w; ++j) y += (double)ldg_stream(vv + j * kSliceRows) * (double)p[ldg_stream(cc + j * kSliceRows)];
-        q[row] = (T)y;
-        const double pr = (double)p[row], rr = (double)r[row];
-        s.v[0] += pr * y;
-        s.v[1] += rr * y;
-        s.v[2] += y * y;
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = sell_row<R>(tile, k);
+            q[row] = (T)y[k];
+            const double pr = (double)p[row], rr = (double)r[row];
+            s.v[0] += pr * y[k];
+            s.v[1] += rr * y[k];
+            s.v[2] += y[k] * y[k];
+        }
     }
     Sums<3> tot;
-    if (tile_finish<3>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+    if (block_finish<3>(s, partial, c, tot) && threadIdx.x == 0) {
         const double pq = tot.v[0], rq = tot.v[1], qq = tot.v[2];
         const double rho = c->rho;
         if (rho == 0.0) {
@@ -136,27 +208,35 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_spmv(SellView<T> A, const 
 template <typename T, int R>
 __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, T *__restrict__ r, T *__restrict__ p,
                                                              const T *__restrict__ q, double *__restrict__ partial,
-                                                             InstCtl *__restrict__ ctl,
-                                                             const int32_t *__restrict__ tile_inst, int32_t *n_done) {
-    const int tile = blockIdx.x;
-    InstCtl *c = ctl + tile_inst[tile];
+                                                             InstCtl *__restrict__ ctl, Plan plan, int32_t *n_done) {
+    InstCtl *c = ctl + plan.inst[blockIdx.x];
     if (c->done) return;
     const double alpha = c->alpha, beta = c->beta;
     Sums<1> s = {{0.0}};
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
+        T pv[R], xv[R], rv[R], qv[R];
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t row = ((int64_t)tile * R + k) * kBlockThreads + threadIdx.x;
-        const double pr = (double)p[row];
-        const double xr = (double)x[row] + alpha * pr;
-        const double rr = (double)r[row] - alpha * (double)ldg_stream(q + row);
-        x[row] = (T)xr;
-        r[row] = (T)rr;
-        p[row] = (T)(rr + beta * pr);
-        const double rs = (double)(T)rr;
-        s.v[0] += rs * rs;
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = flat_row<R>(tile, k);
+            pv[k] = p[row];
+            xv[k] = x[row];
+            rv[k] = r[row];
+            qv[k] = ldg_stream(q + row);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = flat_row<R>(tile, k);
+            const double pr = (double)pv[k];
+            const double rr = (double)rv[k] - alpha * (double)qv[k];
+            x[row] = (T)((double)xv[k] + alpha * pr);
+            r[row] = (T)rr;
+            p[row] = (T)(rr + beta * pr);
+            const double rs = (double)(T)rr;
+            s.v[0] += rs * rs;
+        }
     }
     Sums<1> tot;
-    if (tile_finish<1>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+    if (block_finish<1>(s, partial, c, tot) && threadIdx.x == 0) {
         const double rr = tot.v[0];
         c->rho = rr;
         c->rr = rr;
@@ -167,41 +247,36 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, 
     }
 }
 
-// r = b - S^ x; p = r; start a CG run.  tol2 = max(rtol2 * (use_b ? b.b : r.r), atol2).
-// With use_active, instances whose flag inst_sums[kSumStride*i + kSumActive] is 0 are marked done at once.
-template <typename T, int R>
-__global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<T> A, const T *__restrict__ b, const T *__restrict__ x,
-                                                           T *__restrict__ r, T *__restrict__ p,
-                                                           double *__restrict__ partial, InstCtl *__restrict__ ctl,
-                                                           const int32_t *__restrict__ tile_inst, int32_t *n_done,
-                                                           int use_b, double rtol2, double atol2, int max_it,
+// r = bh - S^ x; p = r; start an FP64 CG run.  tol2 = max(rtol2 * bh.bh, atol2).
+// With use_active, instances whose flag inst_sums[kSumStride*i + kSumActive] is 0 are
+// marked done at once.
+template <int R>
+__global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<double> A, const double *__restrict__ b,
+                                                           const double *__restrict__ x, double *__restrict__ r,
+                                                           double *__restrict__ p, double *__restrict__ partial,
+                                                           InstCtl *__restrict__ ctl, Plan plan, int32_t *n_done,
+                                                           double rtol2, double atol2, int max_it,
                                                            const double *__restrict__ inst_sums, int use_active) {
-    const int tile = blockIdx.x;
-    const int inst = tile_inst[tile];
+    const int inst = plan.inst[blockIdx.x];
     InstCtl *c = ctl + inst;
     const bool active = !use_active || inst_sums[kSumStride * inst + kSumActive] != 0.0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sums<2> s = {{0.0, 0.0}};
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
+        double y[R];
+        sell_rows<double, double, R>(A, x, tile, y);
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t sl = ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
-        const int64_t off = A.slice_off[sl];
-        const int w = (int)((A.slice_off[sl + 1] - off) / kSliceRows);
-        const int64_t row = sl * kSliceRows + lane;
-        double y = 0.0;
-        for (int j = 0; j < w; ++j) {
-            const int64_t slot = off + (int64_t)j * kSliceRows + lane;
-            y += (double)A.val[slot] * (double)x[A.col[slot]];
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = sell_row<R>(tile, k);
+            const double bb = b[row];
+            const double rr = bb - y[k];
+            r[row] = rr;
+            p[row] = rr;
+            s.v[0] += rr * rr;
+            s.v[1] += bb * bb;
         }
-        const double bb = (double)b[row];
-        const double rr = bb - y;
-        r[row] = (T)rr;
-        p[row] = (T)rr;
-        s.v[0] += rr * rr;
-        s.v[1] += bb * bb;
     }
     Sums<2> tot;
-    if (tile_finish<2>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+    if (block_finish<2>(s, partial, c, tot) && threadIdx.x == 0) {
         const double rr = tot.v[0], bb = tot.v[1];
         c->rho = rr;
         c->rr = rr;
@@ -212,8 +287,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<T> A, const 
         c->max_it = max_it;
         c->status = 0;
         c->done = 0;
-        const double ref = use_b ? bb : rr;
-        c->tol2 = fmax(rtol2 * ref, atol2);
+        c->tol2 = fmax(rtol2 * bb, atol2);
         if (!active) finish_inst(c, 0, n_done);
         else if (!isfinite(rr)) finish_inst(c, -6, n_done);
         else if (rr <= c->tol2) finish_inst(c, 0, n_done);
@@ -228,68 +302,65 @@ template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A, const double *__restrict__ bh,
                                                               const double *__restrict__ x, const double *__restrict__ dsq,
                                                               double *__restrict__ r, double *__restrict__ partial,
-                                                              InstCtl *__restrict__ ctl,
-                                                              const int32_t *__restrict__ tile_inst,
+                                                              InstCtl *__restrict__ ctl, Plan plan,
                                                               double *__restrict__ inst_sums) {
-    const int tile = blockIdx.x;
-    const int inst = tile_inst[tile];
+    const int inst = plan.inst[blockIdx.x];
     InstCtl *c = ctl + inst;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sums<4> s = {{0.0, 0.0, 0.0, 0.0}};
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
+        double y[R];
+        sell_rows<double, double, R>(A, x, tile, y);
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t sl = ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
-        const int64_t off = A.slice_off[sl];
-        const int w = (int)((A.slice_off[sl + 1] - off) / kSliceRows);
-        const int64_t row = sl * kSliceRows + lane;
-        double y = 0.0;
-        for (int j = 0; j < w; ++j) {
-            const int64_t slot = off + (int64_t)j * kSliceRows + lane;
-            y += A.val[slot] * x[A.col[slot]];
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = sell_row<R>(tile, k);
+            const double b = bh[row];
+            const double rr = b - y[k];
+            r[row] = rr;
+            const double d = dsq[row] * dsq[row];
+            s.v[0] += rr * rr;
+            s.v[1] += d * rr * rr;
+            s.v[2] += d * b * b;
+            s.v[3] += b * b;
         }
-        const double b = bh[row];
-        const double rr = b - y;
-        r[row] = rr;
-        const double d = dsq[row] * dsq[row];
-        s.v[0] += rr * rr;
-        s.v[1] += d * rr * rr;
-        s.v[2] += d * b * b;
-        s.v[3] += b * b;
     }
     Sums<4> tot;
-    if (tile_finish<4>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+    if (block_finish<4>(s, partial, c, tot) && threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) inst_sums[kSumStride * inst + k] = tot.v[k];
     }
 }
 
-// Start an FP32 inner solve of S^ d = r / |r| for every instance whose outer residual is
-// above its target (inst_sums[kSumStride*i + kSumActive] = 1 marks an active instance).
+// Starts (keep_p = 0) or continues after a reliable update (keep_p = 1) an FP32 inner solve
+// of S^ d = r / |r| for every instance whose outer residual is above its target
+// (inst_sums[kSumStride*i + kSumActive] = 1).  On a reliable update the FP32 recursion
+// continues from the recomputed FP64 residual and the search direction is kept, rescaled from
+// the old normalisation |r_old| to the new |r_new|, so no Krylov information is lost.
 template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__restrict__ r64, float *__restrict__ x32,
                                                             float *__restrict__ r32, float *__restrict__ p32,
                                                             double *__restrict__ partial, InstCtl *__restrict__ ctl,
-                                                            const int32_t *__restrict__ tile_inst,
-                                                            const double *__restrict__ inst_sums, int32_t *n_done,
-                                                            double rtol2, int max_it) {
-    const int tile = blockIdx.x;
-    const int inst = tile_inst[tile];
+                                                            Plan plan, const double *__restrict__ inst_sums,
+                                                            int32_t *n_done, double rtol2, int max_it, int keep_p) {
+    const int inst = plan.inst[blockIdx.x];
     InstCtl *c = ctl + inst;
     const bool active = inst_sums[kSumStride * inst + kSumActive] != 0.0;
     const double nrm = sqrt(inst_sums[kSumStride * inst + 0]);
     const double inv = (active && nrm > 0.0) ? 1.0 / nrm : 0.0;
+    const double ratio = (active && nrm > 0.0) ? c->scale / nrm : 0.0;
     Sums<1> s = {{0.0}};
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t row = ((int64_t)tile * R + k) * kBlockThreads + threadIdx.x;
-        const float v = (float)(r64[row] * inv);
-        x32[row] = 0.0f;
-        r32[row] = v;
-        p32[row] = v;
-        s.v[0] += (double)v * (double)v;
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = flat_row<R>(tile, k);
+            const float v = (float)(r64[row] * inv);
+            x32[row] = 0.0f;
+            r32[row] = v;
+            p32[row] = keep_p ? (float)((double)p32[row] * ratio) : v;
+            s.v[0] += (double)v * (double)v;
+        }
     }
     Sums<1> tot;
-    if (tile_finish<1>(s, partial, c, tile, tot) && threadIdx.x == 0) {
+    if (block_finish<1>(s, partial, c, tot) && threadIdx.x == 0) {
         c->rho = tot.v[0];
         c->rr = tot.v[0];
         c->rr0 = tot.v[0];
@@ -306,131 +377,164 @@ __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__rest
 // x64 += |r| * x32 for the instances of the last inner solve.
 template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_ir_correct(double *__restrict__ x, const float *__restrict__ x32,
-                                                              const InstCtl *__restrict__ ctl,
-                                                              const int32_t *__restrict__ tile_inst) {
-    const int tile = blockIdx.x;
-    const double sc = ctl[tile_inst[tile]].scale;
+                                                              const InstCtl *__restrict__ ctl, Plan plan) {
+    const double sc = ctl[plan.inst[blockIdx.x]].scale;
     if (sc == 0.0) return;
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile)
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int64_t row = ((int64_t)tile * R + k) * kBlockThreads + threadIdx.x;
-        x[row] += sc * (double)x32[row];
-    }
+        for (int k = 0; k < R; ++k) {
+            const int64_t row = flat_row<R>(tile, k);
+            x[row] += sc * (double)x32[row];
+        }
 }
 
 template <typename T> SellView<T> view(const DevSystem &s);
 template <> SellView<double> view<double>(const DevSystem &s) { return {s.n_rows, s.slice_off, s.col, s.val64}; }
 template <> SellView<float> view<float>(const DevSystem &s) { return {s.n_rows, s.slice_off, s.col, s.val32}; }
 
+Plan plan_of(const DevSystem &s) { return {s.blk_inst, s.blk_tile_begin, s.blk_tile_end}; }
+
 template <int R> cudaError_t cg_init_r(const DevSystem &sys, double rtol2, double atol2, int max_it, int use_active,
                                        cudaStream_t st) {
-    k_cg_init<double, R><<<(unsigned)sys.n_tiles, kBlockThreads, 0, st>>>(
-        view<double>(sys), sys.bh, sys.x, sys.r, sys.p, sys.partial, sys.ctl, sys.tile_inst, sys.n_done, 1, rtol2,
-        atol2, max_it, sys.inst_sums, use_active);
+    k_cg_init<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.r, sys.p,
+                                                                    sys.partial, sys.ctl, plan_of(sys), sys.n_done,
+                                                                    rtol2, atol2, max_it, sys.inst_sums, use_active);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t cg_spmv_r(const DevSystem &sys, int prec, cudaStream_t st) {
-    const unsigned g = (unsigned)sys.n_tiles;
+    const unsigned g = (unsigned)sys.n_blocks;
     if (prec == 64)
         k_cg_spmv<double, R><<<g, kBlockThreads, 0, st>>>(view<double>(sys), sys.p, sys.q, sys.r, sys.partial, sys.ctl,
-                                                          sys.tile_inst, sys.n_done);
+                                                          plan_of(sys), sys.n_done);
     else
         k_cg_spmv<float, R><<<g, kBlockThreads, 0, st>>>(view<float>(sys), sys.p32, sys.q32, sys.r32, sys.partial,
-                                                         sys.ctl, sys.tile_inst, sys.n_done);
+                                                         sys.ctl, plan_of(sys), sys.n_done);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t cg_update_r(const DevSystem &sys, int prec, cudaStream_t st) {
-    const unsigned g = (unsigned)sys.n_tiles;
+    const unsigned g = (unsigned)sys.n_blocks;
     if (prec == 64)
         k_cg_update<double, R><<<g, kBlockThreads, 0, st>>>(sys.x, sys.r, sys.p, sys.q, sys.partial, sys.ctl,
-                                                            sys.tile_inst, sys.n_done);
+                                                            plan_of(sys), sys.n_done);
     else
         k_cg_update<float, R><<<g, kBlockThreads, 0, st>>>(sys.x32, sys.r32, sys.p32, sys.q32, sys.partial, sys.ctl,
-                                                           sys.tile_inst, sys.n_done);
+                                                           plan_of(sys), sys.n_done);
     return cudaGetLastError();
 }
 
-template <int R> cudaError_t cg_iter_r(const DevSystem &sys, int prec, cudaStream_t st) {
-    cudaError_t e = cg_spmv_r<R>(sys, prec, st);
-    return e == cudaSuccess ? cg_update_r<R>(sys, prec, st) : e;
+template <int R> cudaError_t residual_r(const DevSystem &sys, cudaStream_t st) {
+    k_residual64<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r,
+                                                                       sys.partial, sys.ctl, plan_of(sys),
+                                                                       sys.inst_sums);
+    return cudaGetLastError();
+}
+
+template <int R> cudaError_t ir_start_r(const DevSystem &sys, double rtol2, int max_it, int keep_p, cudaStream_t st) {
+    k_ir_start<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial,
+                                                                     sys.ctl, plan_of(sys), sys.inst_sums, sys.n_done,
+                                                                     rtol2, max_it, keep_p);
+    return cudaGetLastError();
+}
+
+template <int R> cudaError_t ir_correct_r(const DevSystem &sys, cudaStream_t st) {
+    k_ir_correct<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(sys.x, sys.x32, sys.ctl, plan_of(sys));
+    return cudaGetLastError();
 }
 
 }  // namespace
 
+#define MH_BY_R(CALL)                                      \
+    switch (sys.rows_per_thread) {                         \
+        case 1: return CALL(1);                            \
+        case 2: return CALL(2);                            \
+        case 4: return CALL(4);                            \
+        default: return cudaErrorInvalidValue;             \
+    }
+
 cudaError_t launch_cg_init(const DevSystem &sys, double rtol2, double atol2, int max_it, int use_active,
                            cudaStream_t s) {
-    switch (sys.rows_per_thread) {
-        case 1: return cg_init_r<1>(sys, rtol2, atol2, max_it, use_active, s);
-        case 2: return cg_init_r<2>(sys, rtol2, atol2, max_it, use_active, s);
-        case 4: return cg_init_r<4>(sys, rtol2, atol2, max_it, use_active, s);
-        default: return cudaErrorInvalidValue;
-    }
+#define C_(R) cg_init_r<R>(sys, rtol2, atol2, max_it, use_active, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_cg_spmv(const DevSystem &sys, int prec, cudaStream_t s) {
-    switch (sys.rows_per_thread) {
-        case 1: return cg_spmv_r<1>(sys, prec, s);
-        case 2: return cg_spmv_r<2>(sys, prec, s);
-        case 4: return cg_spmv_r<4>(sys, prec, s);
-        default: return cudaErrorInvalidValue;
-    }
+#define C_(R) cg_spmv_r<R>(sys, prec, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_cg_update(const DevSystem &sys, int prec, cudaStream_t s) {
-    switch (sys.rows_per_thread) {
-        case 1: return cg_update_r<1>(sys, prec, s);
-        case 2: return cg_update_r<2>(sys, prec, s);
-        case 4: return cg_update_r<4>(sys, prec, s);
-        default: return cudaErrorInvalidValue;
-    }
+#define C_(R) cg_update_r<R>(sys, prec, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_cg_iteration(const DevSystem &sys, int prec, cudaStream_t s) {
-    switch (sys.rows_per_thread) {
-        case 1: return cg_iter_r<1>(sys, prec, s);
-        case 2: return cg_iter_r<2>(sys, prec, s);
-        case 4: return cg_iter_r<4>(sys, prec, s);
-        default: return cudaErrorInvalidValue;
-    }
+    cudaError_t e = launch_cg_spmv(sys, prec, s);
+    return e == cudaSuccess ? launch_cg_update(sys, prec, s) : e;
 }
 
 cudaError_t launch_residual64(const DevSystem &sys, cudaStream_t s) {
-    const unsigned g = (unsigned)sys.n_tiles;
-    switch (sys.rows_per_thread) {
-        case 1: k_residual64<1><<<g, kBlockThreads, 0, s>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums); break;
-        case 2: k_residual64<2><<<g, kBlockThreads, 0, s>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums); break;
-        case 4: k_residual64<4><<<g, kBlockThreads, 0, s>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+#define C_(R) residual_r<R>(sys, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_ir_start(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s) {
-    const unsigned g = (unsigned)sys.n_tiles;
-    switch (sys.rows_per_thread) {
-        case 1: k_ir_start<1><<<g, kBlockThreads, 0, s>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums, sys.n_done, rtol2, max_it); break;
-        case 2: k_ir_start<2><<<g, kBlockThreads, 0, s>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums, sys.n_done, rtol2, max_it); break;
-        case 4: k_ir_start<4><<<g, kBlockThreads, 0, s>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial, sys.ctl, sys.tile_inst, sys.inst_sums, sys.n_done, rtol2, max_it); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+#define C_(R) ir_start_r<R>(sys, rtol2, max_it, 0, s)
+    MH_BY_R(C_)
+#undef C_
+}
+
+cudaError_t launch_ir_replace(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s) {
+#define C_(R) ir_start_r<R>(sys, rtol2, max_it, 1, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_ir_correct(const DevSystem &sys, cudaStream_t s) {
-    const unsigned g = (unsigned)sys.n_tiles;
-    switch (sys.rows_per_thread) {
-        case 1: k_ir_correct<1><<<g, kBlockThreads, 0, s>>>(sys.x, sys.x32, sys.ctl, sys.tile_inst); break;
-        case 2: k_ir_correct<2><<<g, kBlockThreads, 0, s>>>(sys.x, sys.x32, sys.ctl, sys.tile_inst); break;
-        case 4: k_ir_correct<4><<<g, kBlockThreads, 0, s>>>(sys.x, sys.x32, sys.ctl, sys.tile_inst); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+#define C_(R) ir_correct_r<R>(sys, s)
+    MH_BY_R(C_)
+#undef C_
 }
 
 cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s) {
     return cudaMemsetAsync(sys.n_done, 0, sizeof(int32_t), s);
+}
+
+int krylov_target_blocks(int rows_per_thread) {
+    int dev = 0, sms = 148, per_sm = 4;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
+        int a = 0, b = 0;
+        cudaError_t e1 = cudaErrorInvalidValue, e2 = cudaErrorInvalidValue;
+        switch (rows_per_thread) {
+            case 1:
+                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 1>, kBlockThreads, 0);
+                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 1>, kBlockThreads, 0);
+                break;
+            case 2:
+                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 2>, kBlockThreads, 0);
+                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 2>, kBlockThreads, 0);
+                break;
+            default:
+                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 4>, kBlockThreads, 0);
+                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 4>, kBlockThreads, 0);
+                break;
+        }
+        if (e1 == cudaSuccess && e2 == cudaSuccess && a > 0 && b > 0) per_sm = a < b ? a : b;
+    } else {
+        cudaGetLastError();
+        sms = 148;
+    }
+    if (const char *env = getenv("MH_BLOCKS_PER_SM")) {
+        int v = atoi(env);
+        if (v >= 1 && v <= 32) per_sm = v;
+    }
+    return sms * per_sm;
 }
 
 }  // namespace mh

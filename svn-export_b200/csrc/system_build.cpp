@@ -17,8 +17,30 @@ int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out) {
     return c;
 }
 
+void build_block_plan(HostSystem &hs, int target_blocks) {
+    const int n_inst = (int)hs.inst_row.size() - 1;
+    const int64_t total = hs.n_tiles;
+    hs.blk_inst.clear();
+    hs.blk_tile_begin.clear();
+    hs.blk_tile_end.clear();
+    hs.inst_blk.assign(n_inst + 1, 0);
+    for (int i = 0; i < n_inst; ++i) {
+        const int64_t t0 = hs.inst_row[i] / hs.tile_rows, t1 = hs.inst_row[i + 1] / hs.tile_rows;
+        const int64_t nt = t1 - t0;
+        int64_t nb = (int64_t)((double)target_blocks * (double)nt / (double)total + 0.5);
+        nb = std::max<int64_t>(1, std::min(nb, nt));
+        hs.inst_blk[i] = (int32_t)hs.blk_inst.size();
+        for (int64_t b = 0; b < nb; ++b) {
+            hs.blk_inst.push_back(i);
+            hs.blk_tile_begin.push_back((int32_t)(t0 + nt * b / nb));
+            hs.blk_tile_end.push_back((int32_t)(t0 + nt * (b + 1) / nb));
+        }
+    }
+    hs.inst_blk[n_inst] = (int32_t)hs.blk_inst.size();
+}
+
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
-                      int rows_per_thread, HostSystem &hs, std::string *err) {
+                      int rows_per_thread, int target_blocks, HostSystem &hs, std::string *err) {
     char msg[256];
     hs = HostSystem();
     hs.inst_el = inst_el;
@@ -115,6 +137,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     for (int i = 0; i < n_inst; ++i)
         for (int64_t tl = hs.inst_row[i] / hs.tile_rows; tl < hs.inst_row[i + 1] / hs.tile_rows; ++tl)
             hs.tile_inst[tl] = i;
+    build_block_plan(hs, target_blocks);
 
     // symmetric pattern: every pair of an element's local edges
     std::vector<int64_t> cnt(hs.n_rows + 1, 0);
