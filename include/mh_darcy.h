@@ -215,6 +215,28 @@ int mh_get_schur_system(const mh_handle *h, int32_t *row_ptr, int32_t *col, doub
 /* Fills opts with defaults. */
 void mh_solve_opts_default(mh_solve_opts *opts);
 
+/* ---- batches of independent systems ---------------------------------------------------- */
+/* n_inst independent meshes (for example conductivity realisations on meshes of uneven
+ * size) in one handle.  Every Krylov launch covers all instances; each instance keeps its own
+ * CG coefficients and stops on its own residual (per-instance masks); mh_solve returns when
+ * all have finished.  Element-wise arrays (mh_set_coeffs), boundary arrays (mh_set_bc) and the
+ * MH solution cover the union: each part is the concatenation over instances in order, i.e.
+ * the solution is [sides of inst 0, 1, ... | elements of 0, 1, ... | edges of 0, 1, ...]. */
+int mh_create_batch(const mh_mesh_desc *meshes, int32_t n_inst, mh_handle **out);
+/* Offsets [n_inst+1] of each instance's elements, sides, edges and boundary objects in the
+ * union numbering (any pointer may be NULL). */
+int mh_get_instance_offsets(const mh_handle *h, int64_t *el_off, int64_t *side_off, int64_t *edge_off,
+                            int64_t *bdr_off);
+/* Per-instance results of the last solve: Krylov iterations, final Jacobi-scaled relative
+ * residual, status (0 converged, 1 not converged, < 0 breakdown).  Arrays of n_inst. */
+int mh_get_instance_stats(const mh_handle *h, int32_t *iterations, double *rel_residual, int32_t *status);
+
+/* Autotuner: times `iterations` FP64 and FP32 CG iterations on the assembled system for
+ * every launch shape (rows per thread R in {1, 2, 4}, blocks per SM from the occupancy of
+ * that R's SpMV kernels) and keeps the fastest.  Writes the chosen R and the FP32 and FP64
+ * microseconds per iteration (either pointer may be NULL). */
+int mh_autotune(mh_handle *h, int32_t iterations, int32_t *rows_per_thread, double *us_per_iter);
+
 /* ---- unsteady MH (DarcyFlowMH_Unsteady, darcy_flow_mh.cc:1601-1675) ----------------- */
 /* lumped = 0: MH time term on element rows (setup_time_term :1614-1658);
  * lumped = 1: LMH time term on edge rows (DarcyFlowLMH_Unsteady :1695-1827).

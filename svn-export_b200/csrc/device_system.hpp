@@ -31,9 +31,16 @@ struct InstCtl {
     int32_t max_it;
     int32_t done;      // 1 once converged, stopped or broken down
     int32_t status;    // 0 converged, 1 max_it, -8 breakdown, -6 non-finite
-    int32_t blk_begin, blk_end;  // blocks of the launch plan that work on this instance
-    uint32_t ticket;
+    uint32_t ticket;   // blocks of the current launch that have published their partials
     int32_t pad;
+};
+
+// Launch plan of the Krylov kernels: block b works on the tiles [tile_begin[b], tile_end[b])
+// of instance blk_inst[b]; instance i owns blocks [inst_blk[i], inst_blk[i+1]).  There is one
+// plan per precision because the FP64 and FP32 SpMV kernels fit different block counts per SM.
+struct DevPlan {
+    int32_t n_blocks = 0;
+    int32_t *blk_inst = nullptr, *tile_begin = nullptr, *tile_end = nullptr, *inst_blk = nullptr;
 };
 
 // SELL-C-sigma matrix view in solver-row space (rows padded per instance to whole tiles).
@@ -49,9 +56,7 @@ struct DevSystem {
     int64_t n_rows = 0, n_slices = 0, n_tiles = 0, n_slots = 0;
     int32_t rows_per_thread = 1;     // R: slices per warp per tile
     int32_t n_inst = 0;
-    int32_t n_blocks = 0;            // blocks of every Krylov launch (the block plan)
-    int32_t *blk_inst = nullptr;     // [n_blocks] instance of each block
-    int32_t *blk_tile_begin = nullptr, *blk_tile_end = nullptr;  // its contiguous tile run
+    DevPlan plan[2];                 // [0]: FP64 kernels, [1]: FP32 kernels
     int64_t *slice_off = nullptr;
     int32_t *col = nullptr;
     double *val_raw = nullptr;       // S  (reference schur2 after scale(-1))
@@ -68,7 +73,7 @@ struct DevSystem {
     double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *w = nullptr;
     // FP32 inner vectors
     float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
-    double *partial = nullptr;       // [n_blocks * 4]
+    double *partial = nullptr;       // [max plan blocks * 4]
     InstCtl *ctl = nullptr;          // [n_inst]
     int32_t *n_done = nullptr;       // instances finished in the current Krylov run
     double *inst_sums = nullptr;     // [n_inst * 4] results of the residual kernel
@@ -118,8 +123,8 @@ cudaError_t launch_ir_correct(const DevSystem &sys, cudaStream_t s);
 // Reliable update: continue the FP32 recursion from the recomputed FP64 residual, keeping p.
 cudaError_t launch_ir_replace(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
 cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s);
-// Blocks per Krylov launch: SMs of the current device times the blocks of the spmv kernel
-// that fit on one SM (148 x 4 without a device); MH_BLOCKS_PER_SM overrides the factor.
-int krylov_target_blocks(int rows_per_thread);
+// Blocks per Krylov launch for precision 64 or 32: SMs of the current device times the blocks
+// of that precision's SpMV kernel that fit on one SM (148 x 4 without a device).
+int krylov_target_blocks(int rows_per_thread, int prec);
 
 }  // namespace mh

@@ -51,6 +51,8 @@ struct mh_handle {
     int64_t n_launch = 0;               // kernels launched so far
     double kernel_ms[4] = {0, 0, 0, 0};
     int32_t kernel_count[4] = {0, 0, 0, 0};
+    std::vector<int32_t> inst_iters, inst_status;  // per instance, last solve
+    std::vector<double> inst_rel;
     std::string err;
 };
 
@@ -179,13 +181,20 @@ int device_setup(mh_handle *h) {
     s.n_slots = hs.n_slots;
     s.rows_per_thread = hs.rows_per_thread;
     s.n_inst = (int32_t)hs.inst_el.size() - 1;
-    s.n_blocks = (int32_t)hs.blk_inst.size();
     if ((rc = upload(h, s.slice_off, hs.slice_off)) || (rc = upload(h, s.col, hs.sell_col)) ||
         (rc = upload(h, s.diag_slot, hs.diag_slot)) || (rc = upload(h, s.row_edge, hs.row_edge)) ||
-        (rc = upload(h, s.edge_row, hs.edge_row)) || (rc = upload(h, s.tile_inst, hs.tile_inst)) ||
-        (rc = upload(h, s.blk_inst, hs.blk_inst)) || (rc = upload(h, s.blk_tile_begin, hs.blk_tile_begin)) ||
-        (rc = upload(h, s.blk_tile_end, hs.blk_tile_end)))
+        (rc = upload(h, s.edge_row, hs.edge_row)) || (rc = upload(h, s.tile_inst, hs.tile_inst)))
         return rc;
+    int32_t max_blocks = 1;
+    for (int k = 0; k < 2; ++k) {
+        mh::DevPlan &dp = s.plan[k];
+        const auto &hp = hs.plan[k];
+        dp.n_blocks = (int32_t)hp.blk_inst.size();
+        max_blocks = std::max(max_blocks, dp.n_blocks);
+        if ((rc = upload(h, dp.blk_inst, hp.blk_inst)) || (rc = upload(h, dp.tile_begin, hp.blk_tile_begin)) ||
+            (rc = upload(h, dp.tile_end, hp.blk_tile_end)) || (rc = upload(h, dp.inst_blk, hp.inst_blk)))
+            return rc;
+    }
     const int64_t nr = hs.n_rows;
     s.val_raw = dalloc<double>(h, hs.n_slots);
     s.val64 = dalloc<double>(h, hs.n_slots);
@@ -203,7 +212,7 @@ int device_setup(mh_handle *h) {
     s.p32 = dalloc<float>(h, nr);
     s.q32 = dalloc<float>(h, nr);
     s.z32 = dalloc<float>(h, nr);
-    s.partial = dalloc<double>(h, (size_t)s.n_blocks * 4);
+    s.partial = dalloc<double>(h, (size_t)max_blocks * 4);
     s.ctl = dalloc<mh::InstCtl>(h, s.n_inst);
     s.n_done = dalloc<int32_t>(h, 1);
     s.inst_sums = dalloc<double>(h, mh::kSumStride * (size_t)s.n_inst);
@@ -215,8 +224,6 @@ int device_setup(mh_handle *h) {
     std::vector<mh::InstCtl> ctl(s.n_inst);
     for (int i = 0; i < s.n_inst; ++i) {
         std::memset(&ctl[i], 0, sizeof(mh::InstCtl));
-        ctl[i].blk_begin = hs.inst_blk[i];
-        ctl[i].blk_end = hs.inst_blk[i + 1];
         ctl[i].done = 1;
     }
     CK(cudaMemcpy(s.ctl, ctl.data(), sizeof(mh::InstCtl) * ctl.size(), cudaMemcpyHostToDevice));
@@ -231,6 +238,39 @@ int device_setup(mh_handle *h) {
     CK(cudaMemset(h->sol, 0, msize * sizeof(double)));
     CK(cudaMemset(h->sol_prev, 0, msize * sizeof(double)));
     h->device = true;
+    return MH_OK;
+}
+
+// Switches rows per thread and the block plans (matrix layout unchanged) and drops the
+// captured graphs, which hold the old launch shape.
+int apply_launch_shape(mh_handle *h, int R, const int targets[2]) {
+    CK(cudaStreamSynchronize(h->stream));
+    mh::set_launch_shape(h->hs, R, targets);
+    const HostSystem &hs = h->hs;
+    mh::DevSystem &s = h->sys;
+    int rc;
+    s.rows_per_thread = R;
+    s.n_tiles = hs.n_tiles;
+    if ((rc = upload(h, s.tile_inst, hs.tile_inst))) return rc;
+    int32_t max_blocks = 1;
+    for (int k = 0; k < 2; ++k) {
+        mh::DevPlan &dp = s.plan[k];
+        const auto &hp = hs.plan[k];
+        dp.n_blocks = (int32_t)hp.blk_inst.size();
+        max_blocks = std::max(max_blocks, dp.n_blocks);
+        if ((rc = upload(h, dp.blk_inst, hp.blk_inst)) || (rc = upload(h, dp.tile_begin, hp.blk_tile_begin)) ||
+            (rc = upload(h, dp.tile_end, hp.blk_tile_end)) || (rc = upload(h, dp.inst_blk, hp.inst_blk)))
+            return rc;
+    }
+    s.partial = dalloc<double>(h, (size_t)max_blocks * 4);
+    if (!s.partial) return MH_ERR_NOMEM;
+    for (auto &gp : h->graph)
+        for (auto &g : gp)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    for (auto &gi : h->graph_iters) gi[0] = gi[1] = 0;
     return MH_OK;
 }
 
@@ -410,7 +450,8 @@ struct SolveResult {
 // residual |D^-1/2 (b - S x)| / |D^-1/2 b| and the unscaled |b - S x| / |b| must both be
 // <= r_tol (or the unscaled absolute residual <= a_tol).  Marks unconverged instances
 // active in `sums`; returns the worst ratio achieved/target (<= 1 when all converged).
-double evaluate(const mh_solve_opts &o, int n_inst, std::vector<double> &sums, SolveResult &res, bool &finite) {
+double evaluate(mh_handle *h, const mh_solve_opts &o, std::vector<double> &sums, SolveResult &res, bool &finite) {
+    const int n_inst = h->sys.n_inst;
     double worst = 0.0;
     res.rel = res.rel_orig = 0.0;
     finite = true;
@@ -425,12 +466,20 @@ double evaluate(const mh_solve_opts &o, int n_inst, std::vector<double> &sums, S
         if (ro <= o.a_tol) ratio = 0.0;
         s[mh::kSumActive] = ratio > 1.0 ? 1.0 : 0.0;
         worst = std::max(worst, ratio);
+        h->inst_rel[i] = rel_s;
+        if (h->inst_status[i] >= 0) h->inst_status[i] = ratio > 1.0 ? MH_NOT_CONVERGED : MH_OK;
     }
     return worst;
 }
 
+void count_iterations(mh_handle *h, const std::vector<mh::InstCtl> &ctl) {
+    for (size_t i = 0; i < ctl.size(); ++i) {
+        h->inst_iters[i] += ctl[i].iter;
+        if (ctl[i].status < 0) h->inst_status[i] = ctl[i].status;
+    }
+}
+
 int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
-    const int n_inst = h->sys.n_inst;
     std::vector<double> sums;
     std::vector<mh::InstCtl> ctl;
     double tau = o.r_tol;
@@ -442,6 +491,7 @@ int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         int rc = run_krylov(h, 64, o.iters_per_graph, o.max_it - total, o.profile_kernels != 0);
         if (rc) return rc;
         if ((rc = read_ctl(h, ctl))) return rc;
+        count_iterations(h, ctl);
         int worst = 0, maxit = 0;
         for (auto &c : ctl) {
             maxit = std::max(maxit, c.iter);
@@ -450,7 +500,7 @@ int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         total += maxit;
         if ((rc = true_residual(h, sums))) return rc;
         bool finite;
-        double worst_ratio = evaluate(o, n_inst, sums, res, finite);
+        double worst_ratio = evaluate(h, o, sums, res, finite);
         res.outer = run + 1;
         res.iterations = total;
         if (!finite) {
@@ -482,7 +532,6 @@ int solve_pcg64(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
 // continues from r64 with the same search direction (reliable update).  If the FP64
 // residual stops decreasing, the solve finishes with FP64 PCG from the current x.
 int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
-    const int n_inst = h->sys.n_inst;
     std::vector<double> sums;
     std::vector<mh::InstCtl> ctl;
     int total = 0;
@@ -492,7 +541,7 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         int rc = true_residual(h, sums);
         if (rc) return rc;
         bool finite;
-        double worst_ratio = evaluate(o, n_inst, sums, res, finite);
+        double worst_ratio = evaluate(h, o, sums, res, finite);
         if (!finite) {
             res.status = MH_ERR_NONFINITE;
             return MH_OK;
@@ -533,6 +582,7 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
         CK(mh::launch_ir_correct(h->sys, h->stream));
         h->n_launch += 2;
         if ((rc = read_ctl(h, ctl))) return rc;
+        count_iterations(h, ctl);
         int maxit = 0;
         for (auto &c : ctl) maxit = std::max(maxit, c.iter);
         total += maxit;
@@ -553,6 +603,8 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
     const bool guess = o.use_initial_guess || have_guess_default;
     const int64_t launches0 = h->n_launch;
+    std::fill(h->inst_iters.begin(), h->inst_iters.end(), 0);
+    std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
     for (int k = 0; k < 4; ++k) {
         h->kernel_ms[k] = 0.0;
         h->kernel_count[k] = 0;
@@ -693,33 +745,45 @@ void mh_solve_opts_default(mh_solve_opts *o) {
     o->iters_per_graph = 16;
 }
 
-int mh_create(const mh_mesh_desc *md, mh_handle **out) {
-    if (!md || !out || md->n_nodes <= 0 || md->n_elements <= 0 || !md->node_xyz || !md->el_dim || !md->el_nodes)
-        return MH_ERR_INVALID;
-    if (md->n_bc_elements < 0 || (md->n_bc_elements > 0 && (!md->bc_dim || !md->bc_nodes))) return MH_ERR_INVALID;
-    *out = nullptr;
-    auto *h = new (std::nothrow) mh_handle();
-    if (!h) return MH_ERR_NOMEM;
+}  // extern "C"
+
+namespace {
+
+bool desc_valid(const mh_mesh_desc *md) {
+    if (!md || md->n_nodes <= 0 || md->n_elements <= 0 || !md->node_xyz || !md->el_dim || !md->el_nodes)
+        return false;
+    if (md->n_bc_elements < 0 || (md->n_bc_elements > 0 && (!md->bc_dim || !md->bc_nodes))) return false;
+    return true;
+}
+
+// Appends a mesh to `m` (node indices shifted past the nodes already there).
+void append_mesh(mh::MeshData &m, const mh_mesh_desc *md) {
+    const int32_t shift = (int32_t)m.n_nodes;
+    m.xyz.insert(m.xyz.end(), md->node_xyz, md->node_xyz + 3 * md->n_nodes);
+    m.dim.insert(m.dim.end(), md->el_dim, md->el_dim + md->n_elements);
+    for (int64_t k = 0; k < 4 * md->n_elements; ++k) {
+        const int32_t v = md->el_nodes[k];
+        m.nodes.push_back(v >= 0 ? v + shift : v);
+    }
+    if (md->n_bc_elements > 0) {
+        m.bc_dim.insert(m.bc_dim.end(), md->bc_dim, md->bc_dim + md->n_bc_elements);
+        for (int64_t k = 0; k < 4 * md->n_bc_elements; ++k) {
+            const int32_t v = md->bc_nodes[k];
+            m.bc_nodes.push_back(v >= 0 ? v + shift : v);
+        }
+    }
+    m.n_nodes += md->n_nodes;
+    m.n_el += md->n_elements;
+    m.n_bc += md->n_bc_elements;
+}
+
+// Topology, edge-system layout and device set-up for a mesh whose instances own the element
+// ranges inst_el (one instance: {0, n_el}).
+int create_impl(mh_handle *h, const std::vector<int64_t> &inst) {
     mh::MeshData &m = h->mesh;
-    m.n_nodes = md->n_nodes;
-    m.xyz.assign(md->node_xyz, md->node_xyz + 3 * md->n_nodes);
-    m.n_el = md->n_elements;
-    m.dim.assign(md->el_dim, md->el_dim + md->n_elements);
-    m.nodes.assign(md->el_nodes, md->el_nodes + 4 * md->n_elements);
-    m.n_bc = md->n_bc_elements;
-    if (m.n_bc > 0) {
-        m.bc_dim.assign(md->bc_dim, md->bc_dim + m.n_bc);
-        m.bc_nodes.assign(md->bc_nodes, md->bc_nodes + 4 * m.n_bc);
-    }
-    if (!check_finite(m.xyz.data(), (int64_t)m.xyz.size())) {
-        delete h;
-        return MH_ERR_NONFINITE;
-    }
+    if (!check_finite(m.xyz.data(), (int64_t)m.xyz.size())) return MH_ERR_NONFINITE;
     int rc = mh::build_topology(m, h->topo, &h->err);
-    if (rc) {
-        delete h;
-        return rc;
-    }
+    if (rc) return rc;
     const mh::Topology &t = h->topo;
     h->ngh_hi_el.resize(t.n_ngh());
     h->ngh_meas.resize(t.n_ngh());
@@ -729,18 +793,53 @@ int mh_create(const mh_mesh_desc *md, mh_handle **out) {
         h->ngh_hi_el[i] = (int32_t)e;
         h->ngh_meas[i] = side_measure_host(m, e, side - t.el_side_start[e]);
     }
-    int rpt = 1;  // best on B200 at cfg2 (R = 1/2/4 measured)
+    int rpt = 1;  // best on B200 at cfg2 (R = 1/2/4 measured); mh_autotune can change it
     if (const char *env = getenv("MH_ROWS_PER_THREAD")) {
         int v = atoi(env);
         if (v == 1 || v == 2 || v == 4) rpt = v;
     }
-    std::vector<int64_t> inst = {0, m.n_el};
-    rc = mh::build_host_system(m, h->topo, inst, rpt, mh::krylov_target_blocks(rpt), h->hs, &h->err);
+    const int targets[2] = {mh::krylov_target_blocks(rpt, 64), mh::krylov_target_blocks(rpt, 32)};
+    rc = mh::build_host_system(m, h->topo, inst, rpt, targets, h->hs, &h->err);
+    if (rc) return rc;
+    const int n_inst = (int)inst.size() - 1;
+    h->inst_iters.assign(n_inst, 0);
+    h->inst_status.assign(n_inst, 0);
+    h->inst_rel.assign(n_inst, 0.0);
+    return device_setup(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mh_create(const mh_mesh_desc *md, mh_handle **out) {
+    if (!out || !desc_valid(md)) return MH_ERR_INVALID;
+    *out = nullptr;
+    auto *h = new (std::nothrow) mh_handle();
+    if (!h) return MH_ERR_NOMEM;
+    append_mesh(h->mesh, md);
+    int rc = create_impl(h, {0, h->mesh.n_el});
     if (rc) {
-        delete h;
+        mh_destroy(h);
         return rc;
     }
-    rc = device_setup(h);
+    *out = h;
+    return MH_OK;
+}
+
+int mh_create_batch(const mh_mesh_desc *meshes, int32_t n_inst, mh_handle **out) {
+    if (!out || !meshes || n_inst <= 0) return MH_ERR_INVALID;
+    *out = nullptr;
+    for (int32_t i = 0; i < n_inst; ++i)
+        if (!desc_valid(&meshes[i])) return MH_ERR_INVALID;
+    auto *h = new (std::nothrow) mh_handle();
+    if (!h) return MH_ERR_NOMEM;
+    std::vector<int64_t> inst(1, 0);
+    for (int32_t i = 0; i < n_inst; ++i) {
+        append_mesh(h->mesh, &meshes[i]);
+        inst.push_back(h->mesh.n_el);
+    }
+    int rc = create_impl(h, inst);
     if (rc) {
         mh_destroy(h);
         return rc;
@@ -996,6 +1095,97 @@ int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts, mh_solv
 }
 
 const char *mh_last_error(const mh_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int mh_get_instance_offsets(const mh_handle *h, int64_t *el_off, int64_t *side_off, int64_t *edge_off,
+                            int64_t *bdr_off) {
+    if (!h) return MH_ERR_INVALID;
+    const mh::HostSystem &hs = h->hs;
+    const mh::Topology &t = h->topo;
+    const int n = (int)hs.inst_el.size() - 1;
+    for (int i = 0; i <= n; ++i) {
+        if (el_off) el_off[i] = hs.inst_el[i];
+        if (side_off) side_off[i] = t.el_side_start[hs.inst_el[i]];
+        if (edge_off) edge_off[i] = hs.inst_edge[i];
+    }
+    if (bdr_off) {
+        // boundary objects follow the instances' elements (edge ranges are per instance)
+        int64_t b = 0;
+        for (int i = 0; i < n; ++i) {
+            bdr_off[i] = b;
+            while (b < t.n_bdr() && t.bdr_edge[b] < hs.inst_edge[i + 1]) ++b;
+        }
+        bdr_off[n] = t.n_bdr();
+    }
+    return MH_OK;
+}
+
+int mh_get_instance_stats(const mh_handle *h, int32_t *iterations, double *rel_residual, int32_t *status) {
+    if (!h) return MH_ERR_INVALID;
+    const size_t n = h->inst_iters.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (iterations) iterations[i] = h->inst_iters[i];
+        if (rel_residual) rel_residual[i] = h->inst_rel[i];
+        if (status) status[i] = h->inst_status[i];
+    }
+    return MH_OK;
+}
+
+int mh_autotune(mh_handle *h, int32_t iterations, int32_t *rows_per_thread, double *us_per_iter) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    if (iterations <= 0) iterations = 64;
+    const int ipg = 16;
+    iterations = ((iterations + ipg - 1) / ipg) * ipg;
+    double best = 1e300, best32 = 0.0, best64 = 0.0;
+    int best_r = h->hs.rows_per_thread;
+    std::vector<double> sums;
+    for (int R : {1, 2, 4}) {
+        const int targets[2] = {mh::krylov_target_blocks(R, 64), mh::krylov_target_blocks(R, 32)};
+        if ((rc = apply_launch_shape(h, R, targets))) return rc;
+        double t[2] = {0.0, 0.0};
+        for (int k = 0; k < 2; ++k) {
+            const int prec = k == 0 ? 64 : 32;
+            // a fixed number of iterations from the current rhs (tolerance 0: never converges)
+            CK(cudaMemsetAsync(h->sys.x, 0, h->sys.n_rows * sizeof(double), h->stream));
+            CK(mh::launch_reset_ctl(h->sys, h->stream));
+            if (prec == 64) {
+                CK(mh::launch_cg_init(h->sys, 0.0, 0.0, iterations, 0, h->stream));
+            } else {
+                if ((rc = true_residual(h, sums))) return rc;
+                for (int i = 0; i < h->sys.n_inst; ++i) sums[mh::kSumStride * i + mh::kSumActive] = 1.0;
+                CK(cudaMemcpyAsync(h->sys.inst_sums, sums.data(), sizeof(double) * sums.size(),
+                                   cudaMemcpyHostToDevice, h->stream));
+                CK(mh::launch_ir_start(h->sys, 0.0, iterations, h->stream));
+            }
+            // warm the captured graph, then time
+            if ((rc = capture_iterations(h, prec, ipg, false))) return rc;
+            CK(cudaEventRecord(h->ev[0], h->stream));
+            if ((rc = run_krylov(h, prec, ipg, iterations, false))) return rc;
+            CK(cudaEventRecord(h->ev[1], h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+            t[k] = 1e3 * ms / iterations;
+        }
+        // the default solver runs FP32 iterations with an occasional FP64 residual
+        const double score = t[1] + 0.05 * t[0];
+        if (score < best) {
+            best = score;
+            best_r = R;
+            best32 = t[1];
+            best64 = t[0];
+        }
+    }
+    const int targets[2] = {mh::krylov_target_blocks(best_r, 64), mh::krylov_target_blocks(best_r, 32)};
+    if ((rc = apply_launch_shape(h, best_r, targets))) return rc;
+    if (rows_per_thread) *rows_per_thread = best_r;
+    if (us_per_iter) {
+        us_per_iter[0] = best32;
+        us_per_iter[1] = best64;
+    }
+    return MH_OK;
+}
 
 int mh_set_stream(mh_handle *h, void *cuda_stream) {
     int rc = need_device(h);

@@ -8,6 +8,7 @@ constexpr int kMaxNgh1 = 6;        // VB neighbours of a segment (triangle sides
 constexpr int kMaxNgh2 = 2;        // VB neighbours of a triangle (coinciding tetrahedron faces)
 constexpr int kSliceRowsHost = 32; // SELL-C-sigma chunk height C
 constexpr int kTileRowsBase = 256; // rows of one 256-thread block per slice-per-warp
+constexpr int kPadRows = 1024;     // instances are padded to a multiple of this many rows
 
 // Read-only device views of the mesh, coefficients and boundary data used by the
 // element kernels (assembly, time term, back-substitution).

@@ -50,20 +50,25 @@ template <int NV> __device__ __forceinline__ Sums<NV> block_sum(Sums<NV> s) {
     return out;
 }
 
+struct Plan {
+    const int32_t *inst, *tile_begin, *tile_end, *inst_blk;
+};
+
 // Publishes this block's partial sums and returns true in every thread of the block that
 // arrived last for its instance; that block then holds the instance totals in `tot`
 // (thread 0 only).
 template <int NV>
-__device__ __forceinline__ bool block_finish(Sums<NV> s, double *partial, InstCtl *c, Sums<NV> &tot) {
+__device__ __forceinline__ bool block_finish(Sums<NV> s, double *partial, InstCtl *c, const Plan &plan, int inst,
+                                             Sums<NV> &tot) {
     __shared__ bool am_last;
     Sums<NV> b = block_sum<NV>(s);
+    const int pb = plan.inst_blk[inst], pe = plan.inst_blk[inst + 1];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) partial[(int64_t)blockIdx.x * 4 + k] = b.v[k];
         __threadfence();
-        const unsigned n_blk = (unsigned)(c->blk_end - c->blk_begin);
         const unsigned t = atomicAdd(&c->ticket, 1u);
-        am_last = (t == n_blk - 1);
+        am_last = (t == (unsigned)(pe - pb) - 1);
     }
     __syncthreads();
     if (!am_last) return false;
@@ -75,7 +80,6 @@ __device__ __forceinline__ bool block_finish(Sums<NV> s, double *partial, InstCt
     for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int k = 0; k < NV; ++k) acc[u][k] = 0.0;
-    const int pb = c->blk_begin, pe = c->blk_end;
     for (int t0 = pb + threadIdx.x; t0 < pe; t0 += U * blockDim.x) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -105,10 +109,6 @@ __device__ __forceinline__ void finish_inst(InstCtl *c, int status, int32_t *n_d
 }
 
 template <typename T> __device__ __forceinline__ T ldg_stream(const T *p) { return __ldcs(p); }
-
-struct Plan {
-    const int32_t *inst, *tile_begin, *tile_end;
-};
 
 __device__ __forceinline__ int64_t slice_of(int tile, int warp, int R, int k) {
     return ((int64_t)tile * kWarpsPerBlock + warp) * R + k;
@@ -161,29 +161,89 @@ template <int R> __device__ __forceinline__ int64_t flat_row(int tile, int k) {
     return ((int64_t)tile * R + k) * kBlockThreads + threadIdx.x;
 }
 
-// q = S^ p and the three dot products.
+// One thread's share of a SELL tile for the pipelined SpMV (R = 1): the first kJ slots of its
+// row (column index and value) and the own-row entries of p and r.
+template <typename T> struct SpmvStage {
+    static constexpr int kJ = 8;
+    int64_t off;
+    int w;
+    int32_t c[kJ];
+    T v[kJ];
+    T pr, rr;
+};
+
+template <typename T>
+__device__ __forceinline__ void spmv_stage_load(const SellView<T> &A, const T *__restrict__ p, const T *__restrict__ r,
+                                                int tile, SpmvStage<T> &st) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t sl = slice_of(tile, warp, 1, 0);
+    st.off = A.slice_off[sl];
+    st.w = (int)((A.slice_off[sl + 1] - st.off) / kSliceRows);
+#pragma unroll
+    for (int j = 0; j < SpmvStage<T>::kJ; ++j) {
+        const bool in = j < st.w;
+        const int64_t slot = st.off + (int64_t)j * kSliceRows + lane;
+        st.c[j] = in ? ldg_stream(A.col + slot) : 0;
+        st.v[j] = in ? ldg_stream(A.val + slot) : (T)0;
+    }
+    const int64_t row = sl * kSliceRows + lane;
+    st.pr = p[row];
+    st.rr = r[row];
+}
+
+// q = S^ p and the three dot products.  Software-pipelined over the block's tiles: the
+// indices, values and own-row vector entries of tile t+1 are loaded while the gathers of
+// tile t are in flight, so every thread always has a full tile of loads outstanding.
 template <typename T, int R>
-__global__ void __launch_bounds__(kBlockThreads) k_cg_spmv(SellView<T> A, const T *__restrict__ p, T *__restrict__ q,
+__global__ void __launch_bounds__(kBlockThreads, sizeof(T) == 4 ? 4 : 3)
+    k_cg_spmv(SellView<T> A, const T *__restrict__ p, T *__restrict__ q,
                                                            const T *__restrict__ r, double *__restrict__ partial,
                                                            InstCtl *__restrict__ ctl, Plan plan, int32_t *n_done) {
-    InstCtl *c = ctl + plan.inst[blockIdx.x];
+    const int inst = plan.inst[blockIdx.x];
+    InstCtl *c = ctl + inst;
     if (c->done) return;
     Sums<3> s = {{0.0, 0.0, 0.0}};
-    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
-        double y[R];
-        sell_rows<T, T, R>(A, p, tile, y);
+    const int tb = plan.tile_begin[blockIdx.x], te = plan.tile_end[blockIdx.x];
+    if (R == 1) {
+        constexpr int kJ = SpmvStage<T>::kJ;
+        const int lane = threadIdx.x & 31;
+        SpmvStage<T> st;
+        if (tb < te) spmv_stage_load<T>(A, p, r, tb, st);
+        for (int tile = tb; tile < te; ++tile) {
+            T g[kJ];
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const int64_t row = sell_row<R>(tile, k);
-            q[row] = (T)y[k];
-            const double pr = (double)p[row], rr = (double)r[row];
-            s.v[0] += pr * y[k];
-            s.v[1] += rr * y[k];
-            s.v[2] += y[k] * y[k];
+            for (int j = 0; j < kJ; ++j) g[j] = p[st.c[j]];
+            const SpmvStage<T> cur = st;
+            if (tile + 1 < te) spmv_stage_load<T>(A, p, r, tile + 1, st);
+            double y = 0.0;
+#pragma unroll
+            for (int j = 0; j < kJ; ++j) y += (double)cur.v[j] * (double)g[j];
+            for (int j = kJ; j < cur.w; ++j) {
+                const int64_t slot = cur.off + (int64_t)j * kSliceRows + lane;
+                y += (double)ldg_stream(A.val + slot) * (double)p[ldg_stream(A.col + slot)];
+            }
+            q[sell_row<1>(tile, 0)] = (T)y;
+            s.v[0] += (double)cur.pr * y;
+            s.v[1] += (double)cur.rr * y;
+            s.v[2] += y * y;
+        }
+    } else {
+        for (int tile = tb; tile < te; ++tile) {
+            double y[R];
+            sell_rows<T, T, R>(A, p, tile, y);
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int64_t row = sell_row<R>(tile, k);
+                q[row] = (T)y[k];
+                const double pr = (double)p[row], rr = (double)r[row];
+                s.v[0] += pr * y[k];
+                s.v[1] += rr * y[k];
+                s.v[2] += y[k] * y[k];
+            }
         }
     }
     Sums<3> tot;
-    if (block_finish<3>(s, partial, c, tot) && threadIdx.x == 0) {
+    if (block_finish<3>(s, partial, c, plan, inst, tot) && threadIdx.x == 0) {
         const double pq = tot.v[0], rq = tot.v[1], qq = tot.v[2];
         const double rho = c->rho;
         if (rho == 0.0) {
@@ -209,12 +269,15 @@ template <typename T, int R>
 __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, T *__restrict__ r, T *__restrict__ p,
                                                              const T *__restrict__ q, double *__restrict__ partial,
                                                              InstCtl *__restrict__ ctl, Plan plan, int32_t *n_done) {
-    InstCtl *c = ctl + plan.inst[blockIdx.x];
+    const int inst = plan.inst[blockIdx.x];
+    InstCtl *c = ctl + inst;
     if (c->done) return;
     const double alpha = c->alpha, beta = c->beta;
     Sums<1> s = {{0.0}};
-    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
-        T pv[R], xv[R], rv[R], qv[R];
+    // software-pipelined: the four loads of tile t+1 are issued before tile t is computed
+    const int tb = plan.tile_begin[blockIdx.x], te = plan.tile_end[blockIdx.x];
+    T pv[R], xv[R], rv[R], qv[R];
+    auto load = [&](int tile) {
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int64_t row = flat_row<R>(tile, k);
@@ -223,12 +286,24 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, 
             rv[k] = r[row];
             qv[k] = ldg_stream(q + row);
         }
+    };
+    if (tb < te) load(tb);
+    for (int tile = tb; tile < te; ++tile) {
+        T cp[R], cx[R], cr[R], cq[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            cp[k] = pv[k];
+            cx[k] = xv[k];
+            cr[k] = rv[k];
+            cq[k] = qv[k];
+        }
+        if (tile + 1 < te) load(tile + 1);
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int64_t row = flat_row<R>(tile, k);
-            const double pr = (double)pv[k];
-            const double rr = (double)rv[k] - alpha * (double)qv[k];
-            x[row] = (T)((double)xv[k] + alpha * pr);
+            const double pr = (double)cp[k];
+            const double rr = (double)cr[k] - alpha * (double)cq[k];
+            x[row] = (T)((double)cx[k] + alpha * pr);
             r[row] = (T)rr;
             p[row] = (T)(rr + beta * pr);
             const double rs = (double)(T)rr;
@@ -236,7 +311,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_update(T *__restrict__ x, 
         }
     }
     Sums<1> tot;
-    if (block_finish<1>(s, partial, c, tot) && threadIdx.x == 0) {
+    if (block_finish<1>(s, partial, c, plan, inst, tot) && threadIdx.x == 0) {
         const double rr = tot.v[0];
         c->rho = rr;
         c->rr = rr;
@@ -276,7 +351,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_cg_init(SellView<double> A, c
         }
     }
     Sums<2> tot;
-    if (block_finish<2>(s, partial, c, tot) && threadIdx.x == 0) {
+    if (block_finish<2>(s, partial, c, plan, inst, tot) && threadIdx.x == 0) {
         const double rr = tot.v[0], bb = tot.v[1];
         c->rho = rr;
         c->rr = rr;
@@ -324,7 +399,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A
         }
     }
     Sums<4> tot;
-    if (block_finish<4>(s, partial, c, tot) && threadIdx.x == 0) {
+    if (block_finish<4>(s, partial, c, plan, inst, tot) && threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) inst_sums[kSumStride * inst + k] = tot.v[k];
     }
@@ -360,7 +435,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__rest
         }
     }
     Sums<1> tot;
-    if (block_finish<1>(s, partial, c, tot) && threadIdx.x == 0) {
+    if (block_finish<1>(s, partial, c, plan, inst, tot) && threadIdx.x == 0) {
         c->rho = tot.v[0];
         c->rr = tot.v[0];
         c->rr0 = tot.v[0];
@@ -392,54 +467,59 @@ template <typename T> SellView<T> view(const DevSystem &s);
 template <> SellView<double> view<double>(const DevSystem &s) { return {s.n_rows, s.slice_off, s.col, s.val64}; }
 template <> SellView<float> view<float>(const DevSystem &s) { return {s.n_rows, s.slice_off, s.col, s.val32}; }
 
-Plan plan_of(const DevSystem &s) { return {s.blk_inst, s.blk_tile_begin, s.blk_tile_end}; }
+// plan 0 serves the FP64 kernels, plan 1 the FP32 ones
+Plan plan_of(const DevSystem &s, int prec) {
+    const DevPlan &p = s.plan[prec == 64 ? 0 : 1];
+    return {p.blk_inst, p.tile_begin, p.tile_end, p.inst_blk};
+}
+unsigned grid_of(const DevSystem &s, int prec) { return (unsigned)s.plan[prec == 64 ? 0 : 1].n_blocks; }
 
 template <int R> cudaError_t cg_init_r(const DevSystem &sys, double rtol2, double atol2, int max_it, int use_active,
                                        cudaStream_t st) {
-    k_cg_init<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.r, sys.p,
-                                                                    sys.partial, sys.ctl, plan_of(sys), sys.n_done,
-                                                                    rtol2, atol2, max_it, sys.inst_sums, use_active);
+    k_cg_init<R><<<grid_of(sys, 64), kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.r, sys.p,
+                                                              sys.partial, sys.ctl, plan_of(sys, 64), sys.n_done,
+                                                              rtol2, atol2, max_it, sys.inst_sums, use_active);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t cg_spmv_r(const DevSystem &sys, int prec, cudaStream_t st) {
-    const unsigned g = (unsigned)sys.n_blocks;
+    const unsigned g = grid_of(sys, prec);
     if (prec == 64)
         k_cg_spmv<double, R><<<g, kBlockThreads, 0, st>>>(view<double>(sys), sys.p, sys.q, sys.r, sys.partial, sys.ctl,
-                                                          plan_of(sys), sys.n_done);
+                                                          plan_of(sys, 64), sys.n_done);
     else
         k_cg_spmv<float, R><<<g, kBlockThreads, 0, st>>>(view<float>(sys), sys.p32, sys.q32, sys.r32, sys.partial,
-                                                         sys.ctl, plan_of(sys), sys.n_done);
+                                                         sys.ctl, plan_of(sys, 32), sys.n_done);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t cg_update_r(const DevSystem &sys, int prec, cudaStream_t st) {
-    const unsigned g = (unsigned)sys.n_blocks;
+    const unsigned g = grid_of(sys, prec);
     if (prec == 64)
         k_cg_update<double, R><<<g, kBlockThreads, 0, st>>>(sys.x, sys.r, sys.p, sys.q, sys.partial, sys.ctl,
-                                                            plan_of(sys), sys.n_done);
+                                                            plan_of(sys, 64), sys.n_done);
     else
         k_cg_update<float, R><<<g, kBlockThreads, 0, st>>>(sys.x32, sys.r32, sys.p32, sys.q32, sys.partial, sys.ctl,
-                                                           plan_of(sys), sys.n_done);
+                                                           plan_of(sys, 32), sys.n_done);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t residual_r(const DevSystem &sys, cudaStream_t st) {
-    k_residual64<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r,
-                                                                       sys.partial, sys.ctl, plan_of(sys),
-                                                                       sys.inst_sums);
+    k_residual64<R><<<grid_of(sys, 64), kBlockThreads, 0, st>>>(view<double>(sys), sys.bh, sys.x, sys.dsq, sys.r,
+                                                                 sys.partial, sys.ctl, plan_of(sys, 64),
+                                                                 sys.inst_sums);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t ir_start_r(const DevSystem &sys, double rtol2, int max_it, int keep_p, cudaStream_t st) {
-    k_ir_start<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial,
-                                                                     sys.ctl, plan_of(sys), sys.inst_sums, sys.n_done,
-                                                                     rtol2, max_it, keep_p);
+    k_ir_start<R><<<grid_of(sys, 32), kBlockThreads, 0, st>>>(sys.r, sys.x32, sys.r32, sys.p32, sys.partial, sys.ctl,
+                                                               plan_of(sys, 32), sys.inst_sums, sys.n_done, rtol2,
+                                                               max_it, keep_p);
     return cudaGetLastError();
 }
 
 template <int R> cudaError_t ir_correct_r(const DevSystem &sys, cudaStream_t st) {
-    k_ir_correct<R><<<(unsigned)sys.n_blocks, kBlockThreads, 0, st>>>(sys.x, sys.x32, sys.ctl, plan_of(sys));
+    k_ir_correct<R><<<grid_of(sys, 32), kBlockThreads, 0, st>>>(sys.x, sys.x32, sys.ctl, plan_of(sys, 32));
     return cudaGetLastError();
 }
 
@@ -505,32 +585,35 @@ cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s) {
     return cudaMemsetAsync(sys.n_done, 0, sizeof(int32_t), s);
 }
 
-int krylov_target_blocks(int rows_per_thread) {
+int krylov_target_blocks(int rows_per_thread, int prec) {
     int dev = 0, sms = 148, per_sm = 4;
     if (cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
-        int a = 0, b = 0;
-        cudaError_t e1 = cudaErrorInvalidValue, e2 = cudaErrorInvalidValue;
+        int a = 0;
+        cudaError_t e = cudaErrorInvalidValue;
+        const bool f64 = prec == 64;
         switch (rows_per_thread) {
             case 1:
-                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 1>, kBlockThreads, 0);
-                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 1>, kBlockThreads, 0);
+                e = f64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 1>, kBlockThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<float, 1>, kBlockThreads, 0);
                 break;
             case 2:
-                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 2>, kBlockThreads, 0);
-                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 2>, kBlockThreads, 0);
+                e = f64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 2>, kBlockThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<float, 2>, kBlockThreads, 0);
                 break;
             default:
-                e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 4>, kBlockThreads, 0);
-                e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_spmv<float, 4>, kBlockThreads, 0);
+                e = f64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<double, 4>, kBlockThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_spmv<float, 4>, kBlockThreads, 0);
                 break;
         }
-        if (e1 == cudaSuccess && e2 == cudaSuccess && a > 0 && b > 0) per_sm = a < b ? a : b;
+        if (e == cudaSuccess && a > 0) per_sm = a;
+        else cudaGetLastError();
     } else {
         cudaGetLastError();
         sms = 148;
     }
-    if (const char *env = getenv("MH_BLOCKS_PER_SM")) {
+    const char *env = getenv(prec == 64 ? "MH_BLOCKS_PER_SM_64" : "MH_BLOCKS_PER_SM_32");
+    if (env) {
         int v = atoi(env);
         if (v >= 1 && v <= 32) per_sm = v;
     }

@@ -17,30 +17,41 @@ int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out) {
     return c;
 }
 
-void build_block_plan(HostSystem &hs, int target_blocks) {
+void build_block_plan(HostSystem &hs, int target_blocks, HostSystem::Plan &plan) {
     const int n_inst = (int)hs.inst_row.size() - 1;
     const int64_t total = hs.n_tiles;
-    hs.blk_inst.clear();
-    hs.blk_tile_begin.clear();
-    hs.blk_tile_end.clear();
-    hs.inst_blk.assign(n_inst + 1, 0);
+    plan = HostSystem::Plan();
+    plan.inst_blk.assign(n_inst + 1, 0);
     for (int i = 0; i < n_inst; ++i) {
         const int64_t t0 = hs.inst_row[i] / hs.tile_rows, t1 = hs.inst_row[i + 1] / hs.tile_rows;
         const int64_t nt = t1 - t0;
         int64_t nb = (int64_t)((double)target_blocks * (double)nt / (double)total + 0.5);
         nb = std::max<int64_t>(1, std::min(nb, nt));
-        hs.inst_blk[i] = (int32_t)hs.blk_inst.size();
+        plan.inst_blk[i] = (int32_t)plan.blk_inst.size();
         for (int64_t b = 0; b < nb; ++b) {
-            hs.blk_inst.push_back(i);
-            hs.blk_tile_begin.push_back((int32_t)(t0 + nt * b / nb));
-            hs.blk_tile_end.push_back((int32_t)(t0 + nt * (b + 1) / nb));
+            plan.blk_inst.push_back(i);
+            plan.blk_tile_begin.push_back((int32_t)(t0 + nt * b / nb));
+            plan.blk_tile_end.push_back((int32_t)(t0 + nt * (b + 1) / nb));
         }
     }
-    hs.inst_blk[n_inst] = (int32_t)hs.blk_inst.size();
+    plan.inst_blk[n_inst] = (int32_t)plan.blk_inst.size();
+}
+
+void set_launch_shape(HostSystem &hs, int rows_per_thread, const int target_blocks[2]) {
+    const int n_inst = (int)hs.inst_row.size() - 1;
+    hs.rows_per_thread = rows_per_thread;
+    hs.tile_rows = (int64_t)kTileRowsBase * rows_per_thread;
+    hs.n_tiles = hs.n_rows / hs.tile_rows;
+    hs.tile_inst.resize(hs.n_tiles);
+    for (int i = 0; i < n_inst; ++i)
+        for (int64_t tl = hs.inst_row[i] / hs.tile_rows; tl < hs.inst_row[i + 1] / hs.tile_rows; ++tl)
+            hs.tile_inst[tl] = i;
+    build_block_plan(hs, target_blocks[0], hs.plan[0]);
+    build_block_plan(hs, target_blocks[1], hs.plan[1]);
 }
 
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
-                      int rows_per_thread, int target_blocks, HostSystem &hs, std::string *err) {
+                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err) {
     char msg[256];
     hs = HostSystem();
     hs.inst_el = inst_el;
@@ -114,17 +125,17 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
         hs.inst_edge[n_inst] = g;
     }
 
-    // padded solver rows per instance (whole tiles)
+    // padded solver rows per instance: a multiple of kPadRows, so tiles of 256*R rows never
+    // straddle instances for any R in {1, 2, 4} and R can be retuned without a rebuild
     hs.inst_row.assign(n_inst + 1, 0);
     for (int i = 0; i < n_inst; ++i) {
         int64_t ne = hs.inst_edge[i + 1] - hs.inst_edge[i];
-        int64_t pad = ((ne + hs.tile_rows - 1) / hs.tile_rows) * hs.tile_rows;
-        if (pad == 0) pad = hs.tile_rows;
+        int64_t pad = ((ne + kPadRows - 1) / kPadRows) * kPadRows;
+        if (pad == 0) pad = kPadRows;
         hs.inst_row[i + 1] = hs.inst_row[i] + pad;
     }
     hs.n_rows = hs.inst_row[n_inst];
     hs.n_slices = hs.n_rows / kSliceRowsHost;
-    hs.n_tiles = hs.n_rows / hs.tile_rows;
     hs.edge_row.resize(n_edges);
     hs.row_edge.assign(hs.n_rows, -1);
     for (int i = 0; i < n_inst; ++i)
@@ -133,11 +144,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
             hs.edge_row[g] = (int32_t)r;
             hs.row_edge[r] = (int32_t)g;
         }
-    hs.tile_inst.resize(hs.n_tiles);
-    for (int i = 0; i < n_inst; ++i)
-        for (int64_t tl = hs.inst_row[i] / hs.tile_rows; tl < hs.inst_row[i + 1] / hs.tile_rows; ++tl)
-            hs.tile_inst[tl] = i;
-    build_block_plan(hs, target_blocks);
+    set_launch_shape(hs, rows_per_thread, target_blocks);
 
     // symmetric pattern: every pair of an element's local edges
     std::vector<int64_t> cnt(hs.n_rows + 1, 0);

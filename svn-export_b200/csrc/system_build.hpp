@@ -28,10 +28,12 @@ struct HostSystem {
     std::vector<int32_t> sell_col;
     std::vector<int32_t> diag_slot;
     std::vector<int32_t> tile_inst;
-    // launch plan: every Krylov kernel runs n_blocks blocks; block b works on the tiles
+    // launch plans ([0] FP64 kernels, [1] FP32 kernels): block b works on the tiles
     // [blk_tile_begin[b], blk_tile_end[b]) of instance blk_inst[b]; instance i owns the blocks
     // [inst_blk[i], inst_blk[i+1])
-    std::vector<int32_t> blk_inst, blk_tile_begin, blk_tile_end, inst_blk;
+    struct Plan {
+        std::vector<int32_t> blk_inst, blk_tile_begin, blk_tile_end, inst_blk;
+    } plan[2];
     std::vector<int32_t> slot_cstart, slot_cidx;
     std::vector<int32_t> row_cstart, row_cidx;
     std::vector<int32_t> dim_list[4];
@@ -41,10 +43,14 @@ struct HostSystem {
 int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out);
 
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
-                      int rows_per_thread, int target_blocks, HostSystem &hs, std::string *err);
+                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err);
 
 // Splits every instance's tiles into contiguous runs, one run per block, with about
 // target_blocks blocks in total (at least one per instance) in proportion to instance size.
-void build_block_plan(HostSystem &hs, int target_blocks);
+void build_block_plan(HostSystem &hs, int target_blocks, HostSystem::Plan &plan);
+
+// Sets rows per thread (tile = 256 R rows) and rebuilds the tile map and both block plans;
+// the matrix layout does not change (instances are padded to kPadRows rows).
+void set_launch_shape(HostSystem &hs, int rows_per_thread, const int target_blocks[2]);
 
 }  // namespace mh

@@ -117,6 +117,10 @@ def _load():
         "mh_unsteady_init": (C.c_int, [vp, C.c_int32, C.c_double, _f64p]),
         "mh_unsteady_step": (C.c_int, [vp, C.c_double, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
         "mh_csr_residual_noalloc": (C.c_int, [C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "mh_create_batch": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(vp)]),
+        "mh_get_instance_offsets": (C.c_int, [vp] + [C.POINTER(C.c_int64)] * 4),
+        "mh_get_instance_stats": (C.c_int, [vp, _i32p, _f64p, _i32p]),
+        "mh_autotune": (C.c_int, [vp, C.c_int32, _i32p, _f64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -133,7 +137,8 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_set_stream", "mh_kernel_launches",
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device", "mh_get_schur_system",
-            "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc")
+            "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
+            "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune")
 
 MH_NOALLOC_MAX_ROWS = 16384 * 256
 

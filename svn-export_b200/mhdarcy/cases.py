@@ -28,7 +28,7 @@ def correlated_normal(grid, corr_len, rng):
     k = 2.0 * np.pi * np.fft.fftfreq(grid, d=1.0 / grid)
     kx, ky, kz = np.meshgrid(k, k, np.fft.rfftfreq(grid, d=1.0 / grid) * 2.0 * np.pi, indexing="ij")
     filt = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) * corr_len ** 2 / 8.0)
-    f = np.fft.irfftn(np.fft.rfftn(w) * filt, s=w.shape)
+    f = np.fft.irfftn(np.fft.rfftn(w) * filt, s=w.shape, axes=(0, 1, 2))
     f -= f.mean()
     return f / f.std()
 

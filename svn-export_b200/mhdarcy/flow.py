@@ -33,18 +33,65 @@ def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000
 
 
 class MHSystem:
-    """One mixed-hybrid Darcy system on the GPU (an mh_handle)."""
+    """One mixed-hybrid Darcy system on the GPU (an mh_handle), or a batch of independent
+    systems (see :meth:`batch`) solved together with per-instance convergence."""
 
-    def __init__(self, mesh):
+    def __init__(self, mesh, _batch=None):
         self.mesh = mesh
         h = C.c_void_p()
-        d = mesh.desc()
-        check(lib.mh_create(C.byref(d), C.byref(h)))
+        if _batch is None:
+            d = mesh.desc()
+            check(lib.mh_create(C.byref(d), C.byref(h)))
+            self.n_instances = 1
+        else:
+            descs = (_lib.MeshDesc * len(_batch))(*[m.desc() for m in _batch])
+            check(lib.mh_create_batch(descs, len(_batch), C.byref(h)))
+            self.n_instances = len(_batch)
+            self._meshes = _batch
         self.h = h
         s = _lib.Sizes()
         check(lib.mh_get_sizes(h, C.byref(s)))
         self.sizes = s
         self._topo = None
+
+    @classmethod
+    def batch(cls, meshes):
+        """Independent meshes in one handle.  Element, boundary and solution arrays cover the
+        union, each part concatenated over the instances in order."""
+        from .mesh import concat_meshes
+        s = cls(None, _batch=list(meshes))
+        s.mesh = concat_meshes(s._meshes)
+        return s
+
+    def instance_offsets(self):
+        n = self.n_instances + 1
+        arrs = [np.zeros(n, np.int64) for _ in range(4)]
+        check(lib.mh_get_instance_offsets(self.h, *[a.ctypes.data_as(C.POINTER(C.c_int64)) for a in arrs]),
+              self.h)
+        return dict(zip(("elements", "sides", "edges", "boundaries"), arrs))
+
+    def instance_stats(self):
+        n = self.n_instances
+        it = np.zeros(n, np.int32)
+        rel = np.zeros(n)
+        st = np.zeros(n, np.int32)
+        check(lib.mh_get_instance_stats(self.h, ptr(it, C.c_int32), ptr(rel, C.c_double), ptr(st, C.c_int32)),
+              self.h)
+        return dict(iterations=it, rel_residual=rel, status=st)
+
+    def autotune(self, iterations=64):
+        """Times the launch shapes on the assembled system and keeps the fastest."""
+        r = np.zeros(1, np.int32)
+        us = np.zeros(2)
+        check(lib.mh_autotune(self.h, iterations, ptr(r, C.c_int32), ptr(us, C.c_double)), self.h)
+        return dict(rows_per_thread=int(r[0]), us_per_iter_fp32=float(us[0]), us_per_iter_fp64=float(us[1]))
+
+    def instance_solution(self, sol, i):
+        """(side fluxes, element pressures, edge pressures) of instance i from a union solution."""
+        o = self.instance_offsets()
+        ns, ne = self.n_sides, self.n_elements
+        return (sol[o["sides"][i]:o["sides"][i + 1]], sol[ns + o["elements"][i]:ns + o["elements"][i + 1]],
+                sol[ns + ne + o["edges"][i]:ns + ne + o["edges"][i + 1]])
 
     def set_stream(self, cuda_stream):
         """Issue all work on the caller's cudaStream_t (an int handle, e.g. torch's

@@ -71,6 +71,21 @@ class Mesh:
         return (pts * mask).sum(axis=1) / n[:, None]
 
 
+def concat_meshes(meshes):
+    """Disjoint union of meshes (node indices shifted), in the order mh_create_batch uses."""
+    nodes, dims, conn, bdims, bconn = [], [], [], [], []
+    shift = 0
+    for m in meshes:
+        nodes.append(m.nodes)
+        dims.append(m.el_dim)
+        conn.append(np.where(m.el_nodes >= 0, m.el_nodes + shift, -1))
+        bdims.append(m.bc_dim)
+        bconn.append(np.where(m.bc_nodes >= 0, m.bc_nodes + shift, -1))
+        shift += len(m.nodes)
+    return Mesh(np.concatenate(nodes), np.concatenate(dims), np.concatenate(conn),
+                np.concatenate(bdims), np.concatenate(bconn).reshape(-1, 4))
+
+
 def cube_mesh(n, planes=(), lines=()):
     """Kuhn mesh of the unit cube (6 tetrahedra per cube of an n^3 grid).
 
