@@ -36,7 +36,7 @@ extern "C" {
 /* ---- status codes ------------------------------------------------------------------ */
 #define MH_OK               0
 #define MH_NOT_CONVERGED    1   /* max_it reached; the result is the last iterate        */
-#define MH_FELL_BACK        2   /* converged, but only after falling back to plain PCG   */
+#define MH_FELL_BACK        2   /* converged, but only after a fallback (see fell_back)   */
 #define MH_ERR_INVALID     -1   /* bad argument, inconsistent mesh                        */
 #define MH_ERR_SINGULAR    -2   /* singular local MH block (|det| < DBL_MIN/DBL_EPSILON)  */
 #define MH_ERR_CUDA        -3   /* CUDA runtime error or no device                        */
@@ -55,8 +55,11 @@ extern "C" {
 /* ---- solver methods ------------------------------------------------------------------ */
 #define MH_SOLVER_PCG64     0   /* Jacobi-preconditioned CG, all FP64                     */
 #define MH_SOLVER_IR32      1   /* FP32 inner CG inside FP64 iterative refinement         */
-#define MH_SOLVER_CHEB64    2   /* Chebyshev-Jacobi preconditioned CG, FP64                */
-#define MH_SOLVER_FCG_LEARNED 3 /* learned preconditioner inside flexible CG (IR outer)   */
+#define MH_SOLVER_CHEB      2   /* Chebyshev-Jacobi polynomial preconditioner in flexible CG:
+                                   FP32 inner iteration, FP64 residual replacements       */
+#define MH_SOLVER_FCG_LEARNED 3 /* learned (message-passing) preconditioner in flexible CG,
+                                   FP32 inner, FP64 replacements; falls back to Chebyshev-
+                                   Jacobi when the learned iteration stalls              */
 
 typedef struct mh_handle mh_handle;
 typedef struct mh_mesh mh_mesh;
@@ -117,7 +120,7 @@ typedef struct mh_solve_opts {
     double  r_tol;          /* relative tolerance (default 1e-10)                    */
     double  a_tol;          /* absolute tolerance on |b - S x| (default 0)           */
     int32_t use_initial_guess;  /* start from the current edge pressures             */
-    int32_t cheb_degree;    /* MH_SOLVER_CHEB64: polynomial degree (default 4)       */
+    int32_t cheb_degree;    /* MH_SOLVER_CHEB: polynomial degree (default 4)         */
     double  inner_rtol;     /* MH_SOLVER_IR32: FP32 residual reduction between two FP64
                                residual replacements (reliable updates), default 0.1 */
     int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000) */
@@ -136,7 +139,8 @@ typedef struct mh_solve_stats {
     int32_t status;
     int32_t iterations;         /* total Krylov iterations (inner ones for IR)       */
     int32_t outer_iterations;   /* refinement steps (IR/FCG), restarts (PCG)          */
-    int32_t fell_back;          /* 1 if the flexible iteration stalled -> plain PCG   */
+    int32_t fell_back;          /* 1: IR32 stalled and finished in FP64 PCG, or the
+                                   learned preconditioner stalled -> Chebyshev-Jacobi */
     double  rel_residual;       /* final Jacobi-scaled relative FP64 true residual    */
     double  ms_assembly;        /* device time of the last assembly                   */
     double  ms_solve;           /* device time of the Krylov solve                    */
@@ -245,6 +249,58 @@ int mh_unsteady_init(mh_handle *h, int32_t lumped, double dt, const double *init
 /* One implicit-Euler step of length dt with the boundary data currently set. */
 int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts,
                      mh_solve_stats *stats);
+
+/* ---- learned preconditioner (MH_SOLVER_FCG_LEARNED) ---------------------------------- */
+/* No counterpart in the reference, which preconditions the Schur system with PETSc ILU
+ * (src/la/solve.cc).  A 3-layer message-passing network over the Jacobi-scaled edge system
+ * S^ (node state 4 channels, MLP width 32, bf16 weights on the tensor cores, fp32 sums):
+ *   h0 = (r/|r|, 0, 0, 0);  h^{l+1} = h^l + W2 relu(W1 [h^l ; S^ h^l] + b1) + b2;
+ *   z = |r| h3[0].
+ * MH_NN_PARAMS floats, per layer: W1 [32][8], b1 [32], W2 [4][32], b2 [4] (row-major).
+ * A new handle starts from the identity network (W2 = 0: z = r, Jacobi). */
+#define MH_NN_PARAMS 1260
+int mh_learned_set_weights(mh_handle *h, const float *w, int64_t n);
+int mh_learned_get_weights(const mh_handle *h, float *w, int64_t n);
+
+/* Loss and gradient of one training pair (r, e) on the assembled system, for checking the
+ * training kernels: r, e [n_edges] in edge order, in the Jacobi-scaled space (S^ e = r for
+ * an exact pair).  loss = (z - e)' S^ (z - e) / (e' S^ e) = (z - e)' (S^ z - r) / (e' r) with
+ * z = NN(r) evaluated without the |r| normalisation; grad [MH_NN_PARAMS]. */
+int mh_learned_grad(mh_handle *h, const double *r, const double *e, float *grad, double *loss);
+
+/* z = NN(r) through the inference kernels (bf16 tensor-core MLP): r, z [n_edges] in edge
+ * order, Jacobi-scaled space; each instance's input is normalised by its own |r| and the
+ * output scaled back.  For checking the inference path against the training path and a
+ * CPU restatement. */
+int mh_learned_apply(mh_handle *h, const double *r, double *z);
+
+typedef struct mh_learn_opts {
+    int32_t n_pairs;        /* training pairs: snapshots of the plain solver (default 12) */
+    int32_t epochs;         /* passes over the pairs, one Adam step per pair (default 40) */
+    float   lr;             /* Adam step size (default 2e-3)                          */
+    int32_t train_bias;     /* 0 (default): b1 = b2 = 0 stay fixed, the network is
+                               positively homogeneous                                 */
+    double  solve_rtol;     /* accuracy of the reference solution x* (default 1e-9)   */
+    uint64_t seed;          /* order of the pairs within an epoch                     */
+    int32_t reserved[6];
+} mh_learn_opts;
+
+typedef struct mh_learn_stats {
+    double  loss_initial;   /* mean pair loss of the first epoch                      */
+    double  loss_final;     /* mean pair loss of the last epoch                       */
+    int32_t n_pairs, epochs;
+    double  ms_pairs;       /* device time: reference solve and snapshots             */
+    double  ms_train;       /* device time: forward, backward and Adam steps          */
+    double  reserved[4];
+} mh_learn_stats;
+
+void mh_learn_opts_default(mh_learn_opts *o);
+/* Trains the network on the assembled system (the current coefficients and boundary data):
+ * solves it with FP64 PCG to solve_rtol for x*, reruns FP64 PCG from zero and takes
+ * n_pairs snapshots x_s at geometrically spaced iterations, giving pairs
+ * (r_s = b^ - S^ x_s, e_s = x* - x_s) scaled by 1/|r_s|, and runs epochs x n_pairs Adam
+ * steps on the energy-norm loss.  The solution left in the handle is x*. */
+int mh_learned_train(mh_handle *h, const mh_learn_opts *opts, mh_learn_stats *stats);
 
 /* ---- residual check without device allocation --------------------------------------- */
 /* No counterpart in the reference: Flow123d leaves this check to PETSc's KSP monitor.

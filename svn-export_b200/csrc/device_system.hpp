@@ -122,6 +122,7 @@ cudaError_t launch_ir_start(const DevSystem &sys, double rtol2, int max_it, cuda
 cudaError_t launch_ir_correct(const DevSystem &sys, cudaStream_t s);
 // Reliable update: continue the FP32 recursion from the recomputed FP64 residual, keeping p.
 cudaError_t launch_ir_replace(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
+cudaError_t launch_ir_continue(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
 cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s);
 // Blocks per Krylov launch for precision 64 or 32: SMs of the current device times the blocks
 // of that precision's SpMV kernel that fit on one SM (148 x 4 without a device).

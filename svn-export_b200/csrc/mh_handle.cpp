@@ -9,11 +9,13 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <random>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "device_system.hpp"
+#include "learned.hpp"
 #include "mh_darcy.h"
 #include "system_build.hpp"
 #include "topology.hpp"
@@ -53,6 +55,19 @@ struct mh_handle {
     int32_t kernel_count[4] = {0, 0, 0, 0};
     std::vector<int32_t> inst_iters, inst_status;  // per instance, last solve
     std::vector<double> inst_rel;
+    // learned preconditioner: fp32 master weights, bf16 fragments, Adam state, work buffers
+    float *nn_w = nullptr, *nn_m = nullptr, *nn_v = nullptr, *nn_grad = nullptr;
+    uint32_t *nn_wb = nullptr;
+    int nn_step = 0;
+    float4 *nn_h0 = nullptr, *nn_h1 = nullptr;
+    float *cheb_z0 = nullptr, *cheb_z1 = nullptr, *cheb_d = nullptr;
+    unsigned int *spec_bound = nullptr;
+    double *d_loss = nullptr;
+    mh::NnTrainBuffers tr{};            // activations of a training pass
+    bool tr_ready = false;
+    float *pair_r = nullptr, *pair_e = nullptr;  // training pairs, [cap][n_rows] each
+    int pair_cap = 0;
+    double *x_star = nullptr, *pair_acc = nullptr;
     std::string err;
 };
 
@@ -591,6 +606,344 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
     return MH_OK;
 }
 
+// ---- learned preconditioner and flexible CG ----------------------------------------------
+
+// Identity network (Jacobi preconditioning): W1 small random, b1 = W2 = b2 = 0.
+void nn_identity_weights(std::vector<float> &w, uint64_t seed) {
+    w.assign(mh::kNnParams, 0.f);
+    uint64_t s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+    for (int l = 0; l < mh::kNnLayers; ++l)
+        for (int k = 0; k < mh::kNnH * 2 * mh::kNnK; ++k) {
+            s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+            const double u = ((s >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
+            w[l * mh::kNnPerLayer + k] = (float)(0.2 * u);
+        }
+}
+
+int nn_upload_weights(mh_handle *h, const float *w_host) {
+    CK(cudaMemcpyAsync(h->nn_w, w_host, mh::kNnParams * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->nn_m, 0, mh::kNnParams * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(h->nn_v, 0, mh::kNnParams * sizeof(float), h->stream));
+    CK(mh::launch_nn_pack(h->nn_w, h->nn_wb, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->nn_step = 0;
+    return MH_OK;
+}
+
+int ensure_learned(mh_handle *h) {
+    if (h->nn_w) return MH_OK;
+    const int64_t nr = h->sys.n_rows;
+    h->nn_w = dalloc<float>(h, mh::kNnParams);
+    h->nn_m = dalloc<float>(h, mh::kNnParams);
+    h->nn_v = dalloc<float>(h, mh::kNnParams);
+    h->nn_grad = dalloc<float>(h, mh::kNnParams);
+    h->nn_wb = dalloc<uint32_t>(h, mh::kNnLayers * mh::kNnPackedPerLayer);
+    h->nn_h0 = dalloc<float4>(h, nr);
+    h->nn_h1 = dalloc<float4>(h, nr);
+    h->cheb_z0 = dalloc<float>(h, nr);
+    h->cheb_z1 = dalloc<float>(h, nr);
+    h->cheb_d = dalloc<float>(h, nr);
+    h->spec_bound = dalloc<unsigned int>(h, 1);
+    h->d_loss = dalloc<double>(h, 1);
+    if (!h->nn_w || !h->nn_m || !h->nn_v || !h->nn_grad || !h->nn_wb || !h->nn_h0 || !h->nn_h1 || !h->cheb_z0 ||
+        !h->cheb_z1 || !h->cheb_d || !h->spec_bound || !h->d_loss)
+        return MH_ERR_NOMEM;
+    std::vector<float> w;
+    nn_identity_weights(w, 1);
+    return nn_upload_weights(h, w.data());
+}
+
+// Upper bound of the spectrum of the scaled FP32 system (Gershgorin).
+int spectrum_bound(mh_handle *h, double &hi) {
+    CK(mh::launch_spectrum_bound(h->sys, h->spec_bound, h->stream));
+    unsigned int bits = 0;
+    CK(cudaMemcpyAsync(&bits, h->spec_bound, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    float f;
+    std::memcpy(&f, &bits, sizeof(f));
+    hi = f > 0.f ? (double)f : 2.0;
+    return MH_OK;
+}
+
+// One flexible-CG iteration: z = M(r) (network or Chebyshev polynomial, which also forms
+// beta = z.q_old / (p.q)_old), p = z - beta p, q = S^ p with alpha = p.r / p.q, x and r.
+cudaError_t fcg_iteration(mh_handle *h, bool learned, int degree, double lo, double hi, cudaStream_t s) {
+    mh::DevSystem &sys = h->sys;
+    cudaError_t e = learned ? mh::launch_nn_apply(sys, h->nn_w, h->nn_wb, sys.r32, h->nn_h0, h->nn_h1, sys.z32,
+                                                   sys.q32, s)
+                            : mh::launch_cheb_apply(sys, sys.r32, h->cheb_z0, h->cheb_z1, h->cheb_d, sys.z32,
+                                                    sys.q32, degree, lo, hi, s);
+    if (e == cudaSuccess) e = mh::launch_fcg_direction(sys, sys.z32, s);
+    if (e == cudaSuccess) e = mh::launch_cg_spmv(sys, 32, s);
+    if (e == cudaSuccess) e = mh::launch_fcg_update(sys, s);
+    return e;
+}
+
+int run_fcg(mh_handle *h, bool learned, int degree, double lo, double hi, int ipg, int max_it) {
+    cudaGraph_t g;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < ipg && e == cudaSuccess; ++k) e = fcg_iteration(h, learned, degree, lo, hi, h->own_stream);
+    cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (e2 == cudaSuccess) cudaGraphDestroy(g);
+        h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
+        return MH_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->err = cudaGetErrorString(e);
+        return MH_ERR_CUDA;
+    }
+    const int per_iter = (learned ? 3 : degree) + 3;
+    int64_t launched = 0;
+    int rc = MH_OK;
+    while (true) {
+        cudaError_t ce = cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+        if (ce != cudaSuccess) {
+            h->err = cudaGetErrorString(ce);
+            rc = MH_ERR_CUDA;
+            break;
+        }
+        if (*h->h_done >= h->sys.n_inst) break;
+        if (launched > (int64_t)max_it + 2 * ipg) break;
+        ce = cudaGraphLaunch(ge, h->stream);
+        if (ce != cudaSuccess) {
+            h->err = cudaGetErrorString(ce);
+            rc = MH_ERR_CUDA;
+            break;
+        }
+        launched += ipg;
+        h->n_launch += (int64_t)per_iter * ipg;
+    }
+    cudaGraphExecDestroy(ge);
+    return rc;
+}
+
+// Mixed-precision flexible CG: FP32 FCG with the learned (or Chebyshev-Jacobi) preconditioner
+// inside FP64 reliable updates, as solve_ir32; the direction sequence runs on across them.
+// If a learned segment breaks down (non-finite network output), uses up inner_max_it, or the
+// FP64 residual stops improving over three replacements, Chebyshev-Jacobi replaces the
+// network for the rest of the solve (fell_back = 1).
+int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, bool learned) {
+    int rc = ensure_learned(h);
+    if (rc) return rc;
+    if (h->sys.rows_per_thread != 1) {  // the preconditioner kernels work on tiles of 256 rows
+        const int t[2] = {mh::krylov_target_blocks(1, 64), mh::krylov_target_blocks(1, 32)};
+        if ((rc = apply_launch_shape(h, 1, t))) return rc;
+    }
+    double hi = 2.0;
+    if ((rc = spectrum_bound(h, hi))) return rc;
+    const double lo = hi / 30.0;
+    const int degree = std::max(1, std::min(o.cheb_degree, 16));
+    std::vector<double> sums;
+    std::vector<mh::InstCtl> ctl;
+    int total = 0, stall = 0;
+    double best = 1e300;
+    bool use_nn = learned, restart = false;
+    for (int outer = 0; outer < 1000; ++outer) {
+        if ((rc = true_residual(h, sums))) return rc;
+        bool finite;
+        double worst_ratio = evaluate(h, o, sums, res, finite);
+        if (!finite) {
+            res.status = MH_ERR_NONFINITE;
+            return MH_OK;
+        }
+        res.outer = outer;
+        res.iterations = total;
+        if (worst_ratio <= 1.0) return MH_OK;
+        if (total >= o.max_it) {
+            res.status = MH_NOT_CONVERGED;
+            return MH_OK;
+        }
+        if (worst_ratio < 0.9 * best) {
+            best = worst_ratio;
+            stall = 0;
+        } else if (++stall >= 3) {
+            if (use_nn) {
+                use_nn = false;
+                res.fell_back = 1;
+                stall = 0;
+                restart = true;
+                std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
+            } else {
+                res.status = MH_NOT_CONVERGED;
+                return MH_OK;
+            }
+        }
+        CK(cudaMemcpyAsync(h->sys.inst_sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(mh::launch_reset_ctl(h->sys, h->stream));
+        const int seg_max = std::min(o.inner_max_it, o.max_it - total);
+        // the direction sequence continues across replacements unless the preconditioner changed
+        if (outer == 0 || restart)
+            CK(mh::launch_ir_start(h->sys, o.inner_rtol * o.inner_rtol, seg_max, h->stream));
+        else
+            CK(mh::launch_ir_continue(h->sys, o.inner_rtol * o.inner_rtol, seg_max, h->stream));
+        restart = false;
+        if ((rc = run_fcg(h, use_nn, degree, lo, hi, o.iters_per_graph, seg_max))) return rc;
+        CK(mh::launch_ir_correct(h->sys, h->stream));
+        h->n_launch += 2;
+        if ((rc = read_ctl(h, ctl))) return rc;
+        count_iterations(h, ctl);
+        int maxit = 0;
+        bool seg_bad = false;  // an instance broke down or used up the segment's iterations
+        for (auto &c : ctl) {
+            maxit = std::max(maxit, c.iter);
+            if (c.status != 0) seg_bad = true;
+        }
+        total += maxit;
+        if (seg_bad && use_nn) {
+            use_nn = false;
+            res.fell_back = 1;
+            stall = 0;
+            restart = true;
+            std::fill(h->inst_status.begin(), h->inst_status.end(), 0);  // the fallback takes over
+        }
+    }
+    res.status = MH_NOT_CONVERGED;
+    return MH_OK;
+}
+
+int ensure_train(mh_handle *h, int n_pairs) {
+    const int64_t nr = h->sys.n_rows;
+    if (!h->tr_ready) {
+        mh::NnTrainBuffers &b = h->tr;
+        for (auto &v : b.h) v = dalloc<float4>(h, nr);
+        for (auto &v : b.a) v = dalloc<float4>(h, nr);
+        for (auto &v : b.g) v = dalloc<float4>(h, nr);
+        b.ga = dalloc<float4>(h, nr);
+        b.z = dalloc<float>(h, nr);
+        h->pair_acc = dalloc<double>(h, 2);
+        for (auto v : b.h)
+            if (!v) return MH_ERR_NOMEM;
+        for (auto v : b.a)
+            if (!v) return MH_ERR_NOMEM;
+        if (!b.g[0] || !b.g[1] || !b.ga || !b.z || !h->pair_acc) return MH_ERR_NOMEM;
+        h->tr_ready = true;
+    }
+    if (h->pair_cap < n_pairs) {
+        h->pair_r = dalloc<float>(h, (size_t)n_pairs * nr);
+        h->pair_e = dalloc<float>(h, (size_t)n_pairs * nr);
+        if (!h->pair_r || !h->pair_e) return MH_ERR_NOMEM;
+        h->pair_cap = n_pairs;
+    }
+    return MH_OK;
+}
+
+// One forward/backward pass over pair k of the pair storage: grad (zeroed first) and the
+// pair's loss added to d_loss.
+int train_pass(mh_handle *h, int k, double er) {
+    const int64_t nr = h->sys.n_rows;
+    CK(cudaMemsetAsync(h->nn_grad, 0, mh::kNnParams * sizeof(float), h->stream));
+    CK(mh::launch_nn_train_pair(h->sys, h->nn_w, h->pair_r + (size_t)k * nr, h->pair_e + (size_t)k * nr, er, h->tr,
+                                h->nn_grad, h->d_loss, h->stream));
+    h->n_launch += 3 + 2 * mh::kNnLayers + 2 * mh::kNnLayers;
+    return MH_OK;
+}
+
+int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st) {
+    int rc;
+    const int np = std::max(1, std::min(o.n_pairs, 64));
+    if ((rc = ensure_learned(h)) || (rc = ensure_train(h, np))) return rc;
+    const int64_t nr = h->sys.n_rows;
+    if (!h->x_star && !(h->x_star = dalloc<double>(h, nr))) return MH_ERR_NOMEM;
+    cudaEvent_t e0 = h->ev[0], e1 = h->ev[1], e2 = h->ev[5];
+    CK(cudaEventRecord(e0, h->stream));
+    // reference solution x* (scaled space)
+    mh_solve_opts so;
+    mh_solve_opts_default(&so);
+    so.r_tol = o.solve_rtol > 0.0 ? o.solve_rtol : 1e-9;
+    std::fill(h->inst_iters.begin(), h->inst_iters.end(), 0);
+    std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
+    CK(cudaMemsetAsync(h->sys.x, 0, nr * sizeof(double), h->stream));
+    SolveResult res;
+    if ((rc = solve_pcg64(h, so, res))) return rc;
+    if (res.status < 0) {
+        h->err = "reference solve broke down";
+        return res.status;
+    }
+    CK(cudaMemcpyAsync(h->x_star, h->sys.x, nr * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    // snapshots of FP64 PCG from zero at geometrically spaced iterations 0 .. total
+    const int total = std::max(1, res.iterations);
+    std::vector<int> snap;
+    for (int k = 0; k < np; ++k) {
+        const int it = np == 1 ? 0 : (int)std::floor(std::pow((double)total + 1.0, (double)k / (np - 1))) - 1;
+        if (snap.empty() || it > snap.back()) snap.push_back(std::min(it, total - 1));
+    }
+    CK(cudaMemsetAsync(h->sys.x, 0, nr * sizeof(double), h->stream));
+    CK(mh::launch_reset_ctl(h->sys, h->stream));
+    CK(mh::launch_cg_init(h->sys, so.r_tol * so.r_tol, 0.0, total + 1, 0, h->stream));
+    h->n_launch += 1;
+    std::vector<double> er;
+    int it = 0, n_ok = 0;
+    for (int target : snap) {
+        for (; it < target; ++it) {
+            CK(mh::launch_cg_iteration(h->sys, 64, h->stream));
+            h->n_launch += 2;
+        }
+        float *pr = h->pair_r + (size_t)n_ok * nr, *pe = h->pair_e + (size_t)n_ok * nr;
+        CK(mh::launch_pair_make(nr, h->x_star, h->sys.x, h->sys.r, pe, pr, h->pair_acc, h->stream));
+        double acc[2];
+        CK(cudaMemcpyAsync(acc, h->pair_acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->n_launch += 1;
+        if (!(acc[0] > 0.0) || !(acc[1] > 0.0) || !std::isfinite(acc[0]) || !std::isfinite(acc[1])) continue;
+        const double sc = 1.0 / std::sqrt(acc[0]);
+        CK(mh::launch_pair_scale(nr, pe, pr, (float)sc, h->stream));
+        h->n_launch += 1;
+        er.push_back(acc[1] * sc * sc);
+        ++n_ok;
+    }
+    CK(cudaEventRecord(e1, h->stream));
+    if (n_ok == 0) {
+        h->err = "no usable training pair";
+        return MH_ERR_STATE;
+    }
+    // Adam, one step per pair, pairs shuffled every epoch
+    const int epochs = std::max(1, o.epochs);
+    const float lr = o.lr > 0.f ? o.lr : 2e-3f;
+    std::mt19937_64 rng(o.seed);
+    std::vector<int> order(n_ok);
+    for (int k = 0; k < n_ok; ++k) order[k] = k;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), h->stream));
+        for (int k : order) {
+            if ((rc = train_pass(h, k, er[k]))) return rc;
+            h->nn_step += 1;
+            CK(mh::launch_nn_adam(h->nn_w, h->nn_m, h->nn_v, h->nn_grad, h->nn_step, lr, 1.f, o.train_bias,
+                                  h->stream));
+            h->n_launch += 1;
+        }
+        if (ep == 0 || ep == epochs - 1) {
+            double l = 0.0;
+            CK(cudaMemcpyAsync(&l, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if (!std::isfinite(l)) {
+                h->err = "training loss is not finite";
+                return MH_ERR_NONFINITE;
+            }
+            (ep == 0 ? st.loss_initial : st.loss_final) = l / n_ok;
+        }
+    }
+    CK(mh::launch_nn_pack(h->nn_w, h->nn_wb, h->stream));
+    h->n_launch += 1;
+    CK(cudaEventRecord(e2, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    st.ms_pairs = ms;
+    CK(cudaEventElapsedTime(&ms, e1, e2));
+    st.ms_train = ms;
+    st.n_pairs = n_ok;
+    st.epochs = epochs;
+    return MH_OK;
+}
+
 int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats, bool have_guess_default) {
     mh_solve_opts o;
     mh_solve_opts_default(&o);
@@ -621,11 +974,14 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     switch (o.method) {
         case MH_SOLVER_PCG64: rc = solve_pcg64(h, o, res); break;
         case MH_SOLVER_IR32: rc = solve_ir32(h, o, res); break;
+        case MH_SOLVER_CHEB: rc = solve_fcg(h, o, res, false); break;
+        case MH_SOLVER_FCG_LEARNED: rc = solve_fcg(h, o, res, true); break;
         default:
             h->err = "solver method not available";
             return MH_ERR_INVALID;
     }
     if (rc) return rc;
+    if (res.status == MH_OK && res.fell_back) res.status = MH_FELL_BACK;
     CK(cudaEventRecord(h->ev[3], h->stream));
     CK(mh::launch_backsub(h->ed, h->as, h->sys, h->sol, h->topo.n_sides(), h->mesh.n_el, h->topo.n_edges(),
                           h->stream));
@@ -1196,5 +1552,130 @@ int mh_set_stream(mh_handle *h, void *cuda_stream) {
 }
 
 int64_t mh_kernel_launches(const mh_handle *h) { return h ? h->n_launch : 0; }
+
+int mh_learned_set_weights(mh_handle *h, const float *w, int64_t n) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled && !h->sys.n_rows) return MH_ERR_STATE;
+    if (!w || n != mh::kNnParams) {
+        h->err = "weights: expected MH_NN_PARAMS floats";
+        return MH_ERR_INVALID;
+    }
+    for (int64_t k = 0; k < n; ++k)
+        if (!std::isfinite(w[k])) {
+            h->err = "weights: non-finite value";
+            return MH_ERR_NONFINITE;
+        }
+    if ((rc = ensure_learned(h))) return rc;
+    return nn_upload_weights(h, w);
+}
+
+int mh_learned_get_weights(const mh_handle *hc, float *w, int64_t n) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!w || n != mh::kNnParams) {
+        h->err = "weights: expected MH_NN_PARAMS floats";
+        return MH_ERR_INVALID;
+    }
+    if ((rc = ensure_learned(h))) return rc;
+    CK(cudaMemcpyAsync(w, h->nn_w, mh::kNnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_learned_grad(mh_handle *h, const double *r, const double *e, float *grad, double *loss) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    if (!r || !e || !grad) return MH_ERR_INVALID;
+    if ((rc = ensure_learned(h)) || (rc = ensure_train(h, 1))) return rc;
+    const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
+    std::vector<float> rv(nr, 0.f), ev(nr, 0.f);
+    double er = 0.0;
+    for (int64_t k = 0; k < ne; ++k) {
+        const int64_t row = h->hs.edge_row[k];
+        rv[row] = (float)r[k];
+        ev[row] = (float)e[k];
+        er += (double)rv[row] * (double)ev[row];
+    }
+    if (!(er != 0.0) || !std::isfinite(er)) {
+        h->err = "grad: e.r must be finite and non-zero";
+        return MH_ERR_INVALID;
+    }
+    CK(cudaMemcpyAsync(h->pair_r, rv.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->pair_e, ev.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), h->stream));
+    if ((rc = train_pass(h, 0, er))) return rc;
+    double l = 0.0;
+    CK(cudaMemcpyAsync(grad, h->nn_grad, mh::kNnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&l, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (loss) *loss = l;
+    return MH_OK;
+}
+
+int mh_learned_apply(mh_handle *h, const double *r, double *z) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    if (!r || !z) return MH_ERR_INVALID;
+    if ((rc = ensure_learned(h)) || (rc = ensure_train(h, 1))) return rc;
+    if (h->sys.rows_per_thread != 1) {
+        const int t[2] = {mh::krylov_target_blocks(1, 64), mh::krylov_target_blocks(1, 32)};
+        if ((rc = apply_launch_shape(h, 1, t))) return rc;
+    }
+    const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
+    const int n_inst = h->sys.n_inst;
+    std::vector<float> rv(nr, 0.f), zv(nr);
+    std::vector<double> rr(n_inst, 0.0);
+    for (int i = 0; i < n_inst; ++i)
+        for (int64_t k = h->hs.inst_edge[i]; k < h->hs.inst_edge[i + 1]; ++k) {
+            const float v = (float)r[k];
+            rv[h->hs.edge_row[k]] = v;
+            rr[i] += (double)v * (double)v;
+        }
+    // the network reads each instance's |r|^2 and done flag from the Krylov control block
+    std::vector<mh::InstCtl> ctl;
+    if ((rc = read_ctl(h, ctl))) return rc;
+    for (int i = 0; i < n_inst; ++i) {
+        ctl[i].rr = rr[i];
+        ctl[i].done = 0;
+        ctl[i].iter = 0;
+    }
+    CK(cudaMemcpyAsync(h->sys.ctl, ctl.data(), sizeof(mh::InstCtl) * n_inst, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->pair_r, rv.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(mh::launch_nn_apply(h->sys, h->nn_w, h->nn_wb, h->pair_r, h->nn_h0, h->nn_h1, h->pair_e, nullptr, h->stream));
+    h->n_launch += mh::kNnLayers;
+    CK(cudaMemcpyAsync(zv.data(), h->pair_e, nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t k = 0; k < ne; ++k) z[k] = zv[h->hs.edge_row[k]];
+    return MH_OK;
+}
+
+void mh_learn_opts_default(mh_learn_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->n_pairs = 12;
+    o->epochs = 40;
+    o->lr = 2e-3f;
+    o->train_bias = 0;
+    o->solve_rtol = 1e-9;
+    o->seed = 1;
+}
+
+int mh_learned_train(mh_handle *h, const mh_learn_opts *opts, mh_learn_stats *stats) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    mh_learn_opts o;
+    mh_learn_opts_default(&o);
+    if (opts) o = *opts;
+    mh_learn_stats st;
+    std::memset(&st, 0, sizeof(st));
+    rc = learned_train_impl(h, o, st);
+    if (stats) *stats = st;
+    return rc;
+}
 
 }  // extern "C"

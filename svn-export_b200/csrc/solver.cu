@@ -410,6 +410,8 @@ __global__ void __launch_bounds__(kBlockThreads) k_residual64(SellView<double> A
 // (inst_sums[kSumStride*i + kSumActive] = 1).  On a reliable update the FP32 recursion
 // continues from the recomputed FP64 residual and the search direction is kept, rescaled from
 // the old normalisation |r_old| to the new |r_new|, so no Krylov information is lost.
+// keep_p = 2 (flexible CG) leaves p and the stored (p, q) pair untouched: the next direction
+// is made conjugate to them, which needs no common scale.
 template <int R>
 __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__restrict__ r64, float *__restrict__ x32,
                                                             float *__restrict__ r32, float *__restrict__ p32,
@@ -430,7 +432,8 @@ __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__rest
             const float v = (float)(r64[row] * inv);
             x32[row] = 0.0f;
             r32[row] = v;
-            p32[row] = keep_p ? (float)((double)p32[row] * ratio) : v;
+            if (keep_p == 0) p32[row] = v;
+            else if (keep_p == 1) p32[row] = (float)((double)p32[row] * ratio);
             s.v[0] += (double)v * (double)v;
         }
     }
@@ -445,6 +448,7 @@ __global__ void __launch_bounds__(kBlockThreads) k_ir_start(const double *__rest
         c->done = 0;
         c->scale = active ? nrm : 0.0;
         c->tol2 = rtol2 * tot.v[0];
+        if (keep_p != 2) c->aux[1] = 0.0;  // flexible CG: no stored direction, restart
         if (!active || !(tot.v[0] > 0.0)) finish_inst(c, 0, n_done);
     }
 }
@@ -571,6 +575,12 @@ cudaError_t launch_ir_start(const DevSystem &sys, double rtol2, int max_it, cuda
 
 cudaError_t launch_ir_replace(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s) {
 #define C_(R) ir_start_r<R>(sys, rtol2, max_it, 1, s)
+    MH_BY_R(C_)
+#undef C_
+}
+
+cudaError_t launch_ir_continue(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s) {
+#define C_(R) ir_start_r<R>(sys, rtol2, max_it, 2, s)
     MH_BY_R(C_)
 #undef C_
 }

@@ -29,11 +29,12 @@ MH_BC_NONE, MH_BC_DIRICHLET, MH_BC_NEUMANN, MH_BC_ROBIN = 0, 1, 2, 3
 
 MH_SOLVER_PCG64 = 0
 MH_SOLVER_IR32 = 1
-MH_SOLVER_CHEB64 = 2
+MH_SOLVER_CHEB = 2
 MH_SOLVER_FCG_LEARNED = 3
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
 
 
 class MeshDesc(C.Structure):
@@ -79,6 +80,20 @@ class SolveStats(C.Structure):
         return d
 
 
+class LearnOpts(C.Structure):
+    _fields_ = [("n_pairs", C.c_int32), ("epochs", C.c_int32), ("lr", C.c_float), ("train_bias", C.c_int32),
+                ("solve_rtol", C.c_double), ("seed", C.c_uint64), ("reserved", C.c_int32 * 6)]
+
+
+class LearnStats(C.Structure):
+    _fields_ = [("loss_initial", C.c_double), ("loss_final", C.c_double), ("n_pairs", C.c_int32),
+                ("epochs", C.c_int32), ("ms_pairs", C.c_double), ("ms_train", C.c_double),
+                ("reserved", C.c_double * 4)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class MHError(RuntimeError):
     def __init__(self, status, msg=""):
         self.status = status
@@ -121,6 +136,12 @@ def _load():
         "mh_get_instance_offsets": (C.c_int, [vp] + [C.POINTER(C.c_int64)] * 4),
         "mh_get_instance_stats": (C.c_int, [vp, _i32p, _f64p, _i32p]),
         "mh_autotune": (C.c_int, [vp, C.c_int32, _i32p, _f64p]),
+        "mh_learned_set_weights": (C.c_int, [vp, _f32p, C.c_int64]),
+        "mh_learned_get_weights": (C.c_int, [vp, _f32p, C.c_int64]),
+        "mh_learned_grad": (C.c_int, [vp, _f64p, _f64p, _f32p, _f64p]),
+        "mh_learned_apply": (C.c_int, [vp, _f64p, _f64p]),
+        "mh_learn_opts_default": (None, [C.POINTER(LearnOpts)]),
+        "mh_learned_train": (C.c_int, [vp, C.POINTER(LearnOpts), C.POINTER(LearnStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -138,7 +159,11 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device", "mh_get_schur_system",
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
-            "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune")
+            "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune",
+            "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",
+            "mh_learned_train")
+
+MH_NN_PARAMS = 1260
 
 MH_NOALLOC_MAX_ROWS = 16384 * 256
 

@@ -226,6 +226,45 @@ class MHSystem:
         d["status"] = rc
         return d
 
+    # ---- learned preconditioner (MH_SOLVER_FCG_LEARNED) ----
+    def learned_weights(self):
+        w = np.zeros(_lib.MH_NN_PARAMS, np.float32)
+        check(lib.mh_learned_get_weights(self.h, ptr(w, C.c_float), len(w)), self.h)
+        return w
+
+    def set_learned_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib.mh_learned_set_weights(self.h, ptr(w, C.c_float), len(w)), self.h)
+
+    def learned_grad(self, r, e):
+        """Loss and parameter gradient of one pair (r, e) [n_edges], Jacobi-scaled space."""
+        r, e = f64(r), f64(e)
+        if len(r) != self.n_edges or len(e) != self.n_edges:
+            raise ValueError("r and e need n_edges entries")
+        g = np.zeros(_lib.MH_NN_PARAMS, np.float32)
+        loss = C.c_double(0.0)
+        check(lib.mh_learned_grad(self.h, ptr(r, C.c_double), ptr(e, C.c_double), ptr(g, C.c_float),
+                                  C.byref(loss)), self.h)
+        return loss.value, g
+
+    def learned_apply(self, r):
+        """z = NN(r) [n_edges] through the tensor-core inference kernels."""
+        r = f64(r)
+        if len(r) != self.n_edges:
+            raise ValueError("r needs n_edges entries")
+        z = np.zeros(self.n_edges)
+        check(lib.mh_learned_apply(self.h, ptr(r, C.c_double), ptr(z, C.c_double)), self.h)
+        return z
+
+    def learned_train(self, n_pairs=12, epochs=40, lr=2e-3, train_bias=False, solve_rtol=1e-9, seed=1):
+        o = _lib.LearnOpts()
+        lib.mh_learn_opts_default(C.byref(o))
+        o.n_pairs, o.epochs, o.lr, o.train_bias = int(n_pairs), int(epochs), float(lr), int(bool(train_bias))
+        o.solve_rtol, o.seed = float(solve_rtol), int(seed)
+        st = _lib.LearnStats()
+        check(lib.mh_learned_train(self.h, C.byref(o), C.byref(st)), self.h)
+        return st.as_dict()
+
     # ---- MH_DofHandler accessors on a solution vector ----
     def split(self, sol):
         ns, ne = self.n_sides, self.n_elements

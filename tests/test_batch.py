@@ -56,7 +56,7 @@ def test_batch_matches_solo_and_oracle(gpu, method):
         b.set_bc(bc["bc_type"], bc["pressure"])
         b.assemble()
         st = b.solve(method=method, r_tol=1e-12)
-        assert st["status"] == 0
+        assert st["status"] in (0, _lib.MH_FELL_BACK)
         sol = b.solution()
         ist = b.instance_stats()
         assert np.all(ist["status"] == 0) and np.all(ist["rel_residual"] <= 1e-12)
