@@ -60,6 +60,9 @@ extern "C" {
 #define MH_SOLVER_FCG_LEARNED 3 /* learned (message-passing) preconditioner in flexible CG,
                                    FP32 inner, FP64 replacements; falls back to Chebyshev-
                                    Jacobi when the learned iteration stalls              */
+#define MH_SOLVER_AMG       4   /* aggregation multigrid V-cycle in flexible CG: FP32 inner,
+                                   FP64 residual replacements; hierarchy built on the GPU
+                                   from the current matrix at every solve                */
 
 typedef struct mh_handle mh_handle;
 typedef struct mh_mesh mh_mesh;
@@ -301,6 +304,17 @@ void mh_learn_opts_default(mh_learn_opts *o);
  * (r_s = b^ - S^ x_s, e_s = x* - x_s) scaled by 1/|r_s|, and runs epochs x n_pairs Adam
  * steps on the energy-norm loss.  The solution left in the handle is x*. */
 int mh_learned_train(mh_handle *h, const mh_learn_opts *opts, mh_learn_stats *stats);
+
+/* ---- aggregation multigrid (MH_SOLVER_AMG) ------------------------------------------- */
+/* No counterpart in the reference (PETSc ILU there).  The hierarchy of the last AMG solve:
+ * number of levels, real rows and SELL slots per level (arrays of cap entries). */
+int mh_amg_info(const mh_handle *h, int32_t *n_levels, int64_t *rows, int64_t *slots, int32_t cap);
+/* One level of that hierarchy in CSR without zero entries (level 0 = the FP32 Jacobi-scaled
+ * edge system in padded solver-row order), its aggregation agg [n] (coarse row of each row,
+ * -1: none; not on the last level) and transfer weights [n]: level l+1 is P^T W A_l W P with
+ * P_{i,agg[i]} = 1 and W = diag(weight).  Call with NULL arrays to get n and nnz first. */
+int mh_amg_level(const mh_handle *h, int32_t level, int64_t *n, int64_t *nnz, int32_t *agg, float *weight,
+                 int32_t *row_ptr, int32_t *col, float *val);
 
 /* ---- residual check without device allocation --------------------------------------- */
 /* No counterpart in the reference: Flow123d leaves this check to PETSc's KSP monitor.

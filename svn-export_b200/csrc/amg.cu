@@ -1,0 +1,956 @@
+// Aggregation multigrid preconditioner: GPU setup (pairwise aggregation, Galerkin products,
+// dense coarsest inverse) and the V-cycle.  See amg.hpp for the method.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "amg.hpp"
+
+namespace mh {
+
+template <class T> cudaError_t DBuf<T>::ensure(size_t n) {
+    if (p && n <= cap) return cudaSuccess;
+    release();
+    const size_t m = n ? n : 1;
+    cudaError_t e = cudaMalloc(&p, m * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    cap = m;
+    return cudaSuccess;
+}
+template <class T> void DBuf<T>::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+template struct DBuf<int32_t>;
+template struct DBuf<int64_t>;
+template struct DBuf<float>;
+template struct DBuf<double>;
+template struct DBuf<unsigned int>;
+
+namespace {
+
+constexpr int kS = kSliceRows;  // SELL slice height
+constexpr int32_t kUnmatched = -2, kSingle = -1, kExcluded = -3;
+constexpr int kGalWarps = 4;    // warps per block of the Galerkin row kernel
+constexpr int kGalCap = 1024;   // candidate entries per coarse row (gathered from its rows)
+constexpr unsigned kFull = 0xffffffffu;
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+inline int64_t round_up(int64_t n, int64_t m) { return (n + m - 1) / m * m; }
+
+struct MatView {
+    int64_t n;
+    const int64_t *off;
+    const int32_t *col;
+    const float *val;
+};
+MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val}; }
+
+__device__ __forceinline__ void row_of(const MatView &A, int64_t i, int64_t &base, int &w, int &ln) {
+    const int64_t sl = i / kS;
+    ln = (int)(i - sl * kS);
+    base = A.off[sl];
+    w = (int)((A.off[sl + 1] - base) / kS);
+}
+
+// ---- scans (exclusive, out[n] = total) ----------------------------------------------------
+template <typename T> __device__ __forceinline__ T block_incl_scan(T v, T *ws, T &block_total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < (int)(blockDim.x >> 5) ? ws[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T y = __shfl_up_sync(kFull, w, o);
+            if (lane >= o) w += y;
+        }
+        ws[lane] = w;
+    }
+    __syncthreads();
+    const T res = (warp ? ws[warp - 1] : T(0)) + x;
+    block_total = ws[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return res;
+}
+
+template <typename T> __global__ void __launch_bounds__(1024) k_scan_block(const T *in, T *out, T *bsum, int64_t n) {
+    __shared__ T ws[32];
+    const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+    const T v = i < n ? in[i] : T(0);
+    T tot;
+    const T incl = block_incl_scan<T>(v, ws, tot);
+    if (i < n) out[i] = incl - v;
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+template <typename T> __global__ void __launch_bounds__(1024) k_scan_sums(T *bsum, int64_t nb) {
+    __shared__ T ws[32];
+    T carry = 0;
+    for (int64_t base = 0; base < nb; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        const T v = i < nb ? bsum[i] : T(0);
+        T tot;
+        const T incl = block_incl_scan<T>(v, ws, tot);
+        if (i < nb) bsum[i] = carry + incl - v;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+template <typename T> __global__ void k_scan_add(T *out, const T *bsum, int64_t n, int64_t nb) {
+    const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+    if (i < n) out[i] += bsum[blockIdx.x];
+    if (i == 0) out[n] = bsum[nb];
+}
+
+// ---- level statistics ----------------------------------------------------------------------
+// inv_diag = 1/a_ii, isd = 1/sqrt(a_ii) (0 where there is no positive diagonal) and the
+// Gershgorin bound max_i sum_j |a_ij| / a_ii of D^-1 A.
+__global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned int *bound) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float s = 0.f;
+    if (i < A.n) {
+        int64_t base;
+        int w, ln;
+        row_of(A, i, base, w, ln);
+        float dg = 0.f, sum = 0.f;
+        for (int j = 0; j < w; ++j) {
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            const float v = A.val[slot];
+            if (A.col[slot] == (int32_t)i) dg += v;
+            sum += fabsf(v);
+        }
+        const bool ok = dg > 0.f;
+        inv_diag[i] = ok ? 1.f / dg : 0.f;
+        isd[i] = ok ? rsqrtf(dg) : 0.f;
+        s = ok ? sum / dg : 0.f;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(kFull, s, o));
+    if ((threadIdx.x & 31) == 0 && s > 0.f) atomicMax(bound, __float_as_uint(s));
+}
+
+// ---- pairwise aggregation ------------------------------------------------------------------
+// A row takes part if it is a real row (row_edge >= 0 on the fine level) with at least one
+// non-zero off-diagonal entry; the rest (padding, decoupled Dirichlet edges) are excluded.
+__global__ void k_pair_init(MatView A, const int32_t *row_edge, const float *isd, int32_t *mate) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    bool coupled = false;
+    if ((!row_edge || row_edge[i] >= 0) && isd[i] > 0.f) {
+        int64_t base;
+        int w, ln;
+        row_of(A, i, base, w, ln);
+        for (int j = 0; j < w && !coupled; ++j) {
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            coupled = A.col[slot] != (int32_t)i && A.val[slot] != 0.f;
+        }
+    }
+    mate[i] = coupled ? kUnmatched : kExcluded;
+}
+
+// Strongest negative coupling -a_ij / sqrt(a_ii a_jj) to a still unmatched row (ties: lower j).
+__global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, int32_t *want) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    int32_t best = -1;
+    if (mate[i] == kUnmatched) {
+        int64_t base;
+        int w, ln;
+        row_of(A, i, base, w, ln);
+        float bw = 0.f;
+        const float si = isd[i];
+        for (int j = 0; j < w; ++j) {
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            const int32_t c = A.col[slot];
+            const float v = A.val[slot];
+            if (c == (int32_t)i || !(v < 0.f) || mate[c] != kUnmatched) continue;
+            const float s = -v * si * isd[c];
+            if (s > bw || (s == bw && best >= 0 && c < best)) {
+                bw = s;
+                best = c;
+            }
+        }
+    }
+    want[i] = best;
+}
+
+// Handshake: i and j pair when each is the other's choice; a row with no candidate is final.
+__global__ void k_pair_match(int64_t n, const int32_t *want, int32_t *mate) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || mate[i] != kUnmatched) return;
+    const int32_t j = want[i];
+    if (j < 0) mate[i] = kSingle;
+    else if (want[j] == (int32_t)i) mate[i] = j;
+}
+
+// leader of each aggregate: a single row, or the lower row of a pair
+__global__ void k_pair_lead(int64_t n, const int32_t *mate, int32_t *lead) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t m = mate[i];
+    lead[i] = (m == kSingle || m == kUnmatched || (m >= 0 && (int32_t)i < m)) ? 1 : 0;
+}
+
+__global__ void k_pair_assign(int64_t n, const int32_t *mate, const int32_t *lead, const int32_t *cid, int32_t *agg,
+                              int32_t *cnt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t m = mate[i];
+    if (lead[i]) {
+        agg[i] = cid[i];
+        cnt[cid[i]] = m >= 0 ? 2 : 1;
+    } else {
+        agg[i] = m >= 0 ? cid[m] : -1;
+    }
+}
+
+__global__ void k_pair_members(int64_t n, const int32_t *mate, const int32_t *lead, const int32_t *cid,
+                               const int32_t *mstart, int32_t *mrows) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !lead[i]) return;
+    const int32_t p = mstart[cid[i]];
+    mrows[p] = (int32_t)i;
+    if (mate[i] >= 0) mrows[p + 1] = mate[i];
+}
+
+// Two pairing passes composed: agg = agg2[agg1[i]], members of each final row in order.
+__global__ void k_compose_agg(int64_t n, const int32_t *agg1, const int32_t *agg2, int32_t *agg) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t a = agg1[i];
+    agg[i] = a >= 0 ? agg2[a] : -1;
+}
+
+__global__ void k_compose_count(int64_t nc, const int32_t *ms2, const int32_t *mr2, const int32_t *ms1, int32_t *cnt) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    int32_t k = 0;
+    for (int32_t q = ms2[c]; q < ms2[c + 1]; ++q) k += ms1[mr2[q] + 1] - ms1[mr2[q]];
+    cnt[c] = k;
+}
+
+__global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr2, const int32_t *ms1,
+                               const int32_t *mr1, const int32_t *ms, int32_t *mr) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    int32_t p = ms[c];
+    for (int32_t q = ms2[c]; q < ms2[c + 1]; ++q)
+        for (int32_t t = ms1[mr2[q]]; t < ms1[mr2[q] + 1]; ++t) mr[p++] = mr1[t];
+}
+
+// ---- Galerkin product A_c = P^T A P, one warp per coarse row -------------------------------
+// Gathers (agg[col], val) of the coarse row's rows, sorts by coarse column (bitonic, in
+// shared memory), and sums equal columns in sorted order (FP64 sums: deterministic).
+// Pass 1 (WRITE = false) stores the row lengths; pass 2 writes the SELL slots, padding with
+// (own row, 0).
+template <bool WRITE>
+__global__ void __launch_bounds__(kGalWarps * 32)
+    k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
+               const int32_t *__restrict__ mrows, int64_t nc, int32_t *__restrict__ rowlen,
+               const int64_t *__restrict__ c_off, int32_t *__restrict__ c_col, float *__restrict__ c_val,
+               int32_t *overflow, const float *__restrict__ wt) {
+    __shared__ int32_t sk[kGalWarps][kGalCap];
+    __shared__ float sv[kGalWarps][kGalCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int32_t *K = sk[warp];
+    float *V = sv[warp];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t I = (int64_t)blockIdx.x * kGalWarps + warp; I < nc; I += (int64_t)gridDim.x * kGalWarps) {
+        int cnt = 0;
+        for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
+            int64_t base;
+            int w, ln;
+            const int32_t mi = mrows[m];
+            row_of(A, mi, base, w, ln);
+            const float wi = wt ? wt[mi] : 1.f;
+            for (int j0 = 0; j0 < w; j0 += 32) {
+                const int j = j0 + lane;
+                int32_t key = -1;
+                float v = 0.f;
+                if (j < w) {
+                    const int64_t slot = base + (int64_t)j * kS + ln;
+                    v = A.val[slot];
+                    if (v != 0.f) {
+                        const int32_t c = A.col[slot];
+                        key = agg[c];
+                        if (wt) v = v * wi * wt[c];
+                    }
+                }
+                const unsigned mask = __ballot_sync(kFull, key >= 0);
+                const int pos = cnt + __popc(mask & lt);
+                if (key >= 0 && pos < kGalCap) {
+                    K[pos] = key;
+                    V[pos] = v;
+                }
+                cnt += __popc(mask);
+            }
+        }
+        if (cnt > kGalCap) {
+            if (lane == 0) {
+                atomicExch(overflow, 1);
+                if (!WRITE) rowlen[I] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        int cp = 32;
+        while (cp < cnt) cp <<= 1;
+        for (int k = cnt + lane; k < cp; k += 32) {
+            K[k] = INT_MAX;
+            V[k] = 0.f;
+        }
+        __syncwarp();
+        for (int k = 2; k <= cp; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int t = lane; t < cp; t += 32) {
+                    const int u = t ^ j;
+                    if (u > t) {
+                        const int32_t a = K[t], b = K[u];
+                        const bool up = (t & k) == 0;
+                        if (up ? (a > b) : (a < b)) {
+                            K[t] = b;
+                            K[u] = a;
+                            const float x = V[t];
+                            V[t] = V[u];
+                            V[u] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        int uniq = 0;
+        const int64_t sl = I / kS;
+        const int ln = (int)(I - sl * kS);
+        for (int t0 = 0; t0 < cnt; t0 += 32) {
+            const int t = t0 + lane;
+            const bool head = t < cnt && (t == 0 || K[t] != K[t - 1]);
+            const unsigned hm = __ballot_sync(kFull, head);
+            if (WRITE && head) {
+                const int outk = uniq + __popc(hm & lt);
+                const int32_t key = K[t];
+                double s = 0.0;
+                for (int q = t; q < cnt && K[q] == key; ++q) s += (double)V[q];
+                const int64_t slot = c_off[sl] + (int64_t)outk * kS + ln;
+                c_col[slot] = key;
+                c_val[slot] = (float)s;
+            }
+            uniq += __popc(hm);
+        }
+        if (!WRITE) {
+            if (lane == 0) rowlen[I] = uniq;
+        } else {
+            const int wc = (int)((c_off[sl + 1] - c_off[sl]) / kS);
+            for (int k = uniq + lane; k < wc; k += 32) {
+                const int64_t slot = c_off[sl] + (int64_t)k * kS + ln;
+                c_col[slot] = (int32_t)I;
+                c_val[slot] = 0.f;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// slots of each slice: 32 x the longest row among its real rows
+__global__ void k_slice_width(int64_t n_slices, int64_t nc, const int32_t *rowlen, int64_t *width) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_slices) return;
+    int32_t m = 0;
+    for (int k = 0; k < kS; ++k) {
+        const int64_t i = s * kS + k;
+        if (i < nc) m = max(m, rowlen[i]);
+    }
+    width[s] = (int64_t)m * kS;
+}
+
+// padding rows of a coarse slice that holds no entry at all still need their slots filled
+__global__ void k_fill_pad_rows(int64_t n, int64_t nc, const int64_t *off, int32_t *col, float *val) {
+    const int64_t i = nc + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t sl = i / kS;
+    const int ln = (int)(i - sl * kS);
+    const int w = (int)((off[sl + 1] - off[sl]) / kS);
+    for (int j = 0; j < w; ++j) {
+        col[off[sl] + (int64_t)j * kS + ln] = (int32_t)i;
+        val[off[sl] + (int64_t)j * kS + ln] = 0.f;
+    }
+}
+
+// ---- dense coarsest level ------------------------------------------------------------------
+// [A | I] (n x 2n, FP64, row-major) from the first n rows of a SELL matrix
+__global__ void k_dense_fill(MatView A, int64_t n, double *M) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *row = M + i * 2 * n;
+    for (int64_t c = 0; c < 2 * n; ++c) row[c] = 0.0;
+    row[n + i] = 1.0;
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    for (int j = 0; j < w; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        const int32_t c = A.col[slot];
+        if (c < n) row[c] += (double)A.val[slot];
+    }
+}
+
+// Gauss-Jordan elimination without pivoting (the matrix is SPD), one block of 1024 threads;
+// writes the inverse in FP32.  flag = 1 on a non-positive or non-finite pivot.
+__global__ void __launch_bounds__(1024) k_gauss_jordan(double *M, int64_t n, float *inv, int32_t *flag) {
+    extern __shared__ double fac[];
+    __shared__ double pinv;
+    const int64_t w = 2 * n;
+    for (int64_t k = 0; k < n; ++k) {
+        if (threadIdx.x == 0) {
+            const double p = M[k * w + k];
+            if (!(p > 0.0) || !isfinite(p)) *flag = 1;
+            pinv = (p > 0.0 && isfinite(p)) ? 1.0 / p : 0.0;
+        }
+        __syncthreads();
+        for (int64_t c = threadIdx.x; c < w; c += blockDim.x) M[k * w + c] *= pinv;
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) fac[i] = i == k ? 0.0 : M[i * w + k];
+        __syncthreads();
+        for (int64_t idx = threadIdx.x; idx < n * w; idx += blockDim.x) {
+            const int64_t i = idx / w, c = idx - i * w;
+            if (i != k) M[idx] -= fac[i] * M[k * w + c];
+        }
+        __syncthreads();
+    }
+    for (int64_t idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int64_t i = idx / n, c = idx - i * n;
+        inv[idx] = (float)M[i * w + n + c];
+    }
+}
+
+// x[i] = sum_j inv[i][j] b[j] for i < n (one warp per row); rows n..n_pad-1 get 0
+__global__ void k_dense_gemv(const float *__restrict__ inv, int64_t n, int64_t n_pad, const float *__restrict__ b,
+                             float *__restrict__ x) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n_pad) return;
+    float s = 0.f;
+    if (i < n)
+        for (int64_t j = lane; j < n; j += 32) s += inv[i * n + j] * b[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (lane == 0) x[i] = s;
+}
+
+// ---- V-cycle kernels ------------------------------------------------------------------------
+__device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const float *__restrict__ x) {
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    float y = 0.f;
+    for (int j = 0; j < w; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        y += __ldg(A.val + slot) * x[__ldg(A.col + slot)];
+    }
+    return y;
+}
+
+// first Chebyshev step from x = 0: d = c2 D^-1 b, x = d
+__global__ void k_sm_first(int64_t n, const float *__restrict__ b, const float *__restrict__ invd, float c2,
+                           float *__restrict__ x, float *__restrict__ d) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = c2 * invd[i] * b[i];
+    d[i] = v;
+    x[i] = v;
+}
+
+// Chebyshev step: d = c1 d + c2 D^-1 (b - A x_in), x_out = x_in + d (c1 = 0: d is not read)
+__global__ void k_sm_step(MatView A, const float *__restrict__ b, const float *__restrict__ invd,
+                          const float *__restrict__ x_in, float *__restrict__ x_out, float *__restrict__ d, float c1,
+                          float c2) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const float r = b[i] - row_dot(A, i, x_in);
+    const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * invd[i] * r;
+    d[i] = dn;
+    x_out[i] = x_in[i] + dn;
+}
+
+__global__ void k_residual(MatView A, const float *__restrict__ b, const float *__restrict__ x,
+                           float *__restrict__ r) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    r[i] = b[i] - row_dot(A, i, x);
+}
+
+// b_c[I] = sum of r over the rows of coarse row I (in member order); padding rows get 0
+__global__ void k_restrict(int64_t nc, int64_t nc_pad, const int32_t *__restrict__ ms, const int32_t *__restrict__ mr,
+                           const float *__restrict__ r, float *__restrict__ bc, const float *__restrict__ wt) {
+    const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc_pad) return;
+    float s = 0.f;
+    if (I < nc)
+        for (int32_t k = ms[I]; k < ms[I + 1]; ++k) s += (wt ? wt[mr[k]] : 1.f) * r[mr[k]];
+    bc[I] = s;
+}
+
+__global__ void k_to_float(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+// x += alpha P x_c (alpha from the device scalar when given, else the constant)
+__global__ void k_prolong(int64_t n, const int32_t *__restrict__ agg, const float *__restrict__ xc,
+                          float *__restrict__ x, const double *__restrict__ alpha_dev, float alpha,
+                          const float *__restrict__ wt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t a = agg[i];
+    const float al = alpha_dev ? (float)*alpha_dev : alpha;
+    if (a >= 0) x[i] += al * (wt ? wt[i] : 1.f) * xc[a];
+}
+
+// Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
+// x_c.(A_c x_c) (the fine-level quantities e.r and e.Ae for e = P x_c).
+__global__ void __launch_bounds__(256) k_coarse_dots(MatView A, const float *__restrict__ x,
+                                                     const float *__restrict__ b, double *__restrict__ part) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double xb = 0.0, xax = 0.0;
+    if (i < A.n) {
+        const double xi = (double)x[i];
+        xb = xi * (double)b[i];
+        xax = xi * (double)row_dot(A, i, x);
+    }
+    __shared__ double sh[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        xb += __shfl_xor_sync(kFull, xb, o);
+        xax += __shfl_xor_sync(kFull, xax, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][warp] = xb;
+        sh[1][warp] = xax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a += sh[0][w];
+            c += sh[1][w];
+        }
+        part[2 * blockIdx.x] = a;
+        part[2 * blockIdx.x + 1] = c;
+    }
+}
+
+// alpha = sum(x.b) / sum(x.Ax) over the partials in block order (1 if not positive)
+__global__ void __launch_bounds__(256) k_coarse_alpha(const double *__restrict__ part, int64_t nb, double *alpha) {
+    __shared__ double sh[2][256];
+    double a = 0.0, c = 0.0;
+    for (int64_t k = threadIdx.x; k < nb; k += blockDim.x) {
+        a += part[2 * k];
+        c += part[2 * k + 1];
+    }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = c;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + st];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double num = sh[0][0], den = sh[1][0];
+        *alpha = (den > 0.0 && num > 0.0 && isfinite(num / den)) ? num / den : 1.0;
+    }
+}
+
+}  // namespace
+
+// ---- host side -------------------------------------------------------------------------------
+#define AMG_CK(call)                                          \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) {                              \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_); \
+            return e_;                                        \
+        }                                                     \
+    } while (0)
+
+void Amg::release() {
+    for (auto &L : lv_) {
+        L.slice_off.release();
+        L.col.release();
+        L.val.release();
+        L.inv_diag.release();
+        L.agg.release();
+        L.mem_start.release();
+        L.mem_rows.release();
+        L.b.release();
+        L.xa.release();
+        L.xb.release();
+        L.d.release();
+        L.r.release();
+    }
+    lv_.clear();
+    n_levels_ = 0;
+    for (auto *b : {&mate_, &want_, &lead_, &cid_, &tmp_agg_, &tmp_ms_, &tmp_mr_, &cnt_, &rowlen_, &scan32_blk_,
+                    &mid_col_, &flag_})
+        b->release();
+    for (auto *b : {&width_, &scan64_, &scan64_blk_, &mid_off_}) b->release();
+    dots_.release();
+    alpha_.release();
+    w0_.release();
+    w0_used_ = nullptr;
+    mid_val_.release();
+    isd_.release();
+    dense_.release();
+    dense_inv_.release();
+    bound_.release();
+    if (h_flag_) cudaFreeHost(h_flag_);
+    h_flag_ = nullptr;
+}
+
+cudaError_t Amg::scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s) {
+    const int64_t nb = (n + 1023) / 1024;
+    AMG_CK(scan32_blk_.ensure(nb + 1));
+    if (n > 0) {
+        k_scan_block<int32_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan32_blk_.p, n);
+        k_scan_sums<int32_t><<<1, 1024, 0, s>>>(scan32_blk_.p, nb);
+        k_scan_add<int32_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan32_blk_.p, n, nb);
+        AMG_CK(cudaGetLastError());
+    } else {
+        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int32_t), s));
+    }
+    int32_t t = 0;
+    AMG_CK(cudaMemcpyAsync(&t, out + n, sizeof(t), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    total = t;
+    return cudaSuccess;
+}
+
+cudaError_t Amg::scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s) {
+    const int64_t nb = (n + 1023) / 1024;
+    AMG_CK(scan64_blk_.ensure(nb + 1));
+    if (n > 0) {
+        k_scan_block<int64_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan64_blk_.p, n);
+        k_scan_sums<int64_t><<<1, 1024, 0, s>>>(scan64_blk_.p, nb);
+        k_scan_add<int64_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan64_blk_.p, n, nb);
+        AMG_CK(cudaGetLastError());
+    } else {
+        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+    }
+    AMG_CK(cudaMemcpyAsync(&total, out + n, sizeof(total), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    return cudaSuccess;
+}
+
+cudaError_t Amg::level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s) {
+    const int64_t n = L.A.n;
+    AMG_CK(L.inv_diag.ensure(n));
+    AMG_CK(isd_.ensure(n));
+    AMG_CK(bound_.ensure(1));
+    AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
+    k_level_diag<<<nblk(n, 256), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound_.p);
+    AMG_CK(cudaGetLastError());
+    unsigned int bits = 0;
+    AMG_CK(cudaMemcpyAsync(&bits, bound_.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    float hi;
+    std::memcpy(&hi, &bits, sizeof(hi));
+    L.hi = hi > 0.f ? hi : 2.f;
+    (void)unit_diag;
+    return cudaSuccess;
+}
+
+// One pairing pass on A (rows excluded by row_edge < 0 or without coupling get agg = -1):
+// agg [A.n], nc aggregates, member lists mstart [nc+1], mrows.
+cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *row_edge, DBuf<int32_t> &agg,
+                           int64_t &nc, DBuf<int32_t> &mstart, DBuf<int32_t> &mrows, cudaStream_t s) {
+    const int64_t n = A.n;
+    const MatView V = view(A);
+    AMG_CK(mate_.ensure(n));
+    AMG_CK(want_.ensure(n));
+    AMG_CK(lead_.ensure(n));
+    AMG_CK(cid_.ensure(n + 1));
+    AMG_CK(agg.ensure(n));
+    const unsigned g = nblk(n, 256);
+    k_pair_init<<<g, 256, 0, s>>>(V, row_edge, isd, mate_.p);
+    for (int r = 0; r < opt_.pair_rounds; ++r) {
+        k_pair_want<<<g, 256, 0, s>>>(V, isd, mate_.p, want_.p);
+        k_pair_match<<<g, 256, 0, s>>>(n, want_.p, mate_.p);
+    }
+    k_pair_lead<<<g, 256, 0, s>>>(n, mate_.p, lead_.p);
+    AMG_CK(cudaGetLastError());
+    cudaError_t e = scan_i32(lead_.p, cid_.p, n, nc, s);
+    if (e != cudaSuccess) return e;
+    AMG_CK(cnt_.ensure(nc + 1));
+    AMG_CK(mstart.ensure(nc + 1));
+    k_pair_assign<<<g, 256, 0, s>>>(n, mate_.p, lead_.p, cid_.p, agg.p, cnt_.p);
+    AMG_CK(cudaGetLastError());
+    int64_t members = 0;
+    if ((e = scan_i32(cnt_.p, mstart.p, nc, members, s)) != cudaSuccess) return e;
+    AMG_CK(mrows.ensure(members));
+    k_pair_members<<<g, 256, 0, s>>>(n, mate_.p, lead_.p, cid_.p, mstart.p, mrows.p);
+    AMG_CK(cudaGetLastError());
+    return cudaSuccess;
+}
+
+cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, const int32_t *mstart,
+                          const int32_t *mrows, DBuf<int64_t> &c_off, DBuf<int32_t> &c_col, DBuf<float> &c_val,
+                          AmgMatrix &C, cudaStream_t s, const float *wt) {
+    const int64_t n_pad = round_up(nc, kS), n_sl = n_pad / kS;
+    AMG_CK(rowlen_.ensure(n_pad));
+    AMG_CK(flag_.ensure(1));
+    AMG_CK(width_.ensure(n_sl));
+    AMG_CK(c_off.ensure(n_sl + 1));
+    AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
+    const unsigned gg = (unsigned)std::min<int64_t>((nc + kGalWarps - 1) / kGalWarps, 148 * 16);
+    k_galerkin<false><<<gg ? gg : 1, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p, nullptr,
+                                                              nullptr, nullptr, flag_.p, wt);
+    k_slice_width<<<nblk(n_sl, 256), 256, 0, s>>>(n_sl, nc, rowlen_.p, width_.p);
+    AMG_CK(cudaGetLastError());
+    int64_t slots = 0;
+    cudaError_t e = scan_i64(width_.p, c_off.p, n_sl, slots, s);
+    if (e != cudaSuccess) return e;
+    AMG_CK(c_col.ensure(slots));
+    AMG_CK(c_val.ensure(slots));
+    k_galerkin<true><<<gg ? gg : 1, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p, c_off.p,
+                                                             c_col.p, c_val.p, flag_.p, wt);
+    if (n_pad > nc) k_fill_pad_rows<<<nblk(n_pad - nc, 256), 256, 0, s>>>(n_pad, nc, c_off.p, c_col.p, c_val.p);
+    AMG_CK(cudaGetLastError());
+    AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    if (*h_flag_) {
+        err = "Galerkin row wider than the gather buffer";
+        return cudaErrorInvalidValue;
+    }
+    C.n = n_pad;
+    C.n_slices = n_sl;
+    C.slots = slots;
+    C.slice_off = c_off.p;
+    C.col = c_col.p;
+    C.val = c_val.p;
+    return cudaSuccess;
+}
+
+cudaError_t Amg::dense_coarse(const AmgMatrix &A, cudaStream_t s) {
+    const int64_t n = dense_n_;
+    AMG_CK(dense_.ensure((size_t)n * 2 * n));
+    AMG_CK(dense_inv_.ensure((size_t)n * n));
+    AMG_CK(flag_.ensure(1));
+    AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
+    k_dense_fill<<<nblk(n, 128), 128, 0, s>>>(view(A), n, dense_.p);
+    k_gauss_jordan<<<1, 1024, n * sizeof(double), s>>>(dense_.p, n, dense_inv_.p, flag_.p);
+    AMG_CK(cudaGetLastError());
+    AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    if (*h_flag_) {
+        err = "coarsest matrix is not positive definite";
+        return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s) {
+    opt_ = o;
+    if (!h_flag_) AMG_CK(cudaHostAlloc((void **)&h_flag_, sizeof(int32_t), cudaHostAllocDefault));
+    if ((int)lv_.size() < o.max_levels) lv_.resize(o.max_levels);
+    n_levels_ = 0;
+    // level 0: the solver's FP32 scaled matrix
+    AmgLevel &L0 = lv_[0];
+    L0.A.n = sys.n_rows;
+    L0.A.n_slices = sys.n_slices;
+    L0.A.slots = sys.n_slots;
+    L0.A.slice_off = sys.slice_off;
+    L0.A.col = sys.col;
+    L0.A.val = sys.val32;
+    // level-0 weights: the near-null vector of the scaled system S^ = D^-1/2 S D^-1/2 is
+    // D^1/2 1 (constants are near-null for S), so the level-0 transfers carry sqrt(diag S)
+    AMG_CK(w0_.ensure(sys.n_rows));
+    k_to_float<<<nblk(sys.n_rows, 256), 256, 0, s>>>(sys.n_rows, sys.dsq, w0_.p);
+    AMG_CK(cudaGetLastError());
+    const float *w0 = opt_.weighted ? w0_.p : nullptr;
+    cudaError_t e;
+    for (int l = 0;; ++l) {
+        AmgLevel &L = lv_[l];
+        if ((e = level_stats(L, l == 0, s)) != cudaSuccess) return e;
+        AMG_CK(L.b.ensure(L.A.n));
+        AMG_CK(L.xa.ensure(L.A.n));
+        AMG_CK(L.xb.ensure(L.A.n));
+        AMG_CK(L.d.ensure(L.A.n));
+        AMG_CK(L.r.ensure(L.A.n));
+        L.nc = 0;
+        n_levels_ = l + 1;
+        const int64_t n_real = l == 0 ? sys.n_rows : (l > 0 ? lv_[l - 1].nc : 0);
+        if (n_real <= opt_.coarse_max || l + 1 >= opt_.max_levels) break;
+        // pass 1 on A_l
+        int64_t nc1 = 0;
+        if ((e = pair_pass(L.A, isd_.p, l == 0 ? sys.row_edge : nullptr, L.agg, nc1, L.mem_start, L.mem_rows, s)) !=
+            cudaSuccess)
+            return e;
+        AmgLevel &C = lv_[l + 1];
+        if (opt_.pair_passes >= 2 && nc1 > opt_.coarse_max) {
+            // intermediate matrix of the pairs, then pair again and compose
+            AmgMatrix M;
+            if ((e = galerkin(L.A, L.agg.p, nc1, L.mem_start.p, L.mem_rows.p, mid_off_, mid_col_, mid_val_, M, s,
+                              l == 0 ? w0 : nullptr)) != cudaSuccess)
+                return e;
+            // strength scaling of the intermediate matrix
+            AMG_CK(isd_.ensure(M.n));
+            AMG_CK(tmp_agg_.ensure(M.n));
+            {
+                AMG_CK(C.inv_diag.ensure(M.n));
+                AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
+                k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), C.inv_diag.p, isd_.p, bound_.p);
+                AMG_CK(cudaGetLastError());
+            }
+            DBuf<int32_t> &agg2 = tmp_agg_;
+            int64_t nc2 = 0;
+            if ((e = pair_pass(M, isd_.p, nullptr, agg2, nc2, tmp_ms_, tmp_mr_, s)) != cudaSuccess) return e;
+            // compose: agg = agg2[agg1], members in order
+            AMG_CK(cnt_.ensure(nc2 + 1));
+            AMG_CK(cid_.ensure(nc2 + 1));
+            k_compose_agg<<<nblk(L.A.n, 256), 256, 0, s>>>(L.A.n, L.agg.p, agg2.p, L.agg.p);
+            k_compose_count<<<nblk(nc2, 256), 256, 0, s>>>(nc2, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, cnt_.p);
+            AMG_CK(cudaGetLastError());
+            int64_t members = 0;
+            if ((e = scan_i32(cnt_.p, cid_.p, nc2, members, s)) != cudaSuccess) return e;
+            AMG_CK(want_.ensure(members));
+            k_compose_fill<<<nblk(nc2, 256), 256, 0, s>>>(nc2, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, L.mem_rows.p,
+                                                          cid_.p, want_.p);
+            AMG_CK(cudaGetLastError());
+            AMG_CK(L.mem_start.ensure(nc2 + 1));
+            AMG_CK(L.mem_rows.ensure(members));
+            AMG_CK(cudaMemcpyAsync(L.mem_start.p, cid_.p, (nc2 + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+            AMG_CK(cudaMemcpyAsync(L.mem_rows.p, want_.p, members * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+            // the final coarse matrix from the intermediate one
+            if ((e = galerkin(M, agg2.p, nc2, tmp_ms_.p, tmp_mr_.p, C.slice_off, C.col, C.val, C.A, s, nullptr)) !=
+                cudaSuccess)
+                return e;
+            L.nc = nc2;
+        } else {
+            if ((e = galerkin(L.A, L.agg.p, nc1, L.mem_start.p, L.mem_rows.p, C.slice_off, C.col, C.val, C.A, s,
+                              l == 0 ? w0 : nullptr)) != cudaSuccess)
+                return e;
+            L.nc = nc1;
+        }
+        if (L.nc == 0) {  // nothing couples: this level is the last
+            break;
+        }
+        if ((double)L.nc > 0.85 * (double)n_real) {  // coarsening stalls: stop one level later
+            opt_.max_levels = std::min(opt_.max_levels, l + 2);
+        }
+    }
+    const AmgLevel &Lc = lv_[n_levels_ - 1];
+    dense_n_ = n_levels_ == 1 ? Lc.A.n : lv_[n_levels_ - 2].nc;
+    if (dense_n_ > 640) {  // Gauss-Jordan in one block is O(n^3): keep the coarsest level small
+        err = "coarsest level too large for the dense solve";
+        return cudaErrorInvalidValue;
+    }
+    w0_used_ = w0;
+    // partial sums of the coarse-correction scaling, one slice per level
+    dots_off_.assign(n_levels_, 0);
+    int64_t tot = 0;
+    for (int l = 0; l + 1 < n_levels_; ++l) {
+        dots_off_[l] = tot;
+        tot += 2 * (int64_t)nblk(lv_[l + 1].A.n, 256);
+    }
+    AMG_CK(dots_.ensure(tot + 2));
+    AMG_CK(alpha_.ensure(n_levels_ + 1));
+    return dense_coarse(Lc.A, s);
+}
+
+void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2) const {
+    const int deg = std::max(1, opt_.cheb_degree);
+    const double hi = L.hi, lo = hi / std::max(1.5f, opt_.cheb_ratio);
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    c1.assign(deg, 0.0);
+    c2.assign(deg, 1.0 / theta);
+    for (int k = 1; k < deg; ++k) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        c1[k] = rn * rho;
+        c2[k] = 2.0 * rn / delta;
+        rho = rn;
+    }
+}
+
+int Amg::kernels_per_apply() const {
+    const int deg = std::max(1, opt_.cheb_degree);
+    return (n_levels_ - 1) * (2 * deg + 3) + 1 + (opt_.kcycle ? 2 * std::max(0, n_levels_ - 2) : 0);
+}
+
+cudaError_t Amg::apply(const float *r, float *z, cudaStream_t s) {
+    // descend: smooth from zero, residual, restrict
+    std::vector<double> c1, c2;
+    const int deg = std::max(1, opt_.cheb_degree);
+    const int nl = n_levels_;
+    std::vector<float *> xout(nl);
+    for (int l = 0; l < nl - 1; ++l) {
+        AmgLevel &L = lv_[l];
+        const float *b = l == 0 ? r : L.b.p;
+        const MatView A = view(L.A);
+        const unsigned g = nblk(L.A.n, 256);
+        cheb_coeffs(L, c1, c2);
+        float *xi = L.xa.p, *xo = L.xb.p;
+        k_sm_first<<<g, 256, 0, s>>>(L.A.n, b, L.inv_diag.p, (float)c2[0], xi, L.d.p);
+        for (int k = 1; k < deg; ++k) {
+            k_sm_step<<<g, 256, 0, s>>>(A, b, L.inv_diag.p, xi, xo, L.d.p, (float)c1[k], (float)c2[k]);
+            std::swap(xi, xo);
+        }
+        xout[l] = xi;
+        k_residual<<<g, 256, 0, s>>>(A, b, xi, L.r.p);
+        AmgLevel &C = lv_[l + 1];
+        k_restrict<<<nblk(C.A.n, 256), 256, 0, s>>>(L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, C.b.p,
+                                                    l == 0 ? w0_used_ : nullptr);
+    }
+    // coarsest: dense inverse
+    {
+        AmgLevel &Lc = lv_[nl - 1];
+        const float *b = nl == 1 ? r : Lc.b.p;
+        float *x = nl == 1 ? z : Lc.xa.p;
+        k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(dense_inv_.p, dense_n_, Lc.A.n, b, x);
+        xout[nl - 1] = x;
+    }
+    // ascend: prolong, smooth
+    for (int l = nl - 2; l >= 0; --l) {
+        AmgLevel &L = lv_[l];
+        const float *b = l == 0 ? r : L.b.p;
+        const MatView A = view(L.A);
+        const unsigned g = nblk(L.A.n, 256);
+        cheb_coeffs(L, c1, c2);
+        float *xi = xout[l];
+        const double *al = nullptr;
+        if (opt_.kcycle && l + 2 < nl) {  // the coarsest correction is exact: alpha = 1
+            AmgLevel &C = lv_[l + 1];
+            const unsigned gc = nblk(C.A.n, 256);
+            k_coarse_dots<<<gc, 256, 0, s>>>(view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l]);
+            k_coarse_alpha<<<1, 256, 0, s>>>(dots_.p + dots_off_[l], gc, alpha_.p + l);
+            al = alpha_.p + l;
+        }
+        k_prolong<<<g, 256, 0, s>>>(L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
+        float *other = xi == L.xa.p ? L.xb.p : L.xa.p;
+        for (int k = 0; k < deg; ++k) {
+            float *xo = (l == 0 && k == deg - 1) ? z : other;
+            k_sm_step<<<g, 256, 0, s>>>(A, b, L.inv_diag.p, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k]);
+            other = xi;
+            xi = xo;
+        }
+        xout[l] = xi;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace mh

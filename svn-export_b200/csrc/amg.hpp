@@ -1,0 +1,118 @@
+// Aggregation multigrid preconditioner for the Jacobi-scaled edge system (FP32), built and
+// applied on the GPU.  No counterpart in the reference, which preconditions the Schur system
+// with PETSc ILU (src/la/solve.cc:370); it is the preconditioner of the MH_SOLVER_AMG solve.
+//
+// Setup (every solve, from the current matrix values):
+//   level l -> l+1 by double pairwise aggregation: two rounds of handshake matching on the
+//   strongest negative coupling -a_ij / sqrt(a_ii a_jj), each followed by the Galerkin product
+//   A_c = P^T A P with the piecewise-constant P of the pairs; rows without off-diagonal
+//   coupling (Dirichlet edges, padding) stay on the fine level only.  The fine level is the
+//   Jacobi-scaled S^ = D^-1/2 S D^-1/2, whose near-null vector is D^1/2 1, so its transfers
+//   carry the weights sqrt(diag S): P_0 = W P, and A_1 = P^T S P in the unscaled space.  Coarse matrices are
+//   stored as SELL-32 like the fine one; their rows are built by one warp each (gather,
+//   bitonic sort by column, deterministic segmented sum).  The coarsest level (<= coarse_max
+//   rows) is inverted densely in FP64 (Gauss-Jordan, one block).
+// Apply (one V-cycle, FP32): Chebyshev smoothing of degree d on [hi/ratio, hi] of D^-1 A
+// before and after the coarse correction (symmetric, so the cycle is an SPD operator).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device_system.hpp"
+
+namespace mh {
+
+struct AmgOptions {
+    int max_levels = 20;
+    int coarse_max = 256;   // dense coarsest solve at or below this many rows
+    int pair_rounds = 4;    // handshake rounds per pairing pass
+    int pair_passes = 2;    // pairing passes per level (2: aggregates of up to 4 rows)
+    int cheb_degree = 2;    // smoothing steps before and after the coarse correction
+    float cheb_ratio = 4.f; // smoothing interval [hi / ratio, hi]
+    int kcycle = 1;         // 1: scale each coarse correction by its energy-optimal factor
+    float alpha = 1.f;      // fixed scaling of the coarse corrections when kcycle = 0
+    int weighted = 1;       // level-0 transfers weighted by sqrt(diag S) (near-null vector)
+};
+
+template <class T> struct DBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n);  // grows (contents lost), never shrinks
+    void release();
+};
+
+struct AmgMatrix {
+    int64_t n = 0, n_slices = 0, slots = 0;
+    const int64_t *slice_off = nullptr;
+    const int32_t *col = nullptr;
+    const float *val = nullptr;
+};
+
+struct AmgLevel {
+    AmgMatrix A;                               // level 0 borrows the solver's SELL matrix
+    DBuf<int64_t> slice_off;                   // owned storage of coarse levels
+    DBuf<int32_t> col;
+    DBuf<float> val;
+    DBuf<float> inv_diag;
+    DBuf<int32_t> agg;                         // [n] coarse row of each row, -1: none
+    DBuf<int32_t> mem_start, mem_rows;         // rows of each coarse row: [nc+1], [n]
+    DBuf<float> b, xa, xb, d, r;               // cycle vectors
+    int64_t nc = 0;                            // coarse rows (0 on the coarsest level)
+    float hi = 2.f;                            // Gershgorin bound of D^-1 A
+};
+
+class Amg {
+public:
+    ~Amg() { release(); }
+    // Builds the hierarchy from the FP32 scaled matrix (sys.val32) and sys.row_edge.
+    cudaError_t setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s);
+    // z = M r over all rows of the solver space (one V-cycle); stream-ordered, capturable.
+    cudaError_t apply(const float *r, float *z, cudaStream_t s);
+    void release();
+    int levels() const { return n_levels_; }
+    const AmgLevel &level(int l) const { return lv_[l]; }
+    int64_t coarse_rows() const { return n_levels_ ? lv_[n_levels_ - 1].A.n : 0; }
+    int kernels_per_apply() const;
+    const float *fine_weights() const { return w0_used_; }  // null when the transfers are unweighted
+    std::string err;
+
+private:
+    cudaError_t pair_pass(const AmgMatrix &A, const float *inv_diag, const int32_t *exclude_row_edge,
+                          DBuf<int32_t> &agg, int64_t &nc, DBuf<int32_t> &mstart, DBuf<int32_t> &mrows, cudaStream_t s);
+    cudaError_t galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, const int32_t *mstart,
+                         const int32_t *mrows, DBuf<int64_t> &c_off, DBuf<int32_t> &c_col, DBuf<float> &c_val,
+                         AmgMatrix &C, cudaStream_t s, const float *wt);
+    cudaError_t level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s);
+    cudaError_t dense_coarse(const AmgMatrix &A, cudaStream_t s);
+    cudaError_t scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s);
+    cudaError_t scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s);
+    void cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2) const;
+
+    AmgOptions opt_;
+    std::vector<AmgLevel> lv_;
+    int n_levels_ = 0;
+    // pairing and Galerkin scratch
+    DBuf<int32_t> mate_, want_, lead_, cid_, tmp_agg_, tmp_ms_, tmp_mr_, cnt_;
+    DBuf<int64_t> width_, scan64_;
+    DBuf<int32_t> rowlen_, scan32_blk_;
+    DBuf<int64_t> scan64_blk_;
+    DBuf<int64_t> mid_off_;
+    DBuf<int32_t> mid_col_;
+    DBuf<float> mid_val_;
+    DBuf<float> isd_;
+    DBuf<double> dense_;
+    DBuf<float> dense_inv_;
+    DBuf<int32_t> flag_;
+    DBuf<unsigned int> bound_;
+    DBuf<double> dots_, alpha_;     // coarse-correction scaling: partials, factor per level
+    std::vector<int64_t> dots_off_;
+    DBuf<float> w0_;                // sqrt(diag S) per fine row
+    const float *w0_used_ = nullptr;
+    int64_t dense_n_ = 0;
+    int32_t *h_flag_ = nullptr;
+};
+
+}  // namespace mh

@@ -330,6 +330,24 @@ __global__ void __launch_bounds__(kBlockThreads)
     }
 }
 
+// beta = z.q_old / (p.q)_old for flexible CG after a preconditioner that writes z only
+__global__ void __launch_bounds__(kBlockThreads)
+    k_fcg_beta(const float *__restrict__ z, const float *__restrict__ q_old, double *__restrict__ partial,
+               InstCtl *__restrict__ ctl, Plan plan) {
+    const int inst = plan.inst[blockIdx.x];
+    InstCtl *c = ctl + inst;
+    if (c->done) return;
+    double zq = 0.0;
+    for (int tile = plan.tile_begin[blockIdx.x]; tile < plan.tile_end[blockIdx.x]; ++tile) {
+        const int64_t row = (int64_t)tile * kBlockThreads + threadIdx.x;
+        zq += (double)z[row] * (double)q_old[row];
+    }
+    Sums<1> s = {{zq}};
+    Sums<1> tot;
+    if (block_finish<1>(s, partial, c, plan, inst, tot) && threadIdx.x == 0)
+        c->beta = (c->aux[1] != 0.0 && c->aux[0] != 0.0) ? tot.v[0] / c->aux[0] : 0.0;
+}
+
 // Gershgorin bound max_i sum_j |S^_ij| (upper bound of the spectrum of S^)
 __global__ void k_row_abs_max(SellView<float> A, int64_t n_rows, unsigned int *out) {
     const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -608,6 +626,12 @@ cudaError_t launch_cheb_apply(const DevSystem &sys, const float *r, float *z0, f
                                                 last && q_old ? sys.partial : nullptr, sys.ctl, p, sys.n_done);
         zp = zn;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fcg_beta(const DevSystem &sys, const float *z, const float *q_old, cudaStream_t s) {
+    if (sys.rows_per_thread != 1) return cudaErrorInvalidValue;  // tiles of 256 rows
+    k_fcg_beta<<<(unsigned)sys.plan[1].n_blocks, kBlockThreads, 0, s>>>(z, q_old, sys.partial, sys.ctl, plan32(sys));
     return cudaGetLastError();
 }
 

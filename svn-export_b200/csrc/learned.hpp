@@ -36,6 +36,8 @@ cudaError_t launch_nn_apply(const DevSystem &sys, const float *w, const uint32_t
                             float4 *h1, float *z, const float *q_old, cudaStream_t s);
 cudaError_t launch_cheb_apply(const DevSystem &sys, const float *r, float *z0, float *z1, float *d, float *z_final,
                               const float *q_old, int degree, double lo, double hi, cudaStream_t s);
+// beta of flexible CG from z and the previous q (for preconditioners that only write z)
+cudaError_t launch_fcg_beta(const DevSystem &sys, const float *z, const float *q_old, cudaStream_t s);
 cudaError_t launch_fcg_direction(const DevSystem &sys, const float *z, cudaStream_t s);
 cudaError_t launch_fcg_update(const DevSystem &sys, cudaStream_t s);
 cudaError_t launch_spectrum_bound(const DevSystem &sys, unsigned int *out, cudaStream_t s);

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "device_system.hpp"
+#include "amg.hpp"
 #include "learned.hpp"
 #include "mh_darcy.h"
 #include "system_build.hpp"
@@ -22,6 +23,18 @@
 
 struct mh_mesh {
     mh::MeshData m;
+};
+
+enum class Pc { Nn, Cheb, Amg };  // preconditioners of the flexible-CG solve
+
+struct FcgKey {  // what a captured flexible-CG graph depends on
+    int kind = -1, ipg = 0, degree = 0;
+    double lo = 0.0, hi = 0.0;
+    int64_t amg_epoch = -1;
+    bool operator==(const FcgKey &o) const {
+        return kind == o.kind && ipg == o.ipg && degree == o.degree && lo == o.lo && hi == o.hi &&
+               amg_epoch == o.amg_epoch;
+    }
 };
 
 struct mh_handle {
@@ -63,6 +76,10 @@ struct mh_handle {
     float *cheb_z0 = nullptr, *cheb_z1 = nullptr, *cheb_d = nullptr;
     unsigned int *spec_bound = nullptr;
     double *d_loss = nullptr;
+    mh::Amg amg;                        // aggregation multigrid (MH_SOLVER_AMG)
+    int64_t amg_epoch = 0;              // setups so far (captured graphs refer to one)
+    cudaGraphExec_t fcg_graph = nullptr;
+    FcgKey fcg_key{};
     mh::NnTrainBuffers tr{};            // activations of a training pass
     bool tr_ready = false;
     float *pair_r = nullptr, *pair_e = nullptr;  // training pairs, [cap][n_rows] each
@@ -286,6 +303,8 @@ int apply_launch_shape(mh_handle *h, int R, const int targets[2]) {
                 g = nullptr;
             }
     for (auto &gi : h->graph_iters) gi[0] = gi[1] = 0;
+    if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
+    h->fcg_graph = nullptr;
     return MH_OK;
 }
 
@@ -665,62 +684,107 @@ int spectrum_bound(mh_handle *h, double &hi) {
     return MH_OK;
 }
 
-// One flexible-CG iteration: z = M(r) (network or Chebyshev polynomial, which also forms
-// beta = z.q_old / (p.q)_old), p = z - beta p, q = S^ p with alpha = p.r / p.q, x and r.
-cudaError_t fcg_iteration(mh_handle *h, bool learned, int degree, double lo, double hi, cudaStream_t s) {
+// One flexible-CG iteration: z = M(r) (network, Chebyshev polynomial or AMG V-cycle) with
+// beta = z.q_old / (p.q)_old, p = z - beta p, q = S^ p with alpha = p.r / p.q, x and r.
+cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double hi, cudaStream_t s) {
     mh::DevSystem &sys = h->sys;
-    cudaError_t e = learned ? mh::launch_nn_apply(sys, h->nn_w, h->nn_wb, sys.r32, h->nn_h0, h->nn_h1, sys.z32,
-                                                   sys.q32, s)
-                            : mh::launch_cheb_apply(sys, sys.r32, h->cheb_z0, h->cheb_z1, h->cheb_d, sys.z32,
-                                                    sys.q32, degree, lo, hi, s);
+    cudaError_t e;
+    switch (kind) {
+        case Pc::Nn:
+            e = mh::launch_nn_apply(sys, h->nn_w, h->nn_wb, sys.r32, h->nn_h0, h->nn_h1, sys.z32, sys.q32, s);
+            break;
+        case Pc::Cheb:
+            e = mh::launch_cheb_apply(sys, sys.r32, h->cheb_z0, h->cheb_z1, h->cheb_d, sys.z32, sys.q32, degree, lo, hi,
+                                      s);
+            break;
+        default:
+            e = h->amg.apply(sys.r32, sys.z32, s);
+            if (e == cudaSuccess) e = mh::launch_fcg_beta(sys, sys.z32, sys.q32, s);
+            break;
+    }
     if (e == cudaSuccess) e = mh::launch_fcg_direction(sys, sys.z32, s);
     if (e == cudaSuccess) e = mh::launch_cg_spmv(sys, 32, s);
     if (e == cudaSuccess) e = mh::launch_fcg_update(sys, s);
     return e;
 }
 
-int run_fcg(mh_handle *h, bool learned, int degree, double lo, double hi, int ipg, int max_it) {
-    cudaGraph_t g;
-    cudaGraphExec_t ge = nullptr;
-    CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
-    for (int k = 0; k < ipg && e == cudaSuccess; ++k) e = fcg_iteration(h, learned, degree, lo, hi, h->own_stream);
-    cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-        if (e2 == cudaSuccess) cudaGraphDestroy(g);
-        h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
-        return MH_ERR_CUDA;
+int fcg_kernels_per_iteration(mh_handle *h, Pc kind, int degree) {
+    switch (kind) {
+        case Pc::Nn: return mh::kNnLayers + 3;
+        case Pc::Cheb: return degree + 3;
+        default: return h->amg.kernels_per_apply() + 4;
     }
-    e = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        h->err = cudaGetErrorString(e);
-        return MH_ERR_CUDA;
-    }
-    const int per_iter = (learned ? 3 : degree) + 3;
-    int64_t launched = 0;
-    int rc = MH_OK;
-    while (true) {
-        cudaError_t ce = cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
-        if (ce != cudaSuccess) {
-            h->err = cudaGetErrorString(ce);
-            rc = MH_ERR_CUDA;
-            break;
+}
+
+void drop_fcg_graph(mh_handle *h) {
+    if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
+    h->fcg_graph = nullptr;
+}
+
+// Runs captured FCG iterations until every instance reports done.  The graph is kept while
+// its inputs (preconditioner, launch shape, AMG hierarchy) stay the same.
+int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it) {
+    const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch};
+    if (!h->fcg_graph || !(h->fcg_key == key)) {
+        drop_fcg_graph(h);
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < ipg && e == cudaSuccess; ++k) e = fcg_iteration(h, kind, degree, lo, hi, h->own_stream);
+        cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (e2 == cudaSuccess) cudaGraphDestroy(g);
+            h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
+            cudaGetLastError();
+            return MH_ERR_CUDA;
         }
+        e = cudaGraphInstantiate(&h->fcg_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->fcg_graph = nullptr;
+            h->err = cudaGetErrorString(e);
+            return MH_ERR_CUDA;
+        }
+        h->fcg_key = key;
+    }
+    const int per_iter = fcg_kernels_per_iteration(h, kind, degree);
+    int64_t launched = 0;
+    while (true) {
+        CK(cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
         if (*h->h_done >= h->sys.n_inst) break;
         if (launched > (int64_t)max_it + 2 * ipg) break;
-        ce = cudaGraphLaunch(ge, h->stream);
-        if (ce != cudaSuccess) {
-            h->err = cudaGetErrorString(ce);
-            rc = MH_ERR_CUDA;
-            break;
-        }
+        CK(cudaGraphLaunch(h->fcg_graph, h->stream));
         launched += ipg;
         h->n_launch += (int64_t)per_iter * ipg;
     }
-    cudaGraphExecDestroy(ge);
-    return rc;
+    return MH_OK;
+}
+
+// AMG options: defaults, overridable from the environment for tuning studies
+mh::AmgOptions amg_options() {
+    mh::AmgOptions o;
+    auto env_i = [](const char *k, int &v, int lo, int hi) {
+        if (const char *e = getenv(k)) {
+            const int x = atoi(e);
+            if (x >= lo && x <= hi) v = x;
+        }
+    };
+    env_i("MH_AMG_DEGREE", o.cheb_degree, 1, 8);
+    env_i("MH_AMG_PASSES", o.pair_passes, 1, 2);
+    env_i("MH_AMG_COARSE", o.coarse_max, 16, 640);
+    env_i("MH_AMG_ROUNDS", o.pair_rounds, 1, 16);
+    env_i("MH_AMG_KCYCLE", o.kcycle, 0, 1);
+    env_i("MH_AMG_WEIGHTED", o.weighted, 0, 1);
+    if (const char *e = getenv("MH_AMG_RATIO")) {
+        const float x = (float)atof(e);
+        if (x >= 1.5f && x <= 100.f) o.cheb_ratio = x;
+    }
+    if (const char *e = getenv("MH_AMG_ALPHA")) {
+        const float x = (float)atof(e);
+        if (x > 0.f && x <= 3.f) o.alpha = x;
+    }
+    return o;
 }
 
 // Mixed-precision flexible CG: FP32 FCG with the learned (or Chebyshev-Jacobi) preconditioner
@@ -728,7 +792,7 @@ int run_fcg(mh_handle *h, bool learned, int degree, double lo, double hi, int ip
 // If a learned segment breaks down (non-finite network output), uses up inner_max_it, or the
 // FP64 residual stops improving over three replacements, Chebyshev-Jacobi replaces the
 // network for the rest of the solve (fell_back = 1).
-int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, bool learned) {
+int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     int rc = ensure_learned(h);
     if (rc) return rc;
     if (h->sys.rows_per_thread != 1) {  // the preconditioner kernels work on tiles of 256 rows
@@ -739,10 +803,23 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, bool learn
     if ((rc = spectrum_bound(h, hi))) return rc;
     const double lo = hi / 30.0;
     const int degree = std::max(1, std::min(o.cheb_degree, 16));
+    if (kind == Pc::Amg) {
+        // the hierarchy is rebuilt from the current matrix on every solve
+        h->amg_epoch += 1;
+        cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
+        h->n_launch += h->amg.levels() * 12;
+        if (e != cudaSuccess) {
+            h->err = "AMG setup: " + h->amg.err;
+            cudaGetLastError();
+            kind = Pc::Cheb;  // the polynomial preconditioner needs no setup
+            res.fell_back = 1;
+        }
+    }
     std::vector<double> sums;
     std::vector<mh::InstCtl> ctl;
     int total = 0, stall = 0;
     double best = 1e300;
+    const bool learned = kind == Pc::Nn;
     bool use_nn = learned, restart = false;
     for (int outer = 0; outer < 1000; ++outer) {
         if ((rc = true_residual(h, sums))) return rc;
@@ -784,7 +861,8 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, bool learn
         else
             CK(mh::launch_ir_continue(h->sys, o.inner_rtol * o.inner_rtol, seg_max, h->stream));
         restart = false;
-        if ((rc = run_fcg(h, use_nn, degree, lo, hi, o.iters_per_graph, seg_max))) return rc;
+        const Pc cur = learned ? (use_nn ? Pc::Nn : Pc::Cheb) : kind;
+        if ((rc = run_fcg(h, cur, degree, lo, hi, o.iters_per_graph, seg_max))) return rc;
         CK(mh::launch_ir_correct(h->sys, h->stream));
         h->n_launch += 2;
         if ((rc = read_ctl(h, ctl))) return rc;
@@ -974,8 +1052,9 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     switch (o.method) {
         case MH_SOLVER_PCG64: rc = solve_pcg64(h, o, res); break;
         case MH_SOLVER_IR32: rc = solve_ir32(h, o, res); break;
-        case MH_SOLVER_CHEB: rc = solve_fcg(h, o, res, false); break;
-        case MH_SOLVER_FCG_LEARNED: rc = solve_fcg(h, o, res, true); break;
+        case MH_SOLVER_CHEB: rc = solve_fcg(h, o, res, Pc::Cheb); break;
+        case MH_SOLVER_FCG_LEARNED: rc = solve_fcg(h, o, res, Pc::Nn); break;
+        case MH_SOLVER_AMG: rc = solve_fcg(h, o, res, Pc::Amg); break;
         default:
             h->err = "solver method not available";
             return MH_ERR_INVALID;
@@ -1212,6 +1291,8 @@ void mh_destroy(mh_handle *h) {
             if (g) cudaGraphExecDestroy(g);
     for (auto &evs : h->prof_ev)
         for (auto e : evs) cudaEventDestroy(e);
+    if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
+    h->amg.release();
     for (void *p : h->allocs) cudaFree(p);
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -1650,6 +1731,63 @@ int mh_learned_apply(mh_handle *h, const double *r, double *z) {
     CK(cudaMemcpyAsync(zv.data(), h->pair_e, nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (int64_t k = 0; k < ne; ++k) z[k] = zv[h->hs.edge_row[k]];
+    return MH_OK;
+}
+
+int mh_amg_info(const mh_handle *hc, int32_t *n_levels, int64_t *rows, int64_t *slots, int32_t cap) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const mh::Amg &a = h->amg;
+    if (n_levels) *n_levels = a.levels();
+    for (int l = 0; l < a.levels() && l < cap; ++l) {
+        const int64_t real = l == 0 ? a.level(0).A.n : a.level(l - 1).nc;
+        if (rows) rows[l] = real;
+        if (slots) slots[l] = a.level(l).A.slots;
+    }
+    return MH_OK;
+}
+
+int mh_amg_level(const mh_handle *hc, int32_t level, int64_t *n, int64_t *nnz, int32_t *agg, float *weight,
+                 int32_t *row_ptr, int32_t *col, float *val) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const mh::Amg &a = h->amg;
+    if (level < 0 || level >= a.levels()) return MH_ERR_INVALID;
+    const mh::AmgLevel &L = a.level(level);
+    const int64_t real = level == 0 ? L.A.n : a.level(level - 1).nc;
+    std::vector<int64_t> off(L.A.n_slices + 1);
+    std::vector<int32_t> c(L.A.slots);
+    std::vector<float> v(L.A.slots);
+    CK(cudaMemcpyAsync(off.data(), L.A.slice_off, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(c.data(), L.A.col, c.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(v.data(), L.A.val, v.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (agg && level + 1 < a.levels())
+        CK(cudaMemcpyAsync(agg, L.agg.p, real * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (weight) {
+        if (level == 0 && a.fine_weights())
+            CK(cudaMemcpyAsync(weight, a.fine_weights(), real * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        else
+            std::fill(weight, weight + real, 1.f);
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    int64_t k = 0;
+    if (row_ptr) row_ptr[0] = 0;
+    for (int64_t i = 0; i < real; ++i) {
+        const int64_t sl = i / mh::kSliceRowsHost, ln = i % mh::kSliceRowsHost;
+        const int64_t w = (off[sl + 1] - off[sl]) / mh::kSliceRowsHost;
+        for (int64_t j = 0; j < w; ++j) {
+            const int64_t slot = off[sl] + j * mh::kSliceRowsHost + ln;
+            if (v[slot] == 0.f) continue;
+            if (col) col[k] = c[slot];
+            if (val) val[k] = v[slot];
+            ++k;
+        }
+        if (row_ptr) row_ptr[i + 1] = (int32_t)k;
+    }
+    if (n) *n = real;
+    if (nnz) *nnz = k;
     return MH_OK;
 }
 

@@ -31,6 +31,7 @@ MH_SOLVER_PCG64 = 0
 MH_SOLVER_IR32 = 1
 MH_SOLVER_CHEB = 2
 MH_SOLVER_FCG_LEARNED = 3
+MH_SOLVER_AMG = 4
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
@@ -140,6 +141,9 @@ def _load():
         "mh_learned_get_weights": (C.c_int, [vp, _f32p, C.c_int64]),
         "mh_learned_grad": (C.c_int, [vp, _f64p, _f64p, _f32p, _f64p]),
         "mh_learned_apply": (C.c_int, [vp, _f64p, _f64p]),
+        "mh_amg_info": (C.c_int, [vp, _i32p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]),
+        "mh_amg_level": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _i32p, _f32p, _i32p,
+                                   _i32p, _f32p]),
         "mh_learn_opts_default": (None, [C.POINTER(LearnOpts)]),
         "mh_learned_train": (C.c_int, [vp, C.POINTER(LearnOpts), C.POINTER(LearnStats)]),
     }
@@ -161,6 +165,7 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
             "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune",
             "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",
+            "mh_amg_info", "mh_amg_level",
             "mh_learned_train")
 
 MH_NN_PARAMS = 1260

@@ -226,6 +226,31 @@ class MHSystem:
         d["status"] = rc
         return d
 
+    # ---- aggregation multigrid (MH_SOLVER_AMG) ----
+    def amg_info(self):
+        """Levels of the last AMG solve: real rows and SELL slots per level."""
+        cap = 32
+        nl = np.zeros(1, np.int32)
+        rows = np.zeros(cap, np.int64)
+        slots = np.zeros(cap, np.int64)
+        check(lib.mh_amg_info(self.h, ptr(nl, C.c_int32), rows.ctypes.data_as(C.POINTER(C.c_int64)),
+                              slots.ctypes.data_as(C.POINTER(C.c_int64)), cap), self.h)
+        n = int(nl[0])
+        return dict(levels=n, rows=rows[:n].tolist(), slots=slots[:n].tolist())
+
+    def amg_level(self, level):
+        """((row_ptr, col, val), agg, weight) of level `level` of the last AMG hierarchy."""
+        n, nnz = C.c_int64(0), C.c_int64(0)
+        check(lib.mh_amg_level(self.h, int(level), C.byref(n), C.byref(nnz), None, None, None, None, None), self.h)
+        rp = np.zeros(n.value + 1, np.int32)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value, np.float32)
+        agg = np.full(n.value, -1, np.int32)
+        wt = np.ones(n.value, np.float32)
+        check(lib.mh_amg_level(self.h, int(level), C.byref(n), C.byref(nnz), ptr(agg, C.c_int32), ptr(wt, C.c_float),
+                               ptr(rp, C.c_int32), ptr(col, C.c_int32), ptr(val, C.c_float)), self.h)
+        return (rp, col, val), agg, wt
+
     # ---- learned preconditioner (MH_SOLVER_FCG_LEARNED) ----
     def learned_weights(self):
         w = np.zeros(_lib.MH_NN_PARAMS, np.float32)
