@@ -52,8 +52,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", type=int, default=2, choices=sorted(WORKLOADS))
-    ap.add_argument("--methods", default="pcg64,ir32",
-                    help="comma list of pcg64, ir32, cheb (Chebyshev-Jacobi FCG), fcg (learned FCG)")
+    ap.add_argument("--methods", default="pcg64,ir32,amg",
+                    help="comma list of pcg64, ir32, amg (multigrid FCG), cheb (Chebyshev-Jacobi FCG), "
+                         "fcg (learned FCG)")
+    ap.add_argument("--amg-inner-rtol", type=float, default=1e-3,
+                    help="FP32 residual reduction between FP64 replacements in the AMG solve")
     ap.add_argument("--train-n", type=int, default=24, help="cube size of the system the network trains on")
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -127,25 +130,41 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- roofline -----------------
+AMG_DEGREE = 2  # Chebyshev smoothing degree of the AMG cycle (library default)
+
+
 def algorithmic_bytes(kernel, N, Z):
     """Bytes each launch must move at minimum (every array once; no padding, no re-reads).
-    spmv:   values + column indices of the Z nonzeros, p (gathered, counted once), r read, q written.
-    update: x, r, p read and written, q read."""
+    spmv:    values + column indices of the Z nonzeros, p (gathered, counted once), r read, q written.
+    update:  x, r, p read and written, q read.
+    smooth0: AMG Chebyshev step on the fine level (FP32, unit diagonal): values + indices, x
+             gathered, b read, x and d written, d read by all but the first post-smoothing step
+             (mean over the 2d-1 steps of one cycle)."""
+    if kernel == "smooth0":
+        steps = 2 * AMG_DEGREE - 1
+        return Z * 8 + 16 * N + 4 * N * (steps - 1) / steps
     s = 8 if kernel.endswith("64") else 4
     if kernel.startswith("spmv"):
         return Z * (s + 4) + 3 * s * N
     return 7 * s * N
 
 
+KERNEL_NAMES = {"spmv64": "k_cg_spmv<double>", "update64": "k_cg_update<double>", "spmv32": "k_cg_spmv<float>",
+                "update32": "k_cg_update<float>", "smooth0": "k_sm_step (AMG fine level)"}
+
+
 def roofline(stats_list, N, Z, peaks):
-    names = ["spmv64", "update64", "spmv32", "update32"]
-    tot = [0.0] * 4
-    cnt = [0] * 4
+    """Roofline of the timed kernel class with the largest total device time (classes 0-4 of
+    mh_solve_stats; class 5 is a whole V-cycle, reported beside it)."""
+    names = ["spmv64", "update64", "spmv32", "update32", "smooth0"]
+    nk = len(names)
+    tot = [0.0] * 6
+    cnt = [0] * 6
     for st in stats_list:
-        for k in range(4):
+        for k in range(6):
             tot[k] += st["kernel_ms"][k]
             cnt[k] += st["kernel_count"][k]
-    k = max(range(4), key=lambda i: tot[i])
+    k = max(range(nk), key=lambda i: tot[i])
     if cnt[k] == 0:
         return None
     per_launch_s = tot[k] / cnt[k] / 1e3
@@ -159,11 +178,15 @@ def roofline(stats_list, N, Z, peaks):
     tj = load_json(os.path.join(ROOT, "profiles", "traffic.json"))
     if tj and names[k] in tj.get("bytes_per_unit", {}):
         traffic = tj["bytes_per_unit"][names[k]] * (N if tj.get("unit") == "row" else 1)
-    share = {names[i]: round(tot[i] / max(sum(tot), 1e-30), 4) for i in range(4) if cnt[i]}
-    return {"bound": "hbm", "kernel": "k_cg_" + names[k][:-2] + "<" + ("double" if names[k].endswith("64") else "float") + ">",
-            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "peak_source": peak_note, "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_),
-            "avg_launch_us": round(per_launch_s * 1e6, 3), "launches": cnt[k], "time_share": share}
+    share = {names[i]: round(tot[i] / max(sum(tot[:nk]), 1e-30), 4) for i in range(nk) if cnt[i]}
+    out = {"bound": "hbm", "kernel": KERNEL_NAMES[names[k]],
+           "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+           "peak_source": peak_note, "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_),
+           "avg_launch_us": round(per_launch_s * 1e6, 3), "launches": cnt[k], "time_share": share}
+    if cnt[5]:
+        out["vcycle_avg_us"] = round(tot[5] / cnt[5] * 1e3, 2)
+        out["smooth0_share_of_vcycle"] = round(tot[4] / tot[5], 4) if tot[5] > 0 else None
+    return out
 
 
 # ---------------------------------------------------------------- ours ------------------
@@ -217,7 +240,8 @@ def run_ours(a, rank, world):
         return float(t.item())
 
     methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32, "cheb": mhdarcy.MH_SOLVER_CHEB,
-               "fcg": mhdarcy.MH_SOLVER_FCG_LEARNED}
+               "fcg": mhdarcy.MH_SOLVER_FCG_LEARNED, "amg": mhdarcy.MH_SOLVER_AMG}
+    solve_kw = {"amg": {"inner_rtol": a.amg_inner_rtol}}
     results = {}
     training = None
     if "fcg" in a.methods.split(","):
@@ -236,7 +260,7 @@ def run_ours(a, rank, world):
         m = methods[name]
         for _ in range(a.warmup):
             system.assemble()
-            st = system.solve(method=m, r_tol=1e-10)
+            st = system.solve(method=m, r_tol=1e-10, **solve_kw.get(name, {}))
         barrier()
         if clocks and not results:
             clocks.start()
@@ -247,7 +271,7 @@ def run_ours(a, rank, world):
             ev0.record(stream)
         for _ in range(a.steps):
             system.assemble()
-            stats.append(system.solve(method=m, r_tol=1e-10))
+            stats.append(system.solve(method=m, r_tol=1e-10, **solve_kw.get(name, {})))
         with torch.cuda.stream(stream):
             ev1.record(stream)
         barrier()
@@ -259,13 +283,14 @@ def run_ours(a, rank, world):
         prof = []
         for _ in range(a.steps):
             system.assemble()
-            prof.append(system.solve(method=m, r_tol=1e-10, profile_kernels=True))
+            prof.append(system.solve(method=m, r_tol=1e-10, profile_kernels=True, **solve_kw.get(name, {})))
         barrier()
         results[name] = {"ms_per_solve": ms / a.steps, "solves_per_s": world * per_step * a.steps / (ms / 1e3),
                          "iterations": stats[-1]["iterations"], "outer": stats[-1]["outer_iterations"],
                          "rel_residual": stats[-1]["rel_residual"],
                          "rel_residual_unscaled": stats[-1]["rel_residual_unscaled"], "converged": ok,
                          "ms_assembly": stats[-1]["ms_assembly"], "ms_backsub": stats[-1]["ms_backsub"],
+                         "ms_precond_setup": stats[-1]["ms_setup"],
                          "stats": prof, "launches": launches,
                          "ms_per_solve_profiled": statistics.mean(p["ms_solve"] + p["ms_backsub"] for p in prof),
                          "fell_back": stats[-1]["fell_back"]}
@@ -288,7 +313,7 @@ def run_ours(a, rank, world):
         system.set_coeffs(**hc)
         system.set_bc(hbt, hbp)
         system.assemble()
-        system.solve(method=methods[best], r_tol=1e-10)
+        system.solve(method=methods[best], r_tol=1e-10, **solve_kw.get(best, {}))
         _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
     barrier()
     with torch.cuda.stream(stream):
@@ -297,7 +322,7 @@ def run_ours(a, rank, world):
         system.set_coeffs(**hc)
         system.set_bc(hbt, hbp)
         system.assemble()
-        system.solve(method=methods[best], r_tol=1e-10)
+        system.solve(method=methods[best], r_tol=1e-10, **solve_kw.get(best, {}))
         _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
     with torch.cuda.stream(stream):
         ev1.record(stream)
@@ -308,7 +333,7 @@ def run_ours(a, rank, world):
     d2h = 8 * sz.mh_size
     peaks = load_json(os.path.join(ROOT, "MEASURED_PEAKS.json"))
     # Krylov kernels timed in-graph (PCG64 / IR32); the flexible-CG graphs carry no events
-    timed = [r for r in results if any(st["kernel_count"][k] for st in results[r]["stats"] for k in range(4))]
+    timed = [r for r in results if any(st["kernel_count"][k] for st in results[r]["stats"] for k in range(5))]
     rstats = rb["stats"] if best in timed else (results[max(timed, key=lambda r: results[r]["solves_per_s"])]["stats"]
                                                  if timed else [])
     roof = roofline(rstats, N, Z, peaks) if rstats else None

@@ -127,7 +127,8 @@ typedef struct mh_solve_opts {
     double  inner_rtol;     /* MH_SOLVER_IR32: FP32 residual reduction between two FP64
                                residual replacements (reliable updates), default 0.1 */
     int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000) */
-    int32_t iters_per_graph;/* CG iterations per captured CUDA graph launch (16)     */
+    int32_t iters_per_graph;/* Krylov iterations per captured CUDA graph launch; 0:
+                               16, or 4 for MH_SOLVER_AMG (long iterations)           */
     int32_t profile_kernels;/* 1: time every Krylov kernel with CUDA events in-graph */
     int32_t reserved[6];
 } mh_solve_opts;
@@ -137,6 +138,9 @@ typedef struct mh_solve_opts {
 #define MH_KERNEL_UPDATE64 1
 #define MH_KERNEL_SPMV32   2
 #define MH_KERNEL_UPDATE32 3
+#define MH_KERNEL_SMOOTH0  4   /* MH_SOLVER_AMG: a Chebyshev smoothing step on the fine level */
+#define MH_KERNEL_VCYCLE   5   /* MH_SOLVER_AMG: one whole V-cycle (all its kernels)          */
+#define MH_KERNEL_CLASSES  6
 
 typedef struct mh_solve_stats {
     int32_t status;
@@ -150,9 +154,11 @@ typedef struct mh_solve_stats {
     double  ms_backsub;         /* device time of back-substitution                   */
     double  rel_residual_unscaled; /* final |b - S x| / |b|                           */
     int64_t kernel_launches;    /* kernels launched by this call (graph nodes too)    */
-    double  kernel_ms[4];       /* with profile_kernels: summed device time of the    */
-    int32_t kernel_count[4];    /*   launches that did work, per MH_KERNEL_* class    */
-    double  reserved[4];
+    double  kernel_ms[MH_KERNEL_CLASSES];    /* with profile_kernels: summed device time */
+    int32_t kernel_count[MH_KERNEL_CLASSES]; /* of the launches that did work, per class */
+    double  ms_setup;           /* device time of the preconditioner setup (AMG), part
+                                   of ms_solve                                         */
+    double  reserved[3];
 } mh_solve_stats;
 
 /* ---- library ---------------------------------------------------------------------- */

@@ -37,7 +37,7 @@ namespace {
 constexpr int kS = kSliceRows;  // SELL slice height
 constexpr int32_t kUnmatched = -2, kSingle = -1, kExcluded = -3;
 constexpr int kGalWarps = 4;    // warps per block of the Galerkin row kernel
-constexpr int kGalCap = 1024;   // candidate entries per coarse row (gathered from its rows)
+constexpr int kGalCapSmall = 256, kGalCapLarge = 1024;  // candidate entries per coarse row
 constexpr unsigned kFull = 0xffffffffu;
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -50,6 +50,14 @@ struct MatView {
     const float *val;
 };
 MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val}; }
+
+// Cycle kernels return at once when every instance of the Krylov run has finished: the
+// captured iteration graph then costs only launches.
+struct Gate {
+    const int32_t *n_done;
+    int32_t n_inst;
+};
+__device__ __forceinline__ bool closed(const Gate &g) { return g.n_done && *g.n_done >= g.n_inst; }
 
 __device__ __forceinline__ void row_of(const MatView &A, int64_t i, int64_t &base, int &w, int &ln) {
     const int64_t sl = i / kS;
@@ -143,13 +151,18 @@ __global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned in
 }
 
 // ---- pairwise aggregation ------------------------------------------------------------------
-// A row takes part if it is a real row (row_edge >= 0 on the fine level) with at least one
-// non-zero off-diagonal entry; the rest (padding, decoupled Dirichlet edges) are excluded.
+// On the fine level a row takes part if it is a real row (row_edge >= 0) with at least one
+// non-zero off-diagonal entry; the rest (padding, decoupled Dirichlet edges) are excluded and
+// only smoothed.  On coarse matrices every row with a diagonal takes part.
 __global__ void k_pair_init(MatView A, const int32_t *row_edge, const float *isd, int32_t *mate) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
+    if (!row_edge) {  // coarse matrices: every row with a diagonal takes part (isolated ones alone)
+        mate[i] = isd[i] > 0.f ? kUnmatched : kExcluded;
+        return;
+    }
     bool coupled = false;
-    if ((!row_edge || row_edge[i] >= 0) && isd[i] > 0.f) {
+    if (row_edge[i] >= 0 && isd[i] > 0.f) {
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
@@ -256,7 +269,7 @@ __global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr
 // shared memory), and sums equal columns in sorted order (FP64 sums: deterministic).
 // Pass 1 (WRITE = false) stores the row lengths; pass 2 writes the SELL slots, padding with
 // (own row, 0).
-template <bool WRITE>
+template <bool WRITE, int kGalCap>
 __global__ void __launch_bounds__(kGalWarps * 32)
     k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
                const int32_t *__restrict__ mrows, int64_t nc, int32_t *__restrict__ rowlen,
@@ -388,56 +401,58 @@ __global__ void k_fill_pad_rows(int64_t n, int64_t nc, const int64_t *off, int32
     }
 }
 
-// ---- dense coarsest level ------------------------------------------------------------------
-// [A | I] (n x 2n, FP64, row-major) from the first n rows of a SELL matrix
-__global__ void k_dense_fill(MatView A, int64_t n, double *M) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double *row = M + i * 2 * n;
-    for (int64_t c = 0; c < 2 * n; ++c) row[c] = 0.0;
-    row[n + i] = 1.0;
-    int64_t base;
-    int w, ln;
-    row_of(A, i, base, w, ln);
-    for (int j = 0; j < w; ++j) {
-        const int64_t slot = base + (int64_t)j * kS + ln;
-        const int32_t c = A.col[slot];
-        if (c < n) row[c] += (double)A.val[slot];
-    }
-}
+// ---- dense coarsest level ----------------------------------------------------------------
+// In-place Gauss-Jordan inversion in shared memory (FP64, no pivoting: the matrix is SPD), one
+// block of 1024 threads, n <= kDenseMax.  The first n rows of the SELL matrix are gathered
+// into shared memory, inverted, and written out as FP32.  flag = 1 on a non-positive or
+// non-finite pivot.
+constexpr int kDenseMax = 160;  // n^2 doubles + n factors fit in 227 KB of shared memory
 
-// Gauss-Jordan elimination without pivoting (the matrix is SPD), one block of 1024 threads;
-// writes the inverse in FP32.  flag = 1 on a non-positive or non-finite pivot.
-__global__ void __launch_bounds__(1024) k_gauss_jordan(double *M, int64_t n, float *inv, int32_t *flag) {
-    extern __shared__ double fac[];
+__global__ void __launch_bounds__(1024) k_dense_inverse(MatView A, int n, float *inv, int32_t *flag) {
+    extern __shared__ double sm[];
+    double *M = sm, *fac = sm + n * n;
     __shared__ double pinv;
-    const int64_t w = 2 * n;
-    for (int64_t k = 0; k < n; ++k) {
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) M[idx] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int64_t base;
+        int w, ln;
+        row_of(A, i, base, w, ln);
+        for (int j = 0; j < w; ++j) {
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            const int32_t c = A.col[slot];
+            if (c < n) M[i * n + c] += (double)A.val[slot];
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
         if (threadIdx.x == 0) {
-            const double p = M[k * w + k];
-            if (!(p > 0.0) || !isfinite(p)) *flag = 1;
-            pinv = (p > 0.0 && isfinite(p)) ? 1.0 / p : 0.0;
+            const double p = M[k * n + k];
+            const bool ok = p > 0.0 && isfinite(p);
+            if (!ok) *flag = 1;
+            pinv = ok ? 1.0 / p : 0.0;
         }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) fac[i] = M[i * n + k];
         __syncthreads();
-        for (int64_t c = threadIdx.x; c < w; c += blockDim.x) M[k * w + c] *= pinv;
+        // row k: a_kj / p, with a_kk := 1 / p
+        for (int j = threadIdx.x; j < n; j += blockDim.x) M[k * n + j] = (j == k ? 1.0 : M[k * n + j]) * pinv;
         __syncthreads();
-        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) fac[i] = i == k ? 0.0 : M[i * w + k];
-        __syncthreads();
-        for (int64_t idx = threadIdx.x; idx < n * w; idx += blockDim.x) {
-            const int64_t i = idx / w, c = idx - i * w;
-            if (i != k) M[idx] -= fac[i] * M[k * w + c];
+        // rows i != k: a_ij -= f_i a_kj, with a_ik := -f_i / p
+        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+            const int i = idx / n, j = idx - i * n;
+            if (i == k) continue;
+            const double base = j == k ? 0.0 : M[idx];
+            M[idx] = base - fac[i] * M[k * n + j];
         }
         __syncthreads();
     }
-    for (int64_t idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        const int64_t i = idx / n, c = idx - i * n;
-        inv[idx] = (float)M[i * w + n + c];
-    }
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) inv[idx] = (float)M[idx];
 }
 
 // x[i] = sum_j inv[i][j] b[j] for i < n (one warp per row); rows n..n_pad-1 get 0
-__global__ void k_dense_gemv(const float *__restrict__ inv, int64_t n, int64_t n_pad, const float *__restrict__ b,
+__global__ void k_dense_gemv(Gate gate, const float *__restrict__ inv, int64_t n, int64_t n_pad, const float *__restrict__ b,
                              float *__restrict__ x) {
+    if (closed(gate)) return;
     const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= n_pad) return;
@@ -463,37 +478,60 @@ __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const floa
 }
 
 // first Chebyshev step from x = 0: d = c2 D^-1 b, x = d
-__global__ void k_sm_first(int64_t n, const float *__restrict__ b, const float *__restrict__ invd, float c2,
+// (invd null: unit diagonal, the Jacobi-scaled fine level)
+__global__ void k_sm_first(Gate gate, int64_t n, const float *__restrict__ b, const float *__restrict__ invd, float c2,
                            float *__restrict__ x, float *__restrict__ d) {
+    if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float v = c2 * invd[i] * b[i];
+    const float v = c2 * (invd ? invd[i] : 1.f) * b[i];
     d[i] = v;
     x[i] = v;
 }
 
+// restriction fused with the first smoothing step of the coarse level:
+// b_c[I] = sum over the rows of I of w r, then x = d = c2 D_c^-1 b_c
+__global__ void k_restrict_first(Gate gate, int64_t nc, int64_t nc_pad, const int32_t *__restrict__ ms,
+                                 const int32_t *__restrict__ mr, const float *__restrict__ r,
+                                 const float *__restrict__ wt, const float *__restrict__ invd_c, float c2,
+                                 float *__restrict__ bc, float *__restrict__ x, float *__restrict__ d) {
+    if (closed(gate)) return;
+    const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc_pad) return;
+    float s = 0.f;
+    if (I < nc)
+        for (int32_t k = ms[I]; k < ms[I + 1]; ++k) s += (wt ? wt[mr[k]] : 1.f) * r[mr[k]];
+    bc[I] = s;
+    const float v = c2 * invd_c[I] * s;
+    d[I] = v;
+    x[I] = v;
+}
+
 // Chebyshev step: d = c1 d + c2 D^-1 (b - A x_in), x_out = x_in + d (c1 = 0: d is not read)
-__global__ void k_sm_step(MatView A, const float *__restrict__ b, const float *__restrict__ invd,
+__global__ void k_sm_step(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ invd,
                           const float *__restrict__ x_in, float *__restrict__ x_out, float *__restrict__ d, float c1,
                           float c2) {
+    if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     const float r = b[i] - row_dot(A, i, x_in);
-    const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * invd[i] * r;
+    const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * (invd ? invd[i] : 1.f) * r;
     d[i] = dn;
     x_out[i] = x_in[i] + dn;
 }
 
-__global__ void k_residual(MatView A, const float *__restrict__ b, const float *__restrict__ x,
+__global__ void k_residual(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ x,
                            float *__restrict__ r) {
+    if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     r[i] = b[i] - row_dot(A, i, x);
 }
 
 // b_c[I] = sum of r over the rows of coarse row I (in member order); padding rows get 0
-__global__ void k_restrict(int64_t nc, int64_t nc_pad, const int32_t *__restrict__ ms, const int32_t *__restrict__ mr,
+__global__ void k_restrict(Gate gate, int64_t nc, int64_t nc_pad, const int32_t *__restrict__ ms, const int32_t *__restrict__ mr,
                            const float *__restrict__ r, float *__restrict__ bc, const float *__restrict__ wt) {
+    if (closed(gate)) return;
     const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= nc_pad) return;
     float s = 0.f;
@@ -508,9 +546,10 @@ __global__ void k_to_float(int64_t n, const double *__restrict__ a, float *__res
 }
 
 // x += alpha P x_c (alpha from the device scalar when given, else the constant)
-__global__ void k_prolong(int64_t n, const int32_t *__restrict__ agg, const float *__restrict__ xc,
+__global__ void k_prolong(Gate gate, int64_t n, const int32_t *__restrict__ agg, const float *__restrict__ xc,
                           float *__restrict__ x, const double *__restrict__ alpha_dev, float alpha,
                           const float *__restrict__ wt) {
+    if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t a = agg[i];
@@ -520,8 +559,9 @@ __global__ void k_prolong(int64_t n, const int32_t *__restrict__ agg, const floa
 
 // Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
 // x_c.(A_c x_c) (the fine-level quantities e.r and e.Ae for e = P x_c).
-__global__ void __launch_bounds__(256) k_coarse_dots(MatView A, const float *__restrict__ x,
+__global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const float *__restrict__ x,
                                                      const float *__restrict__ b, double *__restrict__ part) {
+    if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double xb = 0.0, xax = 0.0;
     if (i < A.n) {
@@ -553,7 +593,8 @@ __global__ void __launch_bounds__(256) k_coarse_dots(MatView A, const float *__r
 }
 
 // alpha = sum(x.b) / sum(x.Ax) over the partials in block order (1 if not positive)
-__global__ void __launch_bounds__(256) k_coarse_alpha(const double *__restrict__ part, int64_t nb, double *alpha) {
+__global__ void __launch_bounds__(256) k_coarse_alpha(Gate gate, const double *__restrict__ part, int64_t nb, double *alpha) {
+    if (closed(gate)) return;
     __shared__ double sh[2][256];
     double a = 0.0, c = 0.0;
     for (int64_t k = threadIdx.x; k < nb; k += blockDim.x) {
@@ -606,16 +647,19 @@ void Amg::release() {
     lv_.clear();
     n_levels_ = 0;
     for (auto *b : {&mate_, &want_, &lead_, &cid_, &tmp_agg_, &tmp_ms_, &tmp_mr_, &cnt_, &rowlen_, &scan32_blk_,
-                    &mid_col_, &flag_})
+                    &flag_})
         b->release();
-    for (auto *b : {&width_, &scan64_, &scan64_blk_, &mid_off_}) b->release();
+    for (auto *b : {&width_, &scan64_, &scan64_blk_, &mid_off_[0], &mid_off_[1]}) b->release();
+    mid_col_[0].release();
+    mid_col_[1].release();
+    mid_val_[0].release();
+    mid_val_[1].release();
+    mid_invd_.release();
     dots_.release();
     alpha_.release();
     w0_.release();
     w0_used_ = nullptr;
-    mid_val_.release();
     isd_.release();
-    dense_.release();
     dense_inv_.release();
     bound_.release();
     if (h_flag_) cudaFreeHost(h_flag_);
@@ -716,9 +760,21 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
     AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-    const unsigned gg = (unsigned)std::min<int64_t>((nc + kGalWarps - 1) / kGalWarps, 148 * 16);
-    k_galerkin<false><<<gg ? gg : 1, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p, nullptr,
-                                                              nullptr, nullptr, flag_.p, wt);
+    const unsigned gg = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + kGalWarps - 1) / kGalWarps, 148 * 32));
+    // rows gather into a small buffer first; if any row overflows it, all rows are redone
+    // with the large one (wide rows appear only on coarse levels)
+    bool large = false;
+    k_galerkin<false, kGalCapSmall><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
+                                                                   nullptr, nullptr, nullptr, flag_.p, wt);
+    AMG_CK(cudaGetLastError());
+    AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    if (*h_flag_) {
+        large = true;
+        AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
+        k_galerkin<false, kGalCapLarge><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
+                                                                       nullptr, nullptr, nullptr, flag_.p, wt);
+    }
     k_slice_width<<<nblk(n_sl, 256), 256, 0, s>>>(n_sl, nc, rowlen_.p, width_.p);
     AMG_CK(cudaGetLastError());
     int64_t slots = 0;
@@ -726,8 +782,12 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     if (e != cudaSuccess) return e;
     AMG_CK(c_col.ensure(slots));
     AMG_CK(c_val.ensure(slots));
-    k_galerkin<true><<<gg ? gg : 1, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p, c_off.p,
-                                                             c_col.p, c_val.p, flag_.p, wt);
+    if (large)
+        k_galerkin<true, kGalCapLarge><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
+                                                                      c_off.p, c_col.p, c_val.p, flag_.p, wt);
+    else
+        k_galerkin<true, kGalCapSmall><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
+                                                                      c_off.p, c_col.p, c_val.p, flag_.p, wt);
     if (n_pad > nc) k_fill_pad_rows<<<nblk(n_pad - nc, 256), 256, 0, s>>>(n_pad, nc, c_off.p, c_col.p, c_val.p);
     AMG_CK(cudaGetLastError());
     AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -747,12 +807,12 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
 
 cudaError_t Amg::dense_coarse(const AmgMatrix &A, cudaStream_t s) {
     const int64_t n = dense_n_;
-    AMG_CK(dense_.ensure((size_t)n * 2 * n));
     AMG_CK(dense_inv_.ensure((size_t)n * n));
     AMG_CK(flag_.ensure(1));
     AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-    k_dense_fill<<<nblk(n, 128), 128, 0, s>>>(view(A), n, dense_.p);
-    k_gauss_jordan<<<1, 1024, n * sizeof(double), s>>>(dense_.p, n, dense_inv_.p, flag_.p);
+    const size_t smem = (size_t)(n * n + n) * sizeof(double);
+    AMG_CK(cudaFuncSetAttribute(k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_dense_inverse<<<1, 1024, smem, s>>>(view(A), (int)n, dense_inv_.p, flag_.p);
     AMG_CK(cudaGetLastError());
     AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     AMG_CK(cudaStreamSynchronize(s));
@@ -785,6 +845,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     cudaError_t e;
     for (int l = 0;; ++l) {
         AmgLevel &L = lv_[l];
+        AmgLevel &C = lv_[l + 1 < (int)lv_.size() ? l + 1 : l];
         if ((e = level_stats(L, l == 0, s)) != cudaSuccess) return e;
         AMG_CK(L.b.ensure(L.A.n));
         AMG_CK(L.xa.ensure(L.A.n));
@@ -795,57 +856,55 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         n_levels_ = l + 1;
         const int64_t n_real = l == 0 ? sys.n_rows : (l > 0 ? lv_[l - 1].nc : 0);
         if (n_real <= opt_.coarse_max || l + 1 >= opt_.max_levels) break;
-        // pass 1 on A_l
-        int64_t nc1 = 0;
-        if ((e = pair_pass(L.A, isd_.p, l == 0 ? sys.row_edge : nullptr, L.agg, nc1, L.mem_start, L.mem_rows, s)) !=
+        // pairing passes: pass 1 on A_l, pass p on the Galerkin matrix of pass p-1's pairs;
+        // the aggregation of the level is their composition
+        const int passes = l == 0 ? opt_.pair_passes : opt_.pair_passes_coarse;
+        AmgMatrix cur = L.A;
+        const float *curw = l == 0 ? w0 : nullptr;
+        int64_t nc = 0;
+        if ((e = pair_pass(cur, isd_.p, l == 0 ? sys.row_edge : nullptr, L.agg, nc, L.mem_start, L.mem_rows, s)) !=
             cudaSuccess)
             return e;
-        AmgLevel &C = lv_[l + 1];
-        if (opt_.pair_passes >= 2 && nc1 > opt_.coarse_max) {
-            // intermediate matrix of the pairs, then pair again and compose
+        const int32_t *cagg = L.agg.p, *cms = L.mem_start.p, *cmr = L.mem_rows.p;
+        for (int p = 1; p < passes && nc > opt_.coarse_max; ++p) {
             AmgMatrix M;
-            if ((e = galerkin(L.A, L.agg.p, nc1, L.mem_start.p, L.mem_rows.p, mid_off_, mid_col_, mid_val_, M, s,
-                              l == 0 ? w0 : nullptr)) != cudaSuccess)
-                return e;
-            // strength scaling of the intermediate matrix
-            AMG_CK(isd_.ensure(M.n));
-            AMG_CK(tmp_agg_.ensure(M.n));
-            {
-                AMG_CK(C.inv_diag.ensure(M.n));
-                AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
-                k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), C.inv_diag.p, isd_.p, bound_.p);
-                AMG_CK(cudaGetLastError());
-            }
-            DBuf<int32_t> &agg2 = tmp_agg_;
-            int64_t nc2 = 0;
-            if ((e = pair_pass(M, isd_.p, nullptr, agg2, nc2, tmp_ms_, tmp_mr_, s)) != cudaSuccess) return e;
-            // compose: agg = agg2[agg1], members in order
-            AMG_CK(cnt_.ensure(nc2 + 1));
-            AMG_CK(cid_.ensure(nc2 + 1));
-            k_compose_agg<<<nblk(L.A.n, 256), 256, 0, s>>>(L.A.n, L.agg.p, agg2.p, L.agg.p);
-            k_compose_count<<<nblk(nc2, 256), 256, 0, s>>>(nc2, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, cnt_.p);
-            AMG_CK(cudaGetLastError());
-            int64_t members = 0;
-            if ((e = scan_i32(cnt_.p, cid_.p, nc2, members, s)) != cudaSuccess) return e;
-            AMG_CK(want_.ensure(members));
-            k_compose_fill<<<nblk(nc2, 256), 256, 0, s>>>(nc2, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, L.mem_rows.p,
-                                                          cid_.p, want_.p);
-            AMG_CK(cudaGetLastError());
-            AMG_CK(L.mem_start.ensure(nc2 + 1));
-            AMG_CK(L.mem_rows.ensure(members));
-            AMG_CK(cudaMemcpyAsync(L.mem_start.p, cid_.p, (nc2 + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
-            AMG_CK(cudaMemcpyAsync(L.mem_rows.p, want_.p, members * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
-            // the final coarse matrix from the intermediate one
-            if ((e = galerkin(M, agg2.p, nc2, tmp_ms_.p, tmp_mr_.p, C.slice_off, C.col, C.val, C.A, s, nullptr)) !=
+            const int slot = p & 1;
+            if ((e = galerkin(cur, cagg, nc, cms, cmr, mid_off_[slot], mid_col_[slot], mid_val_[slot], M, s, curw)) !=
                 cudaSuccess)
                 return e;
-            L.nc = nc2;
-        } else {
-            if ((e = galerkin(L.A, L.agg.p, nc1, L.mem_start.p, L.mem_rows.p, C.slice_off, C.col, C.val, C.A, s,
-                              l == 0 ? w0 : nullptr)) != cudaSuccess)
-                return e;
-            L.nc = nc1;
+            AMG_CK(isd_.ensure(M.n));
+            AMG_CK(mid_invd_.ensure(M.n));
+            AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
+            k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, bound_.p);
+            AMG_CK(cudaGetLastError());
+            int64_t np = 0;
+            if ((e = pair_pass(M, isd_.p, nullptr, tmp_agg_, np, tmp_ms_, tmp_mr_, s)) != cudaSuccess) return e;
+            // compose: agg = agg_p[agg], members of each new aggregate in order
+            AMG_CK(cnt_.ensure(np + 1));
+            AMG_CK(cid_.ensure(np + 1));
+            k_compose_agg<<<nblk(L.A.n, 256), 256, 0, s>>>(L.A.n, L.agg.p, tmp_agg_.p, L.agg.p);
+            k_compose_count<<<nblk(np, 256), 256, 0, s>>>(np, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, cnt_.p);
+            AMG_CK(cudaGetLastError());
+            int64_t members = 0;
+            if ((e = scan_i32(cnt_.p, cid_.p, np, members, s)) != cudaSuccess) return e;
+            AMG_CK(want_.ensure(members));
+            k_compose_fill<<<nblk(np, 256), 256, 0, s>>>(np, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, L.mem_rows.p, cid_.p,
+                                                         want_.p);
+            AMG_CK(cudaGetLastError());
+            AMG_CK(L.mem_start.ensure(np + 1));
+            AMG_CK(L.mem_rows.ensure(members));
+            AMG_CK(cudaMemcpyAsync(L.mem_start.p, cid_.p, (np + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+            AMG_CK(cudaMemcpyAsync(L.mem_rows.p, want_.p, members * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+            cur = M;
+            curw = nullptr;
+            cagg = tmp_agg_.p;
+            cms = tmp_ms_.p;
+            cmr = tmp_mr_.p;
+            nc = np;
         }
+        // the coarse matrix from the last pass's pairs
+        if ((e = galerkin(cur, cagg, nc, cms, cmr, C.slice_off, C.col, C.val, C.A, s, curw)) != cudaSuccess) return e;
+        L.nc = nc;
         if (L.nc == 0) {  // nothing couples: this level is the last
             break;
         }
@@ -855,7 +914,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];
     dense_n_ = n_levels_ == 1 ? Lc.A.n : lv_[n_levels_ - 2].nc;
-    if (dense_n_ > 640) {  // Gauss-Jordan in one block is O(n^3): keep the coarsest level small
+    if (dense_n_ > kDenseMax) {  // the coarsest matrix is inverted in shared memory
         err = "coarsest level too large for the dense solve";
         return cudaErrorInvalidValue;
     }
@@ -889,10 +948,23 @@ void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<do
 
 int Amg::kernels_per_apply() const {
     const int deg = std::max(1, opt_.cheb_degree);
-    return (n_levels_ - 1) * (2 * deg + 3) + 1 + (opt_.kcycle ? 2 * std::max(0, n_levels_ - 2) : 0);
+    return (n_levels_ - 1) * (2 * deg + 3) + 1 - std::max(0, n_levels_ - 2) +
+           (opt_.kcycle ? 2 * std::min(opt_.kcycle_levels, std::max(0, n_levels_ - 2)) : 0);
 }
 
-cudaError_t Amg::apply(const float *r, float *z, cudaStream_t s) {
+cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
+                       AmgProf *prof) {
+    const Gate gate_{n_done, n_inst};
+    // inside a capture only cudaEventRecordExternal turns a record into a graph node
+    auto rec = [&](cudaEvent_t ev) {
+        if (prof && ev) cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
+    };
+    int step0 = 0;  // fine-level smoothing steps recorded so far
+    auto rec_step = [&](bool start) {
+        if (prof && step0 < (int)prof->smooth.size() / 2) rec(prof->smooth[2 * step0 + (start ? 0 : 1)]);
+        if (!start) ++step0;
+    };
+    if (prof) rec(prof->cycle[0]);
     // descend: smooth from zero, residual, restrict
     std::vector<double> c1, c2;
     const int deg = std::max(1, opt_.cheb_degree);
@@ -901,55 +973,70 @@ cudaError_t Amg::apply(const float *r, float *z, cudaStream_t s) {
     for (int l = 0; l < nl - 1; ++l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
+        const float *invd = l == 0 ? nullptr : L.inv_diag.p;  // the scaled fine level has unit diagonal
         const MatView A = view(L.A);
         const unsigned g = nblk(L.A.n, 256);
         cheb_coeffs(L, c1, c2);
         float *xi = L.xa.p, *xo = L.xb.p;
-        k_sm_first<<<g, 256, 0, s>>>(L.A.n, b, L.inv_diag.p, (float)c2[0], xi, L.d.p);
+        if (l == 0) k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p);
+        // (coarser levels: the first step was fused into the restriction from the level above)
         for (int k = 1; k < deg; ++k) {
-            k_sm_step<<<g, 256, 0, s>>>(A, b, L.inv_diag.p, xi, xo, L.d.p, (float)c1[k], (float)c2[k]);
+            if (l == 0) rec_step(true);
+            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k]);
+            if (l == 0) rec_step(false);
             std::swap(xi, xo);
         }
         xout[l] = xi;
-        k_residual<<<g, 256, 0, s>>>(A, b, xi, L.r.p);
+        k_residual<<<g, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
         AmgLevel &C = lv_[l + 1];
-        k_restrict<<<nblk(C.A.n, 256), 256, 0, s>>>(L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, C.b.p,
-                                                    l == 0 ? w0_used_ : nullptr);
+        const float *wt = l == 0 ? w0_used_ : nullptr;
+        if (l + 2 < nl) {
+            std::vector<double> cc1, cc2;
+            cheb_coeffs(C, cc1, cc2);
+            k_restrict_first<<<nblk(C.A.n, 256), 256, 0, s>>>(gate_, L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, wt,
+                                                              C.inv_diag.p, (float)cc2[0], C.b.p, C.xa.p, C.d.p);
+        } else {
+            k_restrict<<<nblk(C.A.n, 256), 256, 0, s>>>(gate_, L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, C.b.p, wt);
+        }
     }
     // coarsest: dense inverse
     {
         AmgLevel &Lc = lv_[nl - 1];
         const float *b = nl == 1 ? r : Lc.b.p;
         float *x = nl == 1 ? z : Lc.xa.p;
-        k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(dense_inv_.p, dense_n_, Lc.A.n, b, x);
+        k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(gate_, dense_inv_.p, dense_n_, Lc.A.n, b, x);
         xout[nl - 1] = x;
     }
     // ascend: prolong, smooth
     for (int l = nl - 2; l >= 0; --l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
+        const float *invd = l == 0 ? nullptr : L.inv_diag.p;
         const MatView A = view(L.A);
         const unsigned g = nblk(L.A.n, 256);
         cheb_coeffs(L, c1, c2);
         float *xi = xout[l];
         const double *al = nullptr;
-        if (opt_.kcycle && l + 2 < nl) {  // the coarsest correction is exact: alpha = 1
+        if (opt_.kcycle && l < opt_.kcycle_levels && l + 2 < nl) {  // the coarsest correction is exact
             AmgLevel &C = lv_[l + 1];
             const unsigned gc = nblk(C.A.n, 256);
-            k_coarse_dots<<<gc, 256, 0, s>>>(view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l]);
-            k_coarse_alpha<<<1, 256, 0, s>>>(dots_.p + dots_off_[l], gc, alpha_.p + l);
+            k_coarse_dots<<<gc, 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l]);
+            k_coarse_alpha<<<1, 256, 0, s>>>(gate_, dots_.p + dots_off_[l], gc, alpha_.p + l);
             al = alpha_.p + l;
         }
-        k_prolong<<<g, 256, 0, s>>>(L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
+        k_prolong<<<g, 256, 0, s>>>(gate_, L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
         float *other = xi == L.xa.p ? L.xb.p : L.xa.p;
         for (int k = 0; k < deg; ++k) {
             float *xo = (l == 0 && k == deg - 1) ? z : other;
-            k_sm_step<<<g, 256, 0, s>>>(A, b, L.inv_diag.p, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k]);
+            if (l == 0) rec_step(true);
+            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k]);
+            if (l == 0) rec_step(false);
             other = xi;
             xi = xo;
         }
         xout[l] = xi;
     }
+    if (prof) rec(prof->cycle[1]);
     return cudaGetLastError();
 }
 

@@ -3,18 +3,19 @@
 // with PETSc ILU (src/la/solve.cc:370); it is the preconditioner of the MH_SOLVER_AMG solve.
 //
 // Setup (every solve, from the current matrix values):
-//   level l -> l+1 by double pairwise aggregation: two rounds of handshake matching on the
+//   level l -> l+1 by repeated pairwise aggregation: passes of handshake matching on the
 //   strongest negative coupling -a_ij / sqrt(a_ii a_jj), each followed by the Galerkin product
 //   A_c = P^T A P with the piecewise-constant P of the pairs; rows without off-diagonal
 //   coupling (Dirichlet edges, padding) stay on the fine level only.  The fine level is the
 //   Jacobi-scaled S^ = D^-1/2 S D^-1/2, whose near-null vector is D^1/2 1, so its transfers
-//   carry the weights sqrt(diag S): P_0 = W P, and A_1 = P^T S P in the unscaled space.  Coarse matrices are
-//   stored as SELL-32 like the fine one; their rows are built by one warp each (gather,
+//   carry the weights sqrt(diag S): P_0 = W P, and A_1 = P^T S P in the unscaled space.
+//   Coarse matrices are stored as SELL-32 like the fine one; their rows are built by one warp each (gather,
 //   bitonic sort by column, deterministic segmented sum).  The coarsest level (<= coarse_max
-//   rows) is inverted densely in FP64 (Gauss-Jordan, one block).
+//   rows) is inverted densely in FP64 (in-place Gauss-Jordan in shared memory, one block).
 // Apply (one V-cycle, FP32): Chebyshev smoothing of degree d on [hi/ratio, hi] of D^-1 A
 // before and after the coarse correction (symmetric, so the cycle is an SPD operator).
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -27,12 +28,14 @@ namespace mh {
 
 struct AmgOptions {
     int max_levels = 20;
-    int coarse_max = 256;   // dense coarsest solve at or below this many rows
+    int coarse_max = 160;   // dense coarsest solve at or below this many rows (<= 160)
     int pair_rounds = 4;    // handshake rounds per pairing pass
-    int pair_passes = 2;    // pairing passes per level (2: aggregates of up to 4 rows)
+    int pair_passes = 2;    // pairing passes from the fine level (2: aggregates of up to 4 rows)
+    int pair_passes_coarse = 3;  // ... from the coarser levels (aggregates of up to 8)
     int cheb_degree = 2;    // smoothing steps before and after the coarse correction
     float cheb_ratio = 4.f; // smoothing interval [hi / ratio, hi]
     int kcycle = 1;         // 1: scale each coarse correction by its energy-optimal factor
+    int kcycle_levels = 64; // ... on the corrections of the first kcycle_levels levels
     float alpha = 1.f;      // fixed scaling of the coarse corrections when kcycle = 0
     int weighted = 1;       // level-0 transfers weighted by sqrt(diag S) (near-null vector)
 };
@@ -64,13 +67,26 @@ struct AmgLevel {
     float hi = 2.f;                            // Gershgorin bound of D^-1 A
 };
 
+// Events recorded inside a captured V-cycle (as external event nodes) to time it: the whole
+// cycle, and each Chebyshev smoothing step of the fine level (start/end pairs).
+struct AmgProf {
+    cudaEvent_t cycle[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> smooth;
+};
+
 class Amg {
 public:
     ~Amg() { release(); }
     // Builds the hierarchy from the FP32 scaled matrix (sys.val32) and sys.row_edge.
     cudaError_t setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s);
     // z = M r over all rows of the solver space (one V-cycle); stream-ordered, capturable.
-    cudaError_t apply(const float *r, float *z, cudaStream_t s);
+    // The kernels do nothing once *n_done >= n_inst (n_done may be null).
+    // With prof, events are recorded around the cycle and its fine-level smoothing steps.
+    cudaError_t apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
+                      AmgProf *prof = nullptr);
+    // smoothing steps on the fine level per cycle (none when the fine level is the coarsest)
+    int fine_steps() const { return n_levels_ > 1 ? 2 * std::max(1, opt_.cheb_degree) - 1 : 0; }
+    int cheb_degree() const { return std::max(1, opt_.cheb_degree); }
     void release();
     int levels() const { return n_levels_; }
     const AmgLevel &level(int l) const { return lv_[l]; }
@@ -99,11 +115,11 @@ private:
     DBuf<int64_t> width_, scan64_;
     DBuf<int32_t> rowlen_, scan32_blk_;
     DBuf<int64_t> scan64_blk_;
-    DBuf<int64_t> mid_off_;
-    DBuf<int32_t> mid_col_;
-    DBuf<float> mid_val_;
+    DBuf<int64_t> mid_off_[2];      // intermediate matrices of the pairing passes
+    DBuf<int32_t> mid_col_[2];
+    DBuf<float> mid_val_[2];
+    DBuf<float> mid_invd_;
     DBuf<float> isd_;
-    DBuf<double> dense_;
     DBuf<float> dense_inv_;
     DBuf<int32_t> flag_;
     DBuf<unsigned int> bound_;

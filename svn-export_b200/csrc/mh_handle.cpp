@@ -31,9 +31,10 @@ struct FcgKey {  // what a captured flexible-CG graph depends on
     int kind = -1, ipg = 0, degree = 0;
     double lo = 0.0, hi = 0.0;
     int64_t amg_epoch = -1;
+    bool prof = false;
     bool operator==(const FcgKey &o) const {
         return kind == o.kind && ipg == o.ipg && degree == o.degree && lo == o.lo && hi == o.hi &&
-               amg_epoch == o.amg_epoch;
+               amg_epoch == o.amg_epoch && prof == o.prof;
     }
 };
 
@@ -61,11 +62,11 @@ struct mh_handle {
     int graph_iters[2][2] = {{0, 0}, {0, 0}};
     std::vector<cudaEvent_t> prof_ev[2];
     int32_t *h_done = nullptr;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[8] = {};
     float ms_assembly = 0.f;
     int64_t n_launch = 0;               // kernels launched so far
-    double kernel_ms[4] = {0, 0, 0, 0};
-    int32_t kernel_count[4] = {0, 0, 0, 0};
+    double kernel_ms[MH_KERNEL_CLASSES] = {};
+    int32_t kernel_count[MH_KERNEL_CLASSES] = {};
     std::vector<int32_t> inst_iters, inst_status;  // per instance, last solve
     std::vector<double> inst_rel;
     // learned preconditioner: fp32 master weights, bf16 fragments, Adam state, work buffers
@@ -80,6 +81,7 @@ struct mh_handle {
     int64_t amg_epoch = 0;              // setups so far (captured graphs refer to one)
     cudaGraphExec_t fcg_graph = nullptr;
     FcgKey fcg_key{};
+    std::vector<mh::AmgProf> amg_prof;  // timing events of the V-cycles of one FCG graph
     mh::NnTrainBuffers tr{};            // activations of a training pass
     bool tr_ready = false;
     float *pair_r = nullptr, *pair_e = nullptr;  // training pairs, [cap][n_rows] each
@@ -422,6 +424,7 @@ int capture_iterations(mh_handle *h, int prec, int ipg, bool prof) {
 // Runs captured Krylov iterations until every instance reports done.  With `prof`, the
 // kernels of the iterations that still did work are timed from the in-graph events.
 int run_krylov(mh_handle *h, int prec, int ipg, int max_it, bool prof) {
+    ipg = std::max(1, ipg);  // an empty graph would never make progress
     const int gi = prec == 64 ? 0 : 1, pi = prof ? 1 : 0;
     int rc = capture_iterations(h, prec, ipg, prof);
     if (rc) return rc;
@@ -478,6 +481,7 @@ struct SolveResult {
     int iterations = 0, outer = 0, fell_back = 0;
     double rel = 0.0;       // worst Jacobi-scaled relative true residual
     double rel_orig = 0.0;  // worst unscaled relative true residual
+    double ms_setup = 0.0;  // preconditioner setup
 };
 
 // Convergence test on the FP64 true residual of every instance: the Jacobi-scaled relative
@@ -686,7 +690,8 @@ int spectrum_bound(mh_handle *h, double &hi) {
 
 // One flexible-CG iteration: z = M(r) (network, Chebyshev polynomial or AMG V-cycle) with
 // beta = z.q_old / (p.q)_old, p = z - beta p, q = S^ p with alpha = p.r / p.q, x and r.
-cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double hi, cudaStream_t s) {
+cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double hi, cudaStream_t s,
+                          mh::AmgProf *prof = nullptr) {
     mh::DevSystem &sys = h->sys;
     cudaError_t e;
     switch (kind) {
@@ -698,7 +703,7 @@ cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double h
                                       s);
             break;
         default:
-            e = h->amg.apply(sys.r32, sys.z32, s);
+            e = h->amg.apply(sys.r32, sys.z32, sys.n_done, sys.n_inst, s, prof);
             if (e == cudaSuccess) e = mh::launch_fcg_beta(sys, sys.z32, sys.q32, s);
             break;
     }
@@ -723,14 +728,31 @@ void drop_fcg_graph(mh_handle *h) {
 
 // Runs captured FCG iterations until every instance reports done.  The graph is kept while
 // its inputs (preconditioner, launch shape, AMG hierarchy) stay the same.
-int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it) {
-    const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch};
+// With prof (AMG only), every V-cycle of the graph records timing events; the cycles of the
+// iterations that did work are added to the MH_KERNEL_VCYCLE / MH_KERNEL_SMOOTH0 classes.
+int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it, bool prof) {
+    ipg = std::max(1, ipg);  // an empty graph would never make progress
+    prof = prof && kind == Pc::Amg;
+    const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch, prof};
+    if (prof) {
+        const int steps = h->amg.fine_steps();
+        if ((int)h->amg_prof.size() < ipg) h->amg_prof.resize(ipg);
+        for (auto &p : h->amg_prof) {
+            for (auto &e : p.cycle)
+                if (!e) CK(cudaEventCreate(&e));
+            while ((int)p.smooth.size() < 2 * steps) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                p.smooth.push_back(e);
+            }
+        }
+    }
     if (!h->fcg_graph || !(h->fcg_key == key)) {
-        drop_fcg_graph(h);
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k < ipg && e == cudaSuccess; ++k) e = fcg_iteration(h, kind, degree, lo, hi, h->own_stream);
+        for (int k = 0; k < ipg && e == cudaSuccess; ++k)
+            e = fcg_iteration(h, kind, degree, lo, hi, h->own_stream, prof ? &h->amg_prof[k] : nullptr);
         cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
         if (e != cudaSuccess || e2 != cudaSuccess) {
             if (e2 == cudaSuccess) cudaGraphDestroy(g);
@@ -738,7 +760,18 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
             cudaGetLastError();
             return MH_ERR_CUDA;
         }
-        e = cudaGraphInstantiate(&h->fcg_graph, g, 0);
+        // a new hierarchy of the same shape (the usual case when only values changed) only
+        // changes kernel parameters: update the executable graph in place
+        bool updated = false;
+        if (h->fcg_graph && h->fcg_key.kind == key.kind && h->fcg_key.ipg == key.ipg && h->fcg_key.prof == prof) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(h->fcg_graph, g, &info) == cudaSuccess;
+            if (!updated) cudaGetLastError();
+        }
+        if (!updated) {
+            drop_fcg_graph(h);
+            e = cudaGraphInstantiate(&h->fcg_graph, g, 0);
+        }
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             h->fcg_graph = nullptr;
@@ -749,6 +782,13 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
     }
     const int per_iter = fcg_kernels_per_iteration(h, kind, degree);
     int64_t launched = 0;
+    std::vector<mh::InstCtl> ctl;
+    int it_before = 0;
+    if (prof) {
+        int rc = read_ctl(h, ctl);
+        if (rc) return rc;
+        for (auto &c : ctl) it_before = std::max(it_before, c.iter);
+    }
     while (true) {
         CK(cudaMemcpyAsync(h->h_done, h->sys.n_done, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -757,6 +797,26 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
         CK(cudaGraphLaunch(h->fcg_graph, h->stream));
         launched += ipg;
         h->n_launch += (int64_t)per_iter * ipg;
+        if (prof) {
+            int rc = read_ctl(h, ctl);
+            if (rc) return rc;
+            int it_now = 0;
+            for (auto &c : ctl) it_now = std::max(it_now, c.iter);
+            const int active = std::min(ipg, it_now - it_before);
+            it_before = it_now;
+            for (int k = 0; k < active; ++k) {
+                const mh::AmgProf &p = h->amg_prof[k];
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, p.cycle[0], p.cycle[1]));
+                h->kernel_ms[MH_KERNEL_VCYCLE] += ms;
+                h->kernel_count[MH_KERNEL_VCYCLE] += 1;
+                for (int q = 0; q + 1 < 2 * h->amg.fine_steps() && q + 1 < (int)p.smooth.size(); q += 2) {
+                    CK(cudaEventElapsedTime(&ms, p.smooth[q], p.smooth[q + 1]));
+                    h->kernel_ms[MH_KERNEL_SMOOTH0] += ms;
+                    h->kernel_count[MH_KERNEL_SMOOTH0] += 1;
+                }
+            }
+        }
     }
     return MH_OK;
 }
@@ -771,10 +831,12 @@ mh::AmgOptions amg_options() {
         }
     };
     env_i("MH_AMG_DEGREE", o.cheb_degree, 1, 8);
-    env_i("MH_AMG_PASSES", o.pair_passes, 1, 2);
-    env_i("MH_AMG_COARSE", o.coarse_max, 16, 640);
+    env_i("MH_AMG_PASSES", o.pair_passes, 1, 4);
+    env_i("MH_AMG_CPASSES", o.pair_passes_coarse, 1, 4);
+    env_i("MH_AMG_COARSE", o.coarse_max, 16, 160);
     env_i("MH_AMG_ROUNDS", o.pair_rounds, 1, 16);
     env_i("MH_AMG_KCYCLE", o.kcycle, 0, 1);
+    env_i("MH_AMG_KLEVELS", o.kcycle_levels, 0, 64);
     env_i("MH_AMG_WEIGHTED", o.weighted, 0, 1);
     if (const char *e = getenv("MH_AMG_RATIO")) {
         const float x = (float)atof(e);
@@ -806,7 +868,13 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     if (kind == Pc::Amg) {
         // the hierarchy is rebuilt from the current matrix on every solve
         h->amg_epoch += 1;
+        CK(cudaEventRecord(h->ev[6], h->stream));
         cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
+        CK(cudaEventRecord(h->ev[7], h->stream));
+        CK(cudaEventSynchronize(h->ev[7]));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]));
+        res.ms_setup = ms;
         h->n_launch += h->amg.levels() * 12;
         if (e != cudaSuccess) {
             h->err = "AMG setup: " + h->amg.err;
@@ -862,7 +930,7 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
             CK(mh::launch_ir_continue(h->sys, o.inner_rtol * o.inner_rtol, seg_max, h->stream));
         restart = false;
         const Pc cur = learned ? (use_nn ? Pc::Nn : Pc::Cheb) : kind;
-        if ((rc = run_fcg(h, cur, degree, lo, hi, o.iters_per_graph, seg_max))) return rc;
+        if ((rc = run_fcg(h, cur, degree, lo, hi, o.iters_per_graph, seg_max, o.profile_kernels != 0))) return rc;
         CK(mh::launch_ir_correct(h->sys, h->stream));
         h->n_launch += 2;
         if ((rc = read_ctl(h, ctl))) return rc;
@@ -935,6 +1003,7 @@ int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st)
     mh_solve_opts so;
     mh_solve_opts_default(&so);
     so.r_tol = o.solve_rtol > 0.0 ? o.solve_rtol : 1e-9;
+    so.iters_per_graph = 16;
     std::fill(h->inst_iters.begin(), h->inst_iters.end(), 0);
     std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
     CK(cudaMemsetAsync(h->sys.x, 0, nr * sizeof(double), h->stream));
@@ -1027,7 +1096,7 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     mh_solve_opts_default(&o);
     if (opts_in) o = *opts_in;
     if (o.max_it <= 0) o.max_it = 20000;
-    if (o.iters_per_graph <= 0) o.iters_per_graph = 16;
+    if (o.iters_per_graph <= 0) o.iters_per_graph = o.method == MH_SOLVER_AMG ? 4 : 16;
     if (o.inner_max_it <= 0) o.inner_max_it = 2000;
     if (!(o.inner_rtol > 0.0)) o.inner_rtol = 0.1;
     if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
@@ -1036,7 +1105,7 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     const int64_t launches0 = h->n_launch;
     std::fill(h->inst_iters.begin(), h->inst_iters.end(), 0);
     std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < MH_KERNEL_CLASSES; ++k) {
         h->kernel_ms[k] = 0.0;
         h->kernel_count[k] = 0;
     }
@@ -1078,7 +1147,7 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
         stats->rel_residual = res.rel;
         stats->rel_residual_unscaled = res.rel_orig;
         stats->kernel_launches = h->n_launch - launches0;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < MH_KERNEL_CLASSES; ++k) {
             stats->kernel_ms[k] = h->kernel_ms[k];
             stats->kernel_count[k] = h->kernel_count[k];
         }
@@ -1088,6 +1157,7 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
         cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
         stats->ms_backsub = ms;
         stats->ms_assembly = h->ms_assembly;
+        stats->ms_setup = res.ms_setup;
     }
     return res.status;
 }
@@ -1177,7 +1247,7 @@ void mh_solve_opts_default(mh_solve_opts *o) {
     o->cheb_degree = 4;
     o->inner_rtol = 0.1;
     o->inner_max_it = 2000;
-    o->iters_per_graph = 16;
+    o->iters_per_graph = 0;
 }
 
 }  // extern "C"
@@ -1292,6 +1362,11 @@ void mh_destroy(mh_handle *h) {
     for (auto &evs : h->prof_ev)
         for (auto e : evs) cudaEventDestroy(e);
     if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
+    for (auto &p : h->amg_prof) {
+        for (auto e : p.cycle)
+            if (e) cudaEventDestroy(e);
+        for (auto e : p.smooth) cudaEventDestroy(e);
+    }
     h->amg.release();
     for (void *p : h->allocs) cudaFree(p);
     for (auto &e : h->ev)

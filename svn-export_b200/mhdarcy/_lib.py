@@ -72,7 +72,8 @@ class SolveStats(C.Structure):
                 ("fell_back", C.c_int32), ("rel_residual", C.c_double), ("ms_assembly", C.c_double),
                 ("ms_solve", C.c_double), ("ms_backsub", C.c_double),
                 ("rel_residual_unscaled", C.c_double), ("kernel_launches", C.c_int64),
-                ("kernel_ms", C.c_double * 4), ("kernel_count", C.c_int32 * 4), ("reserved", C.c_double * 4)]
+                ("kernel_ms", C.c_double * 6), ("kernel_count", C.c_int32 * 6), ("ms_setup", C.c_double),
+                ("reserved", C.c_double * 3)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

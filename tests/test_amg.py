@@ -1,7 +1,7 @@
 """Aggregation multigrid preconditioner (MH_SOLVER_AMG): the hierarchy built on the GPU
 against scipy (every coarse matrix is the Galerkin product P^T A P of the level above with the
 piecewise-constant P of the exported aggregation, weighted on the finest level; aggregates
-hold 1..4 rows), and AMG-FCG solves
+hold 1..4 rows on the fine level, 1..8 below), and AMG-FCG solves
 to tolerance against the direct solve, single and batched."""
 import numpy as np
 import pytest
@@ -57,7 +57,8 @@ def test_amg_hierarchy_is_galerkin(gpu):
             Ac = sp.csr_matrix((valc.astype(np.float64), colc, rpc), shape=(nc, nc))
             assert agg.min() >= -1 and agg.max() == nc - 1
             sizes = np.bincount(agg[agg >= 0], minlength=nc)
-            assert sizes.min() >= 1 and sizes.max() <= 4, (l, sizes.min(), sizes.max())
+            # two pairing passes from the fine level, three from coarser ones
+            assert sizes.min() >= 1 and sizes.max() <= (4 if l == 0 else 8), (l, sizes.min(), sizes.max())
             keep = np.nonzero(agg >= 0)[0]
             P = sp.csr_matrix((wt[keep].astype(np.float64), (keep, agg[keep])), shape=(n, nc))
             G = (P.T @ A @ P).tocsr()
