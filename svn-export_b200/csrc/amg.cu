@@ -36,8 +36,9 @@ namespace {
 
 constexpr int kS = kSliceRows;  // SELL slice height
 constexpr int32_t kUnmatched = -2, kSingle = -1, kExcluded = -3;
-constexpr int kGalWarps = 4;    // warps per block of the Galerkin row kernel
-constexpr int kGalCapSmall = 256, kGalCapLarge = 1024;  // candidate entries per coarse row
+// Galerkin row kernel tiers: candidate entries per coarse row and warps per block (the shared
+// gather buffer is warps x entries x 8 bytes)
+constexpr int kGalCap0 = 256, kGalWarps0 = 4, kGalCap1 = 1024, kGalWarps1 = 4, kGalCap2 = 4096, kGalWarps2 = 1;
 constexpr unsigned kFull = 0xffffffffu;
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -151,18 +152,15 @@ __global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned in
 }
 
 // ---- pairwise aggregation ------------------------------------------------------------------
-// On the fine level a row takes part if it is a real row (row_edge >= 0) with at least one
-// non-zero off-diagonal entry; the rest (padding, decoupled Dirichlet edges) are excluded and
-// only smoothed.  On coarse matrices every row with a diagonal takes part.
+// A row takes part if it is a real row (row_edge >= 0 on the fine level) with at least one
+// non-zero off-diagonal entry.  The rest (padding, decoupled Dirichlet edges, and coarse rows
+// left without coupling, e.g. a whole batch instance reduced to one row) get agg = -1: they
+// leave the hierarchy and the smoother solves them exactly (x = b / a_ii).
 __global__ void k_pair_init(MatView A, const int32_t *row_edge, const float *isd, int32_t *mate) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
-    if (!row_edge) {  // coarse matrices: every row with a diagonal takes part (isolated ones alone)
-        mate[i] = isd[i] > 0.f ? kUnmatched : kExcluded;
-        return;
-    }
     bool coupled = false;
-    if (row_edge[i] >= 0 && isd[i] > 0.f) {
+    if ((!row_edge || row_edge[i] >= 0) && isd[i] > 0.f) {
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
@@ -174,8 +172,26 @@ __global__ void k_pair_init(MatView A, const int32_t *row_edge, const float *isd
     mate[i] = coupled ? kUnmatched : kExcluded;
 }
 
+// agg = -1 for rows without a non-zero off-diagonal (solved exactly by the smoother), else 0
+__global__ void k_mark_isolated(MatView A, int32_t *agg) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    bool coupled = false;
+    for (int j = 0; j < w && !coupled; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        coupled = A.col[slot] != (int32_t)i && A.val[slot] != 0.f;
+    }
+    agg[i] = coupled ? 0 : -1;
+}
+
 // Strongest negative coupling -a_ij / sqrt(a_ii a_jj) to a still unmatched row (ties: lower j).
-__global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, int32_t *want) {
+// With mix, a row may also pair along a positive coupling, weighted 1e-3 so that any negative
+// coupling is preferred (coarse Galerkin matrices, and unsteady systems, carry many positive
+// off-diagonals; pairing only along negative ones stalls the coarsening there).
+__global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, int32_t *want, int mix) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     int32_t best = -1;
@@ -189,8 +205,8 @@ __global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, in
             const int64_t slot = base + (int64_t)j * kS + ln;
             const int32_t c = A.col[slot];
             const float v = A.val[slot];
-            if (c == (int32_t)i || !(v < 0.f) || mate[c] != kUnmatched) continue;
-            const float s = -v * si * isd[c];
+            if (c == (int32_t)i || v == 0.f || (!mix && !(v < 0.f)) || mate[c] != kUnmatched) continue;
+            const float s = (v < 0.f ? -v : 1e-3f * v) * si * isd[c];
             if (s > bw || (s == bw && best >= 0 && c < best)) {
                 bw = s;
                 best = c;
@@ -269,7 +285,7 @@ __global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr
 // shared memory), and sums equal columns in sorted order (FP64 sums: deterministic).
 // Pass 1 (WRITE = false) stores the row lengths; pass 2 writes the SELL slots, padding with
 // (own row, 0).
-template <bool WRITE, int kGalCap>
+template <bool WRITE, int kGalCap, int kGalWarps>
 __global__ void __launch_bounds__(kGalWarps * 32)
     k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
                const int32_t *__restrict__ mrows, int64_t nc, int32_t *__restrict__ rowlen,
@@ -407,6 +423,8 @@ __global__ void k_fill_pad_rows(int64_t n, int64_t nc, const int64_t *off, int32
 // into shared memory, inverted, and written out as FP32.  flag = 1 on a non-positive or
 // non-finite pivot.
 constexpr int kDenseMax = 160;  // n^2 doubles + n factors fit in 227 KB of shared memory
+constexpr int kCoarseDegree = 12;     // Chebyshev degree of a smoothed (not inverted) coarsest level
+constexpr float kCoarseRatio = 50.f;  // ... on [hi / 50, hi]
 
 __global__ void __launch_bounds__(1024) k_dense_inverse(MatView A, int n, float *inv, int32_t *flag) {
     extern __shared__ double sm[];
@@ -480,11 +498,17 @@ __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const floa
 // first Chebyshev step from x = 0: d = c2 D^-1 b, x = d
 // (invd null: unit diagonal, the Jacobi-scaled fine level)
 __global__ void k_sm_first(Gate gate, int64_t n, const float *__restrict__ b, const float *__restrict__ invd, float c2,
-                           float *__restrict__ x, float *__restrict__ d) {
+                           float *__restrict__ x, float *__restrict__ d, const int32_t *__restrict__ agg) {
     if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float v = c2 * (invd ? invd[i] : 1.f) * b[i];
+    const float di = invd ? invd[i] : 1.f;
+    if (agg && agg[i] < 0) {  // a row outside the hierarchy: exact
+        d[i] = 0.f;
+        x[i] = di * b[i];
+        return;
+    }
+    const float v = c2 * di * b[i];
     d[i] = v;
     x[i] = v;
 }
@@ -494,7 +518,8 @@ __global__ void k_sm_first(Gate gate, int64_t n, const float *__restrict__ b, co
 __global__ void k_restrict_first(Gate gate, int64_t nc, int64_t nc_pad, const int32_t *__restrict__ ms,
                                  const int32_t *__restrict__ mr, const float *__restrict__ r,
                                  const float *__restrict__ wt, const float *__restrict__ invd_c, float c2,
-                                 float *__restrict__ bc, float *__restrict__ x, float *__restrict__ d) {
+                                 float *__restrict__ bc, float *__restrict__ x, float *__restrict__ d,
+                                 const int32_t *__restrict__ agg_c) {
     if (closed(gate)) return;
     const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= nc_pad) return;
@@ -502,20 +527,27 @@ __global__ void k_restrict_first(Gate gate, int64_t nc, int64_t nc_pad, const in
     if (I < nc)
         for (int32_t k = ms[I]; k < ms[I + 1]; ++k) s += (wt ? wt[mr[k]] : 1.f) * r[mr[k]];
     bc[I] = s;
-    const float v = c2 * invd_c[I] * s;
-    d[I] = v;
+    const bool exact = agg_c[I] < 0;
+    const float v = (exact ? 1.f : c2) * invd_c[I] * s;
+    d[I] = exact ? 0.f : v;
     x[I] = v;
 }
 
 // Chebyshev step: d = c1 d + c2 D^-1 (b - A x_in), x_out = x_in + d (c1 = 0: d is not read)
 __global__ void k_sm_step(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ invd,
                           const float *__restrict__ x_in, float *__restrict__ x_out, float *__restrict__ d, float c1,
-                          float c2) {
+                          float c2, const int32_t *__restrict__ agg) {
     if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
+    const float di = invd ? invd[i] : 1.f;
+    if (agg && agg[i] < 0) {  // a row outside the hierarchy: exact
+        d[i] = 0.f;
+        x_out[i] = di * b[i];
+        return;
+    }
     const float r = b[i] - row_dot(A, i, x_in);
-    const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * (invd ? invd[i] : 1.f) * r;
+    const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * r;
     d[i] = dn;
     x_out[i] = x_in[i] + dn;
 }
@@ -560,7 +592,8 @@ __global__ void k_prolong(Gate gate, int64_t n, const int32_t *__restrict__ agg,
 // Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
 // x_c.(A_c x_c) (the fine-level quantities e.r and e.Ae for e = P x_c).
 __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const float *__restrict__ x,
-                                                     const float *__restrict__ b, double *__restrict__ part) {
+                                                     const float *__restrict__ b, double *__restrict__ part,
+                                                     unsigned int *ticket, double *alpha) {
     if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double xb = 0.0, xax = 0.0;
@@ -570,6 +603,7 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
         xax = xi * (double)row_dot(A, i, x);
     }
     __shared__ double sh[2][8];
+    __shared__ bool am_last;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         xb += __shfl_xor_sync(kFull, xb, o);
@@ -589,33 +623,36 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
         }
         part[2 * blockIdx.x] = a;
         part[2 * blockIdx.x + 1] = c;
+        __threadfence();
+        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
-}
-
-// alpha = sum(x.b) / sum(x.Ax) over the partials in block order (1 if not positive)
-__global__ void __launch_bounds__(256) k_coarse_alpha(Gate gate, const double *__restrict__ part, int64_t nb, double *alpha) {
-    if (closed(gate)) return;
-    __shared__ double sh[2][256];
+    __syncthreads();
+    if (!am_last) return;
+    // the last block: alpha from the partials in block order (deterministic)
+    __threadfence();
+    __shared__ double red[2][256];
     double a = 0.0, c = 0.0;
-    for (int64_t k = threadIdx.x; k < nb; k += blockDim.x) {
-        a += part[2 * k];
-        c += part[2 * k + 1];
+    for (int64_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        a += __ldcg(part + 2 * k);
+        c += __ldcg(part + 2 * k + 1);
     }
-    sh[0][threadIdx.x] = a;
-    sh[1][threadIdx.x] = c;
+    red[0][threadIdx.x] = a;
+    red[1][threadIdx.x] = c;
     __syncthreads();
     for (int st = 128; st > 0; st >>= 1) {
         if ((int)threadIdx.x < st) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + st];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + st];
+            red[0][threadIdx.x] += red[0][threadIdx.x + st];
+            red[1][threadIdx.x] += red[1][threadIdx.x + st];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        const double num = sh[0][0], den = sh[1][0];
+        const double num = red[0][0], den = red[1][0];
         *alpha = (den > 0.0 && num > 0.0 && isfinite(num / den)) ? num / den : 1.0;
+        *ticket = 0u;
     }
 }
+
 
 }  // namespace
 
@@ -657,6 +694,7 @@ void Amg::release() {
     mid_invd_.release();
     dots_.release();
     alpha_.release();
+    tickets_.release();
     w0_.release();
     w0_used_ = nullptr;
     isd_.release();
@@ -732,7 +770,7 @@ cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *
     const unsigned g = nblk(n, 256);
     k_pair_init<<<g, 256, 0, s>>>(V, row_edge, isd, mate_.p);
     for (int r = 0; r < opt_.pair_rounds; ++r) {
-        k_pair_want<<<g, 256, 0, s>>>(V, isd, mate_.p, want_.p);
+        k_pair_want<<<g, 256, 0, s>>>(V, isd, mate_.p, want_.p, row_edge ? 0 : opt_.mix_coarse);
         k_pair_match<<<g, 256, 0, s>>>(n, want_.p, mate_.p);
     }
     k_pair_lead<<<g, 256, 0, s>>>(n, mate_.p, lead_.p);
@@ -760,20 +798,52 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
     AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-    const unsigned gg = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + kGalWarps - 1) / kGalWarps, 148 * 32));
-    // rows gather into a small buffer first; if any row overflows it, all rows are redone
-    // with the large one (wide rows appear only on coarse levels)
-    bool large = false;
-    k_galerkin<false, kGalCapSmall><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
-                                                                   nullptr, nullptr, nullptr, flag_.p, wt);
-    AMG_CK(cudaGetLastError());
-    AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    AMG_CK(cudaStreamSynchronize(s));
-    if (*h_flag_) {
-        large = true;
+    // rows gather into a small buffer first; if any row overflows it, all rows are redone with
+    // the next larger one (wide rows appear only on coarse levels)
+    const MatView V = view(A);
+    auto grid = [&](int warps) {
+        return (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + warps - 1) / warps, 148 * 32 * 4 / warps));
+    };
+    auto pass = [&](int tier, bool write) {
+        switch (tier) {
+            case 0:
+                if (write)
+                    k_galerkin<true, kGalCap0, kGalWarps0><<<grid(kGalWarps0), kGalWarps0 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
+                else
+                    k_galerkin<false, kGalCap0, kGalWarps0><<<grid(kGalWarps0), kGalWarps0 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
+                break;
+            case 1:
+                if (write)
+                    k_galerkin<true, kGalCap1, kGalWarps1><<<grid(kGalWarps1), kGalWarps1 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
+                else
+                    k_galerkin<false, kGalCap1, kGalWarps1><<<grid(kGalWarps1), kGalWarps1 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
+                break;
+            default:
+                if (write)
+                    k_galerkin<true, kGalCap2, kGalWarps2><<<grid(kGalWarps2), kGalWarps2 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
+                else
+                    k_galerkin<false, kGalCap2, kGalWarps2><<<grid(kGalWarps2), kGalWarps2 * 32, 0, s>>>(
+                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
+                break;
+        }
+    };
+    int tier = 0;
+    for (;; ++tier) {
         AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-        k_galerkin<false, kGalCapLarge><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
-                                                                       nullptr, nullptr, nullptr, flag_.p, wt);
+        pass(tier, false);
+        AMG_CK(cudaGetLastError());
+        AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        AMG_CK(cudaStreamSynchronize(s));
+        if (!*h_flag_) break;
+        if (tier == 2) {
+            err = "Galerkin row wider than the gather buffer";
+            return cudaErrorInvalidValue;
+        }
     }
     k_slice_width<<<nblk(n_sl, 256), 256, 0, s>>>(n_sl, nc, rowlen_.p, width_.p);
     AMG_CK(cudaGetLastError());
@@ -782,12 +852,7 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     if (e != cudaSuccess) return e;
     AMG_CK(c_col.ensure(slots));
     AMG_CK(c_val.ensure(slots));
-    if (large)
-        k_galerkin<true, kGalCapLarge><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
-                                                                      c_off.p, c_col.p, c_val.p, flag_.p, wt);
-    else
-        k_galerkin<true, kGalCapSmall><<<gg, kGalWarps * 32, 0, s>>>(view(A), agg, mstart, mrows, nc, rowlen_.p,
-                                                                      c_off.p, c_col.p, c_val.p, flag_.p, wt);
+    pass(tier, true);
     if (n_pad > nc) k_fill_pad_rows<<<nblk(n_pad - nc, 256), 256, 0, s>>>(n_pad, nc, c_off.p, c_col.p, c_val.p);
     AMG_CK(cudaGetLastError());
     AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -914,9 +979,12 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];
     dense_n_ = n_levels_ == 1 ? Lc.A.n : lv_[n_levels_ - 2].nc;
-    if (dense_n_ > kDenseMax) {  // the coarsest matrix is inverted in shared memory
-        err = "coarsest level too large for the dense solve";
-        return cudaErrorInvalidValue;
+    if (dense_n_ > kDenseMax) {  // too large for the shared-memory inverse: smooth it instead
+        dense_n_ = 0;
+        AmgLevel &Lm = lv_[n_levels_ - 1];
+        AMG_CK(Lm.agg.ensure(Lm.A.n));
+        k_mark_isolated<<<nblk(Lm.A.n, 256), 256, 0, s>>>(view(Lm.A), Lm.agg.p);
+        AMG_CK(cudaGetLastError());
     }
     w0_used_ = w0;
     // partial sums of the coarse-correction scaling, one slice per level
@@ -928,12 +996,15 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     }
     AMG_CK(dots_.ensure(tot + 2));
     AMG_CK(alpha_.ensure(n_levels_ + 1));
-    return dense_coarse(Lc.A, s);
+    AMG_CK(tickets_.ensure(n_levels_ + 1));
+    AMG_CK(cudaMemsetAsync(tickets_.p, 0, (n_levels_ + 1) * sizeof(unsigned int), s));
+    return dense_n_ > 0 ? dense_coarse(Lc.A, s) : cudaSuccess;
 }
 
-void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2) const {
-    const int deg = std::max(1, opt_.cheb_degree);
-    const double hi = L.hi, lo = hi / std::max(1.5f, opt_.cheb_ratio);
+void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2, int degree,
+                      float ratio) const {
+    const int deg = std::max(1, degree > 0 ? degree : opt_.cheb_degree);
+    const double hi = L.hi, lo = hi / std::max(1.5f, ratio > 0.f ? ratio : opt_.cheb_ratio);
     const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
     double rho = 1.0 / sigma;
     c1.assign(deg, 0.0);
@@ -947,14 +1018,16 @@ void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<do
 }
 
 int Amg::kernels_per_apply() const {
-    const int deg = std::max(1, opt_.cheb_degree);
-    return (n_levels_ - 1) * (2 * deg + 3) + 1 - std::max(0, n_levels_ - 2) +
-           (opt_.kcycle ? 2 * std::min(opt_.kcycle_levels, std::max(0, n_levels_ - 2)) : 0);
+    const int deg = std::max(1, opt_.cheb_degree), pre = pre_degree();
+    const int coarse = dense_n_ > 0 ? 1 : kCoarseDegree;
+    return (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) +
+           (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0);
 }
 
 cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
                        AmgProf *prof) {
     const Gate gate_{n_done, n_inst};
+    const int pre = pre_degree();
     // inside a capture only cudaEventRecordExternal turns a record into a graph node
     auto rec = [&](cudaEvent_t ev) {
         if (prof && ev) cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
@@ -978,11 +1051,11 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         const unsigned g = nblk(L.A.n, 256);
         cheb_coeffs(L, c1, c2);
         float *xi = L.xa.p, *xo = L.xb.p;
-        if (l == 0) k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p);
+        if (l == 0) k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p, L.agg.p);
         // (coarser levels: the first step was fused into the restriction from the level above)
-        for (int k = 1; k < deg; ++k) {
+        for (int k = 1; k < pre; ++k) {
             if (l == 0) rec_step(true);
-            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k]);
+            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
             if (l == 0) rec_step(false);
             std::swap(xi, xo);
         }
@@ -994,18 +1067,35 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
             std::vector<double> cc1, cc2;
             cheb_coeffs(C, cc1, cc2);
             k_restrict_first<<<nblk(C.A.n, 256), 256, 0, s>>>(gate_, L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, wt,
-                                                              C.inv_diag.p, (float)cc2[0], C.b.p, C.xa.p, C.d.p);
+                                                              C.inv_diag.p, (float)cc2[0], C.b.p, C.xa.p, C.d.p,
+                                                              C.agg.p);
         } else {
             k_restrict<<<nblk(C.A.n, 256), 256, 0, s>>>(gate_, L.nc, C.A.n, L.mem_start.p, L.mem_rows.p, L.r.p, C.b.p, wt);
         }
     }
-    // coarsest: dense inverse
+    // coarsest: dense inverse, or (when coarsening stalled above the dense limit) a Chebyshev
+    // polynomial of degree kCoarseDegree on a wide interval
     {
         AmgLevel &Lc = lv_[nl - 1];
         const float *b = nl == 1 ? r : Lc.b.p;
-        float *x = nl == 1 ? z : Lc.xa.p;
-        k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(gate_, dense_inv_.p, dense_n_, Lc.A.n, b, x);
-        xout[nl - 1] = x;
+        if (dense_n_ > 0) {
+            float *x = nl == 1 ? z : Lc.xa.p;
+            k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(gate_, dense_inv_.p, dense_n_, Lc.A.n, b, x);
+            xout[nl - 1] = x;
+        } else {
+            const unsigned g = nblk(Lc.A.n, 256);
+            cheb_coeffs(Lc, c1, c2, kCoarseDegree, kCoarseRatio);
+            float *xi = Lc.xa.p, *xo = Lc.xb.p;
+            k_sm_first<<<g, 256, 0, s>>>(gate_, Lc.A.n, b, Lc.inv_diag.p, (float)c2[0], xi, Lc.d.p, Lc.agg.p);
+            for (int k = 1; k < kCoarseDegree; ++k) {
+                float *xk = (nl == 1 && k == kCoarseDegree - 1) ? z : xo;
+                k_sm_step<<<g, 256, 0, s>>>(gate_, view(Lc.A), b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k],
+                                            (float)c2[k], Lc.agg.p);
+                xo = xi;
+                xi = xk;
+            }
+            xout[nl - 1] = xi;
+        }
     }
     // ascend: prolong, smooth
     for (int l = nl - 2; l >= 0; --l) {
@@ -1017,11 +1107,12 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         cheb_coeffs(L, c1, c2);
         float *xi = xout[l];
         const double *al = nullptr;
-        if (opt_.kcycle && l < opt_.kcycle_levels && l + 2 < nl) {  // the coarsest correction is exact
+        // (a dense coarsest correction is exact: its optimal scaling is 1)
+        if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0)) {
             AmgLevel &C = lv_[l + 1];
             const unsigned gc = nblk(C.A.n, 256);
-            k_coarse_dots<<<gc, 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l]);
-            k_coarse_alpha<<<1, 256, 0, s>>>(gate_, dots_.p + dots_off_[l], gc, alpha_.p + l);
+            k_coarse_dots<<<gc, 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l],
+                                             tickets_.p + l, alpha_.p + l);
             al = alpha_.p + l;
         }
         k_prolong<<<g, 256, 0, s>>>(gate_, L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
@@ -1029,7 +1120,8 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         for (int k = 0; k < deg; ++k) {
             float *xo = (l == 0 && k == deg - 1) ? z : other;
             if (l == 0) rec_step(true);
-            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k]);
+            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k],
+                                        L.agg.p);
             if (l == 0) rec_step(false);
             other = xi;
             xi = xo;

@@ -11,7 +11,8 @@
 //   carry the weights sqrt(diag S): P_0 = W P, and A_1 = P^T S P in the unscaled space.
 //   Coarse matrices are stored as SELL-32 like the fine one; their rows are built by one warp each (gather,
 //   bitonic sort by column, deterministic segmented sum).  The coarsest level (<= coarse_max
-//   rows) is inverted densely in FP64 (in-place Gauss-Jordan in shared memory, one block).
+//   rows) is inverted densely in FP64 (in-place Gauss-Jordan in shared memory, one block); if
+//   coarsening stalls above that size, the coarsest level gets a degree-12 Chebyshev polynomial.
 // Apply (one V-cycle, FP32): Chebyshev smoothing of degree d on [hi/ratio, hi] of D^-1 A
 // before and after the coarse correction (symmetric, so the cycle is an SPD operator).
 #pragma once
@@ -32,12 +33,14 @@ struct AmgOptions {
     int pair_rounds = 4;    // handshake rounds per pairing pass
     int pair_passes = 2;    // pairing passes from the fine level (2: aggregates of up to 4 rows)
     int pair_passes_coarse = 3;  // ... from the coarser levels (aggregates of up to 8)
-    int cheb_degree = 2;    // smoothing steps before and after the coarse correction
+    int cheb_degree = 2;    // smoothing steps after the coarse correction (and before, unless
+    int pre_degree = 0;     // pre_degree > 0 sets a different number of steps before it)
     float cheb_ratio = 4.f; // smoothing interval [hi / ratio, hi]
     int kcycle = 1;         // 1: scale each coarse correction by its energy-optimal factor
     int kcycle_levels = 64; // ... on the corrections of the first kcycle_levels levels
     float alpha = 1.f;      // fixed scaling of the coarse corrections when kcycle = 0
     int weighted = 1;       // level-0 transfers weighted by sqrt(diag S) (near-null vector)
+    int mix_coarse = 1;     // coarse levels may pair along positive couplings (weakly preferred)
 };
 
 template <class T> struct DBuf {
@@ -85,7 +88,8 @@ public:
     cudaError_t apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
                       AmgProf *prof = nullptr);
     // smoothing steps on the fine level per cycle (none when the fine level is the coarsest)
-    int fine_steps() const { return n_levels_ > 1 ? 2 * std::max(1, opt_.cheb_degree) - 1 : 0; }
+    int fine_steps() const { return n_levels_ > 1 ? pre_degree() - 1 + std::max(1, opt_.cheb_degree) : 0; }
+    int pre_degree() const { return opt_.pre_degree > 0 ? opt_.pre_degree : std::max(1, opt_.cheb_degree); }
     int cheb_degree() const { return std::max(1, opt_.cheb_degree); }
     void release();
     int levels() const { return n_levels_; }
@@ -105,7 +109,8 @@ private:
     cudaError_t dense_coarse(const AmgMatrix &A, cudaStream_t s);
     cudaError_t scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s);
     cudaError_t scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s);
-    void cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2) const;
+    void cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2, int degree = 0,
+                     float ratio = 0.f) const;
 
     AmgOptions opt_;
     std::vector<AmgLevel> lv_;
@@ -124,6 +129,7 @@ private:
     DBuf<int32_t> flag_;
     DBuf<unsigned int> bound_;
     DBuf<double> dots_, alpha_;     // coarse-correction scaling: partials, factor per level
+    DBuf<unsigned int> tickets_;    // last-block tickets of the scaling reductions, per level
     std::vector<int64_t> dots_off_;
     DBuf<float> w0_;                // sqrt(diag S) per fine row
     const float *w0_used_ = nullptr;

@@ -55,6 +55,7 @@ struct mh_handle {
     double *sol = nullptr, *sol_prev = nullptr;
     double *d_aniso = nullptr;
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
+    bool rhs_stale = false;             // boundary values changed since the last assembly
     int time_mode = 0;
     double dt = 0.0;
     // captured Krylov iterations: [precision 64/32][plain / with per-kernel timing events]
@@ -79,6 +80,10 @@ struct mh_handle {
     double *d_loss = nullptr;
     mh::Amg amg;                        // aggregation multigrid (MH_SOLVER_AMG)
     int64_t amg_epoch = 0;              // setups so far (captured graphs refer to one)
+    int64_t matrix_epoch = 0;           // matrix assemblies so far
+    int64_t amg_matrix_epoch = -1;      // the assembly the current hierarchy was built from
+    std::vector<int32_t> bc_type_host;  // boundary data that enters the matrix, as last set
+    std::vector<double> bc_sigma_host;
     cudaGraphExec_t fcg_graph = nullptr;
     FcgKey fcg_key{};
     std::vector<mh::AmgProf> amg_prof;  // timing events of the V-cycles of one FCG graph
@@ -361,7 +366,11 @@ int assemble_impl(mh_handle *h, int mode) {
         h->err = "non-finite value in the assembled system";
         return MH_ERR_NONFINITE;
     }
-    if (mode & 1) h->assembled = true;
+    if (mode & 2) h->rhs_stale = false;
+    if (mode & 1) {
+        h->assembled = true;
+        h->matrix_epoch += 1;  // the edge system's values changed (or may have)
+    }
     return MH_OK;
 }
 
@@ -831,6 +840,7 @@ mh::AmgOptions amg_options() {
         }
     };
     env_i("MH_AMG_DEGREE", o.cheb_degree, 1, 8);
+    env_i("MH_AMG_PRE", o.pre_degree, 0, 8);
     env_i("MH_AMG_PASSES", o.pair_passes, 1, 4);
     env_i("MH_AMG_CPASSES", o.pair_passes_coarse, 1, 4);
     env_i("MH_AMG_COARSE", o.coarse_max, 16, 160);
@@ -838,6 +848,7 @@ mh::AmgOptions amg_options() {
     env_i("MH_AMG_KCYCLE", o.kcycle, 0, 1);
     env_i("MH_AMG_KLEVELS", o.kcycle_levels, 0, 64);
     env_i("MH_AMG_WEIGHTED", o.weighted, 0, 1);
+    env_i("MH_AMG_MIX", o.mix_coarse, 0, 1);
     if (const char *e = getenv("MH_AMG_RATIO")) {
         const float x = (float)atof(e);
         if (x >= 1.5f && x <= 100.f) o.cheb_ratio = x;
@@ -865,9 +876,13 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     if ((rc = spectrum_bound(h, hi))) return rc;
     const double lo = hi / 30.0;
     const int degree = std::max(1, std::min(o.cheb_degree, 16));
-    if (kind == Pc::Amg) {
-        // the hierarchy is rebuilt from the current matrix on every solve
+    if (kind == Pc::Amg && h->amg_matrix_epoch == h->matrix_epoch && h->amg.levels() > 0) {
+        res.ms_setup = 0.0;  // same matrix as the hierarchy was built from (unsteady steps at
+                             // a fixed dt): the hierarchy is reused
+    } else if (kind == Pc::Amg) {
+        // the hierarchy is built from the current matrix values
         h->amg_epoch += 1;
+        h->amg_matrix_epoch = h->matrix_epoch;
         CK(cudaEventRecord(h->ev[6], h->stream));
         cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
         CK(cudaEventRecord(h->ev[7], h->stream));
@@ -879,6 +894,7 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
         if (e != cudaSuccess) {
             h->err = "AMG setup: " + h->amg.err;
             cudaGetLastError();
+            h->amg_matrix_epoch = -1;
             kind = Pc::Cheb;  // the polynomial preconditioner needs no setup
             res.fell_back = 1;
         }
@@ -1480,8 +1496,18 @@ int mh_set_bc(mh_handle *h, const mh_bc *bc) {
         (rc = fill_or_default(h, (double *)d.bc_sigma, bc->robin_sigma, n, 0.0)))
         return rc;
     CK(cudaStreamSynchronize(h->stream));
+    // boundary types and Robin coefficients enter the matrix, pressures and fluxes only the
+    // right-hand side: an unsteady step after a change of values alone reassembles the rhs
+    std::vector<int32_t> typ(n, 0);
+    std::vector<double> sig(n, 0.0);
+    if (bc->type) std::copy(bc->type, bc->type + n, typ.begin());
+    if (bc->robin_sigma) std::copy(bc->robin_sigma, bc->robin_sigma + n, sig.begin());
+    const bool matrix_same = h->bc_set && typ == h->bc_type_host && sig == h->bc_sigma_host;
+    h->bc_type_host.swap(typ);
+    h->bc_sigma_host.swap(sig);
     h->bc_set = true;
-    h->assembled = false;
+    if (!matrix_same) h->assembled = false;
+    h->rhs_stale = true;
     return MH_OK;
 }
 
@@ -1498,7 +1524,7 @@ int mh_assemble(mh_handle *h) {
 int mh_solve(mh_handle *h, const mh_solve_opts *opts, mh_solve_stats *stats) {
     int rc = need_device(h);
     if (rc) return rc;
-    if (!h->assembled) {
+    if (!h->assembled || h->rhs_stale) {
         h->err = "mh_assemble must come before mh_solve";
         return MH_ERR_STATE;
     }
@@ -1531,7 +1557,7 @@ int mh_get_schur_system(const mh_handle *hc, int32_t *row_ptr, int32_t *col, dou
     mh_handle *h = const_cast<mh_handle *>(hc);
     int rc = need_device(h);
     if (rc) return rc;
-    if (!h->assembled) return MH_ERR_STATE;
+    if (!h->assembled || h->rhs_stale) return MH_ERR_STATE;
     const HostSystem &hs = h->hs;
     std::vector<double> v(hs.n_slots), b(hs.n_rows);
     CK(cudaMemcpyAsync(v.data(), h->sys.val_raw, hs.n_slots * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -100,3 +100,44 @@ def test_amg_batch(gpu):
         ist = b.instance_stats()
         assert np.all(ist["status"] == 0) and np.all(ist["rel_residual"] <= 1e-10), ist
         check_solution(b, st, 1e-10)
+
+
+@pytest.mark.gpu
+def test_amg_unsteady_reuses_hierarchy(gpu):
+    """Implicit Euler steps at a fixed dt with time-dependent Dirichlet values: the matrix does
+    not change, so the AMG hierarchy of the first step is reused (no setup time) and every
+    step still matches FP64 PCG stepping of the same problem."""
+    mesh, coeffs = make_case(4, seed=9, n=6)
+    sols = {}
+    for method in (_lib.MH_SOLVER_AMG, _lib.MH_SOLVER_PCG64):
+        with mhdarcy.MHSystem(mesh) as s:
+            bc, left = dirichlet_x_bc(s.topology(), mesh)
+            s.set_coeffs(**coeffs)
+            s.set_bc(bc["bc_type"], bc["pressure"])
+            s.unsteady_init(0.01, init_pressure=np.zeros(s.n_elements))
+            p = bc["pressure"].copy()
+            out = []
+            for k in range(1, 6):
+                p[left] = 1.0 + 0.5 * np.sin(2 * np.pi * 0.01 * k)
+                s.set_bc(bc["bc_type"], p)
+                st = s.unsteady_step(0.01, method=method, r_tol=1e-11)
+                assert st["status"] == 0, st
+                if method == _lib.MH_SOLVER_AMG and k > 1:
+                    assert st["ms_setup"] == 0.0, st
+                out.append(s.solution())
+            sols[method] = out
+    for a, b in zip(sols[_lib.MH_SOLVER_AMG], sols[_lib.MH_SOLVER_PCG64]):
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+
+
+@pytest.mark.gpu
+def test_boundary_values_need_assembly_before_steady_solve(gpu):
+    """New boundary values change the right-hand side: a steady solve needs mh_assemble first."""
+    with assembled(4) as s:
+        bc, _ = dirichlet_x_bc(s.topology(), s.mesh)
+        s.set_bc(bc["bc_type"], 2.0 * bc["pressure"])
+        with pytest.raises(_lib.MHError) as ei:
+            s.solve(method=_lib.MH_SOLVER_AMG)
+        assert ei.value.status == _lib.MH_ERR_STATE
+        s.assemble()
+        assert s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)["status"] == 0
