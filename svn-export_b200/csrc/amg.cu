@@ -49,8 +49,15 @@ struct MatView {
     const int64_t *off;
     const int32_t *col;
     const float *val;
+    const int32_t *rlen;  // entries of each row (coarse matrices), null: the slice width
 };
-MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val}; }
+MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val, A.rlen}; }
+
+// Rows longer than this (hub aggregates: a fracture intersection or a channel that couples to
+// every aggregate along it) are skipped by the thread-per-row kernels and handled by a block
+// each (k_long_rows), so that one row does not serialise its warp.
+constexpr int kLongRow = 96;
+__device__ __forceinline__ bool is_long(const MatView &A, int64_t i) { return A.rlen && A.rlen[i] > kLongRow; }
 
 // Cycle kernels return at once when every instance of the Krylov run has finished: the
 // captured iteration graph then costs only launches.
@@ -65,6 +72,7 @@ __device__ __forceinline__ void row_of(const MatView &A, int64_t i, int64_t &bas
     ln = (int)(i - sl * kS);
     base = A.off[sl];
     w = (int)((A.off[sl + 1] - base) / kS);
+    if (A.rlen && A.rlen[i] < w) w = A.rlen[i];  // a row stops at its own last entry
 }
 
 // ---- scans (exclusive, out[n] = total) ----------------------------------------------------
@@ -546,6 +554,7 @@ __global__ void k_sm_step(Gate gate, MatView A, const float *__restrict__ b, con
         x_out[i] = di * b[i];
         return;
     }
+    if (is_long(A, i)) return;  // k_long_rows
     const float r = b[i] - row_dot(A, i, x_in);
     const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * r;
     d[i] = dn;
@@ -556,7 +565,7 @@ __global__ void k_residual(Gate gate, MatView A, const float *__restrict__ b, co
                            float *__restrict__ r) {
     if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
+    if (i >= A.n || is_long(A, i)) return;  // long rows: k_long_rows
     r[i] = b[i] - row_dot(A, i, x);
 }
 
@@ -589,15 +598,67 @@ __global__ void k_prolong(Gate gate, int64_t n, const int32_t *__restrict__ agg,
     if (a >= 0) x[i] += al * (wt ? wt[i] : 1.f) * xc[a];
 }
 
+// One block per long row (kLongRow): y = (A x)_i by a block reduction, then the epilogue of
+// the thread-per-row kernel it stands in for.  MODE 0: Chebyshev step (k_sm_step), 1: residual
+// (k_residual), 2: the row's terms x_i b_i and x_i (A x)_i of the coarse-correction scaling
+// (k_coarse_dots), written to long_part[2k], [2k+1].
+template <int MODE>
+__global__ void __launch_bounds__(256) k_long_rows(Gate gate, MatView A, const int32_t *__restrict__ rows,
+                                                   const float *__restrict__ b, const float *__restrict__ invd,
+                                                   const float *__restrict__ x_in, float *__restrict__ out,
+                                                   float *__restrict__ d, float c1, float c2,
+                                                   double *__restrict__ long_part) {
+    if (closed(gate)) return;
+    const int64_t i = rows[blockIdx.x];
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    float y = 0.f;
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        y += __ldg(A.val + slot) * x_in[__ldg(A.col + slot)];
+    }
+    __shared__ float red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(kFull, y, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = y;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    y = 0.f;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) y += red[k];
+    if (MODE == 0) {
+        const float di = invd ? invd[i] : 1.f;
+        const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * (b[i] - y);
+        d[i] = dn;
+        out[i] = x_in[i] + dn;
+    } else if (MODE == 1) {
+        out[i] = b[i] - y;
+    } else {
+        long_part[2 * blockIdx.x] = (double)x_in[i] * (double)b[i];
+        long_part[2 * blockIdx.x + 1] = (double)x_in[i] * (double)y;
+    }
+}
+
+// long-row list: flags (1 where rlen > kLongRow) for a scan, then the compacted row indices
+__global__ void k_flag_long(int64_t n, const int32_t *rlen, int32_t *flag) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = rlen[i] > kLongRow ? 1 : 0;
+}
+__global__ void k_compact_long(int64_t n, const int32_t *flag, const int32_t *pos, int32_t *rows) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && flag[i]) rows[pos[i]] = (int32_t)i;
+}
+
 // Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
 // x_c.(A_c x_c) (the fine-level quantities e.r and e.Ae for e = P x_c).
 __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const float *__restrict__ x,
                                                      const float *__restrict__ b, double *__restrict__ part,
-                                                     unsigned int *ticket, double *alpha) {
+                                                     unsigned int *ticket, double *alpha,
+                                                     const double *__restrict__ long_part, int32_t n_long) {
     if (closed(gate)) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double xb = 0.0, xax = 0.0;
-    if (i < A.n) {
+    if (i < A.n && !is_long(A, i)) {  // long rows' terms come from k_long_rows in long_part
         const double xi = (double)x[i];
         xb = xi * (double)b[i];
         xax = xi * (double)row_dot(A, i, x);
@@ -636,6 +697,10 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
         a += __ldcg(part + 2 * k);
         c += __ldcg(part + 2 * k + 1);
     }
+    for (int k = threadIdx.x; k < n_long; k += blockDim.x) {
+        a += __ldcg(long_part + 2 * k);
+        c += __ldcg(long_part + 2 * k + 1);
+    }
     red[0][threadIdx.x] = a;
     red[1][threadIdx.x] = c;
     __syncthreads();
@@ -673,6 +738,8 @@ void Amg::release() {
         L.val.release();
         L.inv_diag.release();
         L.agg.release();
+        L.rlen.release();
+        L.longrows.release();
         L.mem_start.release();
         L.mem_rows.release();
         L.b.release();
@@ -693,6 +760,11 @@ void Amg::release() {
     mid_val_[1].release();
     mid_invd_.release();
     dots_.release();
+    dots_long_.release();
+    lflag_.release();
+    lpos_.release();
+    for (auto &b : mid_rlen_) b.release();
+    for (auto &b : mid_long_) b.release();
     alpha_.release();
     tickets_.release();
     w0_.release();
@@ -791,9 +863,11 @@ cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *
 
 cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, const int32_t *mstart,
                           const int32_t *mrows, DBuf<int64_t> &c_off, DBuf<int32_t> &c_col, DBuf<float> &c_val,
-                          AmgMatrix &C, cudaStream_t s, const float *wt) {
+                          DBuf<int32_t> &c_rlen, DBuf<int32_t> &c_long, AmgMatrix &C, cudaStream_t s,
+                          const float *wt) {
     const int64_t n_pad = round_up(nc, kS), n_sl = n_pad / kS;
     AMG_CK(rowlen_.ensure(n_pad));
+    AMG_CK(cudaMemsetAsync(rowlen_.p, 0, n_pad * sizeof(int32_t), s));  // padding rows: no entries
     AMG_CK(flag_.ensure(1));
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
@@ -867,6 +941,25 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     C.slice_off = c_off.p;
     C.col = c_col.p;
     C.val = c_val.p;
+    // row lengths, and the rows too long for the thread-per-row kernels
+    AMG_CK(c_rlen.ensure(n_pad));
+    AMG_CK(cudaMemcpyAsync(c_rlen.p, rowlen_.p, n_pad * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    C.rlen = c_rlen.p;
+    AMG_CK(lflag_.ensure(n_pad));
+    AMG_CK(lpos_.ensure(n_pad + 1));
+    k_flag_long<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, c_rlen.p, lflag_.p);
+    AMG_CK(cudaGetLastError());
+    int64_t n_long = 0;
+    cudaError_t e2 = scan_i32(lflag_.p, lpos_.p, n_pad, n_long, s);
+    if (e2 != cudaSuccess) return e2;
+    C.n_long = n_long;
+    C.longrows = nullptr;
+    if (n_long > 0) {
+        AMG_CK(c_long.ensure(n_long));
+        k_compact_long<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, lflag_.p, lpos_.p, c_long.p);
+        AMG_CK(cudaGetLastError());
+        C.longrows = c_long.p;
+    }
     return cudaSuccess;
 }
 
@@ -901,6 +994,9 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     L0.A.slice_off = sys.slice_off;
     L0.A.col = sys.col;
     L0.A.val = sys.val32;
+    L0.A.rlen = nullptr;  // fine rows are short: the slice width bounds them
+    L0.A.longrows = nullptr;
+    L0.A.n_long = 0;
     // level-0 weights: the near-null vector of the scaled system S^ = D^-1/2 S D^-1/2 is
     // D^1/2 1 (constants are near-null for S), so the level-0 transfers carry sqrt(diag S)
     AMG_CK(w0_.ensure(sys.n_rows));
@@ -934,8 +1030,8 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         for (int p = 1; p < passes && nc > opt_.coarse_max; ++p) {
             AmgMatrix M;
             const int slot = p & 1;
-            if ((e = galerkin(cur, cagg, nc, cms, cmr, mid_off_[slot], mid_col_[slot], mid_val_[slot], M, s, curw)) !=
-                cudaSuccess)
+            if ((e = galerkin(cur, cagg, nc, cms, cmr, mid_off_[slot], mid_col_[slot], mid_val_[slot], mid_rlen_[slot],
+                              mid_long_[slot], M, s, curw)) != cudaSuccess)
                 return e;
             AMG_CK(isd_.ensure(M.n));
             AMG_CK(mid_invd_.ensure(M.n));
@@ -968,7 +1064,9 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             nc = np;
         }
         // the coarse matrix from the last pass's pairs
-        if ((e = galerkin(cur, cagg, nc, cms, cmr, C.slice_off, C.col, C.val, C.A, s, curw)) != cudaSuccess) return e;
+        if ((e = galerkin(cur, cagg, nc, cms, cmr, C.slice_off, C.col, C.val, C.rlen, C.longrows, C.A, s, curw)) !=
+            cudaSuccess)
+            return e;
         L.nc = nc;
         if (L.nc == 0) {  // nothing couples: this level is the last
             break;
@@ -995,6 +1093,13 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         tot += 2 * (int64_t)nblk(lv_[l + 1].A.n, 256);
     }
     AMG_CK(dots_.ensure(tot + 2));
+    dots_long_off_.assign(n_levels_, 0);
+    int64_t tl = 0;
+    for (int l = 0; l + 1 < n_levels_; ++l) {
+        dots_long_off_[l] = tl;
+        tl += 2 * std::max<int64_t>(0, lv_[l + 1].A.n_long);
+    }
+    AMG_CK(dots_long_.ensure(tl + 2));
     AMG_CK(alpha_.ensure(n_levels_ + 1));
     AMG_CK(tickets_.ensure(n_levels_ + 1));
     AMG_CK(cudaMemsetAsync(tickets_.p, 0, (n_levels_ + 1) * sizeof(unsigned int), s));
@@ -1020,7 +1125,7 @@ void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<do
 int Amg::kernels_per_apply() const {
     const int deg = std::max(1, opt_.cheb_degree), pre = pre_degree();
     const int coarse = dense_n_ > 0 ? 1 : kCoarseDegree;
-    return (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) +
+    return last_long_launches_ + (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) +
            (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0);
 }
 
@@ -1028,6 +1133,20 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
                        AmgProf *prof) {
     const Gate gate_{n_done, n_inst};
     const int pre = pre_degree();
+    int launches = 0;  // kernels of one cycle, for the launch count
+    auto long_rows = [&](const AmgMatrix &M, int mode, const float *b, const float *invd, const float *x_in,
+                         float *out, float *d, float c1, float c2, double *part) {
+        if (M.n_long <= 0) return;
+        const unsigned gl = (unsigned)M.n_long;
+        const MatView V = view(M);
+        if (mode == 0)
+            k_long_rows<0><<<gl, 256, 0, s>>>(gate_, V, M.longrows, b, invd, x_in, out, d, c1, c2, part);
+        else if (mode == 1)
+            k_long_rows<1><<<gl, 256, 0, s>>>(gate_, V, M.longrows, b, invd, x_in, out, d, c1, c2, part);
+        else
+            k_long_rows<2><<<gl, 256, 0, s>>>(gate_, V, M.longrows, b, invd, x_in, out, d, c1, c2, part);
+        ++launches;
+    };
     // inside a capture only cudaEventRecordExternal turns a record into a graph node
     auto rec = [&](cudaEvent_t ev) {
         if (prof && ev) cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
@@ -1056,11 +1175,13 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         for (int k = 1; k < pre; ++k) {
             if (l == 0) rec_step(true);
             k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
+            long_rows(L.A, 0, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             std::swap(xi, xo);
         }
         xout[l] = xi;
         k_residual<<<g, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
+        long_rows(L.A, 1, b, nullptr, xi, L.r.p, nullptr, 0.f, 0.f, nullptr);
         AmgLevel &C = lv_[l + 1];
         const float *wt = l == 0 ? w0_used_ : nullptr;
         if (l + 2 < nl) {
@@ -1091,6 +1212,7 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
                 float *xk = (nl == 1 && k == kCoarseDegree - 1) ? z : xo;
                 k_sm_step<<<g, 256, 0, s>>>(gate_, view(Lc.A), b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k],
                                             (float)c2[k], Lc.agg.p);
+                long_rows(Lc.A, 0, b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k], (float)c2[k], nullptr);
                 xo = xi;
                 xi = xk;
             }
@@ -1111,8 +1233,10 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0)) {
             AmgLevel &C = lv_[l + 1];
             const unsigned gc = nblk(C.A.n, 256);
+            double *lp = dots_long_.p + dots_long_off_[l];
+            long_rows(C.A, 2, C.b.p, nullptr, xout[l + 1], nullptr, nullptr, 0.f, 0.f, lp);
             k_coarse_dots<<<gc, 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l],
-                                             tickets_.p + l, alpha_.p + l);
+                                             tickets_.p + l, alpha_.p + l, lp, (int32_t)C.A.n_long);
             al = alpha_.p + l;
         }
         k_prolong<<<g, 256, 0, s>>>(gate_, L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
@@ -1122,6 +1246,7 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
             if (l == 0) rec_step(true);
             k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k],
                                         L.agg.p);
+            long_rows(L.A, 0, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             other = xi;
             xi = xo;
@@ -1129,6 +1254,7 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         xout[l] = xi;
     }
     if (prof) rec(prof->cycle[1]);
+    last_long_launches_ = launches;
     return cudaGetLastError();
 }
 

@@ -55,6 +55,9 @@ struct AmgMatrix {
     const int64_t *slice_off = nullptr;
     const int32_t *col = nullptr;
     const float *val = nullptr;
+    const int32_t *rlen = nullptr;      // entries per row (coarse matrices; null on the fine level)
+    const int32_t *longrows = nullptr;  // rows with more than kLongRow entries (amg.cu)
+    int64_t n_long = 0;
 };
 
 struct AmgLevel {
@@ -63,6 +66,7 @@ struct AmgLevel {
     DBuf<int32_t> col;
     DBuf<float> val;
     DBuf<float> inv_diag;
+    DBuf<int32_t> rlen, longrows;              // row lengths and long rows of coarse levels
     DBuf<int32_t> agg;                         // [n] coarse row of each row, -1: none
     DBuf<int32_t> mem_start, mem_rows;         // rows of each coarse row: [nc+1], [n]
     DBuf<float> b, xa, xb, d, r;               // cycle vectors
@@ -104,7 +108,8 @@ private:
                           DBuf<int32_t> &agg, int64_t &nc, DBuf<int32_t> &mstart, DBuf<int32_t> &mrows, cudaStream_t s);
     cudaError_t galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, const int32_t *mstart,
                          const int32_t *mrows, DBuf<int64_t> &c_off, DBuf<int32_t> &c_col, DBuf<float> &c_val,
-                         AmgMatrix &C, cudaStream_t s, const float *wt);
+                         DBuf<int32_t> &c_rlen, DBuf<int32_t> &c_long, AmgMatrix &C, cudaStream_t s,
+                         const float *wt);
     cudaError_t level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s);
     cudaError_t dense_coarse(const AmgMatrix &A, cudaStream_t s);
     cudaError_t scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s);
@@ -124,6 +129,11 @@ private:
     DBuf<int32_t> mid_col_[2];
     DBuf<float> mid_val_[2];
     DBuf<float> mid_invd_;
+    DBuf<int32_t> mid_rlen_[2], mid_long_[2];
+    DBuf<int32_t> lflag_, lpos_;    // long-row list construction
+    DBuf<double> dots_long_;        // long rows' terms of the coarse-correction scaling
+    std::vector<int64_t> dots_long_off_;
+    int last_long_launches_ = 0;
     DBuf<float> isd_;
     DBuf<float> dense_inv_;
     DBuf<int32_t> flag_;
