@@ -124,8 +124,8 @@ typedef struct mh_solve_opts {
     double  a_tol;          /* absolute tolerance on |b - S x| (default 0)           */
     int32_t use_initial_guess;  /* start from the current edge pressures             */
     int32_t cheb_degree;    /* MH_SOLVER_CHEB: polynomial degree (default 4)         */
-    double  inner_rtol;     /* MH_SOLVER_IR32: FP32 residual reduction between two FP64
-                               residual replacements (reliable updates), default 0.1 */
+    double  inner_rtol;     /* FP32 residual reduction between two FP64 residual
+                               replacements; 0: 1e-3 for MH_SOLVER_AMG, else 0.1     */
     int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000) */
     int32_t iters_per_graph;/* Krylov iterations per captured CUDA graph launch; 0:
                                16, or 4 for MH_SOLVER_AMG (long iterations)           */

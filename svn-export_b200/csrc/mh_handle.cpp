@@ -1114,7 +1114,7 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     if (o.max_it <= 0) o.max_it = 20000;
     if (o.iters_per_graph <= 0) o.iters_per_graph = o.method == MH_SOLVER_AMG ? 4 : 16;
     if (o.inner_max_it <= 0) o.inner_max_it = 2000;
-    if (!(o.inner_rtol > 0.0)) o.inner_rtol = 0.1;
+    if (!(o.inner_rtol > 0.0)) o.inner_rtol = o.method == MH_SOLVER_AMG ? 1e-3 : 0.1;
     if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
     if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
     const bool guess = o.use_initial_guess || have_guess_default;
@@ -1261,7 +1261,7 @@ void mh_solve_opts_default(mh_solve_opts *o) {
     o->a_tol = 0.0;
     o->use_initial_guess = 0;
     o->cheb_degree = 4;
-    o->inner_rtol = 0.1;
+    o->inner_rtol = 0.0;
     o->inner_max_it = 2000;
     o->iters_per_graph = 0;
 }

@@ -15,7 +15,7 @@ from ._lib import lib, check, f64, i32, ptr
 
 
 def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000,
-               use_initial_guess=False, inner_rtol=0.1, inner_max_it=2000, iters_per_graph=0,
+               use_initial_guess=False, inner_rtol=0.0, inner_max_it=2000, iters_per_graph=0,
                cheb_degree=4, profile_kernels=False):
     o = _lib.SolveOpts()
     lib.mh_solve_opts_default(C.byref(o))
