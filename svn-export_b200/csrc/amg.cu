@@ -37,8 +37,8 @@ namespace {
 constexpr int kS = kSliceRows;  // SELL slice height
 constexpr int32_t kUnmatched = -2, kSingle = -1, kExcluded = -3;
 // Galerkin row kernel tiers: candidate entries per coarse row and warps per block (the shared
-// gather buffer is warps x entries x 8 bytes)
-constexpr int kGalCap0 = 256, kGalWarps0 = 4, kGalCap1 = 1024, kGalWarps1 = 4, kGalCap2 = 4096, kGalWarps2 = 1;
+// gather buffer is warps x entries x 8 bytes; the large tier's 128 KB is dynamic)
+constexpr int kGalCap0 = 256, kGalWarps0 = 4, kGalCapBig = 16384, kGalWarpsBig = 1;
 constexpr unsigned kFull = 0xffffffffu;
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -138,7 +138,7 @@ template <typename T> __global__ void k_scan_add(T *out, const T *bsum, int64_t 
 __global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned int *bound) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     float s = 0.f;
-    if (i < A.n) {
+    if (i < A.n && !is_long(A, i)) {  // long rows: k_level_diag_long
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
@@ -157,6 +157,44 @@ __global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned in
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(kFull, s, o));
     if ((threadIdx.x & 31) == 0 && s > 0.f) atomicMax(bound, __float_as_uint(s));
+}
+
+// the same for the long rows, one block each
+__global__ void __launch_bounds__(256) k_level_diag_long(MatView A, const int32_t *__restrict__ rows, float *inv_diag,
+                                                         float *isd, unsigned int *bound) {
+    const int64_t i = rows[blockIdx.x];
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    float dg = 0.f, sum = 0.f;
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        const float v = A.val[slot];
+        if (A.col[slot] == (int32_t)i) dg += v;
+        sum += fabsf(v);
+    }
+    __shared__ float red[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dg += __shfl_xor_sync(kFull, dg, o);
+        sum += __shfl_xor_sync(kFull, sum, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = dg;
+        red[1][threadIdx.x >> 5] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    dg = 0.f;
+    sum = 0.f;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+        dg += red[0][k];
+        sum += red[1][k];
+    }
+    const bool ok = dg > 0.f;
+    inv_diag[i] = ok ? 1.f / dg : 0.f;
+    isd[i] = ok ? rsqrtf(dg) : 0.f;
+    if (ok) atomicMax(bound, __float_as_uint(sum / dg));
 }
 
 // ---- pairwise aggregation ------------------------------------------------------------------
@@ -203,7 +241,7 @@ __global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, in
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;
     int32_t best = -1;
-    if (mate[i] == kUnmatched) {
+    if (mate[i] == kUnmatched && !is_long(A, i)) {  // a hub row stays an aggregate of its own
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
@@ -293,19 +331,28 @@ __global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr
 // shared memory), and sums equal columns in sorted order (FP64 sums: deterministic).
 // Pass 1 (WRITE = false) stores the row lengths; pass 2 writes the SELL slots, padding with
 // (own row, 0).
-template <bool WRITE, int kGalCap, int kGalWarps>
+// Rows run in two tiers: every row first with the small static buffer (LIST = false); a row
+// whose candidates do not fit is marked in big[] and appended to a list, and the list then
+// runs with a large dynamic buffer (LIST = true, one warp per block).  A row too wide even for
+// that sets *overflow.
+template <bool WRITE, int kGalCap, int kGalWarps, bool LIST>
 __global__ void __launch_bounds__(kGalWarps * 32)
     k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
                const int32_t *__restrict__ mrows, int64_t nc, int32_t *__restrict__ rowlen,
                const int64_t *__restrict__ c_off, int32_t *__restrict__ c_col, float *__restrict__ c_val,
-               int32_t *overflow, const float *__restrict__ wt) {
-    __shared__ int32_t sk[kGalWarps][kGalCap];
-    __shared__ float sv[kGalWarps][kGalCap];
+               int32_t *overflow, const float *__restrict__ wt, int32_t *__restrict__ big,
+               int32_t *__restrict__ big_list, int32_t *big_count) {
+    __shared__ int32_t s_k[LIST ? 1 : kGalWarps][LIST ? 1 : kGalCap];
+    __shared__ float s_v[LIST ? 1 : kGalWarps][LIST ? 1 : kGalCap];
+    extern __shared__ unsigned char dyn_sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int32_t *K = sk[warp];
-    float *V = sv[warp];
+    int32_t *K = LIST ? reinterpret_cast<int32_t *>(dyn_sm) + (size_t)warp * kGalCap : s_k[warp];
+    float *V = LIST ? reinterpret_cast<float *>(dyn_sm) + (size_t)(kGalWarps + warp) * kGalCap : s_v[warp];
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t I = (int64_t)blockIdx.x * kGalWarps + warp; I < nc; I += (int64_t)gridDim.x * kGalWarps) {
+    const int64_t n_iter = LIST ? *big_count : nc;
+    for (int64_t it = (int64_t)blockIdx.x * kGalWarps + warp; it < n_iter; it += (int64_t)gridDim.x * kGalWarps) {
+        const int64_t I = LIST ? big_list[it] : it;
+        if (!LIST && WRITE && big[I]) continue;  // written by the list pass
         int cnt = 0;
         for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
             int64_t base;
@@ -337,7 +384,12 @@ __global__ void __launch_bounds__(kGalWarps * 32)
         }
         if (cnt > kGalCap) {
             if (lane == 0) {
-                atomicExch(overflow, 1);
+                if (LIST) {
+                    atomicExch(overflow, 1);
+                } else if (!WRITE) {
+                    big[I] = 1;
+                    big_list[atomicAdd(big_count, 1)] = (int32_t)I;
+                }
                 if (!WRITE) rowlen[I] = 0;
             }
             __syncwarp();
@@ -761,6 +813,9 @@ void Amg::release() {
     mid_invd_.release();
     dots_.release();
     dots_long_.release();
+    big_.release();
+    big_list_.release();
+    big_count_.release();
     lflag_.release();
     lpos_.release();
     for (auto &b : mid_rlen_) b.release();
@@ -817,6 +872,8 @@ cudaError_t Amg::level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s) {
     AMG_CK(bound_.ensure(1));
     AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
     k_level_diag<<<nblk(n, 256), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound_.p);
+    if (L.A.n_long > 0)
+        k_level_diag_long<<<(unsigned)L.A.n_long, 256, 0, s>>>(view(L.A), L.A.longrows, L.inv_diag.p, isd_.p, bound_.p);
     AMG_CK(cudaGetLastError());
     unsigned int bits = 0;
     AMG_CK(cudaMemcpyAsync(&bits, bound_.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
@@ -872,49 +929,37 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
     AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-    // rows gather into a small buffer first; if any row overflows it, all rows are redone with
-    // the next larger one (wide rows appear only on coarse levels)
+    // every row first with the small buffer; rows that overflow it run again as a list with
+    // the large one (wide rows appear only on coarse levels, next to hub rows)
     const MatView V = view(A);
-    auto grid = [&](int warps) {
-        return (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + warps - 1) / warps, 148 * 32 * 4 / warps));
-    };
-    auto pass = [&](int tier, bool write) {
-        switch (tier) {
-            case 0:
-                if (write)
-                    k_galerkin<true, kGalCap0, kGalWarps0><<<grid(kGalWarps0), kGalWarps0 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
-                else
-                    k_galerkin<false, kGalCap0, kGalWarps0><<<grid(kGalWarps0), kGalWarps0 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
-                break;
-            case 1:
-                if (write)
-                    k_galerkin<true, kGalCap1, kGalWarps1><<<grid(kGalWarps1), kGalWarps1 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
-                else
-                    k_galerkin<false, kGalCap1, kGalWarps1><<<grid(kGalWarps1), kGalWarps1 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
-                break;
-            default:
-                if (write)
-                    k_galerkin<true, kGalCap2, kGalWarps2><<<grid(kGalWarps2), kGalWarps2 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt);
-                else
-                    k_galerkin<false, kGalCap2, kGalWarps2><<<grid(kGalWarps2), kGalWarps2 * 32, 0, s>>>(
-                        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt);
-                break;
-        }
-    };
-    int tier = 0;
-    for (;; ++tier) {
-        AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
-        pass(tier, false);
+    AMG_CK(big_.ensure(std::max<int64_t>(nc, 1)));
+    AMG_CK(big_list_.ensure(std::max<int64_t>(nc, 1)));
+    AMG_CK(big_count_.ensure(1));
+    AMG_CK(cudaMemsetAsync(big_.p, 0, std::max<int64_t>(nc, 1) * sizeof(int32_t), s));
+    AMG_CK(cudaMemsetAsync(big_count_.p, 0, sizeof(int32_t), s));
+    const unsigned g0 =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + kGalWarps0 - 1) / kGalWarps0, 148 * 32));
+    const size_t big_smem = (size_t)kGalWarpsBig * kGalCapBig * 8;
+    AMG_CK(cudaFuncSetAttribute(k_galerkin<false, kGalCapBig, kGalWarpsBig, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
+    AMG_CK(cudaFuncSetAttribute(k_galerkin<true, kGalCapBig, kGalWarpsBig, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
+    k_galerkin<false, kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
+        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt, big_.p, big_list_.p,
+        big_count_.p);
+    AMG_CK(cudaGetLastError());
+    int32_t n_big = 0;
+    AMG_CK(cudaMemcpyAsync(&n_big, big_count_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    const unsigned gb = (unsigned)std::max<int32_t>(1, std::min<int32_t>(n_big, 148 * 4));
+    if (n_big > 0) {
+        k_galerkin<false, kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
+            V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt, big_.p, big_list_.p,
+            big_count_.p);
         AMG_CK(cudaGetLastError());
         AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         AMG_CK(cudaStreamSynchronize(s));
-        if (!*h_flag_) break;
-        if (tier == 2) {
+        if (*h_flag_) {
             err = "Galerkin row wider than the gather buffer";
             return cudaErrorInvalidValue;
         }
@@ -926,7 +971,13 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     if (e != cudaSuccess) return e;
     AMG_CK(c_col.ensure(slots));
     AMG_CK(c_val.ensure(slots));
-    pass(tier, true);
+    k_galerkin<true, kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
+        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt, big_.p, big_list_.p,
+        big_count_.p);
+    if (n_big > 0)
+        k_galerkin<true, kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
+            V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt, big_.p, big_list_.p,
+            big_count_.p);
     if (n_pad > nc) k_fill_pad_rows<<<nblk(n_pad - nc, 256), 256, 0, s>>>(n_pad, nc, c_off.p, c_col.p, c_val.p);
     AMG_CK(cudaGetLastError());
     AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1037,6 +1088,9 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             AMG_CK(mid_invd_.ensure(M.n));
             AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
             k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, bound_.p);
+            if (M.n_long > 0)
+                k_level_diag_long<<<(unsigned)M.n_long, 256, 0, s>>>(view(M), M.longrows, mid_invd_.p, isd_.p,
+                                                                     bound_.p);
             AMG_CK(cudaGetLastError());
             int64_t np = 0;
             if ((e = pair_pass(M, isd_.p, nullptr, tmp_agg_, np, tmp_ms_, tmp_mr_, s)) != cudaSuccess) return e;

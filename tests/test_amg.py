@@ -42,8 +42,11 @@ def check_solution(s, st, r_tol):
 
 
 @pytest.mark.gpu
-def test_amg_hierarchy_is_galerkin(gpu):
-    with assembled(8) as s:
+@pytest.mark.parametrize("cfg,n", [(1, 8), (5, 24)])
+def test_amg_hierarchy_is_galerkin(gpu, cfg, n):
+    """cfg5 (fracture planes, channels) grows hub rows on its coarse levels: those take the
+    long-row kernels and the large Galerkin gather buffer."""
+    with assembled(n, cfg=cfg) as s:
         st = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-8)
         assert st["status"] in CONVERGED and st["fell_back"] == 0, st
         info = s.amg_info()
@@ -59,6 +62,7 @@ def test_amg_hierarchy_is_galerkin(gpu):
             sizes = np.bincount(agg[agg >= 0], minlength=nc)
             # two pairing passes from the fine level, three from coarser ones
             assert sizes.min() >= 1 and sizes.max() <= (4 if l == 0 else 8), (l, sizes.min(), sizes.max())
+            assert np.all(np.diff(rpc) >= 0)
             keep = np.nonzero(agg >= 0)[0]
             P = sp.csr_matrix((wt[keep].astype(np.float64), (keep, agg[keep])), shape=(n, nc))
             G = (P.T @ A @ P).tocsr()
