@@ -331,17 +331,19 @@ __global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr
 // shared memory), and sums equal columns in sorted order (FP64 sums: deterministic).
 // Pass 1 (WRITE = false) stores the row lengths; pass 2 writes the SELL slots, padding with
 // (own row, 0).
-// Rows run in two tiers: every row first with the small static buffer (LIST = false); a row
-// whose candidates do not fit is marked in big[] and appended to a list, and the list then
+// Each coarse row is gathered, sorted and reduced once; its entries go to a compact buffer at
+// t_off[I] (sized by the candidate bound) and its length to rowlen[I]; k_sell_fill then lays
+// the rows out as SELL.  Rows run in two tiers: every row first with the small static buffer
+// (LIST = false); a row whose candidates do not fit is appended to a list, and the list then
 // runs with a large dynamic buffer (LIST = true, one warp per block).  A row too wide even for
 // that sets *overflow.
-template <bool WRITE, int kGalCap, int kGalWarps, bool LIST>
+template <int kGalCap, int kGalWarps, bool LIST>
 __global__ void __launch_bounds__(kGalWarps * 32)
     k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
                const int32_t *__restrict__ mrows, int64_t nc, int32_t *__restrict__ rowlen,
-               const int64_t *__restrict__ c_off, int32_t *__restrict__ c_col, float *__restrict__ c_val,
-               int32_t *overflow, const float *__restrict__ wt, int32_t *__restrict__ big,
-               int32_t *__restrict__ big_list, int32_t *big_count) {
+               const int64_t *__restrict__ t_off, int32_t *__restrict__ t_col, float *__restrict__ t_val,
+               int32_t *overflow, const float *__restrict__ wt, int32_t *__restrict__ big_list,
+               int32_t *big_count) {
     __shared__ int32_t s_k[LIST ? 1 : kGalWarps][LIST ? 1 : kGalCap];
     __shared__ float s_v[LIST ? 1 : kGalWarps][LIST ? 1 : kGalCap];
     extern __shared__ unsigned char dyn_sm[];
@@ -352,7 +354,6 @@ __global__ void __launch_bounds__(kGalWarps * 32)
     const int64_t n_iter = LIST ? *big_count : nc;
     for (int64_t it = (int64_t)blockIdx.x * kGalWarps + warp; it < n_iter; it += (int64_t)gridDim.x * kGalWarps) {
         const int64_t I = LIST ? big_list[it] : it;
-        if (!LIST && WRITE && big[I]) continue;  // written by the list pass
         int cnt = 0;
         for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
             int64_t base;
@@ -384,13 +385,9 @@ __global__ void __launch_bounds__(kGalWarps * 32)
         }
         if (cnt > kGalCap) {
             if (lane == 0) {
-                if (LIST) {
-                    atomicExch(overflow, 1);
-                } else if (!WRITE) {
-                    big[I] = 1;
-                    big_list[atomicAdd(big_count, 1)] = (int32_t)I;
-                }
-                if (!WRITE) rowlen[I] = 0;
+                if (LIST) atomicExch(overflow, 1);
+                else big_list[atomicAdd(big_count, 1)] = (int32_t)I;
+                rowlen[I] = 0;
             }
             __syncwarp();
             continue;
@@ -421,34 +418,62 @@ __global__ void __launch_bounds__(kGalWarps * 32)
                 __syncwarp();
             }
         int uniq = 0;
-        const int64_t sl = I / kS;
-        const int ln = (int)(I - sl * kS);
+        const int64_t ob = t_off[I];
         for (int t0 = 0; t0 < cnt; t0 += 32) {
             const int t = t0 + lane;
             const bool head = t < cnt && (t == 0 || K[t] != K[t - 1]);
             const unsigned hm = __ballot_sync(kFull, head);
-            if (WRITE && head) {
+            if (head) {
                 const int outk = uniq + __popc(hm & lt);
                 const int32_t key = K[t];
                 double s = 0.0;
                 for (int q = t; q < cnt && K[q] == key; ++q) s += (double)V[q];
-                const int64_t slot = c_off[sl] + (int64_t)outk * kS + ln;
-                c_col[slot] = key;
-                c_val[slot] = (float)s;
+                t_col[ob + outk] = key;
+                t_val[ob + outk] = (float)s;
             }
             uniq += __popc(hm);
         }
-        if (!WRITE) {
-            if (lane == 0) rowlen[I] = uniq;
-        } else {
-            const int wc = (int)((c_off[sl + 1] - c_off[sl]) / kS);
-            for (int k = uniq + lane; k < wc; k += 32) {
-                const int64_t slot = c_off[sl] + (int64_t)k * kS + ln;
-                c_col[slot] = (int32_t)I;
-                c_val[slot] = 0.f;
-            }
-        }
+        if (lane == 0) rowlen[I] = uniq;
         __syncwarp();
+    }
+}
+
+// Candidate bound of each coarse row: the summed lengths of its rows
+__global__ void k_cand_bound(MatView A, const int32_t *__restrict__ mstart, const int32_t *__restrict__ mrows,
+                             int64_t nc, int64_t *__restrict__ bound) {
+    const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc) return;
+    int64_t b = 0;
+    for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
+        int64_t base;
+        int w, ln;
+        row_of(A, mrows[m], base, w, ln);
+        b += w;
+    }
+    bound[I] = b;
+}
+
+// SELL layout of the compact rows: entries, then padding slots (own column, value 0)
+__global__ void k_sell_fill(int64_t n_pad, int64_t nc, const int64_t *__restrict__ c_off,
+                            const int32_t *__restrict__ rowlen, const int64_t *__restrict__ t_off,
+                            const int32_t *__restrict__ t_col, const float *__restrict__ t_val,
+                            int32_t *__restrict__ c_col, float *__restrict__ c_val) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    const int64_t sl = i / kS;
+    const int ln = (int)(i - sl * kS);
+    const int w = (int)((c_off[sl + 1] - c_off[sl]) / kS);
+    const int len = i < nc ? rowlen[i] : 0;
+    const int64_t src = i < nc ? t_off[i] : 0;
+    for (int k = 0; k < w; ++k) {
+        const int64_t slot = c_off[sl] + (int64_t)k * kS + ln;
+        if (k < len) {
+            c_col[slot] = t_col[src + k];
+            c_val[slot] = t_val[src + k];
+        } else {
+            c_col[slot] = (int32_t)i;
+            c_val[slot] = 0.f;
+        }
     }
 }
 
@@ -464,18 +489,6 @@ __global__ void k_slice_width(int64_t n_slices, int64_t nc, const int32_t *rowle
     width[s] = (int64_t)m * kS;
 }
 
-// padding rows of a coarse slice that holds no entry at all still need their slots filled
-__global__ void k_fill_pad_rows(int64_t n, int64_t nc, const int64_t *off, int32_t *col, float *val) {
-    const int64_t i = nc + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t sl = i / kS;
-    const int ln = (int)(i - sl * kS);
-    const int w = (int)((off[sl + 1] - off[sl]) / kS);
-    for (int j = 0; j < w; ++j) {
-        col[off[sl] + (int64_t)j * kS + ln] = (int32_t)i;
-        val[off[sl] + (int64_t)j * kS + ln] = 0.f;
-    }
-}
 
 // ---- dense coarsest level ----------------------------------------------------------------
 // In-place Gauss-Jordan inversion in shared memory (FP64, no pivoting: the matrix is SPD), one
@@ -813,9 +826,12 @@ void Amg::release() {
     mid_invd_.release();
     dots_.release();
     dots_long_.release();
-    big_.release();
     big_list_.release();
     big_count_.release();
+    tbound_.release();
+    toff_.release();
+    tcol_.release();
+    tval_.release();
     lflag_.release();
     lpos_.release();
     for (auto &b : mid_rlen_) b.release();
@@ -929,32 +945,37 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
     AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
+    // compact row buffer sized by the candidate bound of every coarse row
+    const MatView V = view(A);
+    AMG_CK(tbound_.ensure(nc + 1));
+    AMG_CK(toff_.ensure(nc + 1));
+    if (nc > 0) k_cand_bound<<<nblk(nc, 256), 256, 0, s>>>(V, mstart, mrows, nc, tbound_.p);
+    AMG_CK(cudaGetLastError());
+    int64_t cand = 0;
+    cudaError_t e = scan_i64(tbound_.p, toff_.p, nc, cand, s);
+    if (e != cudaSuccess) return e;
+    AMG_CK(tcol_.ensure(std::max<int64_t>(cand, 1)));
+    AMG_CK(tval_.ensure(std::max<int64_t>(cand, 1)));
     // every row first with the small buffer; rows that overflow it run again as a list with
     // the large one (wide rows appear only on coarse levels, next to hub rows)
-    const MatView V = view(A);
-    AMG_CK(big_.ensure(std::max<int64_t>(nc, 1)));
     AMG_CK(big_list_.ensure(std::max<int64_t>(nc, 1)));
     AMG_CK(big_count_.ensure(1));
-    AMG_CK(cudaMemsetAsync(big_.p, 0, std::max<int64_t>(nc, 1) * sizeof(int32_t), s));
     AMG_CK(cudaMemsetAsync(big_count_.p, 0, sizeof(int32_t), s));
     const unsigned g0 =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((nc + kGalWarps0 - 1) / kGalWarps0, 148 * 32));
     const size_t big_smem = (size_t)kGalWarpsBig * kGalCapBig * 8;
-    AMG_CK(cudaFuncSetAttribute(k_galerkin<false, kGalCapBig, kGalWarpsBig, true>,
+    AMG_CK(cudaFuncSetAttribute(k_galerkin<kGalCapBig, kGalWarpsBig, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
-    AMG_CK(cudaFuncSetAttribute(k_galerkin<true, kGalCapBig, kGalWarpsBig, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
-    k_galerkin<false, kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
-        V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt, big_.p, big_list_.p,
-        big_count_.p);
+    k_galerkin<kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
+        V, agg, mstart, mrows, nc, rowlen_.p, toff_.p, tcol_.p, tval_.p, flag_.p, wt, big_list_.p, big_count_.p);
     AMG_CK(cudaGetLastError());
     int32_t n_big = 0;
     AMG_CK(cudaMemcpyAsync(&n_big, big_count_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     AMG_CK(cudaStreamSynchronize(s));
-    const unsigned gb = (unsigned)std::max<int32_t>(1, std::min<int32_t>(n_big, 148 * 4));
     if (n_big > 0) {
-        k_galerkin<false, kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
-            V, agg, mstart, mrows, nc, rowlen_.p, nullptr, nullptr, nullptr, flag_.p, wt, big_.p, big_list_.p,
+        const unsigned gb = (unsigned)std::min<int32_t>(n_big, 148 * 4);
+        k_galerkin<kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
+            V, agg, mstart, mrows, nc, rowlen_.p, toff_.p, tcol_.p, tval_.p, flag_.p, wt, big_list_.p,
             big_count_.p);
         AMG_CK(cudaGetLastError());
         AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -967,25 +988,12 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     k_slice_width<<<nblk(n_sl, 256), 256, 0, s>>>(n_sl, nc, rowlen_.p, width_.p);
     AMG_CK(cudaGetLastError());
     int64_t slots = 0;
-    cudaError_t e = scan_i64(width_.p, c_off.p, n_sl, slots, s);
-    if (e != cudaSuccess) return e;
-    AMG_CK(c_col.ensure(slots));
-    AMG_CK(c_val.ensure(slots));
-    k_galerkin<true, kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
-        V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt, big_.p, big_list_.p,
-        big_count_.p);
-    if (n_big > 0)
-        k_galerkin<true, kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
-            V, agg, mstart, mrows, nc, rowlen_.p, c_off.p, c_col.p, c_val.p, flag_.p, wt, big_.p, big_list_.p,
-            big_count_.p);
-    if (n_pad > nc) k_fill_pad_rows<<<nblk(n_pad - nc, 256), 256, 0, s>>>(n_pad, nc, c_off.p, c_col.p, c_val.p);
+    if ((e = scan_i64(width_.p, c_off.p, n_sl, slots, s)) != cudaSuccess) return e;
+    AMG_CK(c_col.ensure(std::max<int64_t>(slots, 1)));
+    AMG_CK(c_val.ensure(std::max<int64_t>(slots, 1)));
+    k_sell_fill<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, nc, c_off.p, rowlen_.p, toff_.p, tcol_.p, tval_.p, c_col.p,
+                                                  c_val.p);
     AMG_CK(cudaGetLastError());
-    AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    AMG_CK(cudaStreamSynchronize(s));
-    if (*h_flag_) {
-        err = "Galerkin row wider than the gather buffer";
-        return cudaErrorInvalidValue;
-    }
     C.n = n_pad;
     C.n_slices = n_sl;
     C.slots = slots;

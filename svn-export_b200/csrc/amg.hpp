@@ -131,7 +131,10 @@ private:
     DBuf<float> mid_invd_;
     DBuf<int32_t> mid_rlen_[2], mid_long_[2];
     DBuf<int32_t> lflag_, lpos_;    // long-row list construction
-    DBuf<int32_t> big_, big_list_, big_count_;  // Galerkin rows that need the large gather buffer
+    DBuf<int32_t> big_list_, big_count_;  // Galerkin rows that need the large gather buffer
+    DBuf<int64_t> tbound_, toff_;         // compact Galerkin rows: candidate bounds, offsets
+    DBuf<int32_t> tcol_;
+    DBuf<float> tval_;
     DBuf<double> dots_long_;        // long rows' terms of the coarse-correction scaling
     std::vector<int64_t> dots_long_off_;
     int last_long_launches_ = 0;
