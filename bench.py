@@ -137,12 +137,14 @@ def algorithmic_bytes(kernel, N, Z):
     """Bytes each launch must move at minimum (every array once; no padding, no re-reads).
     spmv:    values + column indices of the Z nonzeros, p (gathered, counted once), r read, q written.
     update:  x, r, p read and written, q read.
-    smooth0: AMG Chebyshev step on the fine level (FP32, unit diagonal): values + indices, x
-             gathered, b read, x and d written, d read by all but the first post-smoothing step
-             (mean over the 2d-1 steps of one cycle)."""
+    smooth0: AMG Chebyshev step on the fine level (FP32, unit diagonal): values + indices, x (or
+             b) gathered, b read, x and d written; d read by the steps that continue a sequence
+             (the fused first pre-smoothing pass and the first post-smoothing step start one):
+             mean over the 2d-1 fine steps of one cycle."""
     if kernel == "smooth0":
         steps = 2 * AMG_DEGREE - 1
-        return Z * 8 + 16 * N + 4 * N * (steps - 1) / steps
+        reads_d = max(0, AMG_DEGREE - 2) + (AMG_DEGREE - 1)
+        return Z * 8 + 16 * N + 4 * N * reads_d / steps
     s = 8 if kernel.endswith("64") else 4
     if kernel.startswith("spmv"):
         return Z * (s + 4) + 3 * s * N

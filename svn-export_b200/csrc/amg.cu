@@ -556,12 +556,37 @@ __global__ void k_dense_gemv(Gate gate, const float *__restrict__ inv, int64_t n
 }
 
 // ---- V-cycle kernels ------------------------------------------------------------------------
+// (A x)_i.  On the fine level (no row lengths: 7-8 entries per row) the first 8 slots are
+// loaded together, then gathered together, so each thread keeps 8 independent loads in flight
+// instead of one dependent load chain per slot; coarse rows (longer, irregular) loop.
 __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const float *__restrict__ x) {
     int64_t base;
     int w, ln;
     row_of(A, i, base, w, ln);
+    if (A.rlen) {
+        float y = 0.f;
+        for (int j = 0; j < w; ++j) {
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            y += __ldg(A.val + slot) * x[__ldg(A.col + slot)];
+        }
+        return y;
+    }
+    constexpr int kB = 8;
+    int32_t c[kB];
+    float v[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const int64_t slot = base + (int64_t)k * kS + ln;
+        c[k] = k < w ? __ldg(A.col + slot) : 0;
+        v[k] = k < w ? __ldg(A.val + slot) : 0.f;
+    }
+    float g[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) g[k] = k < w ? x[c[k]] : 0.f;
     float y = 0.f;
-    for (int j = 0; j < w; ++j) {
+#pragma unroll
+    for (int k = 0; k < kB; ++k) y += v[k] * g[k];
+    for (int j = kB; j < w; ++j) {
         const int64_t slot = base + (int64_t)j * kS + ln;
         y += __ldg(A.val + slot) * x[__ldg(A.col + slot)];
     }
@@ -624,6 +649,26 @@ __global__ void k_sm_step(Gate gate, MatView A, const float *__restrict__ b, con
     const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * r;
     d[i] = dn;
     x_out[i] = x_in[i] + dn;
+}
+
+// The fine level's first two Chebyshev steps from x = 0 in one pass (unit diagonal):
+// x1 = c0 b (so A x1 = c0 A b), d = c1 c0 b + c2 (b - c0 A b), x_out = x1 + d
+__global__ void k_sm_first_step(Gate gate, MatView A, const float *__restrict__ b, float *__restrict__ x_out,
+                                float *__restrict__ d, float c0, float c1, float c2, const int32_t *__restrict__ agg) {
+    if (closed(gate)) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const float bi = b[i];
+    if (agg && agg[i] < 0) {  // a row outside the hierarchy: exact
+        d[i] = 0.f;
+        x_out[i] = bi;
+        return;
+    }
+    const float x1 = c0 * bi;
+    const float r = bi - c0 * row_dot(A, i, b);
+    const float dn = c1 * x1 + c2 * r;
+    d[i] = dn;
+    x_out[i] = x1 + dn;
 }
 
 __global__ void k_residual(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ x,
@@ -1187,7 +1232,8 @@ void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<do
 int Amg::kernels_per_apply() const {
     const int deg = std::max(1, opt_.cheb_degree), pre = pre_degree();
     const int coarse = dense_n_ > 0 ? 1 : kCoarseDegree;
-    return last_long_launches_ + (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) +
+    return last_long_launches_ + (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) -
+           (n_levels_ > 1 && pre >= 2 ? 1 : 0) +
            (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0);
 }
 
@@ -1232,9 +1278,19 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         const unsigned g = nblk(L.A.n, 256);
         cheb_coeffs(L, c1, c2);
         float *xi = L.xa.p, *xo = L.xb.p;
-        if (l == 0) k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p, L.agg.p);
+        int k0 = 1;
+        if (l == 0 && pre >= 2) {  // first two steps in one pass
+            rec_step(true);
+            k_sm_first_step<<<g, 256, 0, s>>>(gate_, A, b, xo, L.d.p, (float)c2[0], (float)c1[1], (float)c2[1],
+                                              L.agg.p);
+            rec_step(false);
+            std::swap(xi, xo);
+            k0 = 2;
+        } else if (l == 0) {
+            k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p, L.agg.p);
+        }
         // (coarser levels: the first step was fused into the restriction from the level above)
-        for (int k = 1; k < pre; ++k) {
+        for (int k = k0; k < pre; ++k) {
             if (l == 0) rec_step(true);
             k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
             long_rows(L.A, 0, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], nullptr);
