@@ -160,9 +160,7 @@ __global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned in
 }
 
 // the same for the long rows, one block each
-__global__ void __launch_bounds__(256) k_level_diag_long(MatView A, const int32_t *__restrict__ rows, float *inv_diag,
-                                                         float *isd, unsigned int *bound) {
-    const int64_t i = rows[blockIdx.x];
+__device__ void k_level_diag_long_row(MatView A, int64_t i, float *inv_diag, float *isd, unsigned int *bound) {
     int64_t base;
     int w, ln;
     row_of(A, i, base, w, ln);
@@ -184,17 +182,27 @@ __global__ void __launch_bounds__(256) k_level_diag_long(MatView A, const int32_
         red[1][threadIdx.x >> 5] = sum;
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    dg = 0.f;
-    sum = 0.f;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-        dg += red[0][k];
-        sum += red[1][k];
+    if (threadIdx.x == 0) {
+        dg = 0.f;
+        sum = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            dg += red[0][k];
+            sum += red[1][k];
+        }
+        const bool ok = dg > 0.f;
+        inv_diag[i] = ok ? 1.f / dg : 0.f;
+        isd[i] = ok ? rsqrtf(dg) : 0.f;
+        if (ok) atomicMax(bound, __float_as_uint(sum / dg));
     }
-    const bool ok = dg > 0.f;
-    inv_diag[i] = ok ? 1.f / dg : 0.f;
-    isd[i] = ok ? rsqrtf(dg) : 0.f;
-    if (ok) atomicMax(bound, __float_as_uint(sum / dg));
+}
+
+__global__ void __launch_bounds__(256) k_level_diag_long(MatView A, const int32_t *__restrict__ list, float *inv_diag,
+                                                         float *isd, unsigned int *bound) {
+    // list = [count, rows...]; the blocks stride over the rows
+    for (int32_t k = blockIdx.x; k < list[0]; k += gridDim.x) {
+        k_level_diag_long_row(A, list[1 + k], inv_diag, isd, bound);
+        __syncthreads();
+    }
 }
 
 // ---- pairwise aggregation ------------------------------------------------------------------
@@ -271,34 +279,34 @@ __global__ void k_pair_match(int64_t n, const int32_t *want, int32_t *mate) {
     else if (want[j] == (int32_t)i) mate[i] = j;
 }
 
-// leader of each aggregate: a single row, or the lower row of a pair
-__global__ void k_pair_lead(int64_t n, const int32_t *mate, int32_t *lead) {
+// Leader of each aggregate (a single row, or the lower row of a pair), packed for one scan:
+// low 32 bits 1 for a leader, high 32 bits the aggregate's member count.  The exclusive scan
+// then gives every leader its aggregate id (low) and member offset (high).
+__global__ void k_pair_pack(int64_t n, const int32_t *mate, int64_t *packed) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t m = mate[i];
-    lead[i] = (m == kSingle || m == kUnmatched || (m >= 0 && (int32_t)i < m)) ? 1 : 0;
+    const bool lead = m == kSingle || m == kUnmatched || (m >= 0 && (int32_t)i < m);
+    packed[i] = lead ? (int64_t)1 | ((int64_t)(m >= 0 ? 2 : 1) << 32) : 0;
 }
 
-__global__ void k_pair_assign(int64_t n, const int32_t *mate, const int32_t *lead, const int32_t *cid, int32_t *agg,
-                              int32_t *cnt) {
+// agg of every row, and the member lists (leader first, then its pair)
+__global__ void k_pair_finish(int64_t n, int64_t nc, int64_t members, const int32_t *mate, const int64_t *packed,
+                              const int64_t *pscan, int32_t *agg, int32_t *mstart, int32_t *mrows) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) mstart[nc] = (int32_t)members;
     if (i >= n) return;
     const int32_t m = mate[i];
-    if (lead[i]) {
-        agg[i] = cid[i];
-        cnt[cid[i]] = m >= 0 ? 2 : 1;
+    if (packed[i] & 1) {
+        const int64_t pre = pscan[i];
+        const int32_t cid = (int32_t)(pre & 0xffffffff), off = (int32_t)(pre >> 32);
+        agg[i] = cid;
+        mstart[cid] = off;
+        mrows[off] = (int32_t)i;
+        if (m >= 0) mrows[off + 1] = m;
     } else {
-        agg[i] = m >= 0 ? cid[m] : -1;
+        agg[i] = m >= 0 ? (int32_t)(pscan[m] & 0xffffffff) : -1;
     }
-}
-
-__global__ void k_pair_members(int64_t n, const int32_t *mate, const int32_t *lead, const int32_t *cid,
-                               const int32_t *mstart, int32_t *mrows) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !lead[i]) return;
-    const int32_t p = mstart[cid[i]];
-    mrows[p] = (int32_t)i;
-    if (mate[i] >= 0) mrows[p + 1] = mate[i];
 }
 
 // Two pairing passes composed: agg = agg2[agg1[i]], members of each final row in order.
@@ -754,9 +762,10 @@ __global__ void k_flag_long(int64_t n, const int32_t *rlen, int32_t *flag) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) flag[i] = rlen[i] > kLongRow ? 1 : 0;
 }
-__global__ void k_compact_long(int64_t n, const int32_t *flag, const int32_t *pos, int32_t *rows) {
+__global__ void k_compact_long(int64_t n, const int32_t *flag, const int32_t *pos, int32_t *list) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && flag[i]) rows[pos[i]] = (int32_t)i;
+    if (i == 0) list[0] = pos[n];
+    if (i < n && flag[i]) list[1 + pos[i]] = (int32_t)i;
 }
 
 // Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
@@ -860,8 +869,7 @@ void Amg::release() {
     }
     lv_.clear();
     n_levels_ = 0;
-    for (auto *b : {&mate_, &want_, &lead_, &cid_, &tmp_agg_, &tmp_ms_, &tmp_mr_, &cnt_, &rowlen_, &scan32_blk_,
-                    &flag_})
+    for (auto *b : {&mate_, &want_, &cid_, &tmp_agg_, &tmp_ms_, &tmp_mr_, &cnt_, &rowlen_, &scan32_blk_, &flag_})
         b->release();
     for (auto *b : {&width_, &scan64_, &scan64_blk_, &mid_off_[0], &mid_off_[1]}) b->release();
     mid_col_[0].release();
@@ -874,6 +882,9 @@ void Amg::release() {
     big_list_.release();
     big_count_.release();
     tbound_.release();
+    packed_.release();
+    pscan_.release();
+    bounds_.release();
     toff_.release();
     tcol_.release();
     tval_.release();
@@ -890,6 +901,34 @@ void Amg::release() {
     bound_.release();
     if (h_flag_) cudaFreeHost(h_flag_);
     h_flag_ = nullptr;
+}
+
+cudaError_t Amg::scan_i32_dev(const int32_t *in, int32_t *out, int64_t n, cudaStream_t s) {
+    const int64_t nb = (n + 1023) / 1024;
+    AMG_CK(scan32_blk_.ensure(nb + 1));
+    if (n > 0) {
+        k_scan_block<int32_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan32_blk_.p, n);
+        k_scan_sums<int32_t><<<1, 1024, 0, s>>>(scan32_blk_.p, nb);
+        k_scan_add<int32_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan32_blk_.p, n, nb);
+        AMG_CK(cudaGetLastError());
+    } else {
+        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int32_t), s));
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Amg::scan_i64_dev(const int64_t *in, int64_t *out, int64_t n, cudaStream_t s) {
+    const int64_t nb = (n + 1023) / 1024;
+    AMG_CK(scan64_blk_.ensure(nb + 1));
+    if (n > 0) {
+        k_scan_block<int64_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan64_blk_.p, n);
+        k_scan_sums<int64_t><<<1, 1024, 0, s>>>(scan64_blk_.p, nb);
+        k_scan_add<int64_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan64_blk_.p, n, nb);
+        AMG_CK(cudaGetLastError());
+    } else {
+        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+    }
+    return cudaSuccess;
 }
 
 cudaError_t Amg::scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s) {
@@ -926,23 +965,14 @@ cudaError_t Amg::scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &t
     return cudaSuccess;
 }
 
-cudaError_t Amg::level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s) {
+cudaError_t Amg::level_stats(AmgLevel &L, unsigned int *bound, cudaStream_t s) {
     const int64_t n = L.A.n;
     AMG_CK(L.inv_diag.ensure(n));
     AMG_CK(isd_.ensure(n));
-    AMG_CK(bound_.ensure(1));
-    AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
-    k_level_diag<<<nblk(n, 256), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound_.p);
-    if (L.A.n_long > 0)
-        k_level_diag_long<<<(unsigned)L.A.n_long, 256, 0, s>>>(view(L.A), L.A.longrows, L.inv_diag.p, isd_.p, bound_.p);
+    k_level_diag<<<nblk(n, 256), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound);
+    if (L.A.long_count)
+        k_level_diag_long<<<148, 256, 0, s>>>(view(L.A), L.A.long_count, L.inv_diag.p, isd_.p, bound);
     AMG_CK(cudaGetLastError());
-    unsigned int bits = 0;
-    AMG_CK(cudaMemcpyAsync(&bits, bound_.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
-    AMG_CK(cudaStreamSynchronize(s));
-    float hi;
-    std::memcpy(&hi, &bits, sizeof(hi));
-    L.hi = hi > 0.f ? hi : 2.f;
-    (void)unit_diag;
     return cudaSuccess;
 }
 
@@ -954,8 +984,8 @@ cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *
     const MatView V = view(A);
     AMG_CK(mate_.ensure(n));
     AMG_CK(want_.ensure(n));
-    AMG_CK(lead_.ensure(n));
-    AMG_CK(cid_.ensure(n + 1));
+    AMG_CK(packed_.ensure(n + 1));
+    AMG_CK(pscan_.ensure(n + 1));
     AMG_CK(agg.ensure(n));
     const unsigned g = nblk(n, 256);
     k_pair_init<<<g, 256, 0, s>>>(V, row_edge, isd, mate_.p);
@@ -963,18 +993,17 @@ cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *
         k_pair_want<<<g, 256, 0, s>>>(V, isd, mate_.p, want_.p, row_edge ? 0 : opt_.mix_coarse);
         k_pair_match<<<g, 256, 0, s>>>(n, want_.p, mate_.p);
     }
-    k_pair_lead<<<g, 256, 0, s>>>(n, mate_.p, lead_.p);
+    k_pair_pack<<<g, 256, 0, s>>>(n, mate_.p, packed_.p);
     AMG_CK(cudaGetLastError());
-    cudaError_t e = scan_i32(lead_.p, cid_.p, n, nc, s);
+    int64_t tot = 0;
+    cudaError_t e = scan_i64(packed_.p, pscan_.p, n, tot, s);  // the one host read of the pass
     if (e != cudaSuccess) return e;
-    AMG_CK(cnt_.ensure(nc + 1));
+    nc = tot & 0xffffffff;
+    const int64_t members = tot >> 32;
     AMG_CK(mstart.ensure(nc + 1));
-    k_pair_assign<<<g, 256, 0, s>>>(n, mate_.p, lead_.p, cid_.p, agg.p, cnt_.p);
-    AMG_CK(cudaGetLastError());
-    int64_t members = 0;
-    if ((e = scan_i32(cnt_.p, mstart.p, nc, members, s)) != cudaSuccess) return e;
-    AMG_CK(mrows.ensure(members));
-    k_pair_members<<<g, 256, 0, s>>>(n, mate_.p, lead_.p, cid_.p, mstart.p, mrows.p);
+    AMG_CK(mrows.ensure(std::max<int64_t>(members, 1)));
+    k_pair_finish<<<std::max(g, 1u), 256, 0, s>>>(n, nc, members, mate_.p, packed_.p, pscan_.p, agg.p, mstart.p,
+                                                  mrows.p);
     AMG_CK(cudaGetLastError());
     return cudaSuccess;
 }
@@ -986,21 +1015,20 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     const int64_t n_pad = round_up(nc, kS), n_sl = n_pad / kS;
     AMG_CK(rowlen_.ensure(n_pad));
     AMG_CK(cudaMemsetAsync(rowlen_.p, 0, n_pad * sizeof(int32_t), s));  // padding rows: no entries
-    AMG_CK(flag_.ensure(1));
     AMG_CK(width_.ensure(n_sl));
     AMG_CK(c_off.ensure(n_sl + 1));
-    AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
     // compact row buffer sized by the candidate bound of every coarse row
     const MatView V = view(A);
     AMG_CK(tbound_.ensure(nc + 1));
     AMG_CK(toff_.ensure(nc + 1));
     if (nc > 0) k_cand_bound<<<nblk(nc, 256), 256, 0, s>>>(V, mstart, mrows, nc, tbound_.p);
     AMG_CK(cudaGetLastError());
-    int64_t cand = 0;
-    cudaError_t e = scan_i64(tbound_.p, toff_.p, nc, cand, s);
+    cudaError_t e = scan_i64_dev(tbound_.p, toff_.p, nc, s);
     if (e != cudaSuccess) return e;
-    AMG_CK(tcol_.ensure(std::max<int64_t>(cand, 1)));
-    AMG_CK(tval_.ensure(std::max<int64_t>(cand, 1)));
+    // every row of A belongs to at most one coarse row and contributes at most its slice
+    // width: the candidates fit in A's slot count
+    AMG_CK(tcol_.ensure(std::max<int64_t>(A.slots, 1)));
+    AMG_CK(tval_.ensure(std::max<int64_t>(A.slots, 1)));
     // every row first with the small buffer; rows that overflow it run again as a list with
     // the large one (wide rows appear only on coarse levels, next to hub rows)
     AMG_CK(big_list_.ensure(std::max<int64_t>(nc, 1)));
@@ -1013,23 +1041,11 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
     k_galerkin<kGalCap0, kGalWarps0, false><<<g0, kGalWarps0 * 32, 0, s>>>(
         V, agg, mstart, mrows, nc, rowlen_.p, toff_.p, tcol_.p, tval_.p, flag_.p, wt, big_list_.p, big_count_.p);
+    // the list pass reads its row count on the device (usually none: the blocks return at once);
+    // an overflow there is reported at the end of the setup
+    k_galerkin<kGalCapBig, kGalWarpsBig, true><<<148 * 2, kGalWarpsBig * 32, big_smem, s>>>(
+        V, agg, mstart, mrows, nc, rowlen_.p, toff_.p, tcol_.p, tval_.p, flag_.p, wt, big_list_.p, big_count_.p);
     AMG_CK(cudaGetLastError());
-    int32_t n_big = 0;
-    AMG_CK(cudaMemcpyAsync(&n_big, big_count_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    AMG_CK(cudaStreamSynchronize(s));
-    if (n_big > 0) {
-        const unsigned gb = (unsigned)std::min<int32_t>(n_big, 148 * 4);
-        k_galerkin<kGalCapBig, kGalWarpsBig, true><<<gb, kGalWarpsBig * 32, big_smem, s>>>(
-            V, agg, mstart, mrows, nc, rowlen_.p, toff_.p, tcol_.p, tval_.p, flag_.p, wt, big_list_.p,
-            big_count_.p);
-        AMG_CK(cudaGetLastError());
-        AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        AMG_CK(cudaStreamSynchronize(s));
-        if (*h_flag_) {
-            err = "Galerkin row wider than the gather buffer";
-            return cudaErrorInvalidValue;
-        }
-    }
     k_slice_width<<<nblk(n_sl, 256), 256, 0, s>>>(n_sl, nc, rowlen_.p, width_.p);
     AMG_CK(cudaGetLastError());
     int64_t slots = 0;
@@ -1053,17 +1069,16 @@ cudaError_t Amg::galerkin(const AmgMatrix &A, const int32_t *agg, int64_t nc, co
     AMG_CK(lpos_.ensure(n_pad + 1));
     k_flag_long<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, c_rlen.p, lflag_.p);
     AMG_CK(cudaGetLastError());
-    int64_t n_long = 0;
-    cudaError_t e2 = scan_i32(lflag_.p, lpos_.p, n_pad, n_long, s);
+    cudaError_t e2 = scan_i32_dev(lflag_.p, lpos_.p, n_pad, s);
     if (e2 != cudaSuccess) return e2;
-    C.n_long = n_long;
-    C.longrows = nullptr;
-    if (n_long > 0) {
-        AMG_CK(c_long.ensure(n_long));
-        k_compact_long<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, lflag_.p, lpos_.p, c_long.p);
-        AMG_CK(cudaGetLastError());
-        C.longrows = c_long.p;
-    }
+    // the list holds its count in front: [count, rows...]; the host reads the counts of all
+    // levels at the end of the setup
+    AMG_CK(c_long.ensure(n_pad + 1));
+    k_compact_long<<<nblk(n_pad, 256), 256, 0, s>>>(n_pad, lflag_.p, lpos_.p, c_long.p);
+    AMG_CK(cudaGetLastError());
+    C.longrows = c_long.p + 1;
+    C.long_count = c_long.p;
+    C.n_long = -1;  // not known on the host yet
     return cudaSuccess;
 }
 
@@ -1088,6 +1103,12 @@ cudaError_t Amg::dense_coarse(const AmgMatrix &A, cudaStream_t s) {
 cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s) {
     opt_ = o;
     if (!h_flag_) AMG_CK(cudaHostAlloc((void **)&h_flag_, sizeof(int32_t), cudaHostAllocDefault));
+    // device words the setup fills and the host reads once at its end: the Gershgorin bound of
+    // each level, and the Galerkin overflow flag
+    AMG_CK(bounds_.ensure(o.max_levels + 1));
+    AMG_CK(cudaMemsetAsync(bounds_.p, 0, (o.max_levels + 1) * sizeof(unsigned int), s));
+    AMG_CK(flag_.ensure(1));
+    AMG_CK(cudaMemsetAsync(flag_.p, 0, sizeof(int32_t), s));
     if ((int)lv_.size() < o.max_levels) lv_.resize(o.max_levels);
     n_levels_ = 0;
     // level 0: the solver's FP32 scaled matrix
@@ -1101,6 +1122,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     L0.A.rlen = nullptr;  // fine rows are short: the slice width bounds them
     L0.A.longrows = nullptr;
     L0.A.n_long = 0;
+    L0.A.long_count = nullptr;
     // level-0 weights: the near-null vector of the scaled system S^ = D^-1/2 S D^-1/2 is
     // D^1/2 1 (constants are near-null for S), so the level-0 transfers carry sqrt(diag S)
     AMG_CK(w0_.ensure(sys.n_rows));
@@ -1111,7 +1133,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     for (int l = 0;; ++l) {
         AmgLevel &L = lv_[l];
         AmgLevel &C = lv_[l + 1 < (int)lv_.size() ? l + 1 : l];
-        if ((e = level_stats(L, l == 0, s)) != cudaSuccess) return e;
+        if ((e = level_stats(L, bounds_.p + l, s)) != cudaSuccess) return e;
         AMG_CK(L.b.ensure(L.A.n));
         AMG_CK(L.xa.ensure(L.A.n));
         AMG_CK(L.xb.ensure(L.A.n));
@@ -1139,11 +1161,11 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
                 return e;
             AMG_CK(isd_.ensure(M.n));
             AMG_CK(mid_invd_.ensure(M.n));
-            AMG_CK(cudaMemsetAsync(bound_.p, 0, sizeof(unsigned int), s));
-            k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, bound_.p);
-            if (M.n_long > 0)
-                k_level_diag_long<<<(unsigned)M.n_long, 256, 0, s>>>(view(M), M.longrows, mid_invd_.p, isd_.p,
-                                                                     bound_.p);
+            // (the intermediate matrix's bound is not needed: its own slot past the levels')
+            unsigned int *mb = bounds_.p + o.max_levels;
+            k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, mb);
+            if (M.long_count)
+                k_level_diag_long<<<148, 256, 0, s>>>(view(M), M.long_count, mid_invd_.p, isd_.p, mb);
             AMG_CK(cudaGetLastError());
             int64_t np = 0;
             if ((e = pair_pass(M, isd_.p, nullptr, tmp_agg_, np, tmp_ms_, tmp_mr_, s)) != cudaSuccess) return e;
@@ -1153,16 +1175,14 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             k_compose_agg<<<nblk(L.A.n, 256), 256, 0, s>>>(L.A.n, L.agg.p, tmp_agg_.p, L.agg.p);
             k_compose_count<<<nblk(np, 256), 256, 0, s>>>(np, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, cnt_.p);
             AMG_CK(cudaGetLastError());
-            int64_t members = 0;
-            if ((e = scan_i32(cnt_.p, cid_.p, np, members, s)) != cudaSuccess) return e;
-            AMG_CK(want_.ensure(members));
+            // member offsets by a device-side scan; the member lists hold at most A_l's rows
+            if ((e = scan_i32_dev(cnt_.p, cid_.p, np, s)) != cudaSuccess) return e;
+            AMG_CK(want_.ensure(std::max<int64_t>(L.A.n, 1)));
             k_compose_fill<<<nblk(np, 256), 256, 0, s>>>(np, tmp_ms_.p, tmp_mr_.p, L.mem_start.p, L.mem_rows.p, cid_.p,
                                                          want_.p);
             AMG_CK(cudaGetLastError());
-            AMG_CK(L.mem_start.ensure(np + 1));
-            AMG_CK(L.mem_rows.ensure(members));
-            AMG_CK(cudaMemcpyAsync(L.mem_start.p, cid_.p, (np + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
-            AMG_CK(cudaMemcpyAsync(L.mem_rows.p, want_.p, members * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+            std::swap(L.mem_start, cid_);  // the composed lists become the level's
+            std::swap(L.mem_rows, want_);
             cur = M;
             curw = nullptr;
             cagg = tmp_agg_.p;
@@ -1180,6 +1200,26 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         }
         if ((double)L.nc > 0.85 * (double)n_real) {  // coarsening stalls: stop one level later
             opt_.max_levels = std::min(opt_.max_levels, l + 2);
+        }
+    }
+    {
+        std::vector<unsigned int> bits(n_levels_);
+        std::vector<int32_t> nlong(n_levels_, 0);
+        AMG_CK(cudaMemcpyAsync(bits.data(), bounds_.p, n_levels_ * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        for (int l = 1; l < n_levels_; ++l)
+            if (lv_[l].A.long_count)
+                AMG_CK(cudaMemcpyAsync(&nlong[l], lv_[l].A.long_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        AMG_CK(cudaStreamSynchronize(s));
+        if (*h_flag_) {
+            err = "Galerkin row wider than the gather buffer";
+            return cudaErrorInvalidValue;
+        }
+        for (int l = 0; l < n_levels_; ++l) {
+            float hi;
+            std::memcpy(&hi, &bits[l], sizeof(hi));
+            lv_[l].hi = hi > 0.f ? hi : 2.f;
+            lv_[l].A.n_long = nlong[l];
         }
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];

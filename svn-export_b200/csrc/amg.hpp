@@ -57,7 +57,8 @@ struct AmgMatrix {
     const float *val = nullptr;
     const int32_t *rlen = nullptr;      // entries per row (coarse matrices; null on the fine level)
     const int32_t *longrows = nullptr;  // rows with more than kLongRow entries (amg.cu)
-    int64_t n_long = 0;
+    const int32_t *long_count = nullptr;  // their count, on the device (longrows[-1])
+    int64_t n_long = 0;                 // ... on the host, once the setup has read it
 };
 
 struct AmgLevel {
@@ -110,10 +111,13 @@ private:
                          const int32_t *mrows, DBuf<int64_t> &c_off, DBuf<int32_t> &c_col, DBuf<float> &c_val,
                          DBuf<int32_t> &c_rlen, DBuf<int32_t> &c_long, AmgMatrix &C, cudaStream_t s,
                          const float *wt);
-    cudaError_t level_stats(AmgLevel &L, bool unit_diag, cudaStream_t s);
+    cudaError_t level_stats(AmgLevel &L, unsigned int *bound, cudaStream_t s);
     cudaError_t dense_coarse(const AmgMatrix &A, cudaStream_t s);
     cudaError_t scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s);
     cudaError_t scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s);
+    // the same without reading the total back (out[n] holds it on the device)
+    cudaError_t scan_i32_dev(const int32_t *in, int32_t *out, int64_t n, cudaStream_t s);
+    cudaError_t scan_i64_dev(const int64_t *in, int64_t *out, int64_t n, cudaStream_t s);
     void cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2, int degree = 0,
                      float ratio = 0.f) const;
 
@@ -121,7 +125,9 @@ private:
     std::vector<AmgLevel> lv_;
     int n_levels_ = 0;
     // pairing and Galerkin scratch
-    DBuf<int32_t> mate_, want_, lead_, cid_, tmp_agg_, tmp_ms_, tmp_mr_, cnt_;
+    DBuf<int32_t> mate_, want_, cid_, tmp_agg_, tmp_ms_, tmp_mr_, cnt_;
+    DBuf<int64_t> packed_, pscan_;  // pairing: packed (leader, member count) and its scan
+    DBuf<unsigned int> bounds_;     // Gershgorin bound of each level (float bits)
     DBuf<int64_t> width_, scan64_;
     DBuf<int32_t> rowlen_, scan32_blk_;
     DBuf<int64_t> scan64_blk_;
