@@ -199,24 +199,23 @@ def run_ours(a, rank, world):
     import mhdarcy
     from mhdarcy.cases import dirichlet_x_bc, make_case
 
+    from mhdarcy import parallel
+
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    # one process per GPU, each with its own realisations: no collective on the data path,
+    # only the barrier and the max over ranks that time the run
+    rank, world, dist = parallel.init("nccl", timeout_s=300) if world > 1 else (rank, world, None)
     stream = torch.cuda.Stream()
     if a.config == 3:
         # uneven batch: n in {8,12,16,24,32}, one z-plane fracture each, correlation 0.05..0.2
         import numpy as np
-        parts = [make_case(3, seed=1234 + 3 + 1000 * rank + i) for i in range(a.instances)]
+        parts = [make_case(3, seed=parallel.case_seed(3, rank, i)) for i in range(a.instances)]
         system = mhdarcy.MHSystem.batch([m for m, _ in parts])
         mesh = system.mesh
         coeffs = {k: np.concatenate([c[k] for _, c in parts]) for k in parts[0][1]}
     else:
-        mesh, coeffs = make_case(a.config, seed=1234 + a.config + 1000 * rank)
+        mesh, coeffs = make_case(a.config, seed=parallel.case_seed(a.config, rank))
         system = mhdarcy.MHSystem(mesh)
     per_step = system.n_instances
     system.set_stream(stream.cuda_stream)
@@ -235,11 +234,7 @@ def run_ours(a, rank, world):
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return parallel.max_over_ranks(x, dist, device="cuda")
 
     methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32, "cheb": mhdarcy.MH_SOLVER_CHEB,
                "fcg": mhdarcy.MH_SOLVER_FCG_LEARNED, "amg": mhdarcy.MH_SOLVER_AMG}
