@@ -400,6 +400,51 @@ __global__ void __launch_bounds__(kGalWarps * 32)
             __syncwarp();
             continue;
         }
+        if (cnt <= 32) {
+            // one candidate per lane: the same bitonic network in registers (shuffles), then
+            // the same sequential FP64 sums of equal columns
+            __syncwarp();
+            int32_t key = lane < cnt ? K[lane] : INT_MAX;
+            float val = lane < cnt ? V[lane] : 0.f;
+            __syncwarp();
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int32_t pk = __shfl_xor_sync(kFull, key, j);
+                    const float pv = __shfl_xor_sync(kFull, val, j);
+                    const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                    // the pair (lower, upper) swaps when its keys are out of order (strictly)
+                    const bool swap = lower ? (up ? key > pk : key < pk) : (up ? pk > key : pk < key);
+                    if (swap) {
+                        key = pk;
+                        val = pv;
+                    }
+                }
+            const int32_t prev = __shfl_up_sync(kFull, key, 1);
+            const bool head = lane < cnt && (lane == 0 || key != prev);
+            const unsigned hm = __ballot_sync(kFull, head);
+            double sum = (double)val;
+            bool open = head;
+            for (int dlt = 1; dlt < 32; ++dlt) {
+                const int32_t kd = __shfl_down_sync(kFull, key, dlt);
+                const float vd = __shfl_down_sync(kFull, val, dlt);
+                if (open) {
+                    if (lane + dlt < cnt && kd == key) sum += (double)vd;
+                    else open = false;
+                }
+                if (!__any_sync(kFull, open)) break;
+            }
+            if (head) {
+                const int64_t ob = t_off[I];
+                const int outk = __popc(hm & lt);
+                t_col[ob + outk] = key;
+                t_val[ob + outk] = (float)sum;
+            }
+            if (lane == 0) rowlen[I] = __popc(hm);
+            __syncwarp();
+            continue;
+        }
         int cp = 32;
         while (cp < cnt) cp <<= 1;
         for (int k = cnt + lane; k < cp; k += 32) {
