@@ -646,6 +646,63 @@ __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const floa
     return y;
 }
 
+// Coarse rows are long (tens of entries), so one thread walking a row issues a long chain of
+// dependent loads and the small coarse levels run at load latency.  The row kernels therefore
+// take G warps per 32-row slice (G = AmgLevel::g, chosen from the level's mean slice width):
+// warp g of a slice's group takes the slots g, g + G, g + 2G, ... of its 32 rows, eight loaded
+// together, and the G partial sums meet in shared memory in warp order (deterministic).  Blocks
+// hold 8 warps, i.e. 8 / G slices.  G = 1 is one thread per row (row_dot).
+template <int G> __device__ __forceinline__ void split_row(int64_t &i, int &g) {
+    const int64_t gw = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    i = (gw / G) * kS + (threadIdx.x & 31);
+    g = (int)(gw % G);
+}
+
+template <int G>
+__device__ __forceinline__ float split_part(const MatView &A, int64_t i, int g, const float *__restrict__ x) {
+    if (G == 1) return row_dot(A, i, x);
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    constexpr int kB = 8;
+    float y = 0.f;
+    for (int j0 = g; j0 < w; j0 += kB * G) {
+        int32_t c[kB];
+        float v[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            const int j = j0 + k * G;
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            c[k] = j < w ? __ldg(A.col + slot) : 0;
+            v[k] = j < w ? __ldg(A.val + slot) : 0.f;
+        }
+        float gx[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) gx[k] = j0 + k * G < w ? x[c[k]] : 0.f;
+#pragma unroll
+        for (int k = 0; k < kB; ++k) y += v[k] * gx[k];
+    }
+    return y;
+}
+
+// the row's sum of the G partials (valid in the group's warp g = 0); every thread of the block
+// calls it
+template <int G> __device__ __forceinline__ float split_sum(float y) {
+    if constexpr (G == 1) {
+        return y;
+    } else {
+        __shared__ float part[8][32];
+        const int wb = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        part[wb][lane] = y;
+        __syncthreads();
+        float t = 0.f;
+        if (wb % G == 0)
+#pragma unroll
+            for (int k = 0; k < G; ++k) t += part[wb + k][lane];
+        return t;
+    }
+}
+
 // first Chebyshev step from x = 0: d = c2 D^-1 b, x = d
 // (invd null: unit diagonal, the Jacobi-scaled fine level)
 __global__ void k_sm_first(Gate gate, int64_t n, const float *__restrict__ b, const float *__restrict__ invd, float c2,
@@ -685,20 +742,27 @@ __global__ void k_restrict_first(Gate gate, int64_t nc, int64_t nc_pad, const in
 }
 
 // Chebyshev step: d = c1 d + c2 D^-1 (b - A x_in), x_out = x_in + d (c1 = 0: d is not read)
-__global__ void k_sm_step(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ invd,
-                          const float *__restrict__ x_in, float *__restrict__ x_out, float *__restrict__ d, float c1,
-                          float c2, const int32_t *__restrict__ agg) {
+template <int G>
+__global__ void __launch_bounds__(256) k_sm_step(Gate gate, MatView A, const float *__restrict__ b,
+                                                 const float *__restrict__ invd, const float *__restrict__ x_in,
+                                                 float *__restrict__ x_out, float *__restrict__ d, float c1, float c2,
+                                                 const int32_t *__restrict__ agg) {
     if (closed(gate)) return;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
+    const bool outside = i < A.n && agg && agg[i] < 0;
+    const bool live = i < A.n && !outside && !is_long(A, i);  // long rows: k_long_rows
+    const float y = split_sum<G>(live ? split_part<G>(A, i, g, x_in) : 0.f);
+    if (g != 0 || i >= A.n) return;
     const float di = invd ? invd[i] : 1.f;
-    if (agg && agg[i] < 0) {  // a row outside the hierarchy: exact
+    if (outside) {  // a row outside the hierarchy: exact
         d[i] = 0.f;
         x_out[i] = di * b[i];
         return;
     }
-    if (is_long(A, i)) return;  // k_long_rows
-    const float r = b[i] - row_dot(A, i, x_in);
+    if (!live) return;
+    const float r = b[i] - y;
     const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * r;
     d[i] = dn;
     x_out[i] = x_in[i] + dn;
@@ -724,12 +788,16 @@ __global__ void k_sm_first_step(Gate gate, MatView A, const float *__restrict__ 
     x_out[i] = x1 + dn;
 }
 
-__global__ void k_residual(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ x,
-                           float *__restrict__ r) {
+template <int G>
+__global__ void __launch_bounds__(256) k_residual(Gate gate, MatView A, const float *__restrict__ b,
+                                                  const float *__restrict__ x, float *__restrict__ r) {
     if (closed(gate)) return;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n || is_long(A, i)) return;  // long rows: k_long_rows
-    r[i] = b[i] - row_dot(A, i, x);
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
+    const bool live = i < A.n && !is_long(A, i);  // long rows: k_long_rows
+    const float y = split_sum<G>(live ? split_part<G>(A, i, g, x) : 0.f);
+    if (g == 0 && live) r[i] = b[i] - y;
 }
 
 // b_c[I] = sum of r over the rows of coarse row I (in member order); padding rows get 0
@@ -815,17 +883,22 @@ __global__ void k_compact_long(int64_t n, const int32_t *flag, const int32_t *po
 
 // Energy-optimal scaling of a coarse correction: per block partials of x_c.b_c and
 // x_c.(A_c x_c) (the fine-level quantities e.r and e.Ae for e = P x_c).
+template <int G>
 __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const float *__restrict__ x,
                                                      const float *__restrict__ b, double *__restrict__ part,
                                                      unsigned int *ticket, double *alpha,
                                                      const double *__restrict__ long_part, int32_t n_long) {
     if (closed(gate)) return;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
+    const bool live = i < A.n && !is_long(A, i);  // long rows' terms come from k_long_rows in long_part
+    const float y = split_sum<G>(live ? split_part<G>(A, i, g, x) : 0.f);
     double xb = 0.0, xax = 0.0;
-    if (i < A.n && !is_long(A, i)) {  // long rows' terms come from k_long_rows in long_part
+    if (g == 0 && live) {
         const double xi = (double)x[i];
         xb = xi * (double)b[i];
-        xax = xi * (double)row_dot(A, i, x);
+        xax = xi * (double)y;
     }
     __shared__ double sh[2][8];
     __shared__ bool am_last;
@@ -882,6 +955,18 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
     }
 }
 
+// the row kernels of a level with G warps per slice (G = 1, 2, 4 or 8)
+decltype(&k_sm_step<1>) sm_step_kernel(int g) {
+    return g >= 8 ? k_sm_step<8> : g >= 4 ? k_sm_step<4> : g >= 2 ? k_sm_step<2> : k_sm_step<1>;
+}
+decltype(&k_residual<1>) residual_kernel(int g) {
+    return g >= 8 ? k_residual<8> : g >= 4 ? k_residual<4> : g >= 2 ? k_residual<2> : k_residual<1>;
+}
+decltype(&k_coarse_dots<1>) coarse_dots_kernel(int g) {
+    return g >= 8 ? k_coarse_dots<8> : g >= 4 ? k_coarse_dots<4> : g >= 2 ? k_coarse_dots<2> : k_coarse_dots<1>;
+}
+// blocks of 8 warps covering the level's slices with G warps each (n is a multiple of 32)
+unsigned row_blocks(const AmgLevel &L) { return nblk(L.A.n / kS * L.g, 8); }
 
 }  // namespace
 
@@ -1265,6 +1350,15 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             std::memcpy(&hi, &bits[l], sizeof(hi));
             lv_[l].hi = hi > 0.f ? hi : 2.f;
             lv_[l].A.n_long = nlong[l];
+            // warps per slice in the row kernels: at most split_width slots per warp and row
+            // (the fine level, 7-8 entries per row, keeps one thread per row)
+            AmgLevel &L = lv_[l];
+            const double width = L.A.n > 0 ? (double)L.A.slots / (double)L.A.n : 0.0;
+            int g = 1;
+            if (l > 0 && opt_.split > 0) g = opt_.split;
+            else if (l > 0)
+                while (g < 8 && width > opt_.split_width * g) g *= 2;
+            L.g = g >= 8 ? 8 : g >= 4 ? 4 : g >= 2 ? 2 : 1;  // the kernels' G
         }
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];
@@ -1282,7 +1376,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     int64_t tot = 0;
     for (int l = 0; l + 1 < n_levels_; ++l) {
         dots_off_[l] = tot;
-        tot += 2 * (int64_t)nblk(lv_[l + 1].A.n, 256);
+        tot += 2 * (int64_t)row_blocks(lv_[l + 1]);
     }
     AMG_CK(dots_.ensure(tot + 2));
     dots_long_off_.assign(n_levels_, 0);
@@ -1360,7 +1454,8 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         const float *b = l == 0 ? r : L.b.p;
         const float *invd = l == 0 ? nullptr : L.inv_diag.p;  // the scaled fine level has unit diagonal
         const MatView A = view(L.A);
-        const unsigned g = nblk(L.A.n, 256);
+        const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
+        const auto sm_step = sm_step_kernel(L.g);
         cheb_coeffs(L, c1, c2);
         float *xi = L.xa.p, *xo = L.xb.p;
         int k0 = 1;
@@ -1377,13 +1472,13 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         // (coarser levels: the first step was fused into the restriction from the level above)
         for (int k = k0; k < pre; ++k) {
             if (l == 0) rec_step(true);
-            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
+            sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
             long_rows(L.A, 0, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             std::swap(xi, xo);
         }
         xout[l] = xi;
-        k_residual<<<g, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
+        residual_kernel(L.g)<<<gs, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
         long_rows(L.A, 1, b, nullptr, xi, L.r.p, nullptr, 0.f, 0.f, nullptr);
         AmgLevel &C = lv_[l + 1];
         const float *wt = l == 0 ? w0_used_ : nullptr;
@@ -1407,14 +1502,15 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
             k_dense_gemv<<<nblk(Lc.A.n * 32, 256), 256, 0, s>>>(gate_, dense_inv_.p, dense_n_, Lc.A.n, b, x);
             xout[nl - 1] = x;
         } else {
-            const unsigned g = nblk(Lc.A.n, 256);
+            const unsigned g = nblk(Lc.A.n, 256), gs = row_blocks(Lc);
+            const auto sm_step = sm_step_kernel(Lc.g);
             cheb_coeffs(Lc, c1, c2, kCoarseDegree, kCoarseRatio);
             float *xi = Lc.xa.p, *xo = Lc.xb.p;
             k_sm_first<<<g, 256, 0, s>>>(gate_, Lc.A.n, b, Lc.inv_diag.p, (float)c2[0], xi, Lc.d.p, Lc.agg.p);
             for (int k = 1; k < kCoarseDegree; ++k) {
                 float *xk = (nl == 1 && k == kCoarseDegree - 1) ? z : xo;
-                k_sm_step<<<g, 256, 0, s>>>(gate_, view(Lc.A), b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k],
-                                            (float)c2[k], Lc.agg.p);
+                sm_step<<<gs, 256, 0, s>>>(gate_, view(Lc.A), b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k],
+                                           (float)c2[k], Lc.agg.p);
                 long_rows(Lc.A, 0, b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k], (float)c2[k], nullptr);
                 xo = xi;
                 xi = xk;
@@ -1428,18 +1524,19 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         const float *b = l == 0 ? r : L.b.p;
         const float *invd = l == 0 ? nullptr : L.inv_diag.p;
         const MatView A = view(L.A);
-        const unsigned g = nblk(L.A.n, 256);
+        const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
+        const auto sm_step = sm_step_kernel(L.g);
         cheb_coeffs(L, c1, c2);
         float *xi = xout[l];
         const double *al = nullptr;
         // (a dense coarsest correction is exact: its optimal scaling is 1)
         if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0)) {
             AmgLevel &C = lv_[l + 1];
-            const unsigned gc = nblk(C.A.n, 256);
             double *lp = dots_long_.p + dots_long_off_[l];
             long_rows(C.A, 2, C.b.p, nullptr, xout[l + 1], nullptr, nullptr, 0.f, 0.f, lp);
-            k_coarse_dots<<<gc, 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p, dots_.p + dots_off_[l],
-                                             tickets_.p + l, alpha_.p + l, lp, (int32_t)C.A.n_long);
+            coarse_dots_kernel(C.g)<<<row_blocks(C), 256, 0, s>>>(gate_, view(C.A), xout[l + 1], C.b.p,
+                                                                  dots_.p + dots_off_[l], tickets_.p + l,
+                                                                  alpha_.p + l, lp, (int32_t)C.A.n_long);
             al = alpha_.p + l;
         }
         k_prolong<<<g, 256, 0, s>>>(gate_, L.A.n, L.agg.p, xout[l + 1], xi, al, opt_.alpha, l == 0 ? w0_used_ : nullptr);
@@ -1447,8 +1544,8 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         for (int k = 0; k < deg; ++k) {
             float *xo = (l == 0 && k == deg - 1) ? z : other;
             if (l == 0) rec_step(true);
-            k_sm_step<<<g, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k],
-                                        L.agg.p);
+            sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k],
+                                       L.agg.p);
             long_rows(L.A, 0, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             other = xi;

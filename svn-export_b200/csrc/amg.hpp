@@ -41,6 +41,8 @@ struct AmgOptions {
     float alpha = 1.f;      // fixed scaling of the coarse corrections when kcycle = 0
     int weighted = 1;       // level-0 transfers weighted by sqrt(diag S) (near-null vector)
     int mix_coarse = 1;     // coarse levels may pair along positive couplings (weakly preferred)
+    int split = 0;          // warps per slice in the coarse row kernels (1, 2, 4, 8; 0: by row width)
+    int split_width = 12;   // ... by row width: the fewest warps with at most this many slots each
 };
 
 template <class T> struct DBuf {
@@ -73,6 +75,7 @@ struct AmgLevel {
     DBuf<float> b, xa, xb, d, r;               // cycle vectors
     int64_t nc = 0;                            // coarse rows (0 on the coarsest level)
     float hi = 2.f;                            // Gershgorin bound of D^-1 A
+    int g = 1;                                 // warps per slice in the row kernels (amg.cu)
 };
 
 // Events recorded inside a captured V-cycle (as external event nodes) to time it: the whole

@@ -324,20 +324,37 @@ int need_device(mh_handle *h) {
     return MH_OK;
 }
 
+// input checks on the host threads (element fields of millions of entries are checked on
+// every unsteady step)
 int check_finite(const double *a, int64_t n) {
     if (!a) return 1;
-    for (int64_t i = 0; i < n; ++i)
-        if (!std::isfinite(a[i])) return 0;
-    return 1;
+    int ok = 1;
+#pragma omp parallel for reduction(&& : ok) schedule(static) if (n > (1 << 16))
+    for (int64_t i = 0; i < n; ++i) ok = ok && std::isfinite(a[i]);
+    return ok;
 }
 
+int check_positive(const double *a, int64_t n) {
+    if (!a) return 1;
+    int ok = 1;
+#pragma omp parallel for reduction(&& : ok) schedule(static) if (n > (1 << 16))
+    for (int64_t i = 0; i < n; ++i) ok = ok && a[i] > 0.0;
+    return ok;
+}
+
+__global__ void k_fill(double *dst, int64_t n, double v) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = v;
+}
+
+// a field from the caller's host array, or its default value filled on the device
 int fill_or_default(mh_handle *h, double *dst, const double *src, int64_t n, double dflt) {
+    if (n <= 0) return MH_OK;
     if (src) {
         CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     } else {
-        std::vector<double> v(n, dflt);
-        CK(cudaMemcpyAsync(dst, v.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(dst, n, dflt);
+        CK(cudaGetLastError());
     }
     return MH_OK;
 }
@@ -849,6 +866,8 @@ mh::AmgOptions amg_options() {
     env_i("MH_AMG_KLEVELS", o.kcycle_levels, 0, 64);
     env_i("MH_AMG_WEIGHTED", o.weighted, 0, 1);
     env_i("MH_AMG_MIX", o.mix_coarse, 0, 1);
+    env_i("MH_AMG_SPLIT", o.split, 0, 8);
+    env_i("MH_AMG_SPLITW", o.split_width, 2, 64);
     if (const char *e = getenv("MH_AMG_RATIO")) {
         const float x = (float)atof(e);
         if (x >= 1.5f && x <= 100.f) o.cheb_ratio = x;
@@ -1439,15 +1458,13 @@ int mh_set_coeffs(mh_handle *h, const mh_coeffs *c) {
     for (int i = 0; i < 5; ++i)
         if (!check_finite(arrs[i], n)) return MH_ERR_NONFINITE;
     if (c->anisotropy && !check_finite(c->anisotropy, 9 * n)) return MH_ERR_NONFINITE;
-    for (int64_t e = 0; e < n; ++e) {
-        if (c->conductivity && !(c->conductivity[e] > 0.0)) {
-            h->err = "conductivity must be positive";
-            return MH_ERR_INVALID;
-        }
-        if (c->cross_section && !(c->cross_section[e] > 0.0)) {
-            h->err = "cross_section must be positive";
-            return MH_ERR_INVALID;
-        }
+    if (!check_positive(c->conductivity, n)) {
+        h->err = "conductivity must be positive";
+        return MH_ERR_INVALID;
+    }
+    if (!check_positive(c->cross_section, n)) {
+        h->err = "cross_section must be positive";
+        return MH_ERR_INVALID;
     }
     mh::ElemData &d = h->ed;
     if ((rc = fill_or_default(h, (double *)d.conductivity, c->conductivity, n, 1.0)) ||
