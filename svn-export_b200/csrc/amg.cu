@@ -132,31 +132,79 @@ template <typename T> __global__ void k_scan_add(T *out, const T *bsum, int64_t 
     if (i == 0) out[n] = bsum[nb];
 }
 
+// Row kernels with G warps per 32-row slice (blocks of 8 warps): row i of warp g of its slice's
+// group; the warp takes the slots g, g + G, g + 2G, ... of the row.
+template <int G> __device__ __forceinline__ void split_row(int64_t &i, int &g) {
+    const int64_t gw = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    i = (gw / G) * kS + (threadIdx.x & 31);
+    g = (int)(gw % G);
+}
+
 // ---- level statistics ----------------------------------------------------------------------
 // inv_diag = 1/a_ii, isd = 1/sqrt(a_ii) (0 where there is no positive diagonal) and the
 // Gershgorin bound max_i sum_j |a_ij| / a_ii of D^-1 A.
-__global__ void k_level_diag(MatView A, float *inv_diag, float *isd, unsigned int *bound) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    float s = 0.f;
-    if (i < A.n && !is_long(A, i)) {  // long rows: k_level_diag_long
+template <int G>
+__global__ void __launch_bounds__(256) k_level_diag(MatView A, float *inv_diag, float *isd, unsigned int *bound) {
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
+    const bool live = i < A.n && !is_long(A, i);  // long rows: k_level_diag_long
+    float dg = 0.f, sum = 0.f;
+    if (live) {
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
-        float dg = 0.f, sum = 0.f;
-        for (int j = 0; j < w; ++j) {
-            const int64_t slot = base + (int64_t)j * kS + ln;
-            const float v = A.val[slot];
-            if (A.col[slot] == (int32_t)i) dg += v;
-            sum += fabsf(v);
+        constexpr int kB = 8;
+        for (int j0 = g; j0 < w; j0 += kB * G) {
+            int32_t c[kB];
+            float v[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                const int j = j0 + k * G;
+                const int64_t slot = base + (int64_t)j * kS + ln;
+                c[k] = j < w ? __ldg(A.col + slot) : -1;
+                v[k] = j < w ? __ldg(A.val + slot) : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                if (c[k] == (int32_t)i) dg += v[k];
+                sum += fabsf(v[k]);
+            }
         }
+    }
+    if constexpr (G > 1) {
+        __shared__ float part[2][8][32];
+        const int wb = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        part[0][wb][lane] = dg;
+        part[1][wb][lane] = sum;
+        __syncthreads();
+        if (wb % G == 0) {
+            dg = sum = 0.f;
+#pragma unroll
+            for (int k = 0; k < G; ++k) {
+                dg += part[0][wb + k][lane];
+                sum += part[1][wb + k][lane];
+            }
+        }
+    }
+    float s = 0.f;
+    if (live && g == 0) {
         const bool ok = dg > 0.f;
         inv_diag[i] = ok ? 1.f / dg : 0.f;
         isd[i] = ok ? rsqrtf(dg) : 0.f;
         s = ok ? sum / dg : 0.f;
     }
+    // one atomic per block (one per warp on a single word serialises at the L2)
+    __shared__ float wmax[8];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(kFull, s, o));
-    if ((threadIdx.x & 31) == 0 && s > 0.f) atomicMax(bound, __float_as_uint(s));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmaxf(m, wmax[k]);
+        if (m > 0.f) atomicMax(bound, __float_as_uint(m));
+    }
 }
 
 // the same for the long rows, one block each
@@ -245,29 +293,72 @@ __global__ void k_mark_isolated(MatView A, int32_t *agg) {
 // With mix, a row may also pair along a positive coupling, weighted 1e-3 so that any negative
 // coupling is preferred (coarse Galerkin matrices, and unsteady systems, carry many positive
 // off-diagonals; pairing only along negative ones stalls the coarsening there).
-__global__ void k_pair_want(MatView A, const float *isd, const int32_t *mate, int32_t *want, int mix) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
+// The choice is the largest weight, and among equal weights the lowest column: it does not
+// depend on the order the slots are visited in, so the G warps of a slice (split_row) combine
+// their partial choices to the same row.
+__device__ __forceinline__ bool better(float s, int32_t c, float bw, int32_t best) {
+    return c >= 0 && (s > bw || (s == bw && best >= 0 && c < best));
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_pair_want(MatView A, const float *isd, const int32_t *mate, int32_t *want,
+                                                   int mix) {
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
     int32_t best = -1;
-    if (mate[i] == kUnmatched && !is_long(A, i)) {  // a hub row stays an aggregate of its own
+    float bw = 0.f;
+    if (i < A.n && mate[i] == kUnmatched && !is_long(A, i)) {  // a hub row stays an aggregate of its own
         int64_t base;
         int w, ln;
         row_of(A, i, base, w, ln);
-        float bw = 0.f;
         const float si = isd[i];
-        for (int j = 0; j < w; ++j) {
-            const int64_t slot = base + (int64_t)j * kS + ln;
-            const int32_t c = A.col[slot];
-            const float v = A.val[slot];
-            if (c == (int32_t)i || v == 0.f || (!mix && !(v < 0.f)) || mate[c] != kUnmatched) continue;
-            const float s = (v < 0.f ? -v : 1e-3f * v) * si * isd[c];
-            if (s > bw || (s == bw && best >= 0 && c < best)) {
-                bw = s;
-                best = c;
+        constexpr int kB = 8;
+        for (int j0 = g; j0 < w; j0 += kB * G) {
+            int32_t c[kB];
+            float v[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                const int j = j0 + k * G;
+                const int64_t slot = base + (int64_t)j * kS + ln;
+                c[k] = j < w ? __ldg(A.col + slot) : (int32_t)i;
+                v[k] = j < w ? __ldg(A.val + slot) : 0.f;
+            }
+            int32_t mt[kB];
+            float sc[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                const bool cand = c[k] != (int32_t)i && v[k] != 0.f && (mix || v[k] < 0.f);
+                mt[k] = cand ? mate[c[k]] : kExcluded;
+                sc[k] = cand ? isd[c[k]] : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                if (mt[k] != kUnmatched) continue;
+                const float s = (v[k] < 0.f ? -v[k] : 1e-3f * v[k]) * si * sc[k];
+                if (better(s, c[k], bw, best)) {
+                    bw = s;
+                    best = c[k];
+                }
             }
         }
     }
-    want[i] = best;
+    if constexpr (G > 1) {
+        __shared__ float pw[8][32];
+        __shared__ int32_t pc[8][32];
+        const int wb = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        pw[wb][lane] = bw;
+        pc[wb][lane] = best;
+        __syncthreads();
+        if (wb % G != 0) return;
+#pragma unroll
+        for (int k = 1; k < G; ++k)
+            if (better(pw[wb + k][lane], pc[wb + k][lane], bw, best)) {
+                bw = pw[wb + k][lane];
+                best = pc[wb + k][lane];
+            }
+    }
+    if (i < A.n) want[i] = best;
 }
 
 // Handshake: i and j pair when each is the other's choice; a row with no candidate is final.
@@ -345,6 +436,99 @@ __global__ void k_compose_fill(int64_t nc, const int32_t *ms2, const int32_t *mr
 // (LIST = false); a row whose candidates do not fit is appended to a list, and the list then
 // runs with a large dynamic buffer (LIST = true, one warp per block).  A row too wide even for
 // that sets *overflow.
+// Rows of at most S candidates (S = 16 or 32), one row per S-lane segment of the warp and one
+// candidate per lane (key INT_MAX: none; cnt real ones in the segment; I < 0: no row).
+// seg_gather loads lane t's candidate (the rows of the coarse row in member order, then their
+// slots) with all the row's loads in flight at once; seg_reduce sorts the segment by coarse
+// column (bitonic network in registers), sums equal columns in sorted order in FP64, and writes
+// the row at t_off = ob and its length to rowlen[I].
+template <int S>
+__device__ __forceinline__ void seg_gather(const MatView &A, const int32_t *__restrict__ agg,
+                                           const int32_t *__restrict__ mrows, const float *__restrict__ wt,
+                                           int32_t m0, int32_t nm, int32_t &key, float &v) {
+    const int sl = threadIdx.x & (S - 1);
+    int64_t mb = 0;
+    int mw = 0, mln = 0;
+    float mwt = 1.f;
+    if (sl < nm) {
+        const int32_t mi = mrows[m0 + sl];
+        row_of(A, mi, mb, mw, mln);
+        if (wt) mwt = wt[mi];
+    }
+    int incl = mw;
+#pragma unroll
+    for (int o = 1; o < S; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o, S);
+        if (sl >= o) incl += y;
+    }
+    const int excl = incl - mw, total = __shfl_sync(kFull, incl, S - 1, S);
+    const int nmax = __reduce_max_sync(kFull, (unsigned)nm);
+    int mem = 0;  // the last member starting at or before this lane
+    for (int k = 1; k < nmax; ++k) {
+        const int e = __shfl_sync(kFull, excl, k, S);
+        if (k < nm && e <= sl) mem = k;
+    }
+    const int64_t b = __shfl_sync(kFull, mb, mem, S);
+    const int lnm = __shfl_sync(kFull, mln, mem, S), e0 = __shfl_sync(kFull, excl, mem, S);
+    const float wi = __shfl_sync(kFull, mwt, mem, S);
+    key = INT_MAX;
+    v = 0.f;
+    if (sl < total) {
+        const int64_t slot = b + (int64_t)(sl - e0) * kS + lnm;
+        const float a = A.val[slot];
+        if (a != 0.f) {
+            const int32_t c = A.col[slot];
+            const int32_t ac = agg[c];
+            if (ac >= 0) {
+                key = ac;
+                v = wt ? a * wi * wt[c] : a;
+            }
+        }
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void seg_reduce(int32_t key, float val, int cnt, int64_t ob, int64_t I,
+                                           int32_t *__restrict__ t_col, float *__restrict__ t_val,
+                                           int32_t *__restrict__ rowlen) {
+    const int lane = threadIdx.x & 31, sl = lane & (S - 1);
+#pragma unroll
+    for (int k = 2; k <= S; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int32_t pk = __shfl_xor_sync(kFull, key, j);
+            const float pv = __shfl_xor_sync(kFull, val, j);
+            const bool up = (sl & k) == 0, lower = (sl & j) == 0;
+            // the pair (lower, upper) swaps when its keys are out of order (strictly)
+            const bool swap = lower ? (up ? key > pk : key < pk) : (up ? pk > key : pk < key);
+            if (swap) {
+                key = pk;
+                val = pv;
+            }
+        }
+    const int32_t prev = __shfl_up_sync(kFull, key, 1);
+    const bool head = sl < cnt && (sl == 0 || key != prev);
+    const unsigned hall = __ballot_sync(kFull, head);
+    const unsigned hm = S == 32 ? hall : (hall >> (lane & ~(S - 1))) & ((1u << (S & 31)) - 1u);
+    double sum = (double)val;
+    bool open = head;
+    for (int dlt = 1; dlt < S; ++dlt) {
+        const int32_t kd = __shfl_down_sync(kFull, key, dlt);
+        const float vd = __shfl_down_sync(kFull, val, dlt);
+        if (open) {
+            if (sl + dlt < cnt && kd == key) sum += (double)vd;
+            else open = false;
+        }
+        if (!__any_sync(kFull, open)) break;
+    }
+    if (head) {
+        const int outk = __popc(hm & ((1u << sl) - 1u));
+        t_col[ob + outk] = key;
+        t_val[ob + outk] = (float)sum;
+    }
+    if (sl == 0 && I >= 0) rowlen[I] = __popc(hm);
+}
+
 template <int kGalCap, int kGalWarps, bool LIST>
 __global__ void __launch_bounds__(kGalWarps * 32)
     k_galerkin(MatView A, const int32_t *__restrict__ agg, const int32_t *__restrict__ mstart,
@@ -360,134 +544,139 @@ __global__ void __launch_bounds__(kGalWarps * 32)
     float *V = LIST ? reinterpret_cast<float *>(dyn_sm) + (size_t)(kGalWarps + warp) * kGalCap : s_v[warp];
     const unsigned lt = (1u << lane) - 1u;
     const int64_t n_iter = LIST ? *big_count : nc;
-    for (int64_t it = (int64_t)blockIdx.x * kGalWarps + warp; it < n_iter; it += (int64_t)gridDim.x * kGalWarps) {
-        const int64_t I = LIST ? big_list[it] : it;
-        int cnt = 0;
-        for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
-            int64_t base;
-            int w, ln;
-            const int32_t mi = mrows[m];
-            row_of(A, mi, base, w, ln);
-            const float wi = wt ? wt[mi] : 1.f;
-            for (int j0 = 0; j0 < w; j0 += 32) {
-                const int j = j0 + lane;
-                int32_t key = -1;
-                float v = 0.f;
-                if (j < w) {
-                    const int64_t slot = base + (int64_t)j * kS + ln;
-                    v = A.val[slot];
-                    if (v != 0.f) {
-                        const int32_t c = A.col[slot];
-                        key = agg[c];
-                        if (wt) v = v * wi * wt[c];
-                    }
-                }
-                const unsigned mask = __ballot_sync(kFull, key >= 0);
-                const int pos = cnt + __popc(mask & lt);
-                if (key >= 0 && pos < kGalCap) {
-                    K[pos] = key;
-                    V[pos] = v;
-                }
-                cnt += __popc(mask);
+    constexpr int R = LIST ? 1 : 2;  // rows per warp and iteration
+    for (int64_t it = ((int64_t)blockIdx.x * kGalWarps + warp) * R; it < n_iter;
+         it += (int64_t)gridDim.x * kGalWarps * R) {
+        if (!LIST) {
+            // two rows of at most 16 candidates (the summed widths of their rows): one per
+            // half-warp, lane t of a half taking candidate t of its row
+            const int half = lane >> 4;
+            const int64_t Ih = it + half < n_iter ? it + half : -1;
+            int64_t obh = 0;
+            int32_t m0h = 0, nmh = 0;
+            bool fit = true;
+            if (Ih >= 0) {
+                obh = t_off[Ih];
+                m0h = mstart[Ih];
+                nmh = mstart[Ih + 1] - m0h;
+                fit = t_off[Ih + 1] - obh <= 16 && nmh <= 16;
+            }
+            if (__all_sync(kFull, fit)) {
+                int32_t key;
+                float v;
+                seg_gather<16>(A, agg, mrows, wt, m0h, nmh, key, v);
+                const unsigned bal = __ballot_sync(kFull, key != INT_MAX);
+                seg_reduce<16>(key, v, __popc(half ? bal >> 16 : bal & 0xffffu), obh, Ih, t_col, t_val, rowlen);
+                __syncwarp();
+                continue;
             }
         }
-        if (cnt > kGalCap) {
-            if (lane == 0) {
-                if (LIST) atomicExch(overflow, 1);
-                else big_list[atomicAdd(big_count, 1)] = (int32_t)I;
-                rowlen[I] = 0;
-            }
-            __syncwarp();
-            continue;
-        }
-        if (cnt <= 32) {
-            // one candidate per lane: the same bitonic network in registers (shuffles), then
-            // the same sequential FP64 sums of equal columns
-            __syncwarp();
-            int32_t key = lane < cnt ? K[lane] : INT_MAX;
-            float val = lane < cnt ? V[lane] : 0.f;
-            __syncwarp();
-#pragma unroll
-            for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    const int32_t pk = __shfl_xor_sync(kFull, key, j);
-                    const float pv = __shfl_xor_sync(kFull, val, j);
-                    const bool up = (lane & k) == 0, lower = (lane & j) == 0;
-                    // the pair (lower, upper) swaps when its keys are out of order (strictly)
-                    const bool swap = lower ? (up ? key > pk : key < pk) : (up ? pk > key : pk < key);
-                    if (swap) {
-                        key = pk;
-                        val = pv;
-                    }
+        for (int q = 0; q < R; ++q) {
+            const int64_t I = LIST ? big_list[it] : it + q;
+            if (I >= (LIST ? INT64_MAX : nc)) break;
+            const int64_t ob = t_off[I];
+            if (!LIST) {
+                // at most 32 candidates: one row per warp, lane t taking candidate t
+                const int32_t m0 = mstart[I], nm = mstart[I + 1] - m0;
+                if (t_off[I + 1] - ob <= 32 && nm <= 32) {
+                    int32_t key;
+                    float v;
+                    seg_gather<32>(A, agg, mrows, wt, m0, nm, key, v);
+                    seg_reduce<32>(key, v, __popc(__ballot_sync(kFull, key != INT_MAX)), ob, I, t_col, t_val, rowlen);
+                    __syncwarp();
+                    continue;
                 }
-            const int32_t prev = __shfl_up_sync(kFull, key, 1);
-            const bool head = lane < cnt && (lane == 0 || key != prev);
-            const unsigned hm = __ballot_sync(kFull, head);
-            double sum = (double)val;
-            bool open = head;
-            for (int dlt = 1; dlt < 32; ++dlt) {
-                const int32_t kd = __shfl_down_sync(kFull, key, dlt);
-                const float vd = __shfl_down_sync(kFull, val, dlt);
-                if (open) {
-                    if (lane + dlt < cnt && kd == key) sum += (double)vd;
-                    else open = false;
-                }
-                if (!__any_sync(kFull, open)) break;
             }
-            if (head) {
-                const int64_t ob = t_off[I];
-                const int outk = __popc(hm & lt);
-                t_col[ob + outk] = key;
-                t_val[ob + outk] = (float)sum;
-            }
-            if (lane == 0) rowlen[I] = __popc(hm);
-            __syncwarp();
-            continue;
-        }
-        int cp = 32;
-        while (cp < cnt) cp <<= 1;
-        for (int k = cnt + lane; k < cp; k += 32) {
-            K[k] = INT_MAX;
-            V[k] = 0.f;
-        }
-        __syncwarp();
-        for (int k = 2; k <= cp; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int t = lane; t < cp; t += 32) {
-                    const int u = t ^ j;
-                    if (u > t) {
-                        const int32_t a = K[t], b = K[u];
-                        const bool up = (t & k) == 0;
-                        if (up ? (a > b) : (a < b)) {
-                            K[t] = b;
-                            K[u] = a;
-                            const float x = V[t];
-                            V[t] = V[u];
-                            V[u] = x;
+            int cnt = 0;
+            for (int32_t m = mstart[I]; m < mstart[I + 1]; ++m) {
+                int64_t base;
+                int w, ln;
+                const int32_t mi = mrows[m];
+                row_of(A, mi, base, w, ln);
+                const float wi = wt ? wt[mi] : 1.f;
+                for (int j0 = 0; j0 < w; j0 += 32) {
+                    const int j = j0 + lane;
+                    int32_t key = -1;
+                    float v = 0.f;
+                    if (j < w) {
+                        const int64_t slot = base + (int64_t)j * kS + ln;
+                        v = A.val[slot];
+                        if (v != 0.f) {
+                            const int32_t c = A.col[slot];
+                            key = agg[c];
+                            if (wt) v = v * wi * wt[c];
                         }
                     }
+                    const unsigned mask = __ballot_sync(kFull, key >= 0);
+                    const int pos = cnt + __popc(mask & lt);
+                    if (key >= 0 && pos < kGalCap) {
+                        K[pos] = key;
+                        V[pos] = v;
+                    }
+                    cnt += __popc(mask);
+                }
+            }
+            if (cnt > kGalCap) {
+                if (lane == 0) {
+                    if (LIST) atomicExch(overflow, 1);
+                    else big_list[atomicAdd(big_count, 1)] = (int32_t)I;
+                    rowlen[I] = 0;
                 }
                 __syncwarp();
+                continue;
             }
-        int uniq = 0;
-        const int64_t ob = t_off[I];
-        for (int t0 = 0; t0 < cnt; t0 += 32) {
-            const int t = t0 + lane;
-            const bool head = t < cnt && (t == 0 || K[t] != K[t - 1]);
-            const unsigned hm = __ballot_sync(kFull, head);
-            if (head) {
-                const int outk = uniq + __popc(hm & lt);
-                const int32_t key = K[t];
-                double s = 0.0;
-                for (int q = t; q < cnt && K[q] == key; ++q) s += (double)V[q];
-                t_col[ob + outk] = key;
-                t_val[ob + outk] = (float)s;
+            if (cnt <= 32) {  // one candidate per lane: the register network
+                __syncwarp();
+                const int32_t key = lane < cnt ? K[lane] : INT_MAX;
+                const float val = lane < cnt ? V[lane] : 0.f;
+                __syncwarp();
+                seg_reduce<32>(key, val, cnt, ob, I, t_col, t_val, rowlen);
+                __syncwarp();
+                continue;
             }
-            uniq += __popc(hm);
+            int cp = 32;
+            while (cp < cnt) cp <<= 1;
+            for (int k = cnt + lane; k < cp; k += 32) {
+                K[k] = INT_MAX;
+                V[k] = 0.f;
+            }
+            __syncwarp();
+            for (int k = 2; k <= cp; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int t = lane; t < cp; t += 32) {
+                        const int u = t ^ j;
+                        if (u > t) {
+                            const int32_t a = K[t], b = K[u];
+                            const bool up = (t & k) == 0;
+                            if (up ? (a > b) : (a < b)) {
+                                K[t] = b;
+                                K[u] = a;
+                                const float x = V[t];
+                                V[t] = V[u];
+                                V[u] = x;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            int uniq = 0;
+            for (int t0 = 0; t0 < cnt; t0 += 32) {
+                const int t = t0 + lane;
+                const bool head = t < cnt && (t == 0 || K[t] != K[t - 1]);
+                const unsigned hm = __ballot_sync(kFull, head);
+                if (head) {
+                    const int outk = uniq + __popc(hm & lt);
+                    const int32_t key = K[t];
+                    double s = 0.0;
+                    for (int q = t; q < cnt && K[q] == key; ++q) s += (double)V[q];
+                    t_col[ob + outk] = key;
+                    t_val[ob + outk] = (float)s;
+                }
+                uniq += __popc(hm);
+            }
+            if (lane == 0) rowlen[I] = uniq;
+            __syncwarp();
         }
-        if (lane == 0) rowlen[I] = uniq;
-        __syncwarp();
     }
 }
 
@@ -556,6 +745,7 @@ __global__ void __launch_bounds__(1024) k_dense_inverse(MatView A, int n, float 
     extern __shared__ double sm[];
     double *M = sm, *fac = sm + n * n;
     __shared__ double pinv;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // launched with 1024 threads
     for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) M[idx] = 0.0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -581,12 +771,16 @@ __global__ void __launch_bounds__(1024) k_dense_inverse(MatView A, int n, float 
         // row k: a_kj / p, with a_kk := 1 / p
         for (int j = threadIdx.x; j < n; j += blockDim.x) M[k * n + j] = (j == k ? 1.0 : M[k * n + j]) * pinv;
         __syncthreads();
-        // rows i != k: a_ij -= f_i a_kj, with a_ik := -f_i / p
-        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-            const int i = idx / n, j = idx - i * n;
-            if (i == k) continue;
-            const double base = j == k ? 0.0 : M[idx];
-            M[idx] = base - fac[i] * M[k * n + j];
+        // rows i != k: a_ij -= f_i a_kj, with a_ik := -f_i / p (32 x 32 threads: lanes take
+        // consecutive columns, warps rows; a_kj is loaded once per column, f_i is a broadcast)
+        for (int j = tx; j < n; j += 32) {
+            const double akj = M[k * n + j];
+            const bool jk = j == k;
+            for (int i = ty; i < n; i += 32) {
+                if (i == k) continue;
+                const double base = jk ? 0.0 : M[i * n + j];
+                M[i * n + j] = base - fac[i] * akj;
+            }
         }
         __syncthreads();
     }
@@ -652,12 +846,6 @@ __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const floa
 // warp g of a slice's group takes the slots g, g + G, g + 2G, ... of its 32 rows, eight loaded
 // together, and the G partial sums meet in shared memory in warp order (deterministic).  Blocks
 // hold 8 warps, i.e. 8 / G slices.  G = 1 is one thread per row (row_dot).
-template <int G> __device__ __forceinline__ void split_row(int64_t &i, int &g) {
-    const int64_t gw = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    i = (gw / G) * kS + (threadIdx.x & 31);
-    g = (int)(gw % G);
-}
-
 template <int G>
 __device__ __forceinline__ float split_part(const MatView &A, int64_t i, int g, const float *__restrict__ x) {
     if (G == 1) return row_dot(A, i, x);
@@ -965,8 +1153,27 @@ decltype(&k_residual<1>) residual_kernel(int g) {
 decltype(&k_coarse_dots<1>) coarse_dots_kernel(int g) {
     return g >= 8 ? k_coarse_dots<8> : g >= 4 ? k_coarse_dots<4> : g >= 2 ? k_coarse_dots<2> : k_coarse_dots<1>;
 }
-// blocks of 8 warps covering the level's slices with G warps each (n is a multiple of 32)
-unsigned row_blocks(const AmgLevel &L) { return nblk(L.A.n / kS * L.g, 8); }
+decltype(&k_level_diag<1>) level_diag_kernel(int g) {
+    return g >= 8 ? k_level_diag<8> : g >= 4 ? k_level_diag<4> : g >= 2 ? k_level_diag<2> : k_level_diag<1>;
+}
+decltype(&k_pair_want<1>) pair_want_kernel(int g) {
+    return g >= 8 ? k_pair_want<8> : g >= 4 ? k_pair_want<4> : g >= 2 ? k_pair_want<2> : k_pair_want<1>;
+}
+// blocks of 8 warps covering n rows (a multiple of 32) with G warps per slice
+unsigned split_blocks(int64_t n, int g) { return nblk(n / kS * g, 8); }
+unsigned row_blocks(const AmgLevel &L) { return split_blocks(L.A.n, L.g); }
+// warps per slice for a matrix: the fewest with at most `width` slots per warp and row (one on
+// the fine level, whose 7-8 entries per row are loaded together by each thread)
+int split_of(const AmgMatrix &A, int forced, int width) {
+    if (!A.rlen) return 1;
+    int g = 1;
+    if (forced > 0) g = forced;
+    else {
+        const double w = A.n > 0 ? (double)A.slots / (double)A.n : 0.0;
+        while (g < 8 && w > (double)width * g) g *= 2;
+    }
+    return g >= 8 ? 8 : g >= 4 ? 4 : g >= 2 ? 2 : 1;
+}
 
 }  // namespace
 
@@ -1099,7 +1306,8 @@ cudaError_t Amg::level_stats(AmgLevel &L, unsigned int *bound, cudaStream_t s) {
     const int64_t n = L.A.n;
     AMG_CK(L.inv_diag.ensure(n));
     AMG_CK(isd_.ensure(n));
-    k_level_diag<<<nblk(n, 256), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound);
+    const int g = split_of(L.A, opt_.split, opt_.split_width);
+    level_diag_kernel(g)<<<split_blocks(n, g), 256, 0, s>>>(view(L.A), L.inv_diag.p, isd_.p, bound);
     if (L.A.long_count)
         k_level_diag_long<<<148, 256, 0, s>>>(view(L.A), L.A.long_count, L.inv_diag.p, isd_.p, bound);
     AMG_CK(cudaGetLastError());
@@ -1118,9 +1326,11 @@ cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *
     AMG_CK(pscan_.ensure(n + 1));
     AMG_CK(agg.ensure(n));
     const unsigned g = nblk(n, 256);
+    const int gw = split_of(A, opt_.split, opt_.split_width);
     k_pair_init<<<g, 256, 0, s>>>(V, row_edge, isd, mate_.p);
     for (int r = 0; r < opt_.pair_rounds; ++r) {
-        k_pair_want<<<g, 256, 0, s>>>(V, isd, mate_.p, want_.p, row_edge ? 0 : opt_.mix_coarse);
+        pair_want_kernel(gw)<<<split_blocks(n, gw), 256, 0, s>>>(V, isd, mate_.p, want_.p,
+                                                                  row_edge ? 0 : opt_.mix_coarse);
         k_pair_match<<<g, 256, 0, s>>>(n, want_.p, mate_.p);
     }
     k_pair_pack<<<g, 256, 0, s>>>(n, mate_.p, packed_.p);
@@ -1293,7 +1503,8 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             AMG_CK(mid_invd_.ensure(M.n));
             // (the intermediate matrix's bound is not needed: its own slot past the levels')
             unsigned int *mb = bounds_.p + o.max_levels;
-            k_level_diag<<<nblk(M.n, 256), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, mb);
+            const int gm = split_of(M, opt_.split, opt_.split_width);
+            level_diag_kernel(gm)<<<split_blocks(M.n, gm), 256, 0, s>>>(view(M), mid_invd_.p, isd_.p, mb);
             if (M.long_count)
                 k_level_diag_long<<<148, 256, 0, s>>>(view(M), M.long_count, mid_invd_.p, isd_.p, mb);
             AMG_CK(cudaGetLastError());
@@ -1352,13 +1563,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             lv_[l].A.n_long = nlong[l];
             // warps per slice in the row kernels: at most split_width slots per warp and row
             // (the fine level, 7-8 entries per row, keeps one thread per row)
-            AmgLevel &L = lv_[l];
-            const double width = L.A.n > 0 ? (double)L.A.slots / (double)L.A.n : 0.0;
-            int g = 1;
-            if (l > 0 && opt_.split > 0) g = opt_.split;
-            else if (l > 0)
-                while (g < 8 && width > opt_.split_width * g) g *= 2;
-            L.g = g >= 8 ? 8 : g >= 4 ? 4 : g >= 2 ? 2 : 1;  // the kernels' G
+            lv_[l].g = split_of(lv_[l].A, opt_.split, opt_.split_width);
         }
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];
