@@ -132,6 +132,38 @@ template <typename T> __global__ void k_scan_add(T *out, const T *bsum, int64_t 
     if (i == 0) out[n] = bsum[nb];
 }
 
+// the whole scan in one block (small n: one launch instead of three)
+constexpr int64_t kScanOneMax = 8192;
+template <typename T> __global__ void __launch_bounds__(1024) k_scan_one(const T *in, T *out, int64_t n) {
+    __shared__ T ws[32];
+    T carry = 0;
+    for (int64_t base = 0; base < n; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        const T v = i < n ? in[i] : T(0);
+        T tot;
+        const T incl = block_incl_scan<T>(v, ws, tot);
+        if (i < n) out[i] = carry + incl - v;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+// exclusive scan of in[0, n) into out[0, n], out[n] = total, stream-ordered
+template <typename T> cudaError_t launch_scan(const T *in, T *out, int64_t n, DBuf<T> &blk, cudaStream_t s) {
+    if (n <= 0) return cudaMemsetAsync(out, 0, sizeof(T), s);
+    if (n <= kScanOneMax) {
+        k_scan_one<T><<<1, 1024, 0, s>>>(in, out, n);
+        return cudaGetLastError();
+    }
+    const int64_t nb = (n + 1023) / 1024;
+    cudaError_t e = blk.ensure(nb + 1);
+    if (e != cudaSuccess) return e;
+    k_scan_block<T><<<(unsigned)nb, 1024, 0, s>>>(in, out, blk.p, n);
+    k_scan_sums<T><<<1, 1024, 0, s>>>(blk.p, nb);
+    k_scan_add<T><<<(unsigned)nb, 1024, 0, s>>>(out, blk.p, n, nb);
+    return cudaGetLastError();
+}
+
 // Row kernels with G warps per 32-row slice (blocks of 8 warps): row i of warp g of its slice's
 // group; the warp takes the slots g, g + G, g + 2G, ... of the row.
 template <int G> __device__ __forceinline__ void split_row(int64_t &i, int &g) {
@@ -1241,44 +1273,17 @@ void Amg::release() {
 }
 
 cudaError_t Amg::scan_i32_dev(const int32_t *in, int32_t *out, int64_t n, cudaStream_t s) {
-    const int64_t nb = (n + 1023) / 1024;
-    AMG_CK(scan32_blk_.ensure(nb + 1));
-    if (n > 0) {
-        k_scan_block<int32_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan32_blk_.p, n);
-        k_scan_sums<int32_t><<<1, 1024, 0, s>>>(scan32_blk_.p, nb);
-        k_scan_add<int32_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan32_blk_.p, n, nb);
-        AMG_CK(cudaGetLastError());
-    } else {
-        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int32_t), s));
-    }
+    AMG_CK(launch_scan<int32_t>(in, out, n, scan32_blk_, s));
     return cudaSuccess;
 }
 
 cudaError_t Amg::scan_i64_dev(const int64_t *in, int64_t *out, int64_t n, cudaStream_t s) {
-    const int64_t nb = (n + 1023) / 1024;
-    AMG_CK(scan64_blk_.ensure(nb + 1));
-    if (n > 0) {
-        k_scan_block<int64_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan64_blk_.p, n);
-        k_scan_sums<int64_t><<<1, 1024, 0, s>>>(scan64_blk_.p, nb);
-        k_scan_add<int64_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan64_blk_.p, n, nb);
-        AMG_CK(cudaGetLastError());
-    } else {
-        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
-    }
+    AMG_CK(launch_scan<int64_t>(in, out, n, scan64_blk_, s));
     return cudaSuccess;
 }
 
 cudaError_t Amg::scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s) {
-    const int64_t nb = (n + 1023) / 1024;
-    AMG_CK(scan32_blk_.ensure(nb + 1));
-    if (n > 0) {
-        k_scan_block<int32_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan32_blk_.p, n);
-        k_scan_sums<int32_t><<<1, 1024, 0, s>>>(scan32_blk_.p, nb);
-        k_scan_add<int32_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan32_blk_.p, n, nb);
-        AMG_CK(cudaGetLastError());
-    } else {
-        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int32_t), s));
-    }
+    AMG_CK(launch_scan<int32_t>(in, out, n, scan32_blk_, s));
     int32_t t = 0;
     AMG_CK(cudaMemcpyAsync(&t, out + n, sizeof(t), cudaMemcpyDeviceToHost, s));
     AMG_CK(cudaStreamSynchronize(s));
@@ -1287,16 +1292,7 @@ cudaError_t Amg::scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &t
 }
 
 cudaError_t Amg::scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s) {
-    const int64_t nb = (n + 1023) / 1024;
-    AMG_CK(scan64_blk_.ensure(nb + 1));
-    if (n > 0) {
-        k_scan_block<int64_t><<<(unsigned)nb, 1024, 0, s>>>(in, out, scan64_blk_.p, n);
-        k_scan_sums<int64_t><<<1, 1024, 0, s>>>(scan64_blk_.p, nb);
-        k_scan_add<int64_t><<<(unsigned)nb, 1024, 0, s>>>(out, scan64_blk_.p, n, nb);
-        AMG_CK(cudaGetLastError());
-    } else {
-        AMG_CK(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
-    }
+    AMG_CK(launch_scan<int64_t>(in, out, n, scan64_blk_, s));
     AMG_CK(cudaMemcpyAsync(&total, out + n, sizeof(total), cudaMemcpyDeviceToHost, s));
     AMG_CK(cudaStreamSynchronize(s));
     return cudaSuccess;
