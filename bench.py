@@ -131,20 +131,22 @@ class ClockSampler:
 
 # ------------------------------------------------------------- roofline -----------------
 AMG_DEGREE = 2  # Chebyshev smoothing degree of the AMG cycle (library default)
+# the cycle reads the fine matrix's values in FP16 unless MH_AMG_HALF=0 (library default 1)
+AMG_VALUE_BYTES = 4 if os.environ.get("MH_AMG_HALF", "1") == "0" else 2
 
 
 def algorithmic_bytes(kernel, N, Z):
     """Bytes each launch must move at minimum (every array once; no padding, no re-reads).
     spmv:    values + column indices of the Z nonzeros, p (gathered, counted once), r read, q written.
     update:  x, r, p read and written, q read.
-    smooth0: AMG Chebyshev step on the fine level (FP32, unit diagonal): values + indices, x (or
-             b) gathered, b read, x and d written; d read by the steps that continue a sequence
-             (the fused first pre-smoothing pass and the first post-smoothing step start one):
-             mean over the 2d-1 fine steps of one cycle."""
+    smooth0: AMG Chebyshev step on the fine level (unit diagonal): values (FP16 copy, or FP32)
+             + indices, x (or b) gathered, b read, x and d written; d read by the steps that
+             continue a sequence (the fused first pre-smoothing pass and the first post-smoothing
+             step start one): mean over the 2d-1 fine steps of one cycle."""
     if kernel == "smooth0":
         steps = 2 * AMG_DEGREE - 1
         reads_d = max(0, AMG_DEGREE - 2) + (AMG_DEGREE - 1)
-        return Z * 8 + 16 * N + 4 * N * reads_d / steps
+        return Z * (4 + AMG_VALUE_BYTES) + 16 * N + 4 * N * reads_d / steps
     s = 8 if kernel.endswith("64") else 4
     if kernel.startswith("spmv"):
         return Z * (s + 4) + 3 * s * N
@@ -178,8 +180,9 @@ def roofline(stats_list, N, Z, peaks):
         peak, peak_note = 6650.0, "fallback"
     traffic = None
     tj = load_json(os.path.join(ROOT, "profiles", "traffic.json"))
-    if tj and names[k] in tj.get("bytes_per_unit", {}):
-        traffic = tj["bytes_per_unit"][names[k]] * (N if tj.get("unit") == "row" else 1)
+    tkey = names[k] + ("_f16" if names[k] == "smooth0" and AMG_VALUE_BYTES == 2 else "")
+    if tj and tkey in tj.get("bytes_per_unit", {}):
+        traffic = tj["bytes_per_unit"][tkey] * (N if tj.get("unit") == "row" else 1)
     share = {names[i]: round(tot[i] / max(sum(tot[:nk]), 1e-30), 4) for i in range(nk) if cnt[i]}
     out = {"bound": "hbm", "kernel": KERNEL_NAMES[names[k]],
            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),

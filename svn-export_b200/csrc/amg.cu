@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cuda_fp16.h>
+
 #include "amg.hpp"
 
 namespace mh {
@@ -31,6 +33,7 @@ template struct DBuf<int64_t>;
 template struct DBuf<float>;
 template struct DBuf<double>;
 template struct DBuf<unsigned int>;
+template struct DBuf<uint16_t>;
 
 namespace {
 
@@ -50,8 +53,9 @@ struct MatView {
     const int32_t *col;
     const float *val;
     const int32_t *rlen;  // entries of each row (coarse matrices), null: the slice width
+    const __half *hval;   // FP16 copy of val read by the cycle's fine-level kernels, or null
 };
-MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val, A.rlen}; }
+MatView view(const AmgMatrix &A) { return {A.n, A.slice_off, A.col, A.val, A.rlen, nullptr}; }
 
 // Rows longer than this (hub aggregates: a fracture intersection or a channel that couples to
 // every aggregate along it) are skipped by the thread-per-row kernels and handled by a block
@@ -838,6 +842,32 @@ __global__ void k_dense_gemv(Gate gate, const float *__restrict__ inv, int64_t n
 // (A x)_i.  On the fine level (no row lengths: 7-8 entries per row) the first 8 slots are
 // loaded together, then gathered together, so each thread keeps 8 independent loads in flight
 // instead of one dependent load chain per slot; coarse rows (longer, irregular) loop.
+// the fine level's row: slots loaded 8 at a time, values from FP32 or their FP16 copy
+template <bool HALF>
+__device__ __forceinline__ float fine_dot(const MatView &A, int64_t base, int w, int ln, const float *__restrict__ x) {
+    auto value = [&](int64_t slot) { return HALF ? __half2float(A.hval[slot]) : __ldg(A.val + slot); };
+    constexpr int kB = 8;
+    int32_t c[kB];
+    float v[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const int64_t slot = base + (int64_t)k * kS + ln;
+        c[k] = k < w ? __ldg(A.col + slot) : 0;
+        v[k] = k < w ? value(slot) : 0.f;
+    }
+    float g[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) g[k] = k < w ? x[c[k]] : 0.f;
+    float y = 0.f;
+#pragma unroll
+    for (int k = 0; k < kB; ++k) y += v[k] * g[k];
+    for (int j = kB; j < w; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        y += value(slot) * x[__ldg(A.col + slot)];
+    }
+    return y;
+}
+
 __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const float *__restrict__ x) {
     int64_t base;
     int w, ln;
@@ -850,26 +880,7 @@ __device__ __forceinline__ float row_dot(const MatView &A, int64_t i, const floa
         }
         return y;
     }
-    constexpr int kB = 8;
-    int32_t c[kB];
-    float v[kB];
-#pragma unroll
-    for (int k = 0; k < kB; ++k) {
-        const int64_t slot = base + (int64_t)k * kS + ln;
-        c[k] = k < w ? __ldg(A.col + slot) : 0;
-        v[k] = k < w ? __ldg(A.val + slot) : 0.f;
-    }
-    float g[kB];
-#pragma unroll
-    for (int k = 0; k < kB; ++k) g[k] = k < w ? x[c[k]] : 0.f;
-    float y = 0.f;
-#pragma unroll
-    for (int k = 0; k < kB; ++k) y += v[k] * g[k];
-    for (int j = kB; j < w; ++j) {
-        const int64_t slot = base + (int64_t)j * kS + ln;
-        y += __ldg(A.val + slot) * x[__ldg(A.col + slot)];
-    }
-    return y;
+    return A.hval ? fine_dot<true>(A, base, w, ln, x) : fine_dot<false>(A, base, w, ln, x);
 }
 
 // Coarse rows are long (tens of entries), so one thread walking a row issues a long chain of
@@ -1030,6 +1041,11 @@ __global__ void k_restrict(Gate gate, int64_t nc, int64_t nc_pad, const int32_t 
     if (I < nc)
         for (int32_t k = ms[I]; k < ms[I + 1]; ++k) s += (wt ? wt[mr[k]] : 1.f) * r[mr[k]];
     bc[I] = s;
+}
+
+__global__ void k_to_half(int64_t n, const float *__restrict__ a, uint16_t *__restrict__ h) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) h[i] = __half_as_ushort(__float2half_rn(a[i]));
 }
 
 __global__ void k_to_float(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
@@ -1264,6 +1280,7 @@ void Amg::release() {
     alpha_.release();
     tickets_.release();
     w0_.release();
+    fine_half_.release();
     w0_used_ = nullptr;
     isd_.release();
     dense_inv_.release();
@@ -1459,6 +1476,14 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     L0.A.longrows = nullptr;
     L0.A.n_long = 0;
     L0.A.long_count = nullptr;
+    // the cycle's fine-level kernels read the values in FP16 (unit diagonal, off-diagonals of
+    // magnitude <= 1: relative rounding 5e-4, the same for a_ij and a_ji, so the cycle stays
+    // symmetric); the setup and the Krylov products use the FP32 values
+    if (opt_.half_fine) {
+        AMG_CK(fine_half_.ensure(std::max<int64_t>(sys.n_slots, 1)));
+        k_to_half<<<nblk(sys.n_slots, 256), 256, 0, s>>>(sys.n_slots, sys.val32, fine_half_.p);
+        AMG_CK(cudaGetLastError());
+    }
     // level-0 weights: the near-null vector of the scaled system S^ = D^-1/2 S D^-1/2 is
     // D^1/2 1 (constants are near-null for S), so the level-0 transfers carry sqrt(diag S)
     AMG_CK(w0_.ensure(sys.n_rows));
@@ -1654,7 +1679,8 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
         const float *invd = l == 0 ? nullptr : L.inv_diag.p;  // the scaled fine level has unit diagonal
-        const MatView A = view(L.A);
+        MatView A = view(L.A);
+        if (l == 0 && opt_.half_fine) A.hval = reinterpret_cast<const __half *>(fine_half_.p);
         const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
         const auto sm_step = sm_step_kernel(L.g);
         cheb_coeffs(L, c1, c2);
@@ -1724,7 +1750,8 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
         const float *invd = l == 0 ? nullptr : L.inv_diag.p;
-        const MatView A = view(L.A);
+        MatView A = view(L.A);
+        if (l == 0 && opt_.half_fine) A.hval = reinterpret_cast<const __half *>(fine_half_.p);
         const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
         const auto sm_step = sm_step_kernel(L.g);
         cheb_coeffs(L, c1, c2);

@@ -43,6 +43,7 @@ struct AmgOptions {
     int mix_coarse = 1;     // coarse levels may pair along positive couplings (weakly preferred)
     int split = 0;          // warps per slice in the coarse row kernels (1, 2, 4, 8; 0: by row width)
     int split_width = 12;   // ... by row width: the fewest warps with at most this many slots each
+    int half_fine = 1;      // 1: the cycle reads the fine matrix's values in FP16 (a copy made at setup)
 };
 
 template <class T> struct DBuf {
@@ -105,6 +106,7 @@ public:
     int64_t coarse_rows() const { return n_levels_ ? lv_[n_levels_ - 1].A.n : 0; }
     int kernels_per_apply() const;
     const float *fine_weights() const { return w0_used_; }  // null when the transfers are unweighted
+    bool half_fine() const { return opt_.half_fine != 0; }
     std::string err;
 
 private:
@@ -155,6 +157,7 @@ private:
     DBuf<unsigned int> tickets_;    // last-block tickets of the scaling reductions, per level
     std::vector<int64_t> dots_off_;
     DBuf<float> w0_;                // sqrt(diag S) per fine row
+    DBuf<uint16_t> fine_half_;      // FP16 bits of the fine matrix's values (half_fine)
     const float *w0_used_ = nullptr;
     int64_t dense_n_ = 0;
     int32_t *h_flag_ = nullptr;

@@ -868,6 +868,7 @@ mh::AmgOptions amg_options() {
     env_i("MH_AMG_MIX", o.mix_coarse, 0, 1);
     env_i("MH_AMG_SPLIT", o.split, 0, 8);
     env_i("MH_AMG_SPLITW", o.split_width, 2, 64);
+    env_i("MH_AMG_HALF", o.half_fine, 0, 1);
     if (const char *e = getenv("MH_AMG_RATIO")) {
         const float x = (float)atof(e);
         if (x >= 1.5f && x <= 100.f) o.cheb_ratio = x;
