@@ -91,6 +91,30 @@ def test_amg_solve_matches_direct(gpu, n, seed):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cfg,n", [(1, 12), (5, 24)])
+def test_amg_fp16_fine_values(gpu, monkeypatch, cfg, n):
+    """The cycle's FP16 copy of the fine values (the default) changes the preconditioner only:
+    both variants reach the tolerance on the FP64 residual, agree with each other, and need
+    about the same number of iterations."""
+    out = {}
+    for half in ("1", "0"):
+        monkeypatch.setenv("MH_AMG_HALF", half)
+        with assembled(n, cfg=cfg) as s:
+            st = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+            assert st["status"] == 0 and st["fell_back"] == 0, (half, st)
+            lam, S, rhs = check_solution(s, st, 1e-10)
+            out[half] = (lam, st["iterations"])
+            if half == "0":
+                lam_direct = spla.spsolve(S.tocsc(), rhs)
+                s.solve(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10)
+                err64 = np.abs(s.solution()[s.n_sides + s.n_elements:] - lam_direct).max()
+    (l1, it1), (l0, it0) = out["1"], out["0"]
+    for lam in (l1, l0):
+        assert np.abs(lam - lam_direct).max() <= max(20 * err64, 1e-12)
+    assert it1 <= it0 + max(2, it0 // 10), (it1, it0)
+
+
+@pytest.mark.gpu
 def test_amg_batch(gpu):
     parts = [make_case(3, seed=300 + i, n=n, corr_len=0.15) for i, n in enumerate((4, 8, 6))]
     with mhdarcy.MHSystem.batch([m for m, _ in parts]) as b:
