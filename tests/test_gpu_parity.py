@@ -20,7 +20,7 @@ import mhdarcy
 import oracle as O
 from helpers import cube_bc, fixture_bc, fixture_coeffs, load_fixture, oracle_problem
 from mhdarcy import _lib
-from mhdarcy.cases import make_case
+from mhdarcy.cases import dirichlet_x_bc, make_case
 
 pytestmark = pytest.mark.gpu
 
@@ -173,6 +173,32 @@ def test_tight_tolerance_matches_direct(gpu):
         assert st["status"] == 0
         sol = s.solution()
         assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cfg", [5, 2])
+def test_amg_fluxes_within_1e_8(gpu, cfg):
+    """The accuracy target of the mixed-precision multigrid solve: at r_tol 1e-12 the side
+    fluxes and element pressures are within 1e-8 (relative to the largest one) of the oracle's
+    FP64 direct solution, on fractured cases with channels (cfg5 style: six planes, four
+    channels, log10 K ~ N(-7, 2))."""
+    mesh, coeffs = make_case(cfg, n=12)
+    s = mhdarcy.MHSystem(mesh)
+    try:
+        bc, _ = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        ref, _, _ = O.solve_schur_direct(P)
+        st = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-12)
+        assert st["status"] == 0 and st["fell_back"] == 0, st
+        sol = s.solution()
+        ns, ne = s.n_sides, s.n_elements
+        flux_err = np.abs(sol[:ns] - ref[:ns]).max() / np.abs(ref[:ns]).max()
+        p_err = np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max() / np.abs(ref[ns:ns + ne]).max()
+        assert flux_err <= 1e-8 and p_err <= 1e-8, (flux_err, p_err, st["iterations"])
+    finally:
+        s.close()
 
 
 def test_unsteady_mh_matches_reference(gpu):
