@@ -64,6 +64,12 @@ def parse():
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--instances", type=int, default=256, help="batch size of --config 3")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="flux and pressure errors of AMG and FP64 PCG solves at r_tol 1e-10 and 1e-12 against "
+                         "an AMG solve driven to r_tol 1e-14 (full-size systems have no direct solve)")
+    ap.add_argument("--unsteady", type=int, default=0, metavar="K",
+                    help="time K implicit Euler steps (dt 0.01, time-varying boundary pressure) instead of "
+                         "steady solves; reports steps/s")
     return ap.parse_args()
 
 
@@ -192,6 +198,104 @@ def roofline(stats_list, N, Z, peaks):
         out["vcycle_avg_us"] = round(tot[5] / cnt[5] * 1e3, 2)
         out["smooth0_share_of_vcycle"] = round(tot[4] / tot[5], 4) if tot[5] > 0 else None
     return out
+
+
+# ---------------------------------------------------------------- unsteady --------------
+def run_unsteady(a, rank, world):
+    """K steps of the unsteady MH system (mh_unsteady_step: right-hand side from the previous
+    pressures, solve, back-substitution) with the boundary pressure on x = 0 following
+    1 + 0.5 sin(2 pi t); each method starts from zero pressure.  The matrix is the same in every
+    step (same dt), so the multigrid hierarchy is built once and reused."""
+    import numpy as np
+    import torch
+
+    import mhdarcy
+    from mhdarcy.cases import dirichlet_x_bc, make_case
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    stream = torch.cuda.Stream()
+    mesh, coeffs = make_case(a.config)
+    dt = 0.01
+    out = {}
+    with mhdarcy.MHSystem(mesh) as s:
+        s.set_stream(stream.cuda_stream)
+        bc, left = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32, "amg": mhdarcy.MH_SOLVER_AMG}
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for name in a.methods.split(","):
+            kw = {"inner_rtol": a.amg_inner_rtol} if name == "amg" else {}
+
+            def steps(k):
+                s.set_bc(bc["bc_type"], bc["pressure"])
+                s.unsteady_init(dt, init_pressure=np.zeros(s.n_elements), lumped=False)
+                p = bc["pressure"].copy()
+                its = []
+                for i in range(1, k + 1):
+                    p[left] = 1.0 + 0.5 * np.sin(2 * np.pi * i * dt)
+                    s.set_bc(bc["bc_type"], p)
+                    st = s.unsteady_step(dt, method=methods[name], r_tol=1e-10, **kw)
+                    if st["status"] not in (0, mhdarcy.MH_FELL_BACK):
+                        raise RuntimeError(f"{name} step {i}: {st}")
+                    its.append(st["iterations"])
+                return its
+
+            steps(max(3, a.warmup))
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+            its = steps(a.unsteady)
+            with torch.cuda.stream(stream):
+                ev1.record(stream)
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            out[name] = {"steps_per_s": round(a.unsteady / (ms / 1e3), 3), "ms_per_step": round(ms / a.unsteady, 3),
+                         "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its))}
+    best = max(out, key=lambda m: out[m]["steps_per_s"])
+    line = {"metric": "MH Darcy unsteady steps/s (implicit Euler, residual 1e-10)", "value": out[best]["steps_per_s"],
+            "unit": "steps/s", "n_gpus": 1, "steps": a.unsteady, "warmup": max(3, a.warmup),
+            "ms_per_step": out[best]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if best == "pcg64" else "f32+f64",
+            "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
+            "config": {"workload": "cfg%d: %s, dt %g, %d steps" % (a.config, WORKLOADS[a.config], dt, a.unsteady),
+                       "method": best},
+            "methods": out}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- accuracy --------------
+def run_accuracy(a):
+    """Side fluxes and element pressures of solves at r_tol 1e-10 and 1e-12 against a solve to
+    r_tol 1e-14 (both FP64 residual norms), relative to the largest reference value."""
+    import numpy as np
+    import torch
+
+    import mhdarcy
+    from mhdarcy.cases import dirichlet_x_bc, make_case
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    mesh, coeffs = make_case(a.config)
+    rows = []
+    with mhdarcy.MHSystem(mesh) as s:
+        bc, _ = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        amg = {"method": mhdarcy.MH_SOLVER_AMG, "inner_rtol": a.amg_inner_rtol}
+        st = s.solve(r_tol=1e-14, max_it=20000, **amg)
+        ref = s.solution()
+        ns, ne = s.n_sides, s.n_elements
+        rows.append({"method": "amg", "r_tol": 1e-14, "status": st["status"], "iterations": st["iterations"],
+                     "rel_residual": st["rel_residual"], "rel_residual_unscaled": st["rel_residual_unscaled"]})
+        for name, kw in (("amg", amg), ("pcg64", {"method": mhdarcy.MH_SOLVER_PCG64})):
+            for rt in (1e-10, 1e-12):
+                st = s.solve(r_tol=rt, max_it=50000, **kw)
+                sol = s.solution()
+                rows.append({"method": name, "r_tol": rt, "status": st["status"], "iterations": st["iterations"],
+                             "flux_err": float(np.abs(sol[:ns] - ref[:ns]).max() / np.abs(ref[:ns]).max()),
+                             "pressure_err": float(np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max()
+                                                   / np.abs(ref[ns:ns + ne]).max())})
+    print(json.dumps({"config": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "accuracy": rows}), flush=True)
 
 
 # ---------------------------------------------------------------- ours ------------------
@@ -440,6 +544,14 @@ def main():
         out = run_reference(a)
         if out:
             print(json.dumps(out))
+        return
+    if a.accuracy:
+        if rank == 0:
+            run_accuracy(a)
+        return
+    if a.unsteady > 0:
+        if rank == 0:
+            run_unsteady(a, rank, world)
         return
     out, ctx = run_ours(a, rank, world)
     if rank == 0:
