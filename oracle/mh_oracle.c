@@ -14,6 +14,8 @@
  *   time terms      darcy_flow_mh.cc:1614-1675 (MH), :1695-1766 (LMH)
  *   Schur algebra   src/la/schur.cc:566-611, 690-694, 714-773; darcy_flow_mh.cc:1009-1131
  *   LMH postprocess darcy_flow_mh.cc:1772-1827
+ *   element vectors src/flow/darcy_flow_mh_output.cc:301-323 (make_element_vector) with
+ *                   mh_fe_values.cc:76-118 (RT0_value)
  *
  * Parity is pinned against the reference's own golden outputs: the per-element pressures,
  * fluxes and edge pressures of tests/01_steady_flow_123d/ref_output/flow_gmsh.con/raw_output.txt,
@@ -666,6 +668,71 @@ int orc_resolve(const orc_problem *P, double *sol) {
     free(start);
     free(list);
     return bad ? -2 : 0;
+}
+
+/* ------------------------------------------------------- element flux vectors --------- */
+/* Darcy flux vector at each element centre from its side fluxes (DarcyFlowMHOutput::
+ * make_element_vector, darcy_flow_mh_output.cc:301-323): u = sum_i q_i RT0_i(c) / delta_e,
+ * with the RT0 basis of MHFEValues::RT0_value (mh_fe_values.cc:76-118) and its parameters
+ * from the local-matrix routines: line :150-152, triangle :193-211 (bas_func_0_triangle
+ * :293-301), tetrahedron :379-396.  out holds 3 values per element. */
+static void rt0_at(const Elem *E, const double *x, int s, double *v) {
+    double d[3];
+    if (E->dim == 1) {
+        double lv[3], w[3];
+        sub3(E->X[1], E->X[0], lv);
+        const double ll = dot3(lv, lv);
+        sub3(x, E->X[s == 0 ? 1 : 0], w);
+        const double f = (s == 0 ? -norm3(w) : norm3(w)) / ll;
+        v[0] = f * lv[0]; v[1] = f * lv[1]; v[2] = f * lv[2];
+        return;
+    }
+    if (E->dim == 2) {
+        /* the plane frame of the local matrix: ex along AB, ey in the plane */
+        double ex[3], ac[3], ez[3], ey[3], l;
+        sub3(E->X[1], E->X[0], ex); l = norm3(ex); ex[0] /= l; ex[1] /= l; ex[2] /= l;
+        sub3(E->X[2], E->X[0], ac);
+        cross3(ex, ac, ez); l = norm3(ez); ez[0] /= l; ez[1] /= l; ez[2] /= l;
+        cross3(ez, ex, ey); l = norm3(ey); ey[0] /= l; ey[1] /= l; ey[2] /= l;
+        /* node coordinates in that frame; side s is centred on the node opposite it */
+        double nod[3][2];
+        for (int k = 0; k < 3; ++k) {
+            sub3(E->X[k], E->X[0], d);
+            nod[k][0] = k ? dot3(d, ex) : 0.0;
+            nod[k][1] = k ? dot3(d, ey) : 0.0;
+        }
+        const double *p0 = nod[s], *p1 = nod[(s + 1) % 3], *p2 = nod[(s + 2) % 3];
+        const double ga = 1.0 / fabs((p0[0] - p2[0]) * (p1[1] - p0[1]) + (p0[1] - p2[1]) * (p0[0] - p1[0]));
+        sub3(x, E->X[0], d);
+        const double a = dot3(d, ex) - p2[0], b = dot3(d, ey) - p2[1];
+        for (int c = 0; c < 3; ++c) v[c] = ga * (a * ex[c] + b * ey[c]);
+        return;
+    }
+    /* tetrahedron: delta_s (x - X_s), X_s the node opposite side s */
+    double n[3], c[3];
+    side_normal_tet(E, s, n);
+    side_centre(E, s, c);
+    const double dl = 1.0 / (side_measure(E, s) * (dot3(n, c) - dot3(n, E->X[s])));
+    sub3(x, E->X[s], d);
+    v[0] = dl * d[0]; v[1] = dl * d[1]; v[2] = dl * d[2];
+}
+
+int orc_element_flux(const orc_problem *P, const double *sol, double *out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < P->n_el; ++e) {
+        Elem E;
+        load_elem(P->xyz, P->el_nodes, P->el_dim, e, &E);
+        double c[3], u[3] = {0.0, 0.0, 0.0}, v[3];
+        elem_centre(&E, c);
+        const double cs = P->delta ? P->delta[e] : 1.0;
+        for (int s = 0; s < E.n; ++s) {
+            rt0_at(&E, c, s, v);
+            const double q = sol[P->el_side_start[e] + s];
+            for (int k = 0; k < 3; ++k) u[k] += q * v[k] / cs;
+        }
+        for (int k = 0; k < 3; ++k) out[3 * e + k] = u[k];
+    }
+    return 0;
 }
 
 /* ------------------------------------------------------------ Jacobi PCG -------------- */

@@ -40,6 +40,8 @@ def _load():
     L.orc_schur2_csr.argtypes = [C.c_void_p, i32p, i32p, f64p, f64p]
     L.orc_resolve.restype = C.c_int
     L.orc_resolve.argtypes = [C.c_void_p, f64p]
+    L.orc_element_flux.restype = C.c_int
+    L.orc_element_flux.argtypes = [C.c_void_p, f64p, f64p]
     L.orc_pcg_jacobi.restype = C.c_int
     L.orc_pcg_jacobi.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, f64p, C.c_double, C.c_int, f64p]
     L.orc_local_matrix.restype = C.c_int
@@ -174,6 +176,15 @@ def resolve(P, lam):
     if lib.orc_resolve(C.byref(s), _ptr(sol, C.c_double)):
         raise RuntimeError("singular local matrix")
     return sol
+
+
+def element_flux(P, sol):
+    """Darcy flux vector at every element centre from the side fluxes of an MH solution
+    (DarcyFlowMHOutput::make_element_vector, darcy_flow_mh_output.cc:301-323): [n_el, 3]."""
+    out = np.zeros((P.n_el, 3))
+    s = P.struct()
+    lib.orc_element_flux(C.byref(s), _ptr(np.ascontiguousarray(sol, np.float64), C.c_double), _ptr(out, C.c_double))
+    return out
 
 
 def solve_schur_direct(P):

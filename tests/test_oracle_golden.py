@@ -39,6 +39,17 @@ def test_t01_raw_output():
         np.testing.assert_array_less(np.abs(sf - z["ref_side_flux"][e, :n]), tol(z["ref_side_flux"][e, :n]))
 
 
+def test_t01_element_flux_vectors():
+    """Element-centre flux vectors (the raw_output's three flux columns) of every element of
+    t01: lines, triangles and tetrahedra, at the printing precision."""
+    z, mesh, topo, P = problem("t01")
+    u = O.element_flux(P, O.solve_mh_direct(P))
+    ref = z["ref_flux"]
+    assert u.shape == ref.shape
+    assert set(np.unique(z["el_dim"])) == {1, 2, 3}
+    assert np.all(np.abs(u - ref) <= 1e-8 + 5e-9 * np.abs(ref))
+
+
 def test_t01_schur_path_equals_direct():
     z, mesh, topo, P = problem("t01")
     full = O.solve_mh_direct(P)
