@@ -298,6 +298,40 @@ def run_accuracy(a):
     print(json.dumps({"config": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "accuracy": rows}), flush=True)
 
 
+# ---------------------------------------------------------------- post-processing -------
+def element_flux_timing(system, stream, sz, mesh, reps=20):
+    """The element-centre flux vectors of the last solution (mh_get_element_flux_device),
+    timed with CUDA events on the handle's stream: mean of `reps` launches after one warm-up.
+    Algorithmic bytes per launch: node coordinates once (24 per node), per element its node
+    ids, side fluxes, side offset, cross-section and list entry read and 24 bytes written."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from mhdarcy import _lib
+    ne = sz.n_elements
+    buf = torch.empty((ne, 3), dtype=torch.float64, device="cuda")
+    call = lambda: _lib.check(_lib.lib.mh_get_element_flux_device(system.h, C.c_void_p(buf.data_ptr()), buf.numel()),
+                              system.h)
+    call()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(reps):
+        call()
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    nsides = np.asarray(mesh.el_dim) + 1
+    algo = 24 * sz.n_nodes + int(np.sum(4 * nsides + 8 * nsides)) + ne * (4 + 8 + 4 + 24)
+    return {"kernel": "k_element_flux (make_element_vector)", "ms_per_call": round(ms, 4),
+            "algorithmic_bytes": algo, "achieved_gbs": round(algo / (ms / 1e3) / 1e9, 1),
+            "note": "per call: element kernels plus one stream synchronisation"}
+
+
 # ---------------------------------------------------------------- ours ------------------
 def run_ours(a, rank, world):
     import numpy as np
@@ -462,6 +496,7 @@ def run_ours(a, rank, world):
     }
     if "pcg64" in results:
         JACOBI_PCG_ITERS[a.config] = results["pcg64"]["iterations"]
+    out["postprocess"] = element_flux_timing(system, stream, sz, mesh)
     system.close()
     if dist:
         dist.barrier()

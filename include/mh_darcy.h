@@ -218,6 +218,13 @@ int mh_solve(mh_handle *h, const mh_solve_opts *opts, mh_solve_stats *stats);
 int mh_get_solution(const mh_handle *h, double *out, int64_t len);
 /* Same, into a device buffer (a plain device pointer). */
 int mh_get_solution_device(const mh_handle *h, double *dev_out, int64_t len);
+/* Darcy flux vector at every element centre from the side fluxes of the last solution,
+ * out[3 e + k] for k = x, y, z (length 3 n_elements): DarcyFlowMHOutput::make_element_vector
+ * (src/flow/darcy_flow_mh_output.cc:301-323), the three flux columns of the raw output.
+ * Computed on the device; MH_ERR_STATE before the first solve. */
+int mh_get_element_flux(const mh_handle *h, double *out, int64_t len);
+/* Same, written directly into a device buffer (a plain device pointer); nothing allocated. */
+int mh_get_element_flux_device(const mh_handle *h, double *dev_out, int64_t len);
 
 /* Export of the assembled edge system in CSR form (rows = edges), for checking.  The
  * values are the reference's schur2 matrix after scale(-1) (darcy_flow_mh.cc:1128-1130),

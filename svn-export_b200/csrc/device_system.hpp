@@ -102,6 +102,10 @@ cudaError_t launch_gather(const DevAssembly &a, const DevSystem &sys, int mode, 
 cudaError_t launch_scale(const DevSystem &sys, int matrix, cudaStream_t s);
 cudaError_t launch_backsub(const ElemData &d, const DevAssembly &a, const DevSystem &sys, double *sol,
                            int64_t n_sides, int64_t n_el, int64_t n_edges, cudaStream_t s);
+// Darcy flux vector at every element centre from the side fluxes in sol (postprocess.cu):
+// out[3 e + k], k = x, y, z.
+cudaError_t launch_element_flux(const ElemData &d, const DevAssembly &a, const double *sol, double *out,
+                                cudaStream_t s);
 
 // x = lambda * dsq (initial guess in scaled space; padding rows 0).
 cudaError_t launch_scale_in(const DevSystem &sys, const double *lambda, cudaStream_t s);

@@ -53,6 +53,7 @@ struct mh_handle {
     mh::DevSystem sys{};
     mh::DevAssembly as{};
     double *sol = nullptr, *sol_prev = nullptr;
+    double *d_elflux = nullptr;         // element flux vectors for mh_get_element_flux (3 n_el)
     double *d_aniso = nullptr;
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
     bool rhs_stale = false;             // boundary values changed since the last assembly
@@ -1567,6 +1568,42 @@ int mh_get_solution_device(const mh_handle *hc, double *dev_out, int64_t len) {
     const int64_t msize = h->topo.n_sides() + h->mesh.n_el + h->topo.n_edges();
     if (!dev_out || len < msize) return MH_ERR_INVALID;
     CK(cudaMemcpyAsync(dev_out, h->sol, msize * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+// make_element_vector (darcy_flow_mh_output.cc:301-323) on the device, into dev_out [3 n_el]
+static int element_flux_into(mh_handle *h, double *dev_out) {
+    if (!h->solved) {
+        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the element fluxes";
+        return MH_ERR_STATE;
+    }
+    CK(mh::launch_element_flux(h->ed, h->as, h->sol, dev_out, h->stream));
+    return MH_OK;
+}
+
+int mh_get_element_flux(const mh_handle *hc, double *out, int64_t len) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t n = 3 * h->mesh.n_el;
+    if (!out || len < n) return MH_ERR_INVALID;
+    if (!h->d_elflux) {
+        h->d_elflux = dalloc<double>(h, std::max<int64_t>(n, 1));
+        if (!h->d_elflux) return MH_ERR_NOMEM;
+    }
+    if ((rc = element_flux_into(h, h->d_elflux))) return rc;
+    CK(cudaMemcpyAsync(out, h->d_elflux, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_get_element_flux_device(const mh_handle *hc, double *dev_out, int64_t len) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!dev_out || len < 3 * h->mesh.n_el) return MH_ERR_INVALID;
+    if ((rc = element_flux_into(h, dev_out))) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return MH_OK;
 }

@@ -203,6 +203,13 @@ class MHSystem:
         check(lib.mh_get_solution(self.h, ptr(out, C.c_double), len(out)), self.h)
         return out
 
+    def element_flux(self):
+        """Darcy flux vector at every element centre [n_elements, 3] from the last solution's
+        side fluxes (DarcyFlowMHOutput::make_element_vector, darcy_flow_mh_output.cc:301-323)."""
+        out = np.zeros((self.n_elements, 3))
+        check(lib.mh_get_element_flux(self.h, ptr(out, C.c_double), out.size), self.h)
+        return out
+
     def schur_system(self):
         """The assembled edge system (reference schur2 after scale(-1)) as CSR + rhs."""
         s = self.sizes

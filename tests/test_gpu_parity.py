@@ -175,6 +175,45 @@ def test_tight_tolerance_matches_direct(gpu):
         assert np.abs(sol - ref).max() <= 1e-8 * np.abs(ref).max()
 
 
+def test_element_flux_vectors_t01(gpu):
+    """make_element_vector on the device for t01 (lines, triangles, tetrahedra): against the
+    oracle on the GPU's own solution (same side fluxes: 1e-12 of the largest vector), and
+    against the flux columns of the reference's raw output (printed %.8g)."""
+    z, mesh, coeffs, bc = fixture_case("t01")
+    with gpu_system(mesh, coeffs, bc) as s:
+        with pytest.raises(mhdarcy.MHError) as ei:  # no solution yet
+            s.element_flux()
+        assert ei.value.status == _lib.MH_ERR_STATE
+        s.solve(r_tol=1e-12)
+        sol = s.solution()
+        u = s.element_flux()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        ref = O.element_flux(P, sol)
+        assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
+        assert np.all(np.abs(u - z["ref_flux"]) <= 1e-8 + 5e-9 * np.abs(z["ref_flux"]))
+
+
+def test_element_flux_vectors_device_output(gpu):
+    """The device-pointer variant writes the same values, on a fractured cube with channels
+    and log-normal conductivity and cross-sections (all three element shapes)."""
+    torch = pytest.importorskip("torch")
+    mesh, coeffs = make_case(5, n=8)
+    with mhdarcy.MHSystem(mesh) as s:
+        bc, _ = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+        sol = s.solution()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        ref = O.element_flux(P, sol)
+        buf = torch.full((s.n_elements, 3), np.nan, dtype=torch.float64, device="cuda:0")
+        _lib.check(_lib.lib.mh_get_element_flux_device(s.h, buf.data_ptr(), buf.numel()), s.h)
+        u = buf.cpu().numpy()
+        assert np.abs(u - ref).max() <= 1e-12 * np.abs(ref).max()
+        assert np.array_equal(u, s.element_flux())
+
+
 @pytest.mark.parametrize("cfg", [5, 2])
 def test_amg_fluxes_within_1e_8(gpu, cfg):
     """The accuracy target of the mixed-precision multigrid solve: at r_tol 1e-12 the side
