@@ -4,18 +4,23 @@
 // fluxes q_s, at the centre c (the mean of the nodes):
 //     u_E = sum_s q_s RT0_s(c) / delta_E                          (delta_E: cross-section)
 // with the lowest-order Raviart-Thomas basis of MHFEValues::RT0_value
-// (src/flow/mh_fe_values.cc:76-118) and its parameters from the local-matrix routines:
-//   line         RT0_0 = -|c - X_1| v / |v|^2,  RT0_1 = |c - X_0| v / |v|^2,  v = X_1 - X_0
-//   triangle     RT0_s = g_s ((u.e_x - a_s) e_x + (u.e_y - b_s) e_y),  u = c - X_0, in the
-//                element's plane frame (e_x along X_1 - X_0); (a_s, b_s) the node opposite
-//                side s in that frame, g_s = 1 / (2 |E|) computed from the node coordinates
-//                as bas_func_0_triangle does (:293-301)
-//   tetrahedron  RT0_s = d_s (c - X_s),  X_s the node opposite side s,
-//                d_s = 1 / (|S_s| n_s.(c_s - X_s))  (basis_functions_tetrahedron, :379-396)
+// (src/flow/mh_fe_values.cc:76-118).  The reference evaluates the basis from its local-matrix
+// parameters (line :150-152, triangle :193-211 with bas_func_0_triangle :293-301, tetrahedron
+// :379-396); at the centre each of those equals
+//     RT0_s(c) = (c - X_opp(s)) / (dim |E|)
+// with X_opp(s) the node opposite side s (line: the other node; triangle: node (s+2) mod 3;
+// tetrahedron: node s): |S_s| times the height of X_s over side s is dim |E|, the triangle
+// formula is that vector written in the element's plane frame, and the line's is
+// -(|v|/2) v / |v|^2 = (c - X_1) / |v| for side 0.  So
+//     u_E = sum_s q_s (c - X_opp(s)) / (dim |E| delta_E),
+// one division per element instead of the reference's per-side normals, square roots and
+// divisions (which made the literal version FP64-divide bound: 172 us for 1.57M tetrahedra).
+// The oracle (oracle/mh_oracle.c, orc_element_flux) keeps the reference's literal formulas,
+// so the parity tests also check the identity.
 // One thread per element, per-dimension element lists (no divergence between shapes); the
 // output is [n_el][3], the three flux columns of the reference's raw output.
 // Bytes per element: DIM+1 node indices and their coordinates (gathered, mostly from L2),
-// DIM+1 side fluxes and the cross-section read, 24 bytes written.
+// DIM+1 side fluxes, the side offset, the cross-section and the list entry read, 24 written.
 #include <cuda_runtime.h>
 
 #include "device_system.hpp"
@@ -40,60 +45,28 @@ __global__ void __launch_bounds__(128) k_element_flux(ElemData d, const int32_t 
     V3 c = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int i = 0; i < N; ++i) c = {c.x + X[i].x, c.y + X[i].y, c.z + X[i].z};
-    c = v3div(c, (double)N);
-    const double cs = d.cross_section[e];
+    c = v3scale(c, 1.0 / N);
+    double dm;  // dim |E|
+    if constexpr (DIM == 1) {
+        dm = v3norm(v3sub(X[1], X[0]));
+    } else if constexpr (DIM == 2) {
+        dm = v3norm(v3cross(v3sub(X[1], X[0]), v3sub(X[2], X[0])));
+    } else {
+        dm = fabs(v3dot(v3cross(v3sub(X[1], X[0]), v3sub(X[2], X[0])), v3sub(X[3], X[0]))) / 2.0;
+    }
+    const double f = 1.0 / (dm * d.cross_section[e]);
     const int s0 = d.el_side_start[e];
     V3 u = {0.0, 0.0, 0.0};
-    auto add = [&](double q, V3 v) {  // u += q RT0_s(c) / delta, component by component
-        u.x += q * v.x / cs;
-        u.y += q * v.y / cs;
-        u.z += q * v.z / cs;
-    };
-    if constexpr (DIM == 1) {
-        const V3 v = v3sub(X[1], X[0]);
-        const double ll = v3dot(v, v);
-        add(sol[s0], v3scale(v, -v3norm(v3sub(c, X[1])) / ll));
-        add(sol[s0 + 1], v3scale(v, v3norm(v3sub(c, X[0])) / ll));
-    } else if constexpr (DIM == 2) {
-        V3 ex = v3sub(X[1], X[0]);
-        ex = v3div(ex, v3norm(ex));
-        V3 ez = v3cross(ex, v3sub(X[2], X[0]));
-        ez = v3div(ez, v3norm(ez));
-        V3 ey = v3cross(ez, ex);
-        ey = v3div(ey, v3norm(ey));
-        double px[3], py[3];  // node coordinates in the plane frame
-        px[0] = py[0] = 0.0;
 #pragma unroll
-        for (int k = 1; k < 3; ++k) {
-            const V3 dk = v3sub(X[k], X[0]);
-            px[k] = v3dot(dk, ex);
-            py[k] = v3dot(dk, ey);
-        }
-        const V3 w = v3sub(c, X[0]);
-        const double wx = v3dot(w, ex), wy = v3dot(w, ey);
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            const int i0 = s, i1 = (s + 1) % 3, i2 = (s + 2) % 3;
-            const double g = 1.0 / fabs((px[i0] - px[i2]) * (py[i1] - py[i0]) + (py[i0] - py[i2]) * (px[i0] - px[i1]));
-            const double a = wx - px[i2], b = wy - py[i2];
-            add(sol[s0 + s], {g * (a * ex.x + b * ey.x), g * (a * ex.y + b * ey.y), g * (a * ex.z + b * ey.z)});
-        }
-    } else {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const V3 a = X[dev_side_node(3, s, 0)], b = X[dev_side_node(3, s, 1)], q = X[dev_side_node(3, s, 2)];
-            const V3 cr = v3cross(v3sub(b, a), v3sub(q, a));
-            const double nr = v3norm(cr);
-            V3 nv = v3div(cr, nr);
-            if (v3dot(nv, v3sub(c, a)) > 0.0) nv = v3scale(nv, -1.0);  // outward
-            const V3 sc = {(a.x + b.x + q.x) / 3.0, (a.y + b.y + q.y) / 3.0, (a.z + b.z + q.z) / 3.0};
-            const double ds = 1.0 / (0.5 * nr * (v3dot(nv, sc) - v3dot(nv, X[s])));
-            add(sol[s0 + s], v3scale(v3sub(c, X[s]), ds));
-        }
+    for (int s = 0; s < N; ++s) {
+        const int opp = DIM == 1 ? 1 - s : DIM == 2 ? (s + 2) % 3 : s;
+        const double q = sol[s0 + s];
+        const V3 r = v3sub(c, X[opp]);
+        u = {u.x + q * r.x, u.y + q * r.y, u.z + q * r.z};
     }
-    out[3 * (int64_t)e] = u.x;
-    out[3 * (int64_t)e + 1] = u.y;
-    out[3 * (int64_t)e + 2] = u.z;
+    out[3 * (int64_t)e] = u.x * f;
+    out[3 * (int64_t)e + 1] = u.y * f;
+    out[3 * (int64_t)e + 2] = u.z * f;
 }
 
 }  // namespace
