@@ -225,6 +225,15 @@ int mh_get_solution_device(const mh_handle *h, double *dev_out, int64_t len);
 int mh_get_element_flux(const mh_handle *h, double *out, int64_t len);
 /* Same, written directly into a device buffer (a plain device pointer); nothing allocated. */
 int mh_get_element_flux_device(const mh_handle *h, double *dev_out, int64_t len);
+/* Writes (append = 0) or appends one "$FlowField" block of the flow field text output,
+ * DarcyFlowMHOutput::output_internal_flow_data (src/flow/darcy_flow_mh_output.cc:793-829):
+ * per element its id (el_id, or the element index when null), pressure, centre flux vector,
+ * number of sides, side pressures and side fluxes, printed "%.8g " as the reference does.
+ * Host arrays only (no device, no handle): solution as from mh_get_solution, el_flux as from
+ * mh_get_element_flux, el_side_start [n_el+1] and side_edge as from mh_get_topology. */
+int mh_raw_output_write(const char *path, int append, double time, int64_t n_el, const int32_t *el_id,
+                        const int32_t *el_side_start, const int32_t *side_edge, const double *solution,
+                        const double *el_flux);
 
 /* Export of the assembled edge system in CSR form (rows = edges), for checking.  The
  * values are the reference's schur2 matrix after scale(-1) (darcy_flow_mh.cc:1128-1130),

@@ -4,6 +4,6 @@ from ._lib import (MHError, device_available, lib, MH_BC_NONE, MH_BC_DIRICHLET, 
                    MH_SOLVER_FCG_LEARNED, MH_SOLVER_AMG, MH_OK, MH_NOT_CONVERGED, MH_FELL_BACK, LIB_PATH)
 from .mesh import Mesh, concat_meshes, cube_mesh, read_gmsh
 from .flow import (MHSystem, MH_DofHandler, DarcyFlowMH_Steady, DarcyFlowMH_Unsteady,
-                   DarcyFlowLMH_Unsteady, solve_opts)
+                   DarcyFlowLMH_Unsteady, solve_opts, write_raw_output)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -324,6 +324,23 @@ class MH_DofHandler:
         return self.sol[self.sys.n_sides + element]
 
 
+def write_raw_output(path, solution, el_flux, el_side_start, side_edge, el_id=None, time=float("inf"),
+                     append=False):
+    """One "$FlowField" block of the flow field text output (DarcyFlowMHOutput::
+    output_internal_flow_data, darcy_flow_mh_output.cc:793-829) from host arrays: the MH
+    solution, the element flux vectors [n_el, 3], and the topology's el_side_start and
+    side_edge; element ids default to the element indices.  The time defaults to inf, which is
+    what the reference prints for a steady solve; unsteady output passes the step's time."""
+    sol, ef = f64(solution), f64(el_flux)
+    ss, se, ids = i32(el_side_start), i32(side_edge), i32(el_id)
+    n_el = len(ss) - 1
+    if ef.size != 3 * n_el:
+        raise ValueError("el_flux needs 3 values per element")
+    check(lib.mh_raw_output_write(str(path).encode(), int(bool(append)), float(time), n_el, ptr(ids, C.c_int32),
+                                  ptr(ss, C.c_int32), ptr(se, C.c_int32), ptr(sol, C.c_double),
+                                  ptr(ef, C.c_double)))
+
+
 class DarcyFlowMH_Steady:
     """Steady MH Darcy flow with n_schurs = 2, solved on the GPU."""
 
