@@ -16,9 +16,12 @@
  *   LMH postprocess darcy_flow_mh.cc:1772-1827
  *   element vectors src/flow/darcy_flow_mh_output.cc:301-323 (make_element_vector) with
  *                   mh_fe_values.cc:76-118 (RT0_value)
+ *   node pressures  darcy_flow_mh_output.cc:424-546 (make_node_scalar_param)
+ *   water balance   darcy_flow_mh_output.cc:671-790 (water_balance)
  *
  * Parity is pinned against the reference's own golden outputs: the per-element pressures,
  * fluxes and edge pressures of tests/01_steady_flow_123d/ref_output/flow_gmsh.con/raw_output.txt,
+ * the node pressures and the water balance of the same run,
  * the element pressures of the VTK outputs of tests 05, 06 and 10, and the analytic answers of
  * tests 06 (p2 = -3, p1 = -2.5).  The FP64 direct solve of the full saddle-point system is
  * done with scipy in oracle.py.
@@ -731,6 +734,90 @@ int orc_element_flux(const orc_problem *P, const double *sol, double *out) {
             for (int k = 0; k < 3; ++k) u[k] += q * v[k] / cs;
         }
         for (int k = 0; k < 3; ++k) out[3 * e + k] = u[k];
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------ node pressures ---------- */
+/* Pressure at every node (DarcyFlowMHOutput::make_node_scalar_param, darcy_flow_mh_output.cc:
+ * 424-546): a distance-weighted mean of the pressures of the elements containing the node and
+ * of the sides (of every element) containing it, with weights (1 - d / D) / (n - 1), d the
+ * distance from the node to the element or side centre, D the sum of those distances over
+ * the node's elements and sides, n their number.  Two passes in element order, as there. */
+static double dist3(const double *a, const double *b) {
+    double d[3];
+    sub3(a, b, d);
+    return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+}
+
+int orc_node_pressure(const orc_problem *P, const double *sol, double *out) {
+    const int64_t nn = P->n_nodes, ns = n_sides_of(P);
+    int32_t *cnt = (int32_t *)calloc(nn, sizeof(int32_t));
+    double *sd = (double *)calloc(nn, sizeof(double));
+    for (int64_t i = 0; i < nn; ++i) out[i] = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+        /* elements */
+        for (int64_t e = 0; e < P->n_el; ++e) {
+            Elem E;
+            load_elem(P->xyz, P->el_nodes, P->el_dim, e, &E);
+            double c[3];
+            elem_centre(&E, c);
+            for (int k = 0; k < E.n; ++k) {
+                const int32_t nd = P->el_nodes[4 * e + k];
+                const double d = dist3(E.X[k], c);
+                if (pass == 0) { sd[nd] += d; cnt[nd]++; }
+                else out[nd] += sol[ns + e] * (1.0 - d / sd[nd]) / (cnt[nd] - 1);
+            }
+        }
+        /* sides of every element (a line's sides are its nodes: distance 0) */
+        for (int64_t e = 0; e < P->n_el; ++e) {
+            Elem E;
+            load_elem(P->xyz, P->el_nodes, P->el_dim, e, &E);
+            for (int s = 0; s < E.n; ++s) {
+                double c[3];
+                side_centre(&E, s, c);
+                const int64_t side = P->el_side_start[e] + s;
+                const double p = sol[ns + P->n_el + P->side_edge[side]];
+                for (int k = 0; k < E.dim; ++k) {
+                    const int ln = side_node(E.dim, s, k);
+                    const int32_t nd = P->el_nodes[4 * e + ln];
+                    const double d = dist3(E.X[ln], c);
+                    if (pass == 0) { sd[nd] += d; cnt[nd]++; }
+                    else out[nd] += p * (1.0 - d / sd[nd]) / (cnt[nd] - 1);
+                }
+            }
+        }
+    }
+    free(cnt);
+    free(sd);
+    return 0;
+}
+
+/* ------------------------------------------------------------ water balance ----------- */
+/* DarcyFlowMHOutput::water_balance (darcy_flow_mh_output.cc:671-790): for each boundary region
+ * the sum of the side fluxes of its boundary objects (outward positive), of the positive ones
+ * and of the negative ones; for each bulk region the sum of |E| delta_E f_E.  bdr_region[b]
+ * (for each boundary object b, in topology order) and el_region[e] are region indices;
+ * out_bdr[3 r + {0,1,2}] = total, outflow, inflow; out_src[r]. */
+int orc_water_balance(const orc_problem *P, const double *sol, const int32_t *bdr_region, int32_t n_bdr_regions,
+                      const int32_t *el_region, int32_t n_el_regions, double *out_bdr, double *out_src) {
+    const int64_t ns = n_sides_of(P);
+    for (int32_t r = 0; r < 3 * n_bdr_regions; ++r) out_bdr[r] = 0.0;
+    for (int32_t r = 0; r < n_el_regions; ++r) out_src[r] = 0.0;
+    for (int64_t s = 0; s < ns; ++s) {
+        const int32_t b = P->side_bdr[s];
+        if (b < 0) continue;
+        const int32_t r = bdr_region[b];
+        const double q = sol[s];
+        out_bdr[3 * r] += q;
+        if (q > 0) out_bdr[3 * r + 1] += q;
+        else out_bdr[3 * r + 2] += q;
+    }
+    for (int64_t e = 0; e < P->n_el; ++e) {
+        Elem E;
+        load_elem(P->xyz, P->el_nodes, P->el_dim, e, &E);
+        const double delta = P->delta ? P->delta[e] : 1.0, f = P->source ? P->source[e] : 0.0;
+        out_src[el_region[e]] += elem_measure(&E) * delta * f;
     }
     return 0;
 }

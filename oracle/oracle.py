@@ -42,6 +42,10 @@ def _load():
     L.orc_resolve.argtypes = [C.c_void_p, f64p]
     L.orc_element_flux.restype = C.c_int
     L.orc_element_flux.argtypes = [C.c_void_p, f64p, f64p]
+    L.orc_node_pressure.restype = C.c_int
+    L.orc_node_pressure.argtypes = [C.c_void_p, f64p, f64p]
+    L.orc_water_balance.restype = C.c_int
+    L.orc_water_balance.argtypes = [C.c_void_p, f64p, i32p, C.c_int32, i32p, C.c_int32, f64p, f64p]
     L.orc_pcg_jacobi.restype = C.c_int
     L.orc_pcg_jacobi.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, f64p, C.c_double, C.c_int, f64p]
     L.orc_local_matrix.restype = C.c_int
@@ -185,6 +189,29 @@ def element_flux(P, sol):
     s = P.struct()
     lib.orc_element_flux(C.byref(s), _ptr(np.ascontiguousarray(sol, np.float64), C.c_double), _ptr(out, C.c_double))
     return out
+
+
+def node_pressure(P, sol):
+    """Pressure at every node, DarcyFlowMHOutput::make_node_scalar_param
+    (darcy_flow_mh_output.cc:424-546): [n_nodes]."""
+    out = np.zeros(len(P.keep["xyz"]))
+    s = P.struct()
+    lib.orc_node_pressure(C.byref(s), _ptr(np.ascontiguousarray(sol, np.float64), C.c_double), _ptr(out, C.c_double))
+    return out
+
+
+def water_balance(P, sol, bdr_region, el_region):
+    """DarcyFlowMHOutput::water_balance (darcy_flow_mh_output.cc:671-790) for region indices
+    bdr_region [n_bdr] and el_region [n_el]: ([n_bdr_regions, 3] total, outflow, inflow;
+    [n_el_regions] sources)."""
+    br = np.ascontiguousarray(bdr_region, np.int32)
+    er = np.ascontiguousarray(el_region, np.int32)
+    nb, ne = int(br.max()) + 1 if br.size else 0, int(er.max()) + 1 if er.size else 0
+    ob, os_ = np.zeros((nb, 3)), np.zeros(ne)
+    s = P.struct()
+    lib.orc_water_balance(C.byref(s), _ptr(np.ascontiguousarray(sol, np.float64), C.c_double), _ptr(br, C.c_int32),
+                          nb, _ptr(er, C.c_int32), ne, _ptr(ob, C.c_double), _ptr(os_, C.c_double))
+    return ob, os_
 
 
 def solve_schur_direct(P):

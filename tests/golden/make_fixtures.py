@@ -9,6 +9,8 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
 (0,0,-1).x as FieldAddPotential does), and the reference's own results:
   * t01            tests/01_steady_flow_123d (flow_gmsh.con): ref_output raw_output.txt, i.e.
                    per element pressure, barycentric flux, side (edge) pressures, side fluxes;
+                   the node pressures of the output mesh ($NodeData "pressure_nodes_[L]"); the
+                   boundary and source tables of water_balance.out;
   * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output;
   * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
   * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5.
@@ -102,6 +104,47 @@ def raw_output(path):
                 ref_n_sides=np.array(ns, np.int32), ref_side_pressure=sp, ref_side_flux=sf)
 
 
+def gmsh_node_data(path, name, mesh_path):
+    """Values of the $NodeData block `name` of an output mesh, ordered as the nodes of the
+    input mesh (matched by node id)."""
+    txt = open(path).read().split("\n")
+    k = next(i for i, l in enumerate(txt) if l.strip() == "$NodeData" and txt[i + 2].strip().strip('"') == name)
+    n_str = int(txt[k + 1])
+    n_real = int(txt[k + 2 + n_str])
+    n_int = int(txt[k + 3 + n_str + n_real])
+    first = k + 4 + n_str + n_real + n_int
+    vals = {}
+    for line in txt[first:]:
+        if line.startswith("$EndNodeData"):
+            break
+        nid, v = line.split()[:2]
+        vals[int(nid)] = float(v)
+    mtxt = open(mesh_path).read().split("\n")
+    j = next(i for i, l in enumerate(mtxt) if l.strip() == "$Nodes")
+    ids = [int(mtxt[j + 2 + q].split()[0]) for q in range(int(mtxt[j + 1]))]
+    return np.array([vals[i] for i in ids])
+
+
+def water_balance(path):
+    """The boundary table (region id, total, outflow, inflow) and the source table (region id,
+    total) of a water_balance.out."""
+    bdr, src, mode = [], [], None
+    for line in open(path).read().split("\n"):
+        if line.startswith("# Boundary water balance"):
+            mode = "b"
+        elif line.startswith("# Source fluxes"):
+            mode = "s"
+        elif line.startswith("#") or not line.strip():
+            continue
+        elif mode == "b":
+            v = line.split()
+            bdr.append([float(v[0]), float(v[2]), float(v[3]), float(v[4])])
+        elif mode == "s":
+            v = line.split()
+            src.append([float(v[0]), float(v[2])])
+    return dict(ref_bdr_balance=np.array(bdr), ref_src_balance=np.array(src))
+
+
 def case(mesh_path, bulk, bcs, extra, out_name, meta):
     m, names = parse_gmsh(mesh_path)
     rid = {v: k for k, v in names.items()}
@@ -139,8 +182,13 @@ def main():
           "2d_fraction_2": {"anisotropy": 1.0}, "3d_cube": {"anisotropy": 0.1}},
          {r: {"type": "dirichlet", "pressure": lambda x, y, z: x - z}
           for r in (".1d_channel", ".2d_fraction_1", ".2d_fraction_2", ".3d_cube")},
-         raw_output(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "raw_output.txt")),
-         "t01", "tests/01_steady_flow_123d flow_gmsh.con; raw_output %.8g; solver -ksp_rtol 1e-10")
+         {**raw_output(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "raw_output.txt")),
+          "ref_node_pressure": gmsh_node_data(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "test1.msh"),
+                                              "pressure_nodes_[L]", t("01_steady_flow_123d", "input",
+                                                                      "test1_new.msh")),
+          **water_balance(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "water_balance.out"))},
+         "t01", "tests/01_steady_flow_123d flow_gmsh.con; raw_output %.8g, node pressures of the output "
+         "mesh (%g), water_balance.out (%g); solver -ksp_rtol 1e-10")
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
                                       "test05-000000.vtu"), "pressure_elements_[L]")

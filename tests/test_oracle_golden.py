@@ -50,6 +50,42 @@ def test_t01_element_flux_vectors():
     assert np.all(np.abs(u - ref) <= 1e-8 + 5e-9 * np.abs(ref))
 
 
+def t01_regions(z, topo):
+    """Region indices of t01's boundary objects (through their boundary elements) and
+    elements, and the region ids in index order."""
+    bids = sorted(set(z["bc_region"].tolist()))
+    eids = sorted(set(z["el_region"].tolist()))
+    bdr = np.array([bids.index(z["bc_region"][b]) for b in topo["bdr_bc_element"]], np.int32)
+    el = np.array([eids.index(r) for r in z["el_region"]], np.int32)
+    return bdr, el, bids, eids
+
+
+def test_t01_node_pressures():
+    """Node pressures of the output mesh ($NodeData "pressure_nodes_[L]", printed %g)."""
+    z, mesh, topo, P = problem("t01")
+    p = O.node_pressure(P, O.solve_mh_direct(P))
+    ref = z["ref_node_pressure"]
+    assert p.shape == ref.shape
+    assert np.all(np.abs(p - ref) <= 5e-6 * np.abs(ref) + 1e-10)
+
+
+def test_t01_water_balance():
+    """The boundary table of water_balance.out (printed %g): per boundary region the total,
+    outflow and inflow; the totals are differences of flows of about 1, so they also carry the
+    reference solver's own 1e-10 tolerance.  t01 has no sources."""
+    z, mesh, topo, P = problem("t01")
+    assert np.all(topo["bdr_bc_element"] >= 0)  # every boundary object has its element
+    bdr, el, bids, eids = t01_regions(z, topo)
+    ob, osrc = O.water_balance(P, O.solve_mh_direct(P), bdr, el)
+    scale = np.abs(z["ref_bdr_balance"][:, 1:]).max()
+    for rid, *vals in z["ref_bdr_balance"]:
+        got = ob[bids.index(int(rid))]
+        assert np.all(np.abs(got - vals) <= 5e-6 * np.abs(vals) + 1e-9 * scale), (rid, got, vals)
+    assert np.allclose(ob[:, 0], ob[:, 1] + ob[:, 2], rtol=0, atol=1e-15 * scale)
+    for rid, val in z["ref_src_balance"]:
+        assert osrc[eids.index(int(rid))] == val == 0.0
+
+
 def test_t01_schur_path_equals_direct():
     z, mesh, topo, P = problem("t01")
     full = O.solve_mh_direct(P)
