@@ -225,6 +225,20 @@ int mh_get_solution_device(const mh_handle *h, double *dev_out, int64_t len);
 int mh_get_element_flux(const mh_handle *h, double *out, int64_t len);
 /* Same, written directly into a device buffer (a plain device pointer); nothing allocated. */
 int mh_get_element_flux_device(const mh_handle *h, double *dev_out, int64_t len);
+/* Pressure at every node (length n_nodes) from the last solution: the distance-weighted mean
+ * of the pressures of the elements and element sides containing the node,
+ * DarcyFlowMHOutput::make_node_scalar_param (src/flow/darcy_flow_mh_output.cc:424-546).
+ * Computed on the device; MH_ERR_STATE before the first solve. */
+int mh_get_node_pressure(const mh_handle *h, double *out, int64_t len);
+/* Water balance of the last solution, DarcyFlowMHOutput::water_balance
+ * (src/flow/darcy_flow_mh_output.cc:671-790).  bdr_region [n_boundaries] (the boundary objects
+ * in mh_get_topology's order) and el_region [n_elements] are region indices in
+ * [0, n_bdr_regions) and [0, n_el_regions).  bdr_out [3 n_bdr_regions]: per boundary region
+ * the sum of the outward side fluxes, of the positive ones (outflow) and of the negative ones
+ * (inflow); src_out [n_el_regions]: per bulk region the sum of |E| cross_section f.  Computed
+ * on the device; MH_ERR_INVALID for an index out of range, MH_ERR_STATE before a solve. */
+int mh_water_balance(const mh_handle *h, const int32_t *bdr_region, int32_t n_bdr_regions,
+                     const int32_t *el_region, int32_t n_el_regions, double *bdr_out, double *src_out);
 /* Writes (append = 0) or appends one "$FlowField" block of the flow field text output,
  * DarcyFlowMHOutput::output_internal_flow_data (src/flow/darcy_flow_mh_output.cc:793-829):
  * per element its id (el_id, or the element index when null), pressure, centre flux vector,

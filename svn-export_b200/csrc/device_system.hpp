@@ -106,6 +106,16 @@ cudaError_t launch_backsub(const ElemData &d, const DevAssembly &a, const DevSys
 // out[3 e + k], k = x, y, z.
 cudaError_t launch_element_flux(const ElemData &d, const DevAssembly &a, const double *sol, double *out,
                                 cudaStream_t s);
+// Pressure at every node from the element and side pressures of sol (postprocess.cu); dsum and
+// cnt are scratch of n_nodes entries.
+cudaError_t launch_node_pressure(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_nodes,
+                                 int64_t n_sides, int64_t n_el, double *dsum, int32_t *cnt, double *out,
+                                 cudaStream_t s);
+// Water balance per region (postprocess.cu): bdr_out [3 n_bdr_reg] total, outflow, inflow of
+// the boundary side fluxes; src_out [n_el_reg] the sources.  Region indices are device arrays.
+cudaError_t launch_water_balance(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_sides,
+                                 const int32_t *bdr_region, int32_t n_bdr_reg, const int32_t *el_region,
+                                 int32_t n_el_reg, double *bdr_out, double *src_out, cudaStream_t s);
 
 // x = lambda * dsq (initial guess in scaled space; padding rows 0).
 cudaError_t launch_scale_in(const DevSystem &sys, const double *lambda, cudaStream_t s);

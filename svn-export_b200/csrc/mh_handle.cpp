@@ -54,6 +54,11 @@ struct mh_handle {
     mh::DevAssembly as{};
     double *sol = nullptr, *sol_prev = nullptr;
     double *d_elflux = nullptr;         // element flux vectors for mh_get_element_flux (3 n_el)
+    double *d_node_sum = nullptr, *d_node_p = nullptr;  // node pressures: distance sums, result
+    int32_t *d_node_cnt = nullptr;
+    int32_t *d_bdr_region = nullptr, *d_el_region = nullptr;  // water balance inputs
+    double *d_balance = nullptr;        // water balance sums (capacity in balance_cap)
+    int64_t balance_cap = 0;
     double *d_aniso = nullptr;
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
     bool rhs_stale = false;             // boundary values changed since the last assembly
@@ -1604,6 +1609,74 @@ int mh_get_element_flux_device(const mh_handle *hc, double *dev_out, int64_t len
     if (rc) return rc;
     if (!dev_out || len < 3 * h->mesh.n_el) return MH_ERR_INVALID;
     if ((rc = element_flux_into(h, dev_out))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_get_node_pressure(const mh_handle *hc, double *out, int64_t len) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t nn = h->mesh.n_nodes;
+    if (!out || len < nn) return MH_ERR_INVALID;
+    if (!h->solved) {
+        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the node pressures";
+        return MH_ERR_STATE;
+    }
+    if (!h->d_node_p) {
+        h->d_node_sum = dalloc<double>(h, std::max<int64_t>(nn, 1));
+        h->d_node_p = dalloc<double>(h, std::max<int64_t>(nn, 1));
+        h->d_node_cnt = dalloc<int32_t>(h, std::max<int64_t>(nn, 1));
+        if (!h->d_node_sum || !h->d_node_p || !h->d_node_cnt) return MH_ERR_NOMEM;
+    }
+    CK(mh::launch_node_pressure(h->ed, h->as, h->sol, nn, h->topo.n_sides(), h->mesh.n_el, h->d_node_sum,
+                                h->d_node_cnt, h->d_node_p, h->stream));
+    CK(cudaMemcpyAsync(out, h->d_node_p, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_bdr_regions,
+                     const int32_t *el_region, int32_t n_el_regions, double *bdr_out, double *src_out) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t nb = h->topo.n_bdr(), ne = h->mesh.n_el;
+    if (!bdr_region || !el_region || !bdr_out || !src_out || n_bdr_regions < 1 || n_el_regions < 1)
+        return MH_ERR_INVALID;
+    for (int64_t b = 0; b < nb; ++b)
+        if (bdr_region[b] < 0 || bdr_region[b] >= n_bdr_regions) {
+            h->err = "boundary region index out of range";
+            return MH_ERR_INVALID;
+        }
+    for (int64_t e = 0; e < ne; ++e)
+        if (el_region[e] < 0 || el_region[e] >= n_el_regions) {
+            h->err = "element region index out of range";
+            return MH_ERR_INVALID;
+        }
+    if (!h->solved) {
+        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the water balance";
+        return MH_ERR_STATE;
+    }
+    if (!h->d_el_region) {
+        h->d_bdr_region = dalloc<int32_t>(h, std::max<int64_t>(nb, 1));
+        h->d_el_region = dalloc<int32_t>(h, std::max<int64_t>(ne, 1));
+        if (!h->d_bdr_region || !h->d_el_region) return MH_ERR_NOMEM;
+    }
+    const int64_t need = 3 * (int64_t)n_bdr_regions + n_el_regions;
+    if (need > h->balance_cap) {
+        h->d_balance = dalloc<double>(h, need);
+        if (!h->d_balance) return MH_ERR_NOMEM;
+        h->balance_cap = need;
+    }
+    if (nb > 0)
+        CK(cudaMemcpyAsync(h->d_bdr_region, bdr_region, nb * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_el_region, el_region, ne * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    double *bo = h->d_balance, *so = h->d_balance + 3 * (int64_t)n_bdr_regions;
+    CK(mh::launch_water_balance(h->ed, h->as, h->sol, h->topo.n_sides(), h->d_bdr_region, n_bdr_regions,
+                                h->d_el_region, n_el_regions, bo, so, h->stream));
+    CK(cudaMemcpyAsync(bdr_out, bo, 3 * (size_t)n_bdr_regions * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(src_out, so, (size_t)n_el_regions * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return MH_OK;
 }

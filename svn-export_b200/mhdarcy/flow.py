@@ -210,6 +210,26 @@ class MHSystem:
         check(lib.mh_get_element_flux(self.h, ptr(out, C.c_double), out.size), self.h)
         return out
 
+    def node_pressure(self):
+        """Pressure at every node [n_nodes] from the last solution
+        (DarcyFlowMHOutput::make_node_scalar_param, darcy_flow_mh_output.cc:424-546)."""
+        out = np.zeros(self.sizes.n_nodes)
+        check(lib.mh_get_node_pressure(self.h, ptr(out, C.c_double), len(out)), self.h)
+        return out
+
+    def water_balance(self, bdr_region, el_region, n_bdr_regions=None, n_el_regions=None):
+        """Water balance of the last solution (DarcyFlowMHOutput::water_balance,
+        darcy_flow_mh_output.cc:671-790) for region indices of the boundary objects (topology
+        order) and of the elements: ([n_bdr_regions, 3] total, outflow, inflow;
+        [n_el_regions] sources)."""
+        br, er = i32(bdr_region), i32(el_region)
+        nb = int(n_bdr_regions if n_bdr_regions is not None else (br.max() + 1 if br.size else 1))
+        ne = int(n_el_regions if n_el_regions is not None else (er.max() + 1 if er.size else 1))
+        bo, so = np.zeros((nb, 3)), np.zeros(ne)
+        check(lib.mh_water_balance(self.h, ptr(br, C.c_int32), nb, ptr(er, C.c_int32), ne, ptr(bo, C.c_double),
+                                   ptr(so, C.c_double)), self.h)
+        return bo, so
+
     def schur_system(self):
         """The assembled edge system (reference schur2 after scale(-1)) as CSR + rhs."""
         s = self.sizes

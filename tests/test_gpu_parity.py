@@ -214,6 +214,66 @@ def test_element_flux_vectors_device_output(gpu):
         assert np.array_equal(u, s.element_flux())
 
 
+def test_node_pressure_and_water_balance_t01(gpu):
+    """Node pressures and the water balance of t01 on the device: against the oracle on the
+    GPU's own solution, and against the reference's output mesh ($NodeData, %g) and
+    water_balance.out (%g)."""
+    z, mesh, coeffs, bc = fixture_case("t01")
+    with gpu_system(mesh, coeffs, bc) as s:
+        with pytest.raises(mhdarcy.MHError) as ei:  # no solution yet
+            s.node_pressure()
+        assert ei.value.status == _lib.MH_ERR_STATE
+        s.solve(r_tol=1e-12)
+        sol = s.solution()
+        topo = s.topology()
+        P = oracle_problem(mesh, topo, s.n_edges, coeffs, bc)
+        p = s.node_pressure()
+        ref = O.node_pressure(P, sol)
+        assert np.abs(p - ref).max() <= 1e-12 * np.abs(ref).max()
+        rz = z["ref_node_pressure"]
+        assert np.all(np.abs(p - rz) <= 5e-6 * np.abs(rz) + 1e-10)
+        bids, eids = sorted(set(z["bc_region"].tolist())), sorted(set(z["el_region"].tolist()))
+        br = np.array([bids.index(z["bc_region"][b]) for b in topo["bdr_bc_element"]], np.int32)
+        er = np.array([eids.index(r) for r in z["el_region"]], np.int32)
+        bo, so = s.water_balance(br, er, len(bids), len(eids))
+        ob, osrc = O.water_balance(P, sol, br, er)
+        scale = np.abs(ob).max()
+        assert np.abs(bo - ob).max() <= 1e-12 * scale and np.all(so == 0.0)
+        for rid, *vals in z["ref_bdr_balance"]:
+            got = bo[bids.index(int(rid))]
+            assert np.all(np.abs(got - vals) <= 5e-6 * np.abs(vals) + 1e-9 * scale), (rid, got, vals)
+
+
+def test_node_pressure_and_water_balance_sources(gpu):
+    """A fractured cube with channels, random cross-sections and water sources, and synthetic
+    region maps: node pressures and both balance tables against the oracle; region indices
+    out of range are refused."""
+    mesh, coeffs = make_case(5, n=8)
+    rng = np.random.default_rng(11)
+    coeffs = dict(coeffs, water_source_density=rng.normal(0.0, 1e-3, mesh.n_elements))
+    with mhdarcy.MHSystem(mesh) as s:
+        topo = s.topology()
+        bc, _ = dirichlet_x_bc(topo, mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+        sol = s.solution()
+        P = oracle_problem(mesh, topo, s.n_edges, coeffs, bc)
+        ref = O.node_pressure(P, sol)
+        assert np.abs(s.node_pressure() - ref).max() <= 1e-12 * np.abs(ref).max()
+        nb = s.sizes.n_boundaries
+        br = (np.arange(nb) % 5).astype(np.int32)
+        er = (np.asarray(mesh.el_dim) - 1).astype(np.int32)
+        bo, so = s.water_balance(br, er, 5, 3)
+        ob, osrc = O.water_balance(P, sol, br, er)
+        assert np.abs(bo - ob).max() <= 1e-12 * np.abs(ob).max()
+        assert np.abs(so - osrc).max() <= 1e-12 * np.abs(osrc).max() and np.all(osrc != 0.0)
+        with pytest.raises(mhdarcy.MHError) as ei:
+            s.water_balance(br, er, 5, 2)  # a tetrahedron has region index 2
+        assert ei.value.status == _lib.MH_ERR_INVALID
+
+
 @pytest.mark.parametrize("cfg", [5, 2])
 def test_amg_fluxes_within_1e_8(gpu, cfg):
     """The accuracy target of the mixed-precision multigrid solve: at r_tol 1e-12 the side
