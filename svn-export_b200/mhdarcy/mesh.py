@@ -172,3 +172,75 @@ def read_gmsh(path):
     m.el_id = np.array([r[0] for r in bulk], np.int64)
     m.region_names = names
     return m
+
+
+def _data_header(lines, i):
+    """Parses the tags of an $ElementData header starting at line i (the string-tag count):
+    field name, time, component and entity counts, and the index of the first data line
+    (GmshMeshReader::read_data_header, src/mesh/msh_gmshreader.cc:251-303).  Missing tags
+    take the reference's defaults: time 0, one component, zero entities."""
+    n_str = int(lines[i].split()[0])
+    name = lines[i + 1].strip().strip('"') if n_str > 0 else ""
+    i += 1 + n_str
+    n_real = int(lines[i].split()[0])
+    time = float(lines[i + 1].split()[0]) if n_real > 0 else 0.0
+    i += 1 + n_real
+    n_int = int(lines[i].split()[0])
+    ints = [int(lines[i + 1 + k].split()[0]) for k in range(n_int)]
+    i += 1 + n_int
+    n_comp = ints[1] if n_int > 1 else 1
+    n_ent = ints[2] if n_int > 2 else 0
+    return name, time, n_comp, n_ent, i
+
+
+def read_element_data(path, field_name, el_ids, time=0.0, n_components=1):
+    """Values of the element field `field_name` of a gmsh 2.2 file at `time`, for the elements
+    with ids `el_ids` (ascending, e.g. Mesh.el_id): an array [len(el_ids), n_components] in that
+    order, ready for MHSystem.set_coeffs.  Follows GmshMeshReader::read_element_data
+    (src/mesh/msh_gmshreader.cc:306-396): the $ElementData sections of the field are taken in
+    file order, and the last one whose time is <= time (1 + 2 eps) gives the values; a data line
+    is "id v_1 .. v_n" with ids ascending, ids that are not among el_ids are skipped, and an
+    element without a line keeps the value of an earlier section (NaN if none had it).  A
+    section with another component count is read with n_components values per line, as the
+    reference does.  Raises ValueError when the file has no section of the field, when none is at
+    or before `time` (the reference then leaves the field's values unset), or when a row has
+    fewer values than n_components."""
+    ids = np.asarray(el_ids, np.int64)
+    if ids.size > 1 and np.any(np.diff(ids) <= 0):
+        raise ValueError("el_ids must be ascending")
+    with open(path) as f:
+        lines = f.read().split("\n")
+    out = np.full((ids.size, n_components), np.nan)
+    found = used = False
+    limit = time * (1.0 + 2.0 * np.finfo(float).eps)
+    i = 0
+    while i < len(lines):
+        if lines[i].strip() != "$ElementData":
+            i += 1
+            continue
+        name, t, _, n_ent, i = _data_header(lines, i + 1)
+        if name != field_name:
+            continue
+        found = True
+        if t > limit:
+            break
+        used = True
+        pos = 0
+        for row in lines[i:i + n_ent]:
+            p = row.split()
+            eid = int(p[0])
+            while pos < ids.size and ids[pos] < eid:
+                pos += 1
+            if pos == ids.size:
+                break  # an id past the last element: the rest of the section is skipped
+            if ids[pos] == eid:
+                if len(p) - 1 < n_components:
+                    raise ValueError(f"{path}: element {eid} of field '{field_name}' has {len(p) - 1} values, "
+                                     f"{n_components} expected")
+                out[pos] = [float(v) for v in p[1:1 + n_components]]
+        i += n_ent
+    if not found:
+        raise ValueError(f"{path}: no $ElementData section for field '{field_name}'")
+    if not used:
+        raise ValueError(f"{path}: no $ElementData of field '{field_name}' at or before time {time}")
+    return out
