@@ -327,9 +327,34 @@ def element_flux_timing(system, stream, sz, mesh, reps=20):
     ms = ev0.elapsed_time(ev1) / reps
     nsides = np.asarray(mesh.el_dim) + 1
     algo = 24 * sz.n_nodes + int(np.sum(4 * nsides + 8 * nsides)) + ne * (4 + 8 + 4 + 24)
-    return {"kernel": "k_element_flux (make_element_vector)", "ms_per_call": round(ms, 4),
-            "algorithmic_bytes": algo, "achieved_gbs": round(algo / (ms / 1e3) / 1e9, 1),
-            "note": "per call: element kernels plus one stream synchronisation"}
+    ef = {"kernel": "k_element_flux (make_element_vector)", "ms_per_call": round(ms, 4),
+          "algorithmic_bytes": algo, "achieved_gbs": round(algo / (ms / 1e3) / 1e9, 1),
+          "note": "per call: element kernels plus one stream synchronisation"}
+    # the transport's convection matrix (mh_transport_matrix_device): pattern built by the first
+    # call, then values only; bytes per slot: kind, two side indices and the value (4+4+4+8),
+    # per row its offset, sides, cross-section and the side fluxes read
+    nnz = C.c_int64()
+    _lib.check(_lib.lib.mh_transport_matrix(system.h, None, C.byref(nnz), None, None, None, None), system.h)
+    tbuf = torch.empty(nnz.value, dtype=torch.float64, device="cuda")
+    cfl = C.c_double()
+    tcall = lambda: _lib.check(_lib.lib.mh_transport_matrix_device(system.h, None, C.c_void_p(tbuf.data_ptr()),
+                                                                  nnz.value, C.byref(cfl)), system.h)
+    tcall()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(reps):
+        tcall()
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    tms = ev0.elapsed_time(ev1) / reps
+    talgo = 20 * nnz.value + ne * (8 + 8) + 8 * int(np.sum(nsides)) + 8 * sz.n_edges
+    tr = {"kernel": "k_transport_rows + k_edge_outflow (create_transport_matrix_mpi)", "nnz": nnz.value,
+          "ms_per_call": round(tms, 4), "algorithmic_bytes": talgo,
+          "achieved_gbs": round(talgo / (tms / 1e3) / 1e9, 1), "cfl_max_step": cfl.value,
+          "note": "per call: two kernels, a 8-byte read-back and a stream synchronisation"}
+    return {"element_flux": ef, "transport_matrix": tr}
 
 
 # ---------------------------------------------------------------- ours ------------------

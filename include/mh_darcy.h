@@ -239,6 +239,20 @@ int mh_get_node_pressure(const mh_handle *h, double *out, int64_t len);
  * on the device; MH_ERR_INVALID for an index out of range, MH_ERR_STATE before a solve. */
 int mh_water_balance(const mh_handle *h, const int32_t *bdr_region, int32_t n_bdr_regions,
                      const int32_t *el_region, int32_t n_el_regions, double *bdr_out, double *src_out);
+/* Convection matrix of the explicit finite-volume transport from the side fluxes of the last
+ * solution, ConvectionTransport::create_transport_matrix_mpi (src/transport/transport.cc:
+ * 788-923): a CSR matrix [n_elements x n_elements] with the reference's entries (a zero
+ * entry wherever the reference inserts one), columns ascending in each row, and
+ * cfl_max_step = 1 / max |a_ii|.  porosity [n_elements] (the transport's por_m) may be NULL
+ * (1).  Call with row_ptr, col, val and cfl_max_step all NULL to get *nnz; then row_ptr
+ * [n_elements+1], col [nnz], val [nnz] (any may be NULL).  The pattern is built on the first
+ * call; the values are computed on the device.  MH_ERR_STATE before a solve. */
+int mh_transport_matrix(const mh_handle *h, const double *porosity, int64_t *nnz, int32_t *row_ptr,
+                        int32_t *col, double *val, double *cfl_max_step);
+/* Same values into a device buffer (len >= nnz, in the CSR order of mh_transport_matrix);
+ * dev_porosity is a device pointer or NULL.  Nothing is copied to the host but the CFL step. */
+int mh_transport_matrix_device(const mh_handle *h, const double *dev_porosity, double *dev_val,
+                               int64_t len, double *cfl_max_step);
 /* Writes (append = 0) or appends one "$FlowField" block of the flow field text output,
  * DarcyFlowMHOutput::output_internal_flow_data (src/flow/darcy_flow_mh_output.cc:793-829):
  * per element its id (el_id, or the element index when null), pressure, centre flux vector,

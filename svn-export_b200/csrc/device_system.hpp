@@ -111,6 +111,21 @@ cudaError_t launch_element_flux(const ElemData &d, const DevAssembly &a, const d
 cudaError_t launch_node_pressure(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_nodes,
                                  int64_t n_sides, int64_t n_el, double *dsum, int32_t *cnt, double *out,
                                  cudaStream_t s);
+// Convection matrix of the explicit transport (transport.cu).  The pattern is built on the host
+// once per mesh: per row, slots sorted by column, each with its kind and the side indices its
+// value reads (edge: own side a, other side b; VB: the higher-dimensional side a).
+constexpr int kTrDiag = 0, kTrEdge = 1, kTrVbLower = 2, kTrVbHigher = 3;
+struct TransportPattern {
+    int64_t n_el = 0, n_edges = 0, nnz = 0;
+    int32_t *row_ptr = nullptr, *kind = nullptr, *slot_a = nullptr, *slot_b = nullptr;  // device
+    int32_t *edge_start = nullptr, *edge_sides = nullptr, *ngh_side = nullptr;          // device
+    double *edge_flow = nullptr;                                                         // [n_edges]
+    unsigned long long *diag_max = nullptr;                                              // max |a_ii| bits
+};
+// val [nnz] in the pattern's slot order; porosity [n_el] on the device or null (1).
+cudaError_t launch_transport_matrix(const ElemData &d, const TransportPattern &p, const double *porosity,
+                                    const double *sol, double *val, cudaStream_t s);
+
 // Water balance per region (postprocess.cu): bdr_out [3 n_bdr_reg] total, outflow, inflow of
 // the boundary side fluxes; src_out [n_el_reg] the sources.  Region indices are device arrays.
 cudaError_t launch_water_balance(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_sides,

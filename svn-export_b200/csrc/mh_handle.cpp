@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <random>
 #include <new>
@@ -59,6 +60,12 @@ struct mh_handle {
     int32_t *d_bdr_region = nullptr, *d_el_region = nullptr;  // water balance inputs
     double *d_balance = nullptr;        // water balance sums (capacity in balance_cap)
     int64_t balance_cap = 0;
+    // convection matrix of the transport: pattern (built once), host copies of its CSR
+    // structure, device values and porosity
+    bool tr_built = false;
+    mh::TransportPattern conv{};
+    std::vector<int32_t> tr_row_ptr, tr_col;
+    double *d_tr_val = nullptr, *d_tr_por = nullptr;
     double *d_aniso = nullptr;
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
     bool rhs_stale = false;             // boundary values changed since the last assembly
@@ -1679,6 +1686,130 @@ int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_b
     CK(cudaMemcpyAsync(src_out, so, (size_t)n_el_regions * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return MH_OK;
+}
+
+// The convection matrix's sparsity pattern (ConvectionTransport::create_transport_matrix_mpi,
+// transport.cc:788-923, with the entries written in its order): per element row the diagonal,
+// for each side that is not on a boundary object every other side of its edge, for each VB
+// neighbour (the row element lower-dimensional) the higher element, and for each VB coupling in
+// which the row element is the higher one the lower element.  Slots are sorted by column; two
+// slots of one row never share a column in a simplicial mesh (two elements share at most one
+// face, a VB pair one side), which is checked.
+static int build_transport_pattern(mh_handle *h) {
+    const mh::Topology &t = h->topo;
+    const int64_t ne = h->mesh.n_el, ns = t.n_sides();
+    std::vector<int32_t> side_el(ns);
+    for (int64_t e = 0; e < ne; ++e)
+        for (int32_t k = t.el_side_start[e]; k < t.el_side_start[e + 1]; ++k) side_el[k] = (int32_t)e;
+    struct Slot {
+        int32_t col, kind, a, b;
+    };
+    std::vector<std::vector<Slot>> rows(ne);
+    for (int64_t i = 0; i < ne; ++i) {
+        auto &r = rows[i];
+        r.push_back({(int32_t)i, mh::kTrDiag, -1, -1});
+        for (int32_t si = t.el_side_start[i]; si < t.el_side_start[i + 1]; ++si) {
+            if (t.side_bdr[si] >= 0) continue;
+            const int32_t ed = t.side_edge[si];
+            for (int32_t k = t.edge_side_start[ed]; k < t.edge_side_start[ed + 1]; ++k) {
+                const int32_t so = t.edge_sides[k];
+                if (so != si) r.push_back({side_el[so], mh::kTrEdge, si, so});
+            }
+        }
+        for (int32_t k = t.el_ngh_start[i]; k < t.el_ngh_start[i + 1]; ++k) {
+            const int32_t hs = t.ngh_side[t.el_ngh[k]];
+            r.push_back({side_el[hs], mh::kTrVbLower, hs, -1});
+            rows[side_el[hs]].push_back({(int32_t)i, mh::kTrVbHigher, hs, -1});
+        }
+    }
+    std::vector<int32_t> rp(ne + 1, 0), col, kind, sa, sb;
+    for (int64_t i = 0; i < ne; ++i) {
+        auto &r = rows[i];
+        std::sort(r.begin(), r.end(), [](const Slot &x, const Slot &y) { return x.col < y.col; });
+        for (size_t k = 0; k < r.size(); ++k) {
+            if (k && r[k].col == r[k - 1].col) {
+                h->err = "convection matrix: two couplings of one element pair (degenerate mesh)";
+                return MH_ERR_TOPOLOGY;
+            }
+            col.push_back(r[k].col);
+            kind.push_back(r[k].kind);
+            sa.push_back(r[k].a);
+            sb.push_back(r[k].b);
+        }
+        rp[i + 1] = (int32_t)col.size();
+    }
+    mh::TransportPattern &p = h->conv;
+    p.n_el = ne;
+    p.n_edges = t.n_edges();
+    p.nnz = (int64_t)col.size();
+    int rc;
+    if ((rc = upload(h, p.row_ptr, rp)) || (rc = upload(h, p.kind, kind)) || (rc = upload(h, p.slot_a, sa)) ||
+        (rc = upload(h, p.slot_b, sb)) || (rc = upload(h, p.edge_start, t.edge_side_start)) ||
+        (rc = upload(h, p.edge_sides, t.edge_sides)) || (rc = upload(h, p.ngh_side, t.ngh_side)))
+        return rc;
+    p.edge_flow = dalloc<double>(h, std::max<int64_t>(p.n_edges, 1));
+    p.diag_max = dalloc<unsigned long long>(h, 1);
+    h->d_tr_val = dalloc<double>(h, std::max<int64_t>(p.nnz, 1));
+    h->d_tr_por = dalloc<double>(h, std::max<int64_t>(ne, 1));
+    if (!p.edge_flow || !p.diag_max || !h->d_tr_val || !h->d_tr_por) return MH_ERR_NOMEM;
+    h->tr_row_ptr.swap(rp);
+    h->tr_col.swap(col);
+    h->tr_built = true;
+    return MH_OK;
+}
+
+// values of the convection matrix into dev_val for the last solution; cfl = 1 / max |a_ii|
+static int transport_values(mh_handle *h, const double *dev_porosity, double *dev_val, double *cfl) {
+    if (!h->solved) {
+        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the convection matrix";
+        return MH_ERR_STATE;
+    }
+    CK(mh::launch_transport_matrix(h->ed, h->conv, dev_porosity, h->sol, dev_val, h->stream));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, h->conv.diag_max, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (cfl) {
+        double mx;
+        std::memcpy(&mx, &bits, sizeof(mx));
+        *cfl = mx > 0.0 ? 1.0 / mx : std::numeric_limits<double>::infinity();
+    }
+    return MH_OK;
+}
+
+int mh_transport_matrix(const mh_handle *hc, const double *porosity, int64_t *nnz, int32_t *row_ptr, int32_t *col,
+                        double *val, double *cfl_max_step) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!nnz) return MH_ERR_INVALID;
+    if (!h->tr_built && (rc = build_transport_pattern(h))) return rc;
+    *nnz = h->conv.nnz;
+    if (!row_ptr && !col && !val && !cfl_max_step) return MH_OK;  // the size query
+    const int64_t ne = h->mesh.n_el;
+    if (porosity && !check_finite(porosity, ne)) return MH_ERR_NONFINITE;
+    if (porosity && !check_positive(porosity, ne)) {
+        h->err = "porosity must be positive";
+        return MH_ERR_INVALID;
+    }
+    if (porosity) CK(cudaMemcpyAsync(h->d_tr_por, porosity, ne * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if ((rc = transport_values(h, porosity ? h->d_tr_por : nullptr, h->d_tr_val, cfl_max_step))) return rc;
+    if (row_ptr) std::memcpy(row_ptr, h->tr_row_ptr.data(), (ne + 1) * sizeof(int32_t));
+    if (col) std::memcpy(col, h->tr_col.data(), h->conv.nnz * sizeof(int32_t));
+    if (val) {
+        CK(cudaMemcpyAsync(val, h->d_tr_val, h->conv.nnz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return MH_OK;
+}
+
+int mh_transport_matrix_device(const mh_handle *hc, const double *dev_porosity, double *dev_val, int64_t len,
+                               double *cfl_max_step) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->tr_built && (rc = build_transport_pattern(h))) return rc;
+    if (!dev_val || len < h->conv.nnz) return MH_ERR_INVALID;
+    return transport_values(h, dev_porosity, dev_val, cfl_max_step);
 }
 
 int mh_get_schur_system(const mh_handle *hc, int32_t *row_ptr, int32_t *col, double *val, double *rhs) {

@@ -134,6 +134,8 @@ def _load():
         "mh_raw_output_write": (C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_int64, vp, vp, vp, vp, vp]),
         "mh_get_node_pressure": (C.c_int, [vp, vp, C.c_int64]),
         "mh_water_balance": (C.c_int, [vp, vp, C.c_int32, vp, C.c_int32, vp, vp]),
+        "mh_transport_matrix": (C.c_int, [vp, vp, vp, vp, vp, vp, vp]),
+        "mh_transport_matrix_device": (C.c_int, [vp, vp, vp, C.c_int64, vp]),
         "mh_get_schur_system": (C.c_int, [vp, _i32p, _i32p, _f64p, _f64p]),
         "mh_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "mh_unsteady_init": (C.c_int, [vp, C.c_int32, C.c_double, _f64p]),
@@ -169,7 +171,7 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device",
             "mh_get_element_flux", "mh_get_element_flux_device", "mh_raw_output_write",
-            "mh_get_node_pressure", "mh_water_balance", "mh_get_schur_system",
+            "mh_get_node_pressure", "mh_water_balance", "mh_transport_matrix", "mh_transport_matrix_device", "mh_get_schur_system",
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
             "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune",
             "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",

@@ -230,6 +230,21 @@ class MHSystem:
                                    ptr(so, C.c_double)), self.h)
         return bo, so
 
+    def transport_matrix(self, porosity=None):
+        """Convection matrix of the explicit transport from the last solution's side fluxes
+        (ConvectionTransport::create_transport_matrix_mpi, transport.cc:788-923): (row_ptr,
+        col, val) CSR arrays [n_elements x n_elements] and cfl_max_step."""
+        nnz = C.c_int64()
+        check(lib.mh_transport_matrix(self.h, None, C.byref(nnz), None, None, None, None), self.h)
+        rp = np.zeros(self.n_elements + 1, np.int32)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value)
+        cfl = C.c_double()
+        por = f64(porosity)
+        check(lib.mh_transport_matrix(self.h, ptr(por, C.c_double), C.byref(nnz), ptr(rp, C.c_int32),
+                                      ptr(col, C.c_int32), ptr(val, C.c_double), C.byref(cfl)), self.h)
+        return (rp, col, val), cfl.value
+
     def schur_system(self):
         """The assembled edge system (reference schur2 after scale(-1)) as CSR + rhs."""
         s = self.sizes
