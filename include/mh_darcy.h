@@ -221,14 +221,14 @@ int mh_get_solution_device(const mh_handle *h, double *dev_out, int64_t len);
 /* Darcy flux vector at every element centre from the side fluxes of the last solution,
  * out[3 e + k] for k = x, y, z (length 3 n_elements): DarcyFlowMHOutput::make_element_vector
  * (src/flow/darcy_flow_mh_output.cc:301-323), the three flux columns of the raw output.
- * Computed on the device; MH_ERR_STATE before the first solve. */
+ * Computed on the device; MH_ERR_STATE until a solve follows the last mh_set_coeffs. */
 int mh_get_element_flux(const mh_handle *h, double *out, int64_t len);
 /* Same, written directly into a device buffer (a plain device pointer); nothing allocated. */
 int mh_get_element_flux_device(const mh_handle *h, double *dev_out, int64_t len);
 /* Pressure at every node (length n_nodes) from the last solution: the distance-weighted mean
  * of the pressures of the elements and element sides containing the node,
  * DarcyFlowMHOutput::make_node_scalar_param (src/flow/darcy_flow_mh_output.cc:424-546).
- * Computed on the device; MH_ERR_STATE before the first solve. */
+ * Computed on the device; MH_ERR_STATE until a solve follows the last mh_set_coeffs. */
 int mh_get_node_pressure(const mh_handle *h, double *out, int64_t len);
 /* Water balance of the last solution, DarcyFlowMHOutput::water_balance
  * (src/flow/darcy_flow_mh_output.cc:671-790).  bdr_region [n_boundaries] (the boundary objects
@@ -236,7 +236,8 @@ int mh_get_node_pressure(const mh_handle *h, double *out, int64_t len);
  * [0, n_bdr_regions) and [0, n_el_regions).  bdr_out [3 n_bdr_regions]: per boundary region
  * the sum of the outward side fluxes, of the positive ones (outflow) and of the negative ones
  * (inflow); src_out [n_el_regions]: per bulk region the sum of |E| cross_section f.  Computed
- * on the device; MH_ERR_INVALID for an index out of range, MH_ERR_STATE before a solve. */
+ * on the device; MH_ERR_INVALID for an index out of range, MH_ERR_STATE until a solve
+ * follows the last mh_set_coeffs. */
 int mh_water_balance(const mh_handle *h, const int32_t *bdr_region, int32_t n_bdr_regions,
                      const int32_t *el_region, int32_t n_el_regions, double *bdr_out, double *src_out);
 /* Convection matrix of the explicit finite-volume transport from the side fluxes of the last
@@ -246,7 +247,8 @@ int mh_water_balance(const mh_handle *h, const int32_t *bdr_region, int32_t n_bd
  * cfl_max_step = 1 / max |a_ii|.  porosity [n_elements] (the transport's por_m) may be NULL
  * (1).  Call with row_ptr, col, val and cfl_max_step all NULL to get *nnz; then row_ptr
  * [n_elements+1], col [nnz], val [nnz] (any may be NULL).  The pattern is built on the first
- * call; the values are computed on the device.  MH_ERR_STATE before a solve. */
+ * call; the values are computed on the device.  MH_ERR_STATE until a solve follows the last
+ * mh_set_coeffs. */
 int mh_transport_matrix(const mh_handle *h, const double *porosity, int64_t *nnz, int32_t *row_ptr,
                         int32_t *col, double *val, double *cfl_max_step);
 /* Same values into a device buffer (len >= nnz, in the CSR order of mh_transport_matrix);

@@ -1500,6 +1500,7 @@ int mh_set_coeffs(mh_handle *h, const mh_coeffs *c) {
     CK(cudaStreamSynchronize(h->stream));
     h->coeffs_set = true;
     h->assembled = false;
+    h->solved = false;  // the post-processing needs a solution of the new coefficients
     return MH_OK;
 }
 
@@ -1587,7 +1588,7 @@ int mh_get_solution_device(const mh_handle *hc, double *dev_out, int64_t len) {
 // make_element_vector (darcy_flow_mh_output.cc:301-323) on the device, into dev_out [3 n_el]
 static int element_flux_into(mh_handle *h, double *dev_out) {
     if (!h->solved) {
-        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the element fluxes";
+        h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the element fluxes";
         return MH_ERR_STATE;
     }
     CK(mh::launch_element_flux(h->ed, h->as, h->sol, dev_out, h->stream));
@@ -1627,7 +1628,7 @@ int mh_get_node_pressure(const mh_handle *hc, double *out, int64_t len) {
     const int64_t nn = h->mesh.n_nodes;
     if (!out || len < nn) return MH_ERR_INVALID;
     if (!h->solved) {
-        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the node pressures";
+        h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the node pressures";
         return MH_ERR_STATE;
     }
     if (!h->d_node_p) {
@@ -1662,7 +1663,7 @@ int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_b
             return MH_ERR_INVALID;
         }
     if (!h->solved) {
-        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the water balance";
+        h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the water balance";
         return MH_ERR_STATE;
     }
     if (!h->d_el_region) {
@@ -1761,7 +1762,7 @@ static int build_transport_pattern(mh_handle *h) {
 // values of the convection matrix into dev_val for the last solution; cfl = 1 / max |a_ii|
 static int transport_values(mh_handle *h, const double *dev_porosity, double *dev_val, double *cfl) {
     if (!h->solved) {
-        h->err = "no solution yet: mh_solve or mh_unsteady_step must come before the convection matrix";
+        h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the convection matrix";
         return MH_ERR_STATE;
     }
     CK(mh::launch_transport_matrix(h->ed, h->conv, dev_porosity, h->sol, dev_val, h->stream));
