@@ -216,15 +216,43 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
         return hs.slice_off[r / kSliceRowsHost] + j * kSliceRowsHost + r % kSliceRowsHost;
     };
 
-    // contributions: element blocks -> slots, element rhs -> rows (element order)
+    // contributions: element blocks -> slots, element rhs -> rows, in element order (the
+    // device sums each slot's contributions in list order).  The slot of every block entry
+    // (a binary search in its row) is found in parallel for a chunk of elements; counting and
+    // filling then walk the chunk in element order.
+    constexpr int64_t kChunk = 1 << 18;
+    std::vector<int64_t> coff(kChunk + 1);
+    std::vector<int64_t> cslot;
+    auto chunk_slots = [&](int64_t e0, int64_t e1) {
+        coff[0] = 0;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int64_t c = m.dim[e] + 1 + (t.el_ngh_start[e + 1] - t.el_ngh_start[e]);  // local_edges' count
+            coff[e - e0 + 1] = coff[e - e0] + c * c;
+        }
+        cslot.resize(coff[e1 - e0]);
+#pragma omp parallel for schedule(static)
+        for (int64_t e = e0; e < e1; ++e) {
+            int32_t lc[16];
+            const int c = local_edges(m, t, e, lc);
+            int64_t o = coff[e - e0];
+            for (int a = 0; a < c; ++a) {
+                const int64_t ra = hs.edge_row[lc[a]];
+                for (int b = 0; b < c; ++b) cslot[o++] = slot_of(ra, hs.edge_row[lc[b]]);
+            }
+        }
+    };
     hs.slot_cstart.assign(hs.n_slots + 1, 0);
     hs.row_cstart.assign(hs.n_rows + 1, 0);
-    for (int64_t e = 0; e < n_el; ++e) {
-        int c = local_edges(m, t, e, loc);
-        for (int a = 0; a < c; ++a) {
-            int64_t ra = hs.edge_row[loc[a]];
-            hs.row_cstart[ra + 1]++;
-            for (int b = 0; b < c; ++b) hs.slot_cstart[slot_of(ra, hs.edge_row[loc[b]]) + 1]++;
+    for (int64_t e0 = 0; e0 < n_el; e0 += kChunk) {
+        const int64_t e1 = std::min(n_el, e0 + kChunk);
+        chunk_slots(e0, e1);
+        for (int64_t e = e0; e < e1; ++e) {
+            int c = local_edges(m, t, e, loc);
+            const int64_t o = coff[e - e0];
+            for (int a = 0; a < c; ++a) {
+                hs.row_cstart[hs.edge_row[loc[a]] + 1]++;
+                for (int b = 0; b < c; ++b) hs.slot_cstart[cslot[o + (int64_t)a * c + b] + 1]++;
+            }
         }
     }
     for (int64_t s = 0; s < hs.n_slots; ++s) hs.slot_cstart[s + 1] += hs.slot_cstart[s];
@@ -234,14 +262,19 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     {
         std::vector<int32_t> sf(hs.slot_cstart.begin(), hs.slot_cstart.end() - 1);
         std::vector<int32_t> rf(hs.row_cstart.begin(), hs.row_cstart.end() - 1);
-        for (int64_t e = 0; e < n_el; ++e) {
-            int c = local_edges(m, t, e, loc);
-            for (int a = 0; a < c; ++a) {
-                int64_t ra = hs.edge_row[loc[a]];
-                hs.row_cidx[rf[ra]++] = (int32_t)(hs.rhs_off[e] + a);
-                for (int b = 0; b < c; ++b) {
-                    int64_t sl = slot_of(ra, hs.edge_row[loc[b]]);
-                    hs.slot_cidx[sf[sl]++] = (int32_t)(hs.blk_off[e] + (int64_t)a * c + b);
+        for (int64_t e0 = 0; e0 < n_el; e0 += kChunk) {
+            const int64_t e1 = std::min(n_el, e0 + kChunk);
+            chunk_slots(e0, e1);
+            for (int64_t e = e0; e < e1; ++e) {
+                int c = local_edges(m, t, e, loc);
+                const int64_t o = coff[e - e0];
+                for (int a = 0; a < c; ++a) {
+                    int64_t ra = hs.edge_row[loc[a]];
+                    hs.row_cidx[rf[ra]++] = (int32_t)(hs.rhs_off[e] + a);
+                    for (int b = 0; b < c; ++b) {
+                        const int64_t sl = cslot[o + (int64_t)a * c + b];
+                        hs.slot_cidx[sf[sl]++] = (int32_t)(hs.blk_off[e] + (int64_t)a * c + b);
+                    }
                 }
             }
         }
