@@ -12,6 +12,8 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
                    the node pressures of the output mesh ($NodeData "pressure_nodes_[L]"); the
                    boundary and source tables of water_balance.out;
   * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output;
+  * t08            tests/08_steady_flow_sources: element and node pressures, element velocities
+                   of the VTK output, and its water balance (a source field given by a formula);
   * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
   * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5.
 The parsers here are self-contained (independent of the package under test).
@@ -151,11 +153,13 @@ def case(mesh_path, bulk, bcs, extra, out_name, meta):
     ne, nb = len(m["el_dim"]), len(m["bc_dim"])
     f = dict(conductivity=np.ones(ne), anisotropy=np.ones(ne), cross_section=np.ones(ne), sigma=np.ones(ne),
              water_source_density=np.zeros(ne), storativity=np.ones(ne), init_pressure=np.zeros(ne))
+    el_c = centres(m["nodes"], m["el_dim"], m["el_nodes"])
     for reg, vals in bulk.items():
         sel = m["el_region"] == rid[reg]
         assert sel.any(), reg
         for k, v in vals.items():
-            f[k][sel] = v
+            # a formula field is evaluated at the element centre, as the assembly does
+            f[k][sel] = [v(*c) for c in el_c[sel]] if callable(v) else v
     bc_c = centres(m["nodes"], m["bc_dim"], m["bc_nodes"])
     b = dict(bc_type=np.zeros(nb, np.int32), bc_pressure=np.zeros(nb), bc_flux=np.zeros(nb),
              bc_robin_sigma=np.zeros(nb))
@@ -189,6 +193,17 @@ def main():
           **water_balance(t("01_steady_flow_123d", "ref_output", "flow_gmsh.con", "water_balance.out"))},
          "t01", "tests/01_steady_flow_123d flow_gmsh.con; raw_output %.8g, node pressures of the output "
          "mesh (%g), water_balance.out (%g); solver -ksp_rtol 1e-10")
+    # test 08: sources on a square, exact p = (1-x^2)(1-y^2), homogeneous Dirichlet
+    vtu8 = lambda nm: vtu_cell_array(t("08_steady_flow_sources", "ref_output", "flow_vtk.con", "flow",
+                                       "flow-000000.vtu"), nm)
+    case(t("08_steady_flow_sources", "input", "test08.msh"),
+         {"plane": {"anisotropy": 1.0,
+                    "water_source_density": lambda x, y, z: 2 * (1 - x ** 2) + 2 * (1 - y ** 2)}},
+         {".plane_boundary": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure": vtu8("pressure_elements_[L]"), "ref_node_pressure": vtu8("pressure_nodes_[L]"),
+          "ref_flux": vtu8("velocity_elements_[L/T]").reshape(-1, 3),
+          **water_balance(t("08_steady_flow_sources", "ref_output", "flow_vtk.con", "water_balance.txt"))},
+         "t08", "tests/08_steady_flow_sources flow_vtk.con VTK (ascii) and water_balance.txt; solver accuracy 1e-7")
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
                                       "test05-000000.vtu"), "pressure_elements_[L]")

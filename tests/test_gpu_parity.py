@@ -24,7 +24,7 @@ from mhdarcy.cases import dirichlet_x_bc, make_case
 
 pytestmark = pytest.mark.gpu
 
-FIXTURES = ["t01", "t05_dirichlet", "t05_neumann", "t05_robin", "t06_32", "t06_21"]
+FIXTURES = ["t01", "t05_dirichlet", "t05_neumann", "t05_robin", "t06_32", "t06_21", "t08"]
 
 
 def gpu_system(mesh, coeffs, bc):
