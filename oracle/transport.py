@@ -84,3 +84,52 @@ def transport_matrix(mesh, topo, sol, cross_section=1.0, porosity=1.0):
     cols = np.array([k[1] for k in keys])
     vals = np.array([entries[k] for k in keys])
     return sp.csr_matrix((vals, (rows, cols)), shape=(ne, ne)), (1.0 / max_sum if max_sum > 0 else np.inf)
+
+
+def boundary_inflow(mesh, topo, sol, bdr_conc, cross_section=1.0, porosity=1.0):
+    """The boundary term of the explicit step (ConvectionTransport::set_boundary_conditions,
+    transport.cc:455-491): for every boundary side of element i with inflow (q < 0),
+    -q / (|E_i| delta_i por_i) * c_b, c_b the concentration of that boundary object."""
+    xyz = np.asarray(mesh.nodes, np.float64)
+    eln = np.asarray(mesh.el_nodes)
+    dim = np.asarray(mesh.el_dim)
+    ne = len(dim)
+    cs = np.broadcast_to(np.asarray(cross_section, np.float64), (ne,))
+    por = np.broadcast_to(np.asarray(porosity, np.float64), (ne,))
+    ss, sb = topo["el_side_start"], topo["side_bdr"]
+    out = np.zeros(ne)
+    for i in range(ne):
+        for s in range(ss[i], ss[i + 1]):
+            if sb[s] >= 0 and sol[s] < 0.0:
+                out[i] += bdr_conc[sb[s]] * (-(sol[s] / (element_measure(xyz, eln[i], dim[i]) * cs[i] * por[i])))
+    return out
+
+
+def step_count(full_step, cfl):
+    """Steps of the time governor over a fixed interval (TimeGovernor::estimate_dt,
+    src/coupling/time_governor.cc:261-300): the step is min(interval, CFL step), the count the
+    ceiling of interval / step, or its floor when that is within 1e-14 of the ratio."""
+    est = min(full_step, cfl)
+    ratio = full_step / est
+    n = int(np.ceil(ratio))
+    nf = int(np.floor(ratio))
+    return nf if abs(ratio - nf) < 1e-14 else n
+
+
+def explicit_transport(A, bcv, cfl, c0, output_times):
+    """Concentrations at output_times (increasing, from 0) of the explicit scheme
+    c <- (I + dt A) c + dt bcv (ConvectionTransport::compute_one_step, transport.cc:593-716),
+    with dt fixed over each interval between outputs (set_target_time + fix_dt_until_mark:
+    interval / step_count)."""
+    c = np.array(c0, np.float64)
+    t = 0.0
+    out = []
+    for target in output_times:
+        if target > t:
+            n = step_count(target - t, cfl)
+            dt = (target - t) / n
+            for _ in range(n):
+                c = c + dt * (A @ c) + dt * bcv
+            t = target
+        out.append(c.copy())
+    return np.array(out)

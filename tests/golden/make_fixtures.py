@@ -15,7 +15,9 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
   * t08            tests/08_steady_flow_sources: element and node pressures, element velocities
                    of the VTK output, and its water balance (a source field given by a formula);
   * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
-  * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5.
+  * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5;
+  * t13            tests/13_edge_solute_mixing: legacy side-based boundary data, the flow outputs
+                   and the concentrations of the explicit transport every 0.5 up to t = 100.
 The parsers here are self-contained (independent of the package under test).
 """
 import os
@@ -178,6 +180,93 @@ def case(mesh_path, bulk, bcs, extra, out_name, meta):
     print(out_name, ne, "elements", nb, "boundary elements", list(extra))
 
 
+def legacy_flow_bcd(path):
+    """Rows of a legacy flow boundary file ($BoundaryConditions): (condition id, type, value,
+    element id, local side) for conditions given by element and side (OldBcdInput::read_flow,
+    src/flow/old_bcd.cc): type 1 Dirichlet (value = pressure), 2 Neumann (value = flux)."""
+    lines = open(path).read().split("\n")
+    k = next(i for i, l in enumerate(lines) if l.strip() == "$BoundaryConditions")
+    rows = []
+    for line in lines[k + 2:k + 2 + int(lines[k + 1])]:
+        v = line.split()
+        cid, typ = int(v[0]), int(v[1])
+        assert typ in (1, 2) and int(v[3]) == 2, line  # value, then "by element and side"
+        rows.append((cid, typ, float(v[2]), int(v[4]), int(v[5])))
+    return rows
+
+
+def legacy_transport_bcd(path):
+    """{condition id: concentrations} of a legacy transport boundary file ($Transport_BCD):
+    each row names the flow condition whose boundary it applies to (OldBcdInput::read_transport)."""
+    lines = open(path).read().split("\n")
+    k = next(i for i, l in enumerate(lines) if l.strip() == "$Transport_BCD")
+    out = {}
+    for line in lines[k + 2:k + 2 + int(lines[k + 1])]:
+        v = line.split()
+        out[int(v[0])] = [float(x) for x in v[2:]]
+    return out
+
+
+def gmsh_element_data_blocks(path, name):
+    """(times, values [n_blocks, n_entities]) of every $ElementData block of a field, in file order."""
+    txt = open(path).read().split("\n")
+    times, vals = [], []
+    for k, l in enumerate(txt):
+        if l.strip() != "$ElementData" or txt[k + 2].strip().strip('"') != name:
+            continue
+        n_str = int(txt[k + 1])
+        n_real = int(txt[k + 2 + n_str])
+        times.append(float(txt[k + 3 + n_str]) if n_real else 0.0)
+        n_int = int(txt[k + 3 + n_str + n_real])
+        n_ent = int(txt[k + 6 + n_str + n_real])
+        first = k + 4 + n_str + n_real + n_int
+        vals.append([float(r.split()[1]) for r in txt[first:first + n_ent]])
+    return np.array(times), np.array(vals)
+
+
+def case_t13(t):
+    """tests/13_edge_solute_mixing (flow_gmsh.con): a fork of three strips meeting on one edge,
+    flow and transport boundary conditions in the legacy side-based files, explicit convection of
+    one substance up to t = 100 with output every 0.5."""
+    d = lambda *p: t("13_edge_solute_mixing", *p)
+    m, names = parse_gmsh(d("input", "test13.msh"))
+    ne = len(m["el_dim"])
+    aniso = {17: 1.0, 18: 0.1, 19: 1.0}
+    f = dict(conductivity=np.ones(ne), anisotropy=np.array([aniso[r] for r in m["el_region"]]),
+             cross_section=np.ones(ne), sigma=np.ones(ne), water_source_density=np.zeros(ne),
+             storativity=np.ones(ne), init_pressure=np.zeros(ne))
+    fb = legacy_flow_bcd(d("input", "test13.fbc"))
+    tb = legacy_transport_bcd(d("input", "test13.tbc"))
+    eidx = {int(e): i for i, e in enumerate(m["el_id"])}
+    legacy = dict(lbc_id=np.array([r[0] for r in fb], np.int32), lbc_type=np.array([r[1] for r in fb], np.int32),
+                  lbc_value=np.array([r[2] for r in fb]), lbc_element=np.array([eidx[r[3]] for r in fb], np.int32),
+                  lbc_side=np.array([r[4] for r in fb], np.int32),
+                  lbc_conc=np.array([tb.get(r[0], [0.0])[0] for r in fb]))
+    out = d("ref_output", "flow_gmsh.con")
+    ct, cv = gmsh_element_data_blocks(os.path.join(out, "transport.msh"), "A_mobile_[M/L^3]")
+    fl = os.path.join(out, "test13.msh")
+    ref = dict(ref_pressure=gmsh_element_data_blocks(fl, "pressure_elements_[L]")[1][0],
+               ref_flux=np.array(gmsh_element_vectors(fl, "velocity_elements_[L/T]")),
+               ref_node_pressure=gmsh_node_data(fl, "pressure_nodes_[L]", d("input", "test13.msh")),
+               ref_conc_times=ct, ref_conc=cv)
+    np.savez_compressed(os.path.join(OUT, "t13.npz"), **m, **f, **legacy, **ref,
+                        meta=np.array("tests/13_edge_solute_mixing flow_gmsh.con: legacy .fbc/.tbc boundary "
+                                      "data, transport.msh concentrations every 0.5 (por_m = 1), flow outputs"))
+    print("t13", ne, "elements", len(fb), "legacy conditions", len(ct), "concentration outputs")
+
+
+def gmsh_element_vectors(path, name):
+    """The first $ElementData block of a 3-component field: [n_entities, 3]."""
+    txt = open(path).read().split("\n")
+    k = next(i for i, l in enumerate(txt) if l.strip() == "$ElementData" and txt[i + 2].strip().strip('"') == name)
+    n_str = int(txt[k + 1])
+    n_real = int(txt[k + 2 + n_str])
+    n_int = int(txt[k + 3 + n_str + n_real])
+    n_ent = int(txt[k + 6 + n_str + n_real])
+    first = k + 4 + n_str + n_real + n_int
+    return [[float(x) for x in r.split()[1:4]] for r in txt[first:first + n_ent]]
+
+
 def main():
     t = lambda *p: os.path.join(REF, "tests", *p)
     # test 01: 1D-2D-3D steady flow, n_schurs = 2
@@ -204,6 +293,7 @@ def main():
           "ref_flux": vtu8("velocity_elements_[L/T]").reshape(-1, 3),
           **water_balance(t("08_steady_flow_sources", "ref_output", "flow_vtk.con", "water_balance.txt"))},
          "t08", "tests/08_steady_flow_sources flow_vtk.con VTK (ascii) and water_balance.txt; solver accuracy 1e-7")
+    case_t13(t)
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
                                       "test05-000000.vtu"), "pressure_elements_[L]")

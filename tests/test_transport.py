@@ -35,6 +35,42 @@ def test_oracle_conserves_mass():
     assert cfl == 1.0 / np.abs(A.diagonal()).max()
 
 
+def t13_problem():
+    """tests/13_edge_solute_mixing: the boundary objects of the legacy side-based conditions
+    get their flow data (Dirichlet pressures) and transport concentration; the others have no
+    condition (no flux) and concentration 0."""
+    z, mesh = load_fixture("t13")
+    topo = T.build(mesh)
+    nb = len(topo["bdr_edge"])
+    bt, bp, conc = np.zeros(nb, np.int32), np.zeros(nb), np.zeros(nb)
+    ss, sb = topo["el_side_start"], topo["side_bdr"]
+    for e, s, typ, val, c in zip(z["lbc_element"], z["lbc_side"], z["lbc_type"], z["lbc_value"], z["lbc_conc"]):
+        b = sb[ss[e] + s]
+        assert b >= 0
+        bt[b], bp[b], conc[b] = typ, val, c
+    co = fixture_coeffs(z)
+    P = oracle_problem(mesh, topo, topo["n_edges"], co, {"bc_type": bt, "pressure": bp})
+    return z, mesh, topo, P, conc
+
+
+def test_t13_reference_transport_run():
+    """The reference's own transport run: the flow outputs of test 13 (printed with 6 digits)
+    and the concentrations of its explicit transport at all 200 outputs up to t = 100 (three
+    CFL-limited steps per 0.5 interval, mixing where the three strips meet), from the oracle's
+    convection matrix, boundary inflow term and time steps."""
+    z, mesh, topo, P, conc = t13_problem()
+    sol = O.solve_mh_direct(P)
+    ns, ne = P.n_sides, P.n_el
+    assert np.abs(sol[ns:ns + ne] - z["ref_pressure"]).max() < 2e-5
+    assert np.abs(O.element_flux(P, sol) - z["ref_flux"]).max() < 2e-6
+    A, cfl = TR.transport_matrix(mesh, topo, sol)
+    assert TR.step_count(0.5, cfl) == 3
+    c = TR.explicit_transport(A, TR.boundary_inflow(mesh, topo, sol, conc), cfl, np.zeros(ne), z["ref_conc_times"])
+    assert len(z["ref_conc_times"]) == 201 and z["ref_conc_times"][-1] == 100.0
+    assert np.abs(c - z["ref_conc"]).max() < 5e-6
+    assert z["ref_conc"][10].min() < 0.7 < z["ref_conc"][10].max()  # a front is inside the domain at t = 5
+
+
 def check_against_oracle(s, mesh, sol, cross_section, porosity):
     (rp, col, val), cfl = s.transport_matrix(porosity)
     A, cfl_ref = TR.transport_matrix(mesh, s.topology(), sol, cross_section,
