@@ -1,6 +1,8 @@
 // See system_build.hpp.
 #include "system_build.hpp"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cstdio>
 
@@ -147,11 +149,17 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     set_launch_shape(hs, rows_per_thread, target_blocks);
 
     // symmetric pattern: every pair of an element's local edges
+    // (each row is sorted and deduplicated below, so the rows are filled in parallel in any order)
     std::vector<int64_t> cnt(hs.n_rows + 1, 0);
     int32_t loc[16];
+#pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < n_el; ++e) {
-        int c = local_edges(m, t, e, loc);
-        for (int a = 0; a < c; ++a) cnt[hs.edge_row[loc[a]] + 1] += c;
+        int32_t lc[16];
+        int c = local_edges(m, t, e, lc);
+        for (int a = 0; a < c; ++a) {
+#pragma omp atomic
+            cnt[hs.edge_row[lc[a]] + 1] += c;
+        }
     }
     for (int64_t r = 0; r < hs.n_rows; ++r)
         if (hs.row_edge[r] < 0) cnt[r + 1] += 1;
@@ -159,11 +167,19 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     std::vector<int32_t> raw(cnt[hs.n_rows]);
     {
         std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+#pragma omp parallel for schedule(static)
         for (int64_t e = 0; e < n_el; ++e) {
-            int c = local_edges(m, t, e, loc);
+            int32_t lc[16];
+            int c = local_edges(m, t, e, lc);
             for (int a = 0; a < c; ++a) {
-                int64_t ra = hs.edge_row[loc[a]];
-                for (int b = 0; b < c; ++b) raw[fill[ra]++] = hs.edge_row[loc[b]];
+                const int64_t ra = hs.edge_row[lc[a]];
+                int64_t pos;
+#pragma omp atomic capture
+                {
+                    pos = fill[ra];
+                    fill[ra] += c;
+                }
+                for (int b = 0; b < c; ++b) raw[pos + b] = hs.edge_row[lc[b]];
             }
         }
         for (int64_t r = 0; r < hs.n_rows; ++r)
@@ -179,6 +195,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     }
     for (int64_t r = 0; r < hs.n_rows; ++r) hs.row_ptr[r + 1] = hs.row_ptr[r] + len[r];
     hs.row_col.resize(hs.row_ptr[hs.n_rows]);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < hs.n_rows; ++r)
         std::copy(raw.begin() + cnt[r], raw.begin() + cnt[r] + len[r], hs.row_col.begin() + hs.row_ptr[r]);
     hs.nnz = 0;
@@ -201,6 +218,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     }
     hs.sell_col.resize(hs.n_slots);
     hs.diag_slot.resize(hs.n_rows);
+#pragma omp parallel for schedule(static)
     for (int64_t r = 0; r < hs.n_rows; ++r) {
         int64_t s = r / kSliceRowsHost, lane = r % kSliceRowsHost;
         int64_t off = hs.slice_off[s], w = (hs.slice_off[s + 1] - off) / kSliceRowsHost;
@@ -222,7 +240,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     // filling then walk the chunk in element order.
     constexpr int64_t kChunk = 1 << 18;
     std::vector<int64_t> coff(kChunk + 1);
-    std::vector<int64_t> cslot;
+    std::vector<int32_t> cslot;  // n_slots < 2^31 (checked above)
     auto chunk_slots = [&](int64_t e0, int64_t e1) {
         coff[0] = 0;
         for (int64_t e = e0; e < e1; ++e) {
@@ -237,7 +255,7 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
             int64_t o = coff[e - e0];
             for (int a = 0; a < c; ++a) {
                 const int64_t ra = hs.edge_row[lc[a]];
-                for (int b = 0; b < c; ++b) cslot[o++] = slot_of(ra, hs.edge_row[lc[b]]);
+                for (int b = 0; b < c; ++b) cslot[o++] = (int32_t)slot_of(ra, hs.edge_row[lc[b]]);
             }
         }
     };
@@ -260,20 +278,30 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     hs.slot_cidx.resize(hs.slot_cstart[hs.n_slots]);
     hs.row_cidx.resize(hs.row_cstart[hs.n_rows]);
     {
+        // every thread owns a contiguous range of slots and of rows and walks the chunk in element
+        // order, writing only its own lists: each list keeps the element order
         std::vector<int32_t> sf(hs.slot_cstart.begin(), hs.slot_cstart.end() - 1);
         std::vector<int32_t> rf(hs.row_cstart.begin(), hs.row_cstart.end() - 1);
         for (int64_t e0 = 0; e0 < n_el; e0 += kChunk) {
             const int64_t e1 = std::min(n_el, e0 + kChunk);
             chunk_slots(e0, e1);
-            for (int64_t e = e0; e < e1; ++e) {
-                int c = local_edges(m, t, e, loc);
-                const int64_t o = coff[e - e0];
-                for (int a = 0; a < c; ++a) {
-                    int64_t ra = hs.edge_row[loc[a]];
-                    hs.row_cidx[rf[ra]++] = (int32_t)(hs.rhs_off[e] + a);
-                    for (int b = 0; b < c; ++b) {
-                        const int64_t sl = cslot[o + (int64_t)a * c + b];
-                        hs.slot_cidx[sf[sl]++] = (int32_t)(hs.blk_off[e] + (int64_t)a * c + b);
+#pragma omp parallel
+            {
+                const int nt = omp_get_num_threads(), th = omp_get_thread_num();
+                const int64_t s_lo = hs.n_slots * th / nt, s_hi = hs.n_slots * (th + 1) / nt;
+                const int64_t r_lo = hs.n_rows * th / nt, r_hi = hs.n_rows * (th + 1) / nt;
+                int32_t lc[16];
+                for (int64_t e = e0; e < e1; ++e) {
+                    const int c = local_edges(m, t, e, lc);
+                    const int64_t o = coff[e - e0];
+                    for (int a = 0; a < c; ++a) {
+                        const int64_t ra = hs.edge_row[lc[a]];
+                        if (ra >= r_lo && ra < r_hi) hs.row_cidx[rf[ra]++] = (int32_t)(hs.rhs_off[e] + a);
+                        for (int b = 0; b < c; ++b) {
+                            const int64_t sl = cslot[o + (int64_t)a * c + b];
+                            if (sl >= s_lo && sl < s_hi)
+                                hs.slot_cidx[sf[sl]++] = (int32_t)(hs.blk_off[e] + (int64_t)a * c + b);
+                        }
                     }
                 }
             }
