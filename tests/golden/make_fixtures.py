@@ -11,6 +11,9 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
                    per element pressure, barycentric flux, side (edge) pressures, side fluxes;
                    the node pressures of the output mesh ($NodeData "pressure_nodes_[L]"); the
                    boundary and source tables of water_balance.out;
+  * t03            tests/03_transport_small_12d (flow part of flow_vtk.con): element and node
+                   pressures, element velocities of the VTK output and the water balance of a
+                   1D-2D network with a three-channel junction;
   * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output;
   * t08            tests/08_steady_flow_sources: element and node pressures, element velocities
                    of the VTK output, and its water balance (a source field given by a formula);
@@ -293,6 +296,20 @@ def main():
           "ref_flux": vtu8("velocity_elements_[L/T]").reshape(-1, 3),
           **water_balance(t("08_steady_flow_sources", "ref_output", "flow_vtk.con", "water_balance.txt"))},
          "t08", "tests/08_steady_flow_sources flow_vtk.con VTK (ascii) and water_balance.txt; solver accuracy 1e-7")
+    # test 03 (flow part of flow_vtk.con): 1D channels on edges of a 2D square meeting at a
+    # junction of three channels, Dirichlet p = x + y on every boundary region (points and lines)
+    vtu3 = lambda nm: vtu_cell_array(t("03_transport_small_12d", "ref_output", "flow_vtk.con", "test3",
+                                       "test3-000000.vtu"), nm)
+    case(t("03_transport_small_12d", "input", "mesh_with_boundary.msh"),
+         {"1d_upper": {"conductivity": 10.0}, "1d_lower": {"conductivity": 10.0},
+          "1d_left_branch": {"conductivity": 10.0}, "2d": {"conductivity": 1.0}},
+         {r: {"type": "dirichlet", "pressure": lambda x, y, z: x + y}
+          for r in (".1d_top", ".1d_left", ".1d_bottom", ".2d_top", ".2d_right", ".2d_bottom", ".2d_left")},
+         {"ref_pressure": vtu3("pressure_elements_[L]"), "ref_node_pressure": vtu3("pressure_nodes_[L]"),
+          "ref_flux": vtu3("velocity_elements_[L/T]").reshape(-1, 3),
+          **water_balance(t("03_transport_small_12d", "ref_output", "flow_vtk.con", "water_balance.txt"))},
+         "t03", "tests/03_transport_small_12d flow_vtk.con VTK (ascii, 16 digits) and water_balance.txt (%g); "
+         "solver r_tol 1e-12, a_tol 1e-12")
     case_t13(t)
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",

@@ -50,9 +50,9 @@ def test_t01_element_flux_vectors():
     assert np.all(np.abs(u - ref) <= 1e-8 + 5e-9 * np.abs(ref))
 
 
-def t01_regions(z, topo):
-    """Region indices of t01's boundary objects (through their boundary elements) and
-    elements, and the region ids in index order."""
+def fixture_regions(z, topo):
+    """Region indices of a fixture's boundary objects (through their boundary elements, so
+    every boundary object must have one) and elements, and the region ids in index order."""
     bids = sorted(set(z["bc_region"].tolist()))
     eids = sorted(set(z["el_region"].tolist()))
     bdr = np.array([bids.index(z["bc_region"][b]) for b in topo["bdr_bc_element"]], np.int32)
@@ -75,7 +75,7 @@ def test_t01_water_balance():
     reference solver's own 1e-10 tolerance.  t01 has no sources."""
     z, mesh, topo, P = problem("t01")
     assert np.all(topo["bdr_bc_element"] >= 0)  # every boundary object has its element
-    bdr, el, bids, eids = t01_regions(z, topo)
+    bdr, el, bids, eids = fixture_regions(z, topo)
     ob, osrc = O.water_balance(P, O.solve_mh_direct(P), bdr, el)
     scale = np.abs(z["ref_bdr_balance"][:, 1:]).max()
     for rid, *vals in z["ref_bdr_balance"]:
@@ -103,6 +103,37 @@ def test_t08_sources():
     ob, osrc = O.water_balance(P, sol, np.zeros(len(topo["bdr_bc_element"]), np.int32), np.zeros(ne, np.int32))
     assert abs(osrc[0] - z["ref_src_balance"][0, 1]) <= 5e-6 * abs(osrc[0])
     assert abs(ob[0, 0] - osrc[0]) <= 1e-12 * osrc[0] and ob[0, 2] == 0.0
+
+
+def test_t03_channel_network():
+    """tests/03_transport_small_12d, flow part: 1D channels (conductivity 10) on edges of a 2D
+    square (conductivity 1), three channels meeting at one junction edge, channel ends on the
+    boundary as point elements, Dirichlet p = x + y everywhere on the boundary.  The VTK output
+    has 16 digits; the reference's CG stopped at a preconditioned relative residual of 1e-12,
+    which leaves errors of a few 1e-9 in pressures of about 1 and a few 1e-8 in velocities of
+    up to 16.  The water balance (printed %g) has regions with both outflow and inflow."""
+    z, mesh, topo, P = problem("t03")
+    assert set(np.unique(z["el_dim"])) == {1, 2} and set(np.unique(z["bc_dim"])) == {0, 1}
+    assert len(topo["ngh_element"]) > 0                         # VB couplings present
+    ss, se = topo["el_side_start"], topo["side_edge"]
+    assert np.bincount(se[:ss[-1]]).max() >= 3                  # the junction edge
+    sol = O.solve_mh_direct(P)
+    ns, ne = P.n_sides, P.n_el
+    assert np.abs(sol[ns:ns + ne] - z["ref_pressure"]).max() < 1e-8
+    assert np.abs(O.node_pressure(P, sol) - z["ref_node_pressure"]).max() < 1e-8
+    assert np.abs(O.element_flux(P, sol) - z["ref_flux"]).max() < 1e-7
+    assert np.all(topo["bdr_bc_element"] >= 0)
+    bdr, el, bids, eids = fixture_regions(z, topo)
+    ob, osrc = O.water_balance(P, sol, bdr, el)
+    scale = np.abs(z["ref_bdr_balance"][:, 1:]).max()
+    mixed = 0
+    for rid, *vals in z["ref_bdr_balance"]:
+        got = ob[bids.index(int(rid))]
+        assert np.all(np.abs(got - vals) <= 5e-6 * np.abs(vals) + 1e-12 * scale), (rid, got, vals)
+        mixed += vals[1] > 0 and vals[2] < 0
+    assert mixed == 2
+    for rid, val in z["ref_src_balance"]:
+        assert osrc[eids.index(int(rid))] == val == 0.0
 
 
 def test_t01_schur_path_equals_direct():
