@@ -28,6 +28,7 @@
 #define MH_DARCY_H
 
 #include <stdint.h>
+#include <stddef.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -45,6 +46,7 @@ extern "C" {
 #define MH_ERR_NONFINITE   -6   /* NaN/Inf in coefficients or in the iteration            */
 #define MH_ERR_TOPOLOGY    -7   /* the mesh violates a rule of the reference topology     */
 #define MH_ERR_BREAKDOWN   -8   /* CG breakdown (p'Sp <= 0): system not SPD               */
+#define MH_ERR_IO          -9   /* a file cannot be opened or read                        */
 
 /* ---- boundary condition types (DarcyFlowMH::EqData::BC_Type, darcy_flow_mh.cc:81-87) --- */
 #define MH_BC_NONE       0
@@ -179,6 +181,53 @@ int mh_cube_mesh_create(int32_t n, int32_t n_planes, const int32_t *plane_axis,
                         const int32_t *line_a, const int32_t *line_b, mh_mesh **out);
 int mh_mesh_describe(const mh_mesh *m, mh_mesh_desc *desc);
 void mh_mesh_destroy(mh_mesh *m);
+
+/* ---- gmsh 2.2 ASCII input (GmshMeshReader, src/mesh/msh_gmshreader.cc) -------------- */
+/* Reads $PhysicalNames, $Nodes and $Elements (read_mesh, msh_gmshreader.cc:75-244) into a
+ * mesh for mh_create.  Elements of types 1, 2, 4 and 15 (line, triangle, tetrahedron,
+ * point) with at least two tags; the first tag is the physical region, the third (if any)
+ * the partition.  Regions follow RegionDB::add_region (src/mesh/region.cc:107-175): a named
+ * region is a boundary region when its name starts with '.', an id met only in $Elements
+ * becomes the bulk region "region_<id>", and an element whose dimension differs from its
+ * region's is an error.  Elements of boundary regions become boundary elements, the others
+ * bulk elements (points in bulk regions are skipped), both in file order.  Empty lines and
+ * lines starting with '#' are skipped and tokens may be quoted (Tokenizer,
+ * src/system/tokenizer.cc).  Node ids may be sparse; a repeated node or element id is an
+ * error.  Returns MH_ERR_IO when the file cannot be read and MH_ERR_INVALID for a format
+ * error; the message (file line included) goes to err[err_len] when err is not NULL. */
+int mh_gmsh_read(const char *path, mh_mesh **out, char *err, size_t err_len);
+
+typedef struct mh_gmsh_info {
+    const int64_t *node_id;            /* [n_nodes] ids of the file                       */
+    const int64_t *el_id;              /* [n_elements]                                   */
+    const int32_t *el_region;          /* [n_elements] physical id                       */
+    const int32_t *el_partition;       /* [n_elements] third tag, 0 if absent            */
+    const int64_t *bc_id;              /* [n_bc_elements]                                */
+    const int32_t *bc_region;          /* [n_bc_elements]                                */
+    int32_t        n_regions;          /* $PhysicalNames in file order, then the regions
+                                          met only in $Elements, in order of appearance  */
+    const int32_t *region_id;
+    const int32_t *region_dim;
+    const int32_t *region_boundary;    /* 1 for a boundary region                        */
+    const char *const *region_name;
+} mh_gmsh_info;
+/* Ids and regions of a mesh read by mh_gmsh_read (MH_ERR_INVALID for other meshes).  The
+ * arrays live as long as the mesh. */
+int mh_gmsh_info_get(const mh_mesh *m, mh_gmsh_info *info);
+
+/* Values of the element field `field` at `time` for the elements with ids el_ids[n_ids]
+ * (strictly ascending), n_components per element, into out[n_ids*n_components]
+ * (GmshMeshReader::read_element_data, msh_gmshreader.cc:251-396): the $ElementData
+ * sections of the field are taken in file order while their time is <= time*(1 + 2 eps),
+ * each overwriting the elements it lists; a row "id v_1 .. v_n" is matched against el_ids
+ * with a pointer that only moves forward, rows of other ids are skipped, and a row past the
+ * last id ends its section.  Elements no section lists stay NaN.  A section's own component
+ * and entity counts are only used to find its rows.  MH_ERR_INVALID when the file has no
+ * section of the field, none at or before `time`, or a row that is read has fewer than
+ * n_components values or a malformed number. */
+int mh_gmsh_element_data(const char *path, const char *field, double time, int64_t n_ids,
+                         const int64_t *el_ids, int32_t n_components, double *out, char *err,
+                         size_t err_len);
 
 /* ---- the MH system (DarcyFlowMH_Steady, darcy_flow_mh.cc:249-433) ------------------- */
 /* Builds edges, boundaries and VB neighbours on the host (Mesh::setup_topology,

@@ -18,13 +18,11 @@
 #include "device_system.hpp"
 #include "amg.hpp"
 #include "learned.hpp"
+#include "mesh_store.hpp"
 #include "mh_darcy.h"
 #include "system_build.hpp"
 #include "topology.hpp"
 
-struct mh_mesh {
-    mh::MeshData m;
-};
 
 enum class Pc { Nn, Cheb, Amg };  // preconditioners of the flexible-CG solve
 
@@ -1230,6 +1228,7 @@ const char *mh_status_string(int s) {
         case MH_ERR_NONFINITE: return "non-finite value";
         case MH_ERR_TOPOLOGY: return "invalid mesh topology";
         case MH_ERR_BREAKDOWN: return "CG breakdown";
+        case MH_ERR_IO: return "file cannot be read";
         default: return "unknown status";
     }
 }

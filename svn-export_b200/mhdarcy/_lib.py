@@ -24,6 +24,7 @@ MH_ERR_NOMEM = -5
 MH_ERR_NONFINITE = -6
 MH_ERR_TOPOLOGY = -7
 MH_ERR_BREAKDOWN = -8
+MH_ERR_IO = -9
 
 MH_BC_NONE, MH_BC_DIRICHLET, MH_BC_NEUMANN, MH_BC_ROBIN = 0, 1, 2, 3
 
@@ -36,12 +37,19 @@ MH_SOLVER_AMG = 4
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
 _f32p = C.POINTER(C.c_float)
+_i64p = C.POINTER(C.c_int64)
 
 
 class MeshDesc(C.Structure):
     _fields_ = [("n_nodes", C.c_int64), ("node_xyz", _f64p), ("n_elements", C.c_int64),
                 ("el_dim", _i32p), ("el_nodes", _i32p), ("n_bc_elements", C.c_int64),
                 ("bc_dim", _i32p), ("bc_nodes", _i32p)]
+
+
+class GmshInfo(C.Structure):
+    _fields_ = [("node_id", _i64p), ("el_id", _i64p), ("el_region", _i32p), ("el_partition", _i32p),
+                ("bc_id", _i64p), ("bc_region", _i32p), ("n_regions", C.c_int32), ("region_id", _i32p),
+                ("region_dim", _i32p), ("region_boundary", _i32p), ("region_name", C.POINTER(C.c_char_p))]
 
 
 class Sizes(C.Structure):
@@ -117,6 +125,10 @@ def _load():
                                           _i32p, C.POINTER(vp)]),
         "mh_mesh_describe": (C.c_int, [vp, C.POINTER(MeshDesc)]),
         "mh_mesh_destroy": (None, [vp]),
+        "mh_gmsh_read": (C.c_int, [C.c_char_p, C.POINTER(vp), C.c_char_p, C.c_size_t]),
+        "mh_gmsh_info_get": (C.c_int, [vp, C.POINTER(GmshInfo)]),
+        "mh_gmsh_element_data": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, C.c_int64, vp, C.c_int32, vp,
+                                           C.c_char_p, C.c_size_t]),
         "mh_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(vp)]),
         "mh_destroy": (None, [vp]),
         "mh_set_stream": (C.c_int, [vp, vp]),
@@ -167,7 +179,7 @@ lib = _load()
 # every symbol the header declares, for the load/export check
 EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_error",
             "mh_cube_mesh_create", "mh_mesh_describe", "mh_mesh_destroy", "mh_create", "mh_destroy",
-            "mh_set_stream", "mh_kernel_launches",
+            "mh_gmsh_read", "mh_gmsh_info_get", "mh_gmsh_element_data", "mh_set_stream", "mh_kernel_launches",
             "mh_get_sizes", "mh_get_topology", "mh_set_coeffs", "mh_set_bc", "mh_assemble",
             "mh_solve", "mh_get_solution", "mh_get_solution_device",
             "mh_get_element_flux", "mh_get_element_flux_device", "mh_raw_output_write",

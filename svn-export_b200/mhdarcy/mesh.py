@@ -1,11 +1,13 @@
-"""Meshes as flat arrays: the synthetic Kuhn cube meshes and a gmsh 2.2 ASCII reader.
+"""Meshes as flat arrays: the synthetic Kuhn cube meshes and gmsh 2.2 ASCII input (meshes and
+$ElementData fields) through the library's parallel reader.
 
-The gmsh reader follows GmshMeshReader (src/mesh/msh_gmshreader.cc:125-260): elements keep
+The gmsh reader follows GmshMeshReader (src/mesh/msh_gmshreader.cc:75-396): elements keep
 file order; an element whose physical region name starts with '.' is a boundary element
-(read_physical_names, msh_gmshreader.cc:242-262); element types 1/2/4/15 are lines,
+(read_physical_names, msh_gmshreader.cc:220-244); element types 1/2/4/15 are lines,
 triangles, tetrahedra and points.
 """
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -25,6 +27,10 @@ class Mesh:
     bc_region: np.ndarray = None           # physical region id per boundary element
     el_id: np.ndarray = None               # gmsh element ids
     region_names: dict = field(default_factory=dict)
+    bc_id: np.ndarray = None               # gmsh ids of the boundary elements
+    node_id: np.ndarray = None             # gmsh node ids
+    el_partition: np.ndarray = None        # third element tag (0 if absent)
+    regions: list = field(default_factory=list)  # (id, dim, boundary, name) in creation order
 
     def __post_init__(self):
         self.nodes = np.ascontiguousarray(self.nodes, dtype=np.float64).reshape(-1, 3)
@@ -115,132 +121,70 @@ def cube_mesh(n, planes=(), lines=()):
     return Mesh(nodes, dim, eln)
 
 
+def _err_buf():
+    return C.create_string_buffer(1024)
+
+
+def _raise(rc, err):
+    msg = err.value.decode(errors="replace")
+    if rc == _lib.MH_ERR_IO:
+        raise OSError(msg)
+    if rc == _lib.MH_ERR_NOMEM:
+        raise MemoryError(msg)
+    raise ValueError(msg)
+
+
 def read_gmsh(path):
-    """Reads a gmsh 2.2 ASCII mesh (nodes, elements, physical names)."""
-    with open(path) as f:
-        lines = f.read().split("\n")
-    i = 0
-    names = {}
-    node_ids = []
-    coords = []
-    bulk = []
-    bnd = []
-    boundary_regions = set()
-    while i < len(lines):
-        s = lines[i].strip()
-        if s == "$PhysicalNames":
-            n = int(lines[i + 1])
-            for k in range(n):
-                parts = lines[i + 2 + k].split(None, 2)
-                dim, rid, name = int(parts[0]), int(parts[1]), parts[2].strip().strip('"')
-                names[rid] = name
-                if name.startswith("."):
-                    boundary_regions.add(rid)
-            i += n + 2
-        elif s == "$Nodes":
-            n = int(lines[i + 1])
-            for k in range(n):
-                p = lines[i + 2 + k].split()
-                node_ids.append(int(p[0]))
-                coords.append([float(p[1]), float(p[2]), float(p[3])])
-            i += n + 2
-        elif s == "$Elements":
-            n = int(lines[i + 1])
-            nmap = {nid: k for k, nid in enumerate(node_ids)}
-            tdim = {1: 1, 2: 2, 4: 3, 15: 0}
-            for k in range(n):
-                p = [int(v) for v in lines[i + 2 + k].split()]
-                eid, etype, ntags = p[0], p[1], p[2]
-                dim = tdim[etype]
-                region = p[3]
-                nd = [nmap[v] for v in p[3 + ntags:3 + ntags + dim + 1]]
-                nd = nd + [-1] * (4 - len(nd))
-                rec = (eid, dim, nd, region)
-                if region in boundary_regions:
-                    bnd.append(rec)
-                elif dim > 0:
-                    bulk.append(rec)
-            i += n + 2
-        else:
-            i += 1
-    m = Mesh(np.array(coords), np.array([r[1] for r in bulk], np.int32),
-             np.array([r[2] for r in bulk], np.int32),
-             np.array([r[1] for r in bnd], np.int32) if bnd else None,
-             np.array([r[2] for r in bnd], np.int32).reshape(-1, 4) if bnd else None)
-    m.el_region = np.array([r[3] for r in bulk], np.int32)
-    m.bc_region = np.array([r[3] for r in bnd], np.int32)
-    m.el_id = np.array([r[0] for r in bulk], np.int64)
-    m.region_names = names
+    """Reads a gmsh 2.2 ASCII mesh with the library's parallel reader (mh_gmsh_read; the rules
+    of GmshMeshReader::read_mesh, src/mesh/msh_gmshreader.cc:75-244, and RegionDB::add_region,
+    src/mesh/region.cc:107-175).  Bulk and boundary elements keep file order; node indices
+    refer to the file's node order.  Raises OSError when the file cannot be read and
+    ValueError (with the file line) for a format error."""
+    h = C.c_void_p()
+    err = _err_buf()
+    rc = lib.mh_gmsh_read(os.fsencode(str(path)), C.byref(h), err, len(err))
+    if rc != _lib.MH_OK:
+        _raise(rc, err)
+    try:
+        d = _lib.MeshDesc()
+        check(lib.mh_mesh_describe(h, C.byref(d)))
+        g = _lib.GmshInfo()
+        check(lib.mh_gmsh_info_get(h, C.byref(g)))
+        arr = lambda p, n, shape=None: (np.ctypeslib.as_array(p, shape=(n,)).copy() if n else
+                                        np.zeros(0, np.dtype(p._type_)))
+        nn, ne, nb = d.n_nodes, d.n_elements, d.n_bc_elements
+        m = Mesh(arr(d.node_xyz, nn * 3).reshape(-1, 3), arr(d.el_dim, ne), arr(d.el_nodes, ne * 4).reshape(-1, 4),
+                 arr(d.bc_dim, nb) if nb else None, arr(d.bc_nodes, nb * 4).reshape(-1, 4) if nb else None)
+        m.el_region = arr(g.el_region, ne)
+        m.el_id = arr(g.el_id, ne)
+        m.el_partition = arr(g.el_partition, ne)
+        m.bc_region = arr(g.bc_region, nb)
+        m.bc_id = arr(g.bc_id, nb)
+        m.node_id = arr(g.node_id, nn)
+        m.regions = [(g.region_id[i], g.region_dim[i], bool(g.region_boundary[i]), g.region_name[i].decode())
+                     for i in range(g.n_regions)]
+        m.region_names = {r[0]: r[3] for r in m.regions}
+    finally:
+        lib.mh_mesh_destroy(h)
     return m
-
-
-def _data_header(lines, i):
-    """Parses the tags of an $ElementData header starting at line i (the string-tag count):
-    field name, time, component and entity counts, and the index of the first data line
-    (GmshMeshReader::read_data_header, src/mesh/msh_gmshreader.cc:251-303).  Missing tags
-    take the reference's defaults: time 0, one component, zero entities."""
-    n_str = int(lines[i].split()[0])
-    name = lines[i + 1].strip().strip('"') if n_str > 0 else ""
-    i += 1 + n_str
-    n_real = int(lines[i].split()[0])
-    time = float(lines[i + 1].split()[0]) if n_real > 0 else 0.0
-    i += 1 + n_real
-    n_int = int(lines[i].split()[0])
-    ints = [int(lines[i + 1 + k].split()[0]) for k in range(n_int)]
-    i += 1 + n_int
-    n_comp = ints[1] if n_int > 1 else 1
-    n_ent = ints[2] if n_int > 2 else 0
-    return name, time, n_comp, n_ent, i
 
 
 def read_element_data(path, field_name, el_ids, time=0.0, n_components=1):
     """Values of the element field `field_name` of a gmsh 2.2 file at `time`, for the elements
-    with ids `el_ids` (ascending, e.g. Mesh.el_id): an array [len(el_ids), n_components] in that
-    order, ready for MHSystem.set_coeffs.  Follows GmshMeshReader::read_element_data
+    with ids `el_ids` (strictly ascending, e.g. Mesh.el_id): an array [len(el_ids),
+    n_components] in that order, ready for MHSystem.set_coeffs.  The library's reader
+    (mh_gmsh_element_data) follows GmshMeshReader::read_element_data
     (src/mesh/msh_gmshreader.cc:306-396): the $ElementData sections of the field are taken in
-    file order, and the last one whose time is <= time (1 + 2 eps) gives the values; a data line
-    is "id v_1 .. v_n" with ids ascending, ids that are not among el_ids are skipped, and an
-    element without a line keeps the value of an earlier section (NaN if none had it).  A
-    section with another component count is read with n_components values per line, as the
-    reference does.  Raises ValueError when the file has no section of the field, when none is at
-    or before `time` (the reference then leaves the field's values unset), or when a row has
-    fewer values than n_components."""
-    ids = np.asarray(el_ids, np.int64)
-    if ids.size > 1 and np.any(np.diff(ids) <= 0):
-        raise ValueError("el_ids must be ascending")
-    with open(path) as f:
-        lines = f.read().split("\n")
-    out = np.full((ids.size, n_components), np.nan)
-    found = used = False
-    limit = time * (1.0 + 2.0 * np.finfo(float).eps)
-    i = 0
-    while i < len(lines):
-        if lines[i].strip() != "$ElementData":
-            i += 1
-            continue
-        name, t, _, n_ent, i = _data_header(lines, i + 1)
-        if name != field_name:
-            continue
-        found = True
-        if t > limit:
-            break
-        used = True
-        pos = 0
-        for row in lines[i:i + n_ent]:
-            p = row.split()
-            eid = int(p[0])
-            while pos < ids.size and ids[pos] < eid:
-                pos += 1
-            if pos == ids.size:
-                break  # an id past the last element: the rest of the section is skipped
-            if ids[pos] == eid:
-                if len(p) - 1 < n_components:
-                    raise ValueError(f"{path}: element {eid} of field '{field_name}' has {len(p) - 1} values, "
-                                     f"{n_components} expected")
-                out[pos] = [float(v) for v in p[1:1 + n_components]]
-        i += n_ent
-    if not found:
-        raise ValueError(f"{path}: no $ElementData section for field '{field_name}'")
-    if not used:
-        raise ValueError(f"{path}: no $ElementData of field '{field_name}' at or before time {time}")
+    file order, each one whose time is <= time (1 + 2 eps) overwriting the elements it lists;
+    a data line is "id v_1 .. v_n", ids that are not among el_ids are skipped, and an element
+    no section lists is NaN.  Raises ValueError when the file has no section of the field,
+    when none is at or before `time`, or when a row that is read has fewer than n_components
+    values; OSError when the file cannot be read."""
+    ids = np.ascontiguousarray(el_ids, dtype=np.int64)
+    out = np.empty((ids.size, n_components), np.float64)
+    err = _err_buf()
+    rc = lib.mh_gmsh_element_data(os.fsencode(str(path)), field_name.encode(), float(time), ids.size,
+                                  ids.ctypes.data, int(n_components), out.ctypes.data, err, len(err))
+    if rc != _lib.MH_OK:
+        _raise(rc, err)
     return out

@@ -1,4 +1,4 @@
-"""The $ElementData reader (mhdarcy.read_element_data) against the rules of the reference's
+"""The $ElementData reader (mhdarcy.read_element_data, the library's mh_gmsh_element_data) against the rules of the reference's
 GmshMeshReader::read_element_data (src/mesh/msh_gmshreader.cc:251-396), on a file written here:
 sections taken in file order up to the requested time, ids matched in ascending order, rows of
 unknown elements skipped, elements without a row keeping an earlier section's value, the
@@ -112,5 +112,5 @@ def test_errors(path):
         mhdarcy.read_element_data(path, "conductivity", IDS, time=-1.0)
     with pytest.raises(ValueError, match="ascending"):
         mhdarcy.read_element_data(path, "conductivity", [2, 1])
-    with pytest.raises(ValueError, match="4 expected"):
+    with pytest.raises(ValueError, match="fewer than 4 values"):
         mhdarcy.read_element_data(path, "anisotropy", IDS, n_components=4)

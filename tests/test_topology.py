@@ -77,19 +77,24 @@ def test_invalid_node_index_is_rejected():
 
 
 def test_gmsh_reader_round_trip(tmp_path):
+    """A fixture mesh written as gmsh 2.2 and read back by the library's reader: one physical
+    region per dimension (a region has one dimension), boundary regions named with '.'."""
     z, mesh = load_fixture("t06_21")
     path = tmp_path / "m.msh"
-    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", "2", '1 1 "plane"', '1 2 ".bnd"',
-             "$EndPhysicalNames", "$Nodes", str(len(mesh.nodes))]
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", "4", '2 1 "plane"', '1 2 "channel"',
+             '1 3 ".bnd_lines"', '0 4 ".bnd_points"', "$EndPhysicalNames", "$Nodes", str(len(mesh.nodes))]
     lines += ["%d %.17g %.17g %.17g" % (i + 1, *p) for i, p in enumerate(mesh.nodes)]
     lines += ["$EndNodes", "$Elements", str(len(mesh.el_dim) + len(mesh.bc_dim))]
     typ = {0: 15, 1: 1, 2: 2, 3: 4}
+    bulk_region, bc_region = {2: 1, 1: 2}, {1: 3, 0: 4}
     k = 1
     for d, nd in zip(mesh.bc_dim, mesh.bc_nodes):
-        lines.append("%d %d 2 2 2 %s" % (k, typ[d], " ".join(str(v + 1) for v in nd[:d + 1])))
+        r = bc_region[d]
+        lines.append("%d %d 2 %d %d %s" % (k, typ[d], r, r, " ".join(str(v + 1) for v in nd[:d + 1])))
         k += 1
     for d, nd in zip(mesh.el_dim, mesh.el_nodes):
-        lines.append("%d %d 2 1 1 %s" % (k, typ[d], " ".join(str(v + 1) for v in nd[:d + 1])))
+        r = bulk_region[d]
+        lines.append("%d %d 2 %d %d %s" % (k, typ[d], r, r, " ".join(str(v + 1) for v in nd[:d + 1])))
         k += 1
     lines.append("$EndElements")
     path.write_text("\n".join(lines) + "\n")
