@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-setup-timing", action="store_true",
+                    help="skip the host setup timing (gmsh read and handle creation at 56k elements)")
     ap.add_argument("--instances", type=int, default=256, help="batch size of --config 3")
     ap.add_argument("--accuracy", action="store_true",
                     help="flux and pressure errors of AMG and FP64 PCG solves at r_tol 1e-10 and 1e-12 against "
@@ -357,6 +359,60 @@ def element_flux_timing(system, stream, sz, mesh, reps=20):
     return {"element_flux": ef, "transport_matrix": tr}
 
 
+# ---------------------------------------------------------------- host setup ------------
+# Flow123d 1.7.0 on one process at 56,355 elements (bench_mel_table.tex:34,43,44), seconds
+SETUP_PUBLISHED_S = {"GMSHReader - read mesh": 3.46, "MESH - setup topology": 0.49, "Darcy constructor": 3.28}
+
+
+def setup_timing(n=21, reps=3):
+    """Host-side setup at the size of the reference's published profile: a fractured n=21 cube
+    (55,566 tets + 882 fracture triangles + 21 channel segments = 56,469 elements) written as a
+    gmsh 2.2 file, read by the library's reader (mh_gmsh_read) and turned into a solver handle
+    (MHSystem: topology, Schur pattern, SELL layout and device upload), each the median of
+    `reps` host-timed runs."""
+    import tempfile
+
+    import numpy as np
+
+    import mhdarcy
+    mesh = mhdarcy.cube_mesh(n, [(2, n // 2)], [(0, n // 2, n // 2)])
+    typ = np.array([15, 1, 2, 4])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "cube.msh")
+        with open(path, "w") as f:
+            f.write('$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$PhysicalNames\n3\n3 3 "rock"\n2 2 "fracture"\n'
+                    '1 1 "channel"\n$EndPhysicalNames\n$Nodes\n%d\n' % len(mesh.nodes))
+            np.savetxt(f, np.column_stack([np.arange(1, len(mesh.nodes) + 1), mesh.nodes]),
+                       fmt=["%d", "%.17g", "%.17g", "%.17g"])
+            f.write("$EndNodes\n$Elements\n%d\n" % len(mesh.el_dim))
+            dim = np.asarray(mesh.el_dim)
+            for k in (3, 2, 1):  # cube_mesh orders tetrahedra, triangles, segments
+                sel = np.where(dim == k)[0]
+                cols = [sel + 1, typ[dim[sel]], np.full(len(sel), 2), np.full(len(sel), k), np.full(len(sel), k)]
+                cols += [np.asarray(mesh.el_nodes)[sel, j] + 1 for j in range(k + 1)]
+                np.savetxt(f, np.column_stack(cols), fmt="%d")
+            f.write("$EndElements\n")
+        size = os.path.getsize(path)
+        t_read, t_create = [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            m = mhdarcy.read_gmsh(path)
+            t_read.append(time.perf_counter() - t0)
+        if not (np.array_equal(m.el_nodes, mesh.el_nodes) and np.array_equal(m.nodes, mesh.nodes)):
+            raise RuntimeError("gmsh round trip changed the mesh")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        s = mhdarcy.MHSystem(m)
+        t_create.append(time.perf_counter() - t0)
+        s.close()
+    return {"elements": int(len(m.el_dim)), "gmsh_file_bytes": size, "host_threads": os.cpu_count(),
+            "read_gmsh_s": round(statistics.median(t_read), 5), "create_s": round(statistics.median(t_create), 5),
+            "reference_published_s": SETUP_PUBLISHED_S,
+            "note": "host timers; read_gmsh = mh_gmsh_read + array copies, create = mh_create (topology, "
+                    "Schur pattern, SELL layout, device upload); reference: Flow123d 1.7.0, 1 process, "
+                    "56,355 elements"}
+
+
 # ---------------------------------------------------------------- ours ------------------
 def run_ours(a, rank, world):
     import numpy as np
@@ -621,6 +677,11 @@ def main():
             out["cpu_baseline"] = {"value": round(1.0 / cb["t_solve"], 6) if cb["t_solve"] else None,
                                    "unit": "solves/s", "cores": cb["cores"], "kind": "port", "sample": cb["sample"],
                                    "detail": {k: cb[k] for k in ("t_asm", "t_iter", "t_res")}}
+        if world == 1 and not a.no_setup_timing:
+            try:
+                out["setup"] = setup_timing()
+            except Exception as e:  # a host-side extra must never cost the bench line
+                out["setup"] = {"error": "%s: %s" % (type(e).__name__, e)}
         print(json.dumps(out))
 
 
