@@ -11,6 +11,9 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
                    per element pressure, barycentric flux, side (edge) pressures, side fluxes;
                    the node pressures of the output mesh ($NodeData "pressure_nodes_[L]"); the
                    boundary and source tables of water_balance.out;
+  * t02            tests/02_transport_12d (flow part of flow_gmsh.con): legacy side-based Dirichlet
+                   data on a 1D-2D network; element and node pressures, element velocities and
+                   the water balance;
   * t03            tests/03_transport_small_12d (flow part of flow_vtk.con): element and node
                    pressures, element velocities of the VTK output and the water balance of a
                    1D-2D network with a three-channel junction;
@@ -143,12 +146,12 @@ def water_balance(path):
             mode = "s"
         elif line.startswith("#") or not line.strip():
             continue
-        elif mode == "b":
+        elif mode == "b":  # id, label (may hold blanks), total, outflow, inflow, time
             v = line.split()
-            bdr.append([float(v[0]), float(v[2]), float(v[3]), float(v[4])])
-        elif mode == "s":
+            bdr.append([float(v[0]), float(v[-4]), float(v[-3]), float(v[-2])])
+        elif mode == "s":  # id, label, total, time
             v = line.split()
-            src.append([float(v[0]), float(v[2])])
+            src.append([float(v[0]), float(v[-2])])
     return dict(ref_bdr_balance=np.array(bdr), ref_src_balance=np.array(src))
 
 
@@ -258,6 +261,34 @@ def case_t13(t):
     print("t13", ne, "elements", len(fb), "legacy conditions", len(ct), "concentration outputs")
 
 
+def case_t02(t):
+    """tests/02_transport_12d (flow part of flow_gmsh.con): a 1D network (anisotropy 10) on the
+    edges of a 2D domain, Dirichlet conditions in the legacy side-based file, solver r_tol 1e-12;
+    the flow outputs of test2.msh (printed with 6 digits) and its water balance."""
+    d = lambda *p: t("02_transport_12d", *p)
+    m, names = parse_gmsh(d("input", "test2.msh"))
+    ne = len(m["el_dim"])
+    aniso = {48: 10.0, 184: 1.0}
+    f = dict(conductivity=np.ones(ne), anisotropy=np.array([aniso[r] for r in m["el_region"]]),
+             cross_section=np.ones(ne), sigma=np.ones(ne), water_source_density=np.zeros(ne),
+             storativity=np.ones(ne), init_pressure=np.zeros(ne))
+    fb = legacy_flow_bcd(d("input", "test2.fbc"))
+    eidx = {int(e): i for i, e in enumerate(m["el_id"])}
+    legacy = dict(lbc_id=np.array([r[0] for r in fb], np.int32), lbc_type=np.array([r[1] for r in fb], np.int32),
+                  lbc_value=np.array([r[2] for r in fb]), lbc_element=np.array([eidx[r[3]] for r in fb], np.int32),
+                  lbc_side=np.array([r[4] for r in fb], np.int32), lbc_conc=np.zeros(len(fb)))
+    out = d("ref_output", "flow_gmsh.con")
+    fl = os.path.join(out, "test2.msh")
+    ref = dict(ref_pressure=gmsh_element_data_blocks(fl, "pressure_elements_[L]")[1][0],
+               ref_flux=np.array(gmsh_element_vectors(fl, "velocity_elements_[L/T]")),
+               ref_node_pressure=gmsh_node_data(fl, "pressure_nodes_[L]", d("input", "test2.msh")),
+               **water_balance(os.path.join(out, "water_balance.txt")))
+    np.savez_compressed(os.path.join(OUT, "t02.npz"), **m, **f, **legacy, **ref,
+                        meta=np.array("tests/02_transport_12d flow_gmsh.con: legacy .fbc boundary data, flow "
+                                      "outputs of test2.msh (6 digits), water_balance.txt; r_tol 1e-12"))
+    print("t02", ne, "elements", len(fb), "legacy conditions")
+
+
 def gmsh_element_vectors(path, name):
     """The first $ElementData block of a 3-component field: [n_entities, 3]."""
     txt = open(path).read().split("\n")
@@ -311,6 +342,7 @@ def main():
          "t03", "tests/03_transport_small_12d flow_vtk.con VTK (ascii, 16 digits) and water_balance.txt (%g); "
          "solver r_tol 1e-12, a_tol 1e-12")
     case_t13(t)
+    case_t02(t)
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
                                       "test05-000000.vtu"), "pressure_elements_[L]")

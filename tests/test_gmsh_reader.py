@@ -68,7 +68,7 @@ def compare(path):
     return got, ref
 
 
-@pytest.mark.parametrize("name", ["t01", "t03", "t05_robin", "t06_32", "t08", "t13"])
+@pytest.mark.parametrize("name", ["t01", "t02", "t03", "t05_robin", "t06_32", "t08", "t13"])
 def test_fixture_meshes(tmp_path, name):
     mesh, nodes, elements, names = fixture_file(name)
     p = tmp_path / "m.msh"

@@ -136,6 +136,45 @@ def test_t03_channel_network():
         assert osrc[eids.index(int(rid))] == val == 0.0
 
 
+def legacy_problem(name):
+    """A fixture whose boundary conditions come from a legacy side-based .fbc file: each
+    condition names an element and a local side, whose boundary object gets the condition; the
+    other boundary objects have none (no flux)."""
+    z, mesh = load_fixture(name)
+    topo = T.build(mesh)
+    nb = len(topo["bdr_edge"])
+    bt, bp = np.zeros(nb, np.int32), np.zeros(nb)
+    ss, sb = topo["el_side_start"], topo["side_bdr"]
+    for e, s, typ, val in zip(z["lbc_element"], z["lbc_side"], z["lbc_type"], z["lbc_value"]):
+        b = sb[ss[e] + s]
+        assert b >= 0
+        bt[b], bp[b] = typ, val
+    P = oracle_problem(mesh, topo, topo["n_edges"], fixture_coeffs(z), {"bc_type": bt, "pressure": bp})
+    return z, mesh, topo, P
+
+
+def test_t02_legacy_network():
+    """tests/02_transport_12d, flow part: a 1D network (anisotropy 10) on edges of a 2D domain,
+    20 Dirichlet conditions from the legacy .fbc file, solver r_tol 1e-12.  Element and node
+    pressures and element velocities of test2.msh are printed with 6 digits; the water balance
+    has one region, IMPLICIT BOUNDARY, whose total is the reference solver's residual."""
+    z, mesh, topo, P = legacy_problem("t02")
+    assert set(np.unique(z["el_dim"])) == {1, 2} and len(topo["ngh_element"]) > 0
+    sol = O.solve_mh_direct(P)
+    ns, ne = P.n_sides, P.n_el
+    printed = lambda got, ref, floor: np.all(np.abs(got - ref) <= 5e-6 * np.abs(ref) + floor * np.abs(ref).max())
+    assert printed(sol[ns:ns + ne], z["ref_pressure"], 1e-9)
+    assert printed(O.node_pressure(P, sol), z["ref_node_pressure"], 1e-9)
+    # the smallest velocities carry the reference solver's error (up to 5.5e-7 on values of 0.006,
+    # 4e-8 of the largest velocity) beyond their printing precision
+    assert printed(O.element_flux(P, sol), z["ref_flux"], 1e-7)
+    ob, osrc = O.water_balance(P, sol, np.zeros(len(topo["bdr_edge"]), np.int32), np.zeros(ne, np.int32))
+    (rid, total, out, inflow), = z["ref_bdr_balance"]
+    assert rid == -3 and abs(ob[0, 1] - out) <= 5e-6 * out and abs(ob[0, 2] - inflow) <= 5e-6 * out
+    assert abs(ob[0, 0]) <= 1e-12 * out and abs(total) < 1e-6 * out
+    assert np.all(z["ref_src_balance"][:, 1] == 0.0) and osrc[0] == 0.0
+
+
 def test_t01_schur_path_equals_direct():
     z, mesh, topo, P = problem("t01")
     full = O.solve_mh_direct(P)
