@@ -116,20 +116,31 @@ def step_count(full_step, cfl):
     return nf if abs(ratio - nf) < 1e-14 else n
 
 
-def explicit_transport(A, bcv, cfl, c0, output_times):
+def explicit_transport(A, bcv, cfl, c0, output_times, bc_switch=()):
     """Concentrations at output_times (increasing, from 0) of the explicit scheme
     c <- (I + dt A) c + dt bcv (ConvectionTransport::compute_one_step, transport.cc:593-716),
     with dt fixed over each interval between outputs (set_target_time + fix_dt_until_mark:
-    interval / step_count)."""
+    interval / step_count).  bc_switch lists (time, boundary term) pairs in increasing time:
+    the step that starts at t uses the term of the last pair with time <= t, and `bcv` before
+    the first one -- the data are set to the last computed time before the step
+    (transport.cc:600, 621-622) and the time advances after (:665)."""
     c = np.array(c0, np.float64)
     t = 0.0
     out = []
+
+    def term(t0):
+        cur = bcv
+        for ts, v in bc_switch:
+            if ts <= t0:
+                cur = v
+        return cur
+
     for target in output_times:
         if target > t:
             n = step_count(target - t, cfl)
             dt = (target - t) / n
-            for _ in range(n):
-                c = c + dt * (A @ c) + dt * bcv
+            for i in range(n):
+                c = c + dt * (A @ c) + dt * term(t + i * dt)
             t = target
         out.append(c.copy())
     return np.array(out)

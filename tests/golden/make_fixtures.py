@@ -23,7 +23,9 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
   * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
   * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5;
   * t13            tests/13_edge_solute_mixing: legacy side-based boundary data, the flow outputs
-                   and the concentrations of the explicit transport every 0.5 up to t = 100.
+                   and the concentrations of the explicit transport every 0.5 up to t = 100;
+  * t14            tests/14_trans_time_bc (trans_explicit.con): an inflow concentration switched
+                   in time by four legacy transport files; concentrations every 1.0 up to t = 10.
 The parsers here are self-contained (independent of the package under test).
 """
 import os
@@ -289,6 +291,37 @@ def case_t02(t):
     print("t02", ne, "elements", len(fb), "legacy conditions")
 
 
+def case_t14(t):
+    """tests/14_trans_time_bc (trans_explicit.con): a strip with a uniform flow, Dirichlet
+    pressures in the legacy side-based file, and the inflow concentration switched by four legacy
+    transport files at t = 1 (20), 3 (0), 6 (40) and 7 (0), 0 before; explicit convection up to
+    t = 10 with output every 1.0 (VTK, 16 digits)."""
+    d = lambda *p: t("14_trans_time_bc", *p)
+    m, names = parse_gmsh(d("input", "test14.msh"))
+    ne = len(m["el_dim"])
+    f = dict(conductivity=np.ones(ne), anisotropy=np.full(ne, 0.1), cross_section=np.ones(ne), sigma=np.ones(ne),
+             water_source_density=np.zeros(ne), storativity=np.ones(ne), init_pressure=np.zeros(ne))
+    fb = legacy_flow_bcd(d("input", "test14.fbc"))
+    eidx = {int(e): i for i, e in enumerate(m["el_id"])}
+    times = [1.0, 3.0, 6.0, 7.0]
+    tb = [legacy_transport_bcd(d("input", "test14_tbc_%03d" % k)) for k in range(4)]
+    legacy = dict(lbc_id=np.array([r[0] for r in fb], np.int32), lbc_type=np.array([r[1] for r in fb], np.int32),
+                  lbc_value=np.array([r[2] for r in fb]), lbc_element=np.array([eidx[r[3]] for r in fb], np.int32),
+                  lbc_side=np.array([r[4] for r in fb], np.int32),
+                  lbc_conc_times=np.array(times),
+                  lbc_conc_steps=np.array([[b.get(r[0], [0.0])[0] for r in fb] for b in tb]))
+    out = d("ref_output", "trans_explicit.con")
+    vt = lambda k: vtu_cell_array(os.path.join(out, "transport", "transport-%06d.vtu" % k), "A_mobile_[M/L^3]")
+    fl = os.path.join(out, "test14", "test14-000000.vtu")
+    ref = dict(ref_pressure=vtu_cell_array(fl, "pressure_elements_[L]"),
+               ref_flux=vtu_cell_array(fl, "velocity_elements_[L/T]").reshape(-1, 3),
+               ref_conc_times=np.arange(11.0), ref_conc=np.array([vt(k) for k in range(11)]))
+    np.savez_compressed(os.path.join(OUT, "t14.npz"), **m, **f, **legacy, **ref,
+                        meta=np.array("tests/14_trans_time_bc trans_explicit.con: legacy .fbc and four time-switched "
+                                      "transport files, VTK concentrations every 1.0 up to t = 10"))
+    print("t14", ne, "elements", len(fb), "legacy conditions")
+
+
 def gmsh_element_vectors(path, name):
     """The first $ElementData block of a 3-component field: [n_entities, 3]."""
     txt = open(path).read().split("\n")
@@ -343,6 +376,7 @@ def main():
          "solver r_tol 1e-12, a_tol 1e-12")
     case_t13(t)
     case_t02(t)
+    case_t14(t)
     # test 05: Dirichlet / Neumann / Robin on a square, exact u = xy
     vtu5 = lambda c: vtu_cell_array(t("05_flow_boundary_conditions", "ref_output", c, "test05",
                                       "test05-000000.vtu"), "pressure_elements_[L]")

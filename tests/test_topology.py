@@ -24,7 +24,7 @@ def compare(mesh):
         return s.sizes
 
 
-@pytest.mark.parametrize("name", ["t01", "t02", "t03", "t05_robin", "t06_32", "t06_21", "t08", "t10_mh", "t13"])
+@pytest.mark.parametrize("name", ["t01", "t02", "t03", "t05_robin", "t06_32", "t06_21", "t08", "t10_mh", "t13", "t14"])
 def test_fixture_topology(name):
     z, mesh = load_fixture(name)
     compare(mesh)

@@ -71,6 +71,34 @@ def test_t13_reference_transport_run():
     assert z["ref_conc"][10].min() < 0.7 < z["ref_conc"][10].max()  # a front is inside the domain at t = 5
 
 
+def test_t14_time_switched_inflow():
+    """The reference's tests/14_trans_time_bc: a uniform flow along a strip, the inflow
+    concentration switched by four legacy transport files (20 from t = 1, 0 from 3, 40 from 6,
+    0 from 7); the concentrations of its VTK output every 1.0 up to t = 10 (16 digits).  A
+    step uses the boundary data of its start time: the output at t = 1 is still all zero."""
+    z, mesh = load_fixture("t14")
+    topo = T.build(mesh)
+    nb = len(topo["bdr_edge"])
+    bt, bp = np.zeros(nb, np.int32), np.zeros(nb)
+    conc = np.zeros((len(z["lbc_conc_times"]), nb))
+    ss, sb = topo["el_side_start"], topo["side_bdr"]
+    for j, (e, s, typ, val) in enumerate(zip(z["lbc_element"], z["lbc_side"], z["lbc_type"], z["lbc_value"])):
+        b = sb[ss[e] + s]
+        assert b >= 0
+        bt[b], bp[b] = typ, val
+        conc[:, b] = z["lbc_conc_steps"][:, j]
+    P = oracle_problem(mesh, topo, topo["n_edges"], fixture_coeffs(z), {"bc_type": bt, "pressure": bp})
+    sol = O.solve_mh_direct(P)
+    ns, ne = P.n_sides, P.n_el
+    assert np.abs(sol[ns:ns + ne] - z["ref_pressure"]).max() < 1e-12
+    assert np.abs(O.element_flux(P, sol) - z["ref_flux"]).max() < 1e-12
+    A, cfl = TR.transport_matrix(mesh, topo, sol)
+    switch = [(t, TR.boundary_inflow(mesh, topo, sol, conc[k])) for k, t in enumerate(z["lbc_conc_times"])]
+    c = TR.explicit_transport(A, np.zeros(ne), cfl, np.zeros(ne), z["ref_conc_times"], bc_switch=switch)
+    assert np.abs(c - z["ref_conc"]).max() < 1e-9
+    assert np.all(z["ref_conc"][1] == 0.0) and z["ref_conc"][7].max() > 39.0
+
+
 def check_against_oracle(s, mesh, sol, cross_section, porosity):
     (rp, col, val), cfl = s.transport_matrix(porosity)
     A, cfl_ref = TR.transport_matrix(mesh, s.topology(), sol, cross_section,
