@@ -389,11 +389,14 @@ int read_mesh(const char *path, mh_mesh &out, std::string &err) {
     if (nn == 0) return fail(k + 1, "zero number of nodes");
     if (nn > std::numeric_limits<int32_t>::max()) return fail(k + 1, "too many nodes");
     const int64_t n0 = k + 2;
-    std::vector<uint32_t> nid(nn);
-    out.m.xyz.resize(nn * 3);
+    // rows present in the file (a count beyond the end of the file is an error at the end,
+    // after the rows that are there, and allocates nothing for the missing ones)
+    const int64_t n_avail = std::min<int64_t>(nn, std::max<int64_t>(0, nl - n0));
+    std::vector<uint32_t> nid(n_avail);
+    out.m.xyz.resize(n_avail * 3);
     FirstError node_err;
     {
-        const int64_t avail = std::min<int64_t>(nn, nl - n0);
+        const int64_t avail = n_avail;
         if (avail < nn) node_err.offer(nl, 0, "unexpected end of file in $Nodes");
 #pragma omp parallel
         {
@@ -428,15 +431,16 @@ int read_mesh(const char *path, mh_mesh &out, std::string &err) {
     if (ne == 0) return fail(k + 1, "zero number of elements");
     if (ne > std::numeric_limits<int32_t>::max()) return fail(k + 1, "too many elements");
     const int64_t e0 = k + 2;
-    // per row of the file (left uninitialised: every row the later passes read is written)
-    std::unique_ptr<uint32_t[]> eid(new uint32_t[ne]), ereg(new uint32_t[ne]);
-    std::unique_ptr<int32_t[]> epart(new int32_t[ne]), enodes(new int32_t[4 * ne]);
-    std::unique_ptr<int8_t[]> edim(new int8_t[ne]), cls(new int8_t[ne]);
+    // per row present in the file (left uninitialised: every row the later passes read is written)
+    const int64_t e_avail = std::min<int64_t>(ne, std::max<int64_t>(0, nl - e0));
+    std::unique_ptr<uint32_t[]> eid(new uint32_t[e_avail + 1]), ereg(new uint32_t[e_avail + 1]);
+    std::unique_ptr<int32_t[]> epart(new int32_t[e_avail + 1]), enodes(new int32_t[4 * e_avail + 4]);
+    std::unique_ptr<int8_t[]> edim(new int8_t[e_avail + 1]), cls(new int8_t[e_avail + 1]);
     // stage 0: errors before the region is known; stage 1: errors in the node list, which
     // the reference meets after the region and id bookkeeping of the same line
     FirstError el_err;
     {
-        const int64_t avail = std::min<int64_t>(ne, nl - e0);
+        const int64_t avail = e_avail;
         if (avail < ne) el_err.offer(nl, 0, "unexpected end of file in $Elements");
 #pragma omp parallel
         {

@@ -168,6 +168,9 @@ ERRORS = [
     ("wrong format", lambda t: edit(t, "4 2 2 3 3 2 3 4", "4 2 2 3 3 2 3")),
     ("wrong format", lambda t: edit(t, "2 1 0 0\n", "2 1e999 0 0\n")),
     ("zero number of nodes", lambda t: edit(t, "$Nodes\n4\n", "$Nodes\n0\n")),
+    # counts beyond the rows of the file: the first line that is not a row is the error
+    ("wrong format", lambda t: edit(t, "$Nodes\n4\n", "$Nodes\n2000000000\n")),
+    ("wrong format", lambda t: edit(t, "$Elements\n4\n", "$Elements\n2000000000\n")),
     ("missing section '$Nodes'", lambda t: t.replace("$Nodes", "$Nodez").replace("$EndNodez", "$EndNodes")),
     ("missing section '$Elements'", lambda t: t.replace("$Elements", "$Elementz")),
     # the earlier line wins: a dimension error on element 3 before a bad number on element 4
