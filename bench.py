@@ -14,7 +14,8 @@ buffers: coefficients and boundary data copied in from pinned memory every step 
 MH solution copied back.
 
 --impl reference times the CPU path (the FP64 C restatement of the reference in oracle/,
-OpenMP over all host threads) on a bounded sample of the same workload.
+OpenMP over all host threads, Jacobi-preconditioned CG; --cpu-precond ilu0 selects ILU(0), the
+zero-fill member of the reference's PETSc ILU) on a bounded sample of the same workload.
 Multi-GPU (torchrun): independent replicas, one per GPU, no data-path collective.
 """
 import argparse
@@ -43,6 +44,9 @@ WORKLOADS = {
 # a B200 with the FP64 path of this bench (seeded inputs, so deterministic); used to scale the
 # CPU per-iteration sample of --impl reference to a full solve.
 JACOBI_PCG_ITERS = {1: 1630, 2: 4785}
+# ILU(0)-PCG iterations to 1e-10 under the same stopping rule, measured with the CPU restatement
+# (oracle/, 8 host threads, seeded inputs); the projection count of --cpu-precond ilu0.
+ILU0_PCG_ITERS = {1: 168, 2: 1509}
 
 
 def parse():
@@ -61,6 +65,11 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=200)
+    ap.add_argument("--cpu-precond", choices=["jacobi", "ilu0"], default="jacobi",
+                    help="preconditioner of the CPU baseline's CG: Jacobi (threaded throughout; the faster "
+                         "CPU solve on multi-core hosts at the benchmark sizes) or ILU(0) (the zero-fill "
+                         "member of the reference's PETSc ILU, sequential triangular solves; used where its "
+                         "iteration count is recorded)")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-setup-timing", action="store_true",
@@ -590,7 +599,10 @@ def cpu_sample(a, mesh=None, coeffs=None, bc=None, topo=None, n_edges=None, pcg_
     """Times the CPU restatement (oracle/, all host threads) on a bounded sample of the workload:
     the threaded element-local double-Schur assembly, `cpu_sample_iters` Jacobi-PCG iterations and
     the threaded back-substitution, projected to a full solve with the Jacobi-PCG iteration count
-    of this system (same algorithm and stopping rule as the GPU FP64 path)."""
+    of this system (same algorithm and stopping rule as the GPU FP64 path).  With --cpu-precond
+    ilu0 (for workloads whose ILU(0) count is recorded) the sample is the ILU(0) factorisation
+    and ILU(0)-PCG iterations (threaded SpMV and vector updates, sequential triangular solves),
+    projected with the ILU(0)-PCG count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
@@ -606,6 +618,7 @@ def cpu_sample(a, mesh=None, coeffs=None, bc=None, topo=None, n_edges=None, pcg_
     P = O.Problem(mesh, topo, n_edges, conductivity=coeffs["conductivity"], cross_section=coeffs["cross_section"],
                   storativity=coeffs.get("storativity", 1.0), bc_type=bc["bc_type"], bc_pressure=bc["pressure"])
     S, r = O.schur2(P)                      # pattern (setup, untimed)
+    S.sort_indices()
     rp = np.ascontiguousarray(S.indptr, np.int32)
     col = np.ascontiguousarray(S.indices, np.int32)
     val = np.zeros(len(col))
@@ -615,18 +628,36 @@ def cpu_sample(a, mesh=None, coeffs=None, bc=None, topo=None, n_edges=None, pcg_
     t_asm = time.perf_counter() - t0
     S.data[:] = val
     k = a.cpu_sample_iters
+    ilu = a.cpu_precond == "ilu0" and a.config in ILU0_PCG_ITERS
     t0 = time.perf_counter()
-    x, it, res = O.pcg_jacobi(S, rhs, rtol=1e-30, max_it=k)
-    t_iter = (time.perf_counter() - t0) / k
+    if ilu:
+        x, it, res, t_factor = O.pcg_ilu0(S, rhs, rtol=1e-30, max_it=k)
+        t_iter = (time.perf_counter() - t0 - t_factor) / k
+    else:
+        t_factor = 0.0
+        x, it, res = O.pcg_jacobi(S, rhs, rtol=1e-30, max_it=k)
+        t_iter = (time.perf_counter() - t0) / k
     t0 = time.perf_counter()
     O.resolve(P, x)
     t_res = time.perf_counter() - t0
-    iters = pcg_iters or JACOBI_PCG_ITERS.get(a.config)
-    t_solve = t_asm + t_iter * iters + t_res if iters else None
-    return {"t_asm": t_asm, "t_iter": t_iter, "t_res": t_res, "iters": iters, "t_solve": t_solve,
-            "cores": O.num_threads(),
-            "sample": "cfg%d full mesh: threaded double-Schur assembly + %d Jacobi-PCG iterations + "
-                      "back-substitution, projected to %s iterations" % (a.config, k, iters)}
+    iters = ILU0_PCG_ITERS[a.config] if ilu else (pcg_iters or JACOBI_PCG_ITERS.get(a.config))
+    t_solve = t_asm + t_factor + t_iter * iters + t_res if iters else None
+    name = "ILU(0)-PCG" if ilu else "Jacobi-PCG"
+    return {"t_asm": t_asm, "t_factor": t_factor, "t_iter": t_iter, "t_res": t_res, "iters": iters,
+            "t_solve": t_solve, "cores": O.num_threads(), "method": ("ilu0" if ilu else "jacobi") + "-pcg64 (CPU)",
+            "sample": "cfg%d full mesh: threaded double-Schur assembly + %s%d %s iterations + "
+                      "back-substitution, projected to %s iterations" % (
+                          a.config, "ILU(0) factorisation + " if ilu else "", k, name, iters)}
+
+
+def cpu_baseline_entry(a, ctx, pcg_iters):
+    """The `cpu_baseline` object of the bench line: the CPU restatement timed on the workload of
+    the GPU run (ctx = mesh, coefficients, boundary data, topology, edge count)."""
+    mesh, coeffs, bc, topo, N = ctx
+    cb = cpu_sample(a, mesh, coeffs, bc, topo, N, pcg_iters)
+    return {"value": round(1.0 / cb["t_solve"], 6) if cb["t_solve"] else None, "unit": "solves/s",
+            "cores": cb["cores"], "kind": "port", "sample": cb["sample"],
+            "detail": {k: cb[k] for k in ("method", "t_asm", "t_factor", "t_iter", "t_res", "iters")}}
 
 
 def run_reference(a):
@@ -645,7 +676,7 @@ def run_reference(a):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(t * 1e3, 3) if t else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
-            "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": "jacobi-pcg64 (CPU)",
+            "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": s0["method"],
                        "r_tol": 1e-10},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": s0["cores"], "kind": "port",
                              "sample": s0["sample"]},
@@ -672,11 +703,7 @@ def main():
     out, ctx = run_ours(a, rank, world)
     if rank == 0:
         if not a.no_cpu_baseline and world == 1 and a.config != 3:
-            mesh, coeffs, bc, topo, N = ctx
-            cb = cpu_sample(a, mesh, coeffs, bc, topo, N, out["methods"].get("pcg64", {}).get("iterations"))
-            out["cpu_baseline"] = {"value": round(1.0 / cb["t_solve"], 6) if cb["t_solve"] else None,
-                                   "unit": "solves/s", "cores": cb["cores"], "kind": "port", "sample": cb["sample"],
-                                   "detail": {k: cb[k] for k in ("t_asm", "t_iter", "t_res")}}
+            out["cpu_baseline"] = cpu_baseline_entry(a, ctx, out["methods"].get("pcg64", {}).get("iterations"))
         if world == 1 and not a.no_setup_timing:
             try:
                 out["setup"] = setup_timing()

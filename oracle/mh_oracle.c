@@ -895,6 +895,133 @@ int orc_pcg_jacobi(int64_t n, const int32_t *rp, const int32_t *col, const doubl
     return (rr > tol2 || rz > tol2s) ? -1 : it;
 }
 
+/* Incomplete LU factorisation with zero fill, ILU(0), of a CSR matrix whose rows have sorted
+ * column indices and a diagonal entry (IKJ form: row i is eliminated with the finished rows
+ * k < i inside its own pattern).  For the SPD edge system this is IC(0) in LU form, the
+ * zero-fill member of the incomplete factorisations the reference's PETSc solver uses
+ * (PCILU with 3 levels of fill, solve.cc:355-374).  lu[nnz] receives L (unit lower, strictly
+ * below the diagonal) and U; dpos[n] the diagonal positions.  Returns 0, or -1 for a missing
+ * diagonal or a zero pivot. */
+int orc_ilu0(int64_t n, const int32_t *rp, const int32_t *col, const double *val, double *lu, int32_t *dpos) {
+    int32_t *mark = (int32_t *)malloc(n * sizeof(int32_t));
+    int rc = 0;
+    for (int64_t i = 0; i < n; ++i) mark[i] = -1;
+    memcpy(lu, val, (size_t)rp[n] * sizeof(double));
+    for (int64_t i = 0; i < n && !rc; ++i) {
+        dpos[i] = -1;
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            mark[col[k]] = k;
+            if (col[k] == i) dpos[i] = k;
+        }
+        if (dpos[i] < 0) {
+            rc = -1;
+            break;
+        }
+        for (int32_t k = rp[i]; k < dpos[i]; ++k) {
+            const int32_t c = col[k];
+            const double f = (lu[k] /= lu[dpos[c]]);
+            for (int32_t j = dpos[c] + 1; j < rp[c + 1]; ++j) {
+                const int32_t m = mark[col[j]];
+                if (m >= 0) lu[m] -= f * lu[j];
+            }
+        }
+        if (lu[dpos[i]] == 0.0) rc = -1;
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) mark[col[k]] = -1;
+    }
+    free(mark);
+    return rc;
+}
+
+/* z = (LU)^-1 r: forward substitution with the unit lower factor, then backward with U. */
+static void ilu0_apply(int64_t n, const int32_t *rp, const int32_t *col, const double *lu, const int32_t *dpos,
+                       const double *r, double *z) {
+    for (int64_t i = 0; i < n; ++i) {
+        double s = r[i];
+        for (int32_t k = rp[i]; k < dpos[i]; ++k) s -= lu[k] * z[col[k]];
+        z[i] = s;
+    }
+    for (int64_t i = n - 1; i >= 0; --i) {
+        double s = z[i];
+        for (int32_t k = dpos[i] + 1; k < rp[i + 1]; ++k) s -= lu[k] * z[col[k]];
+        z[i] = s / lu[dpos[i]];
+    }
+}
+
+/* CG preconditioned by ILU(0) on a CSR SPD matrix, FP64: the SpMV and the vector updates are
+ * threaded, the two triangular solves sequential.  The same stopping rule as orc_pcg_jacobi:
+ * the recursively updated residual satisfies |D^-1/2 r| <= rtol |D^-1/2 b| and
+ * |r| <= rtol |b|.  Returns iterations, -1 if max_it was reached, -2 if the factorisation
+ * failed; res_out gets the true Jacobi-scaled relative residual and t_factor_out the
+ * factorisation's seconds. */
+int orc_pcg_ilu0(int64_t n, const int32_t *rp, const int32_t *col, const double *val, const double *b, double *x,
+                 double rtol, int max_it, double *res_out, double *t_factor_out) {
+    extern double omp_get_wtime(void);
+    double *lu = (double *)malloc((size_t)rp[n] * sizeof(double));
+    int32_t *dpos = (int32_t *)malloc(n * sizeof(int32_t));
+    const double t0 = omp_get_wtime();
+    if (orc_ilu0(n, rp, col, val, lu, dpos)) {
+        free(lu); free(dpos);
+        return -2;
+    }
+    if (t_factor_out) *t_factor_out = omp_get_wtime() - t0;
+    double *r = (double *)malloc(n * sizeof(double)), *z = (double *)malloc(n * sizeof(double));
+    double *p = (double *)malloc(n * sizeof(double)), *q = (double *)malloc(n * sizeof(double));
+    double *dinv = (double *)malloc(n * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) dinv[i] = 1.0 / val[dpos[i]];
+    csr_mv(n, rp, col, val, x, q);
+    double bb = 0.0, bdb = 0.0, rr = 0.0, rdr = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : bb, bdb, rr, rdr)
+    for (int64_t i = 0; i < n; ++i) {
+        r[i] = b[i] - q[i];
+        bb += b[i] * b[i];
+        bdb += b[i] * dinv[i] * b[i];
+        rr += r[i] * r[i];
+        rdr += r[i] * dinv[i] * r[i];
+    }
+    ilu0_apply(n, rp, col, lu, dpos, r, z);
+    double rz = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : rz)
+    for (int64_t i = 0; i < n; ++i) {
+        p[i] = z[i];
+        rz += r[i] * z[i];
+    }
+    const double tol2 = rtol * rtol * bb, tol2s = rtol * rtol * bdb;
+    int it = 0;
+    while ((rr > tol2 || rdr > tol2s) && it < max_it) {
+        csr_mv(n, rp, col, val, p, q);
+        double pq = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : pq)
+        for (int64_t i = 0; i < n; ++i) pq += p[i] * q[i];
+        const double alpha = rz / pq;
+        rr = 0.0;
+        rdr = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : rr, rdr)
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+            rr += r[i] * r[i];
+            rdr += r[i] * dinv[i] * r[i];
+        }
+        ilu0_apply(n, rp, col, lu, dpos, r, z);
+        double rz_new = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : rz_new)
+        for (int64_t i = 0; i < n; ++i) rz_new += r[i] * z[i];
+        const double beta = rz_new / rz;
+        rz = rz_new;
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+        ++it;
+    }
+    csr_mv(n, rp, col, val, x, q);
+    double res = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : res)
+    for (int64_t i = 0; i < n; ++i) res += (b[i] - q[i]) * dinv[i] * (b[i] - q[i]);
+    if (res_out) *res_out = bdb > 0.0 ? sqrt(res / bdb) : 0.0;
+    free(r); free(z); free(p); free(q); free(dinv); free(lu); free(dpos);
+    return (rr > tol2 || rdr > tol2s) ? -1 : it;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     extern int omp_get_max_threads(void);

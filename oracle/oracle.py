@@ -8,7 +8,9 @@ GPU library; never imported by the product.  Provides:
                         "FP64 direct oracle", independent of any Schur algebra;
   * schur2 / resolve -- the element-local double Schur complement and back-substitution
                         (src/la/schur.cc:566-773, darcy_flow_mh.cc:1009-1131);
-  * pcg_jacobi       -- the CPU FP64 Jacobi-PCG used as the timed CPU baseline.
+  * pcg_jacobi       -- the CPU FP64 Jacobi-PCG used as the timed CPU baseline;
+  * pcg_ilu0 / ilu0  -- CPU FP64 CG with an ILU(0) preconditioner, the zero-fill member of the
+                        incomplete factorisations of the reference's PETSc solver (solve.cc:355-374).
 Parity of the restatement is pinned to the reference's golden outputs in tests/golden.
 """
 import ctypes as C
@@ -48,6 +50,10 @@ def _load():
     L.orc_water_balance.argtypes = [C.c_void_p, f64p, i32p, C.c_int32, i32p, C.c_int32, f64p, f64p]
     L.orc_pcg_jacobi.restype = C.c_int
     L.orc_pcg_jacobi.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, f64p, C.c_double, C.c_int, f64p]
+    L.orc_pcg_ilu0.restype = C.c_int
+    L.orc_pcg_ilu0.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, f64p, C.c_double, C.c_int, f64p, f64p]
+    L.orc_ilu0.restype = C.c_int
+    L.orc_ilu0.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, i32p]
     L.orc_local_matrix.restype = C.c_int
     L.orc_local_matrix.argtypes = [f64p, i32p, i32p, C.c_int64, f64p, C.c_double, C.c_double, f64p, f64p, f64p]
     L.orc_num_threads.restype = C.c_int
@@ -232,6 +238,41 @@ def pcg_jacobi(S, b, x0=None, rtol=1e-10, max_it=100000):
     it = lib.orc_pcg_jacobi(len(b), _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double),
                             _ptr(b, C.c_double), _ptr(x, C.c_double), rtol, max_it, C.byref(res))
     return x, it, res.value
+
+
+def pcg_ilu0(S, b, x0=None, rtol=1e-10, max_it=100000):
+    """CPU FP64 CG preconditioned by ILU(0) (IC(0) in LU form for the SPD edge system; the
+    triangular solves are sequential).  Returns x, iterations (-1 if max_it, -2 if the
+    factorisation failed), the true Jacobi-scaled relative residual and the factorisation's
+    seconds."""
+    S = S.tocsr()
+    S.sort_indices()
+    rp = np.ascontiguousarray(S.indptr, np.int32)
+    col = np.ascontiguousarray(S.indices, np.int32)
+    val = np.ascontiguousarray(S.data, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+    res, tf = C.c_double(0.0), C.c_double(0.0)
+    it = lib.orc_pcg_ilu0(len(b), _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double),
+                          _ptr(b, C.c_double), _ptr(x, C.c_double), rtol, max_it, C.byref(res), C.byref(tf))
+    return x, it, res.value, tf.value
+
+
+def ilu0(S):
+    """(L, U) of ILU(0) as scipy CSR matrices (L unit lower), for checks."""
+    S = S.tocsr()
+    S.sort_indices()
+    rp = np.ascontiguousarray(S.indptr, np.int32)
+    col = np.ascontiguousarray(S.indices, np.int32)
+    val = np.ascontiguousarray(S.data, np.float64)
+    lu = np.empty_like(val)
+    dpos = np.empty(S.shape[0], np.int32)
+    if lib.orc_ilu0(S.shape[0], _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double),
+                    _ptr(lu, C.c_double), _ptr(dpos, C.c_int32)):
+        raise ArithmeticError("ILU(0) breakdown")
+    F = sp.csr_matrix((lu, col, rp), shape=S.shape)
+    L = sp.tril(F, -1, format="csr") + sp.identity(S.shape[0], format="csr")
+    return L, sp.triu(F, 0, format="csr")
 
 
 def local_matrix(mesh, e, conductivity=1.0, cross_section=1.0, anisotropy=None):

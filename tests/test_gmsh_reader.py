@@ -250,16 +250,3 @@ def test_element_data_matches_restatement(tmp_path, seed, rows):
                         continue
                     got = mhdarcy.read_element_data(str(p), field, sub, t, nc)
                     assert np.array_equal(got, ref, equal_nan=True), (field, t, nc)
-
-
-def test_bench_setup_timing():
-    """bench.py's host setup timing (gmsh write, read, handle creation) runs on a small cube."""
-    import importlib.util
-    import os
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
-    bench = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(bench)
-    r = bench.setup_timing(n=6, reps=1)
-    assert r["elements"] == 6 * 6 ** 3 + 2 * 6 * 6 + 6
-    assert r["read_gmsh_s"] > 0 and r["create_s"] > 0 and r["gmsh_file_bytes"] > 0
