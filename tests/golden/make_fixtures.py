@@ -22,6 +22,7 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
                    of the VTK output, and its water balance (a source field given by a formula);
   * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
   * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5;
+  * t10_lmh        the same with the lumped scheme (flow_LMH.con);
   * t13            tests/13_edge_solute_mixing: legacy side-based boundary data, the flow outputs
                    and the concentrations of the explicit transport every 0.5 up to t = 100;
   * t14            tests/14_trans_time_bc (trans_explicit.con): an inflow concentration switched
@@ -426,6 +427,15 @@ def main():
           ".bc_outflow": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
          {"ref_pressure_steps": np.array(steps), "ref_times": np.arange(6) * 0.1, "dt": np.array(0.01)},
          "t10_mh", "tests/10_unsteady_2d flow_MH.con VTK every 0.1")
+    # the same problem with the lumped mixed-hybrid scheme (Unsteady_LMH)
+    steps = [vtu_cell_array(t("10_unsteady_2d", "ref_output", "flow_LMH.con", "test10", "test10-%06d.vtu" % k),
+                            "pressure_elements_[L]") for k in range(6)]
+    case(t("10_unsteady_2d", "input", "test10.msh"),
+         {"plane": {"anisotropy": 0.02, "storativity": 1.0, "init_pressure": 0.0}},
+         {".bc_inflow": {"type": "dirichlet", "pressure": lambda x, y, z: 100.0},
+          ".bc_outflow": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
+         {"ref_pressure_steps": np.array(steps), "ref_times": np.arange(6) * 0.1, "dt": np.array(0.01)},
+         "t10_lmh", "tests/10_unsteady_2d flow_LMH.con VTK every 0.1")
 
 
 if __name__ == "__main__":
