@@ -17,10 +17,11 @@ boundary element's barycentre, bc_piezo_head converted to pressure by adding the
   * t03            tests/03_transport_small_12d (flow part of flow_vtk.con): element and node
                    pressures, element velocities of the VTK output and the water balance of a
                    1D-2D network with a three-channel junction;
-  * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output;
+  * t05_*          tests/05_flow_boundary_conditions: element pressures of the VTK output and the
+                   water balance;
   * t08            tests/08_steady_flow_sources: element and node pressures, element velocities
                    of the VTK output, and its water balance (a source field given by a formula);
-  * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output;
+  * t06_32, t06_21 tests/06_flow_coupling: element pressures of the VTK output and the water balance;
   * t10_mh         tests/10_unsteady_2d (flow_MH.con): element pressures at t = 0.1 .. 0.5;
   * t10_lmh        the same with the lumped scheme (flow_LMH.con);
   * t13            tests/13_edge_solute_mixing: legacy side-based boundary data, the flow outputs
@@ -386,19 +387,19 @@ def main():
           ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
           ".bc_north": {"type": "dirichlet", "pressure": lambda x, y, z: x},
           ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
-         {"ref_pressure": vtu5("flow_dirichlet.con")}, "t05_dirichlet", "tests/05 flow_dirichlet.con VTK")
+         {"ref_pressure": vtu5("flow_dirichlet.con"), **water_balance(t("05_flow_boundary_conditions", "ref_output", "flow_dirichlet.con", "water_balance.out"))}, "t05_dirichlet", "tests/05 flow_dirichlet.con VTK")
     case(t("05_flow_boundary_conditions", "input", "test05.msh"), {"plane": {"anisotropy": 1.0}},
          {".bc_south": {"type": "neumann", "flux": lambda x, y, z: x},
           ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
           ".bc_north": {"type": "neumann", "flux": lambda x, y, z: -x},
           ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
-         {"ref_pressure": vtu5("flow_neumann.con")}, "t05_neumann", "tests/05 flow_neumann.con VTK")
+         {"ref_pressure": vtu5("flow_neumann.con"), **water_balance(t("05_flow_boundary_conditions", "ref_output", "flow_neumann.con", "water_balance.out"))}, "t05_neumann", "tests/05 flow_neumann.con VTK")
     case(t("05_flow_boundary_conditions", "input", "test05.msh"), {"plane": {"anisotropy": 1.0}},
          {".bc_south": {"type": "robin", "pressure": lambda x, y, z: -2 * x, "robin_sigma": lambda x, y, z: 0.5},
           ".bc_east": {"type": "dirichlet", "pressure": lambda x, y, z: y},
           ".bc_north": {"type": "robin", "pressure": lambda x, y, z: 3 * x, "robin_sigma": lambda x, y, z: 0.5},
           ".bc_west": {"type": "dirichlet", "pressure": lambda x, y, z: 0.0}},
-         {"ref_pressure": vtu5("flow_robin.con")}, "t05_robin", "tests/05 flow_robin.con VTK")
+         {"ref_pressure": vtu5("flow_robin.con"), **water_balance(t("05_flow_boundary_conditions", "ref_output", "flow_robin.con", "water_balance.out"))}, "t05_robin", "tests/05 flow_robin.con VTK")
     # test 06: dimension coupling, known answers p2 = -3 (head), p1 = -2.5
     case(t("06_flow_coupling", "input", "test6_32d.msh"),
          {"2d_fraction": {"conductivity": 16.0, "sigma": 1.0, "cross_section": 10.0,
@@ -407,7 +408,8 @@ def main():
          {".2d_fraction": {"type": "neumann", "flux": lambda x, y, z: 0.0},
           ".3d_cube": {"type": "dirichlet", "piezo_head": lambda x, y, z: z}},
          {"ref_pressure": vtu_cell_array(t("06_flow_coupling", "ref_output", "flow_32d.con", "test6_32d",
-                                           "test6_32d-000000.vtu"), "pressure_elements_[L]")},
+                                           "test6_32d-000000.vtu"), "pressure_elements_[L]"),
+          **water_balance(t("06_flow_coupling", "ref_output", "flow_32d.con", "water_balance.out"))},
          "t06_32", "tests/06 flow_32d.con VTK; analytic 2D piezometric head -3")
     case(t("06_flow_coupling", "input", "test6_21d.msh"),
          {"plane": {"conductivity": 5.0, "cross_section": 10.0},
@@ -416,7 +418,8 @@ def main():
          {".plane": {"type": "dirichlet", "piezo_head": lambda x, y, z: x},
           ".channel": {"type": "neumann", "flux": lambda x, y, z: 0.0}},
          {"ref_pressure": vtu_cell_array(t("06_flow_coupling", "ref_output", "flow_21d.con", "test6_21d",
-                                           "test6_21d-000000.vtu"), "pressure_elements_[L]")},
+                                           "test6_21d-000000.vtu"), "pressure_elements_[L]"),
+          **water_balance(t("06_flow_coupling", "ref_output", "flow_21d.con", "water_balance.out"))},
          "t06_21", "tests/06 flow_21d.con VTK; analytic 1D pressure -2.5")
     # test 10: unsteady MH, dt = 0.01, outputs every 0.1 up to 0.5
     steps = [vtu_cell_array(t("10_unsteady_2d", "ref_output", "flow_MH.con", "test10", "test10-%06d.vtu" % k),

@@ -175,6 +175,25 @@ def test_t02_legacy_network():
     assert np.all(z["ref_src_balance"][:, 1] == 0.0) and osrc[0] == 0.0
 
 
+@pytest.mark.parametrize("name", ["t05_dirichlet", "t05_neumann", "t05_robin", "t06_32", "t06_21"])
+def test_water_balance_tables(name):
+    """The boundary and source tables of water_balance.out of tests 05 (Dirichlet, Neumann,
+    Robin) and 06 (3D-2D and 2D-1D coupling with sources): printed %g after solves to the
+    reference's r_tol 1e-7, so each entry agrees at its printing plus 2e-6 of the table's
+    largest entry (the reference's own spurious flows reach 2.9e-6 on 50)."""
+    z, mesh, topo, P = problem(name)
+    assert np.all(topo["bdr_bc_element"] >= 0)
+    bdr, el, bids, eids = fixture_regions(z, topo)
+    ob, osrc = O.water_balance(P, O.solve_mh_direct(P), bdr, el)
+    scale = max(np.abs(z["ref_bdr_balance"][:, 1:]).max(), np.abs(z["ref_src_balance"][:, 1]).max())
+    close = lambda got, ref: np.all(np.abs(np.asarray(got) - ref) <= 5e-6 * np.abs(ref) + 2e-6 * scale)
+    for rid, *vals in z["ref_bdr_balance"]:
+        assert close(ob[bids.index(int(rid))], vals), (rid, ob[bids.index(int(rid))], vals)
+    for rid, val in z["ref_src_balance"]:
+        assert close(osrc[eids.index(int(rid))], val), (rid, osrc[eids.index(int(rid))], val)
+    assert abs(ob[:, 0].sum() - osrc.sum()) <= 1e-12 * scale  # what the sources give leaves through the boundary
+
+
 def test_t01_schur_path_equals_direct():
     z, mesh, topo, P = problem("t01")
     full = O.solve_mh_direct(P)
