@@ -422,6 +422,21 @@ def setup_timing(n=21, reps=3):
                     "56,355 elements"}
 
 
+def setup_timing_isolated(n=21, reps=3, timeout_s=300):
+    """setup_timing in a child process, so that nothing in it (a native fault included) can
+    cost the bench line; an error is reported in place of the timings."""
+    code = ("import json, sys; sys.path.insert(0, %r); import bench; "
+            "print(json.dumps(bench.setup_timing(n=%d, reps=%d)))" % (ROOT, n, reps))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout_s, cwd=ROOT)
+        if r.returncode == 0:
+            return json.loads(r.stdout.strip().splitlines()[-1])
+        tail = (r.stderr.strip().splitlines() or [""])[-1]
+        return {"error": "exit %d: %s" % (r.returncode, tail[:200])}
+    except Exception as e:
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
 # ---------------------------------------------------------------- ours ------------------
 def run_ours(a, rank, world):
     import numpy as np
@@ -705,10 +720,7 @@ def main():
         if not a.no_cpu_baseline and world == 1 and a.config != 3:
             out["cpu_baseline"] = cpu_baseline_entry(a, ctx, out["methods"].get("pcg64", {}).get("iterations"))
         if world == 1 and not a.no_setup_timing:
-            try:
-                out["setup"] = setup_timing()
-            except Exception as e:  # a host-side extra must never cost the bench line
-                out["setup"] = {"error": "%s: %s" % (type(e).__name__, e)}
+            out["setup"] = setup_timing_isolated()
         print(json.dumps(out))
 
 

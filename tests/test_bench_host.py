@@ -37,3 +37,10 @@ def test_bench_cpu_baseline_entry():
         e = bench.cpu_baseline_entry(a, (mesh, coeffs, bc, topo, n_edges), iters if pre == "jacobi" else None)
         assert e["value"] > 0 and e["detail"]["method"].startswith(pre)
         assert e["detail"]["iters"] == (iters if pre == "jacobi" else bench.ILU0_PCG_ITERS[1])
+
+
+def test_bench_setup_timing_isolated():
+    """The child-process wrapper the bench line uses returns the same record."""
+    r = load_bench().setup_timing_isolated(n=6, reps=1, timeout_s=600)
+    assert "error" not in r, r
+    assert r["elements"] == 6 * 6 ** 3 + 2 * 6 * 6 + 6
