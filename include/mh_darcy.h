@@ -427,15 +427,25 @@ int mh_amg_level(const mh_handle *h, int32_t level, int64_t *n, int64_t *nnz, in
  * Computes r = b - S x for an n x n CSR matrix (row_ptr [n+1], col/val [nnz]) and writes
  *   out[0] = |D^-1/2 r| / |D^-1/2 b|   (D = diag S; the norm mh_solve judges convergence by)
  *   out[1] = |r| / |b|,  out[2] = |r|,  out[3] = |b|
- * and, if r is not NULL, the residual vector.  Every pointer is a device pointer owned by
- * the caller; work runs on cuda_stream (NULL: the legacy default stream) and is complete
- * when the call returns.  The call allocates nothing and calls no allocating routine: its
- * scratch is a fixed array inside the library (about 512 KiB, held on every GPU that loads
- * the library until the process exits), so n is limited to MH_NOALLOC_MAX_ROWS and larger n
- * is rejected with MH_ERR_INVALID.  The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU race and must be serialised by
- * the caller. */
+ * and, if r is not NULL, the residual vector.  r must not overlap x or b (MH_ERR_INVALID).
+ * Every pointer is a device pointer owned by the caller; work runs on cuda_stream (NULL: the
+ * legacy default stream) and is complete when the call returns.  The scratch is a fixed
+ * array inside the library (about 512 KiB, held on every GPU that loads the library until
+ * the process exits), so n is limited to MH_NOALLOC_MAX_ROWS and larger n is rejected with
+ * MH_ERR_INVALID.
+ *
+ * Set-up: CUDA loads a library's device code lazily, per context.  The first call in a
+ * context loads this entry point's code and array (which allocates device memory) and looks
+ * up the array's device address (cudaGetSymbolAddress).  Call it once with n == 0 (all other
+ * pointers may be NULL) in each context you will use, at start-up while allocation still
+ * succeeds and before any stream capture: that call does only the set-up.  After it, calls in
+ * that context allocate nothing and call no allocating routine.  A new context (one created
+ * after cudaDeviceReset, or a driver-API context made current) needs its own set-up call.
+ *
+ * Errors: an error already pending from the caller's earlier CUDA work makes the call return
+ * MH_ERR_CUDA and is left pending; errors of this call's own work are cleared and returned as
+ * MH_ERR_CUDA.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 #define MH_NOALLOC_MAX_ROWS (16384 * 256)
 int mh_csr_residual_noalloc(int64_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
                             const double *b, const double *x, double *r, double *out, void *cuda_stream);

@@ -11,6 +11,15 @@
 // (about 512 KiB) until the process exits.  All calls share it and it keeps the last call's
 // contents, so the arrival ticket is cleared at the start of every call; calls that overlap on
 // the GPU (different streams, or different host threads) race on it.
+//
+// In host code g_noalloc_scratch names a host-side stand-in, so the kernel is given the array's
+// device address, looked up with cudaGetSymbolAddress.  That address belongs to a CUDA context
+// (the module holding the array is loaded into each context separately), so it is cached per
+// context id: a context created after cudaDeviceReset, or a driver-API context the caller made
+// current, gets its own lookup.  CUDA loads modules lazily, and the first lookup in a context
+// loads this file's module, which allocates device memory for its code and the array; a call
+// with n == 0 does only that set-up, so callers can run it while allocation still succeeds.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -22,7 +31,7 @@ namespace {
 
 constexpr int kRowsPerBlock = 256;
 constexpr int kMaxBlocks = MH_NOALLOC_MAX_ROWS / kRowsPerBlock;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;
 
 struct NoAllocScratch {
     double partial[kMaxBlocks][4];  // per-block sums: r'D^-1 r, b'D^-1 b, r'r, b'b
@@ -30,10 +39,6 @@ struct NoAllocScratch {
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
-
-// Device address of g_noalloc_scratch on each device, looked up once per device.
-std::mutex g_setup_mutex;
-NoAllocScratch *g_scratch_addr[kMaxDevices] = {};
 
 __global__ void __launch_bounds__(kRowsPerBlock)
     k_csr_residual_noalloc(int64_t n, const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ col,
@@ -109,33 +114,95 @@ __global__ void __launch_bounds__(kRowsPerBlock)
     }
 }
 
+// ---- per-context cache of the scratch array's device address -----------------------------
+typedef CUresult(CUDAAPI *PFN_ctx_current)(CUcontext *);
+typedef CUresult(CUDAAPI *PFN_ctx_id)(CUcontext, unsigned long long *);
+
+struct ContextEntry {
+    unsigned long long ctx_id;
+    NoAllocScratch *addr;
+};
+
+std::mutex g_setup_mutex;
+std::once_flag g_driver_once;
+PFN_ctx_current g_ctx_current = nullptr;
+PFN_ctx_id g_ctx_id = nullptr;
+ContextEntry g_contexts[kMaxContexts];
+int g_n_contexts = 0;
+
+void load_driver_entry_points() {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_current = (PFN_ctx_current)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_id = (PFN_ctx_id)f;
+    cudaGetLastError();  // a failed lookup only disables the cache; it is not this call's error
+}
+
+// Device address of g_noalloc_scratch in the context current on this thread.  Looked up once per
+// context; when no context is current yet (the lookup then initialises the device's primary
+// context) or the driver lacks cuCtxGetId (before CUDA 12.0), it is looked up without caching.
+cudaError_t scratch_address(NoAllocScratch **out) {
+    std::call_once(g_driver_once, load_driver_entry_points);
+    unsigned long long id = 0;
+    bool have_id = false;
+    if (g_ctx_current && g_ctx_id) {
+        CUcontext ctx = nullptr;
+        have_id = g_ctx_current(&ctx) == CUDA_SUCCESS && ctx && g_ctx_id(ctx, &id) == CUDA_SUCCESS;
+    }
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (have_id)
+        for (int i = 0; i < g_n_contexts; ++i)
+            if (g_contexts[i].ctx_id == id) {
+                *out = g_contexts[i].addr;
+                return cudaSuccess;
+            }
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if (!p) return cudaErrorInvalidSymbol;
+    // load the kernel too, so that a set-up call leaves nothing for a later call to load
+    cudaFuncAttributes attr;
+    e = cudaFuncGetAttributes(&attr, k_csr_residual_noalloc);
+    if (e != cudaSuccess) return e;
+    if (have_id && g_n_contexts < kMaxContexts) g_contexts[g_n_contexts++] = {id, (NoAllocScratch *)p};
+    *out = (NoAllocScratch *)p;
+    return cudaSuccess;
+}
+
+bool overlaps(const void *a, const void *b, int64_t n) {
+    const uintptr_t pa = (uintptr_t)a, pb = (uintptr_t)b, bytes = (uintptr_t)n * sizeof(double);
+    return pa < pb + bytes && pb < pa + bytes;
+}
+
 }  // namespace
 
 extern "C" int mh_csr_residual_noalloc(int64_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
                                        const double *b, const double *x, double *r, double *out,
                                        void *cuda_stream) {
-    if (n <= 0 || !row_ptr || !col || !val || !b || !x || !out) return MH_ERR_INVALID;
-    if (n > (int64_t)MH_NOALLOC_MAX_ROWS) return MH_ERR_INVALID;  // larger than the fixed scratch
+    if (n < 0 || n > (int64_t)MH_NOALLOC_MAX_ROWS) return MH_ERR_INVALID;  // beyond the fixed scratch
+    if (n > 0) {
+        if (!row_ptr || !col || !val || !b || !x || !out) return MH_ERR_INVALID;
+        // the kernel reads x and b while other threads write r
+        if (r && (overlaps(r, x, n) || overlaps(r, b, n))) return MH_ERR_INVALID;
+    }
+    // an error left by the caller's earlier work is not this call's: report it, leave it pending
+    if (cudaPeekAtLastError() != cudaSuccess) return MH_ERR_CUDA;
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         cudaGetLastError();
         return MH_ERR_CUDA;
     }
     NoAllocScratch *scratch = nullptr;
-    {
-        // set-up on the first call per device: in host code g_noalloc_scratch names a host-side
-        // stand-in, so the kernel gets the device address from cudaGetSymbolAddress
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_addr[dev]) {
-            void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return MH_ERR_CUDA;
-            }
-            g_scratch_addr[dev] = (NoAllocScratch *)p;
-        }
-        scratch = g_scratch_addr[dev];
+    if (scratch_address(&scratch) != cudaSuccess) {
+        cudaGetLastError();
+        return MH_ERR_CUDA;
     }
+    if (n == 0) return MH_OK;  // set-up only
     cudaStream_t s = (cudaStream_t)cuda_stream;
     if (cudaMemsetAsync(&scratch->ticket, 0, sizeof(unsigned int), s) != cudaSuccess) {
         cudaGetLastError();

@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ from the Flow123d reference tree.
 
-Run once in a checkout that has the reference sources (default /root/reference):
-    python tests/golden/make_fixtures.py [REFERENCE_ROOT]
+Run once where the reference sources are available, giving the root of their tree:
+    python tests/golden/make_fixtures.py REFERENCE_ROOT
 Each case is written as <case>.npz holding the mesh (nodes, bulk and boundary elements with
 their physical regions), the coefficient and boundary data of the case's .con file (evaluated
 the way the reference evaluates them: element fields per region, boundary fields at the
@@ -36,7 +36,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "tests")):
+    sys.exit("usage: make_fixtures.py REFERENCE_ROOT  (the Flow123d source tree, holding tests/)")
+REF = sys.argv[1]
 OUT = os.path.dirname(os.path.abspath(__file__))
 TDIM = {1: 1, 2: 2, 4: 3, 15: 0}
 
