@@ -10,7 +10,9 @@ GPU library; never imported by the product.  Provides:
                         (src/la/schur.cc:566-773, darcy_flow_mh.cc:1009-1131);
   * pcg_jacobi       -- the CPU FP64 Jacobi-PCG used as the timed CPU baseline;
   * pcg_ilu0 / ilu0  -- CPU FP64 CG with an ILU(0) preconditioner, the zero-fill member of the
-                        incomplete factorisations of the reference's PETSc solver (solve.cc:355-374).
+                        incomplete factorisations of the reference's PETSc solver (solve.cc:355-374);
+  * pcg_iluk / iluk  -- the same with k levels of fill (orc_iluk.c); k = 3 is the reference's
+                        serial default (-pc_factor_levels 3, solve.cc:370).
 Parity of the restatement is pinned to the reference's golden outputs in tests/golden.
 """
 import ctypes as C
@@ -57,6 +59,14 @@ def _load():
     L.orc_local_matrix.restype = C.c_int
     L.orc_local_matrix.argtypes = [f64p, i32p, i32p, C.c_int64, f64p, C.c_double, C.c_double, f64p, f64p, f64p]
     L.orc_num_threads.restype = C.c_int
+    L.orc_topology.restype = C.c_int
+    L.orc_topology.argtypes = [C.c_int64, C.c_int64, i32p, i32p, C.c_int64, i32p, i32p] + [i32p] * 8 + \
+        [C.POINTER(C.c_int64)]
+    L.orc_iluk.restype = C.c_int64
+    L.orc_iluk.argtypes = [C.c_int64, i32p, i32p, f64p, C.c_int, i32p, i32p, f64p, i32p, C.c_int64]
+    L.orc_pcg_iluk.restype = C.c_int
+    L.orc_pcg_iluk.argtypes = [C.c_int64, i32p, i32p, f64p, f64p, f64p, C.c_int, C.c_double, C.c_int, f64p, f64p,
+                               f64p]
     return L
 
 
@@ -151,9 +161,17 @@ def solve_mh_direct(P):
     return spla.spsolve(A.tocsc(), rhs)
 
 
+def _local_sizes(P):
+    """Edges of each element's local system: its sides plus its VB neighbours' higher sides."""
+    m = P.keep["el_dim"].astype(np.int64) + 1
+    if len(P.keep["ngh_element"]):
+        m += np.bincount(P.keep["ngh_element"], minlength=P.n_el)
+    return m
+
+
 def schur2(P):
     """Second Schur complement S2 (reference schur2 after scale(-1)) and its rhs."""
-    cap = 64 * P.n_el + 16
+    cap = int(np.sum(_local_sizes(P) ** 2)) + 16
     I = np.zeros(cap, np.int32)
     J = np.zeros(cap, np.int32)
     V = np.zeros(cap)
@@ -256,6 +274,52 @@ def pcg_ilu0(S, b, x0=None, rtol=1e-10, max_it=100000):
     it = lib.orc_pcg_ilu0(len(b), _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double),
                           _ptr(b, C.c_double), _ptr(x, C.c_double), rtol, max_it, C.byref(res), C.byref(tf))
     return x, it, res.value, tf.value
+
+
+def _csr_arrays(S):
+    S = S.tocsr()
+    S.sort_indices()
+    return (np.ascontiguousarray(S.indptr, np.int32), np.ascontiguousarray(S.indices, np.int32),
+            np.ascontiguousarray(S.data, np.float64))
+
+
+def pcg_iluk(S, b, k=3, x0=None, rtol=1e-10, max_it=100000):
+    """CPU FP64 CG preconditioned by ILU(k) (level-of-fill incomplete LU, orc_iluk.c; k = 3 is
+    PETSc's setting in the reference's serial solver).  Returns x, iterations (-1 if max_it,
+    -2 if the factorisation failed), the true Jacobi-scaled relative residual, the
+    factorisation's seconds and the factor's fill ratio nnz(LU) / nnz(S)."""
+    rp, col, val = _csr_arrays(S)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+    res, tf, fill = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+    it = lib.orc_pcg_iluk(len(b), _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double),
+                          _ptr(b, C.c_double), _ptr(x, C.c_double), k, rtol, max_it, C.byref(res), C.byref(tf),
+                          C.byref(fill))
+    return x, it, res.value, tf.value, fill.value
+
+
+def iluk(S, k, raw=False):
+    """(L, U) of ILU(k) as scipy CSR matrices (L unit lower), for checks; raw=True returns the
+    factor as stored (strict L and U in one CSR, its pattern kept with any zero values)."""
+    rp, col, val = _csr_arrays(S)
+    n = S.shape[0]
+    frp = np.zeros(n + 1, np.int32)
+    dpos = np.zeros(n, np.int32)
+    nnz = lib.orc_iluk(n, _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double), k,
+                       _ptr(frp, C.c_int32), None, None, _ptr(dpos, C.c_int32), 0)
+    if nnz < 0:
+        raise ArithmeticError("ILU(k) breakdown (%d)" % nnz)
+    fcol = np.zeros(nnz, np.int32)
+    fval = np.zeros(nnz)
+    rc = lib.orc_iluk(n, _ptr(rp, C.c_int32), _ptr(col, C.c_int32), _ptr(val, C.c_double), k,
+                      _ptr(frp, C.c_int32), _ptr(fcol, C.c_int32), _ptr(fval, C.c_double), _ptr(dpos, C.c_int32), nnz)
+    if rc < 0:
+        raise ArithmeticError("ILU(k) breakdown (%d)" % rc)
+    F = sp.csr_matrix((fval, fcol, frp), shape=S.shape)
+    if raw:
+        return F
+    L = sp.tril(F, -1, format="csr") + sp.identity(n, format="csr")
+    return L, sp.triu(F, 0, format="csr")
 
 
 def ilu0(S):

@@ -15,8 +15,6 @@ homogeneous Neumann elsewhere.  Seeds: 1234 + config index (+ instance for cfg3)
 """
 import numpy as np
 
-from .mesh import cube_mesh
-
 _SIDE = {1: np.array([[0, -1, -1], [1, -1, -1]]), 2: np.array([[0, 1, -1], [1, 2, -1], [0, 2, -1]]),
          3: np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])}
 
@@ -69,8 +67,14 @@ def dirichlet_x_bc(topo, mesh, p_left=1.0, p_right=0.0):
     return dict(bc_type=typ, pressure=p), sb[bs[left]]
 
 
-def make_case(cfg, seed=None, n=None, corr_len=None):
-    """Mesh and coefficients of a benchmark configuration (1..5)."""
+def make_case(cfg, seed=None, n=None, corr_len=None, mesh_builder=None):
+    """Mesh and coefficients of a benchmark configuration (1..5).  mesh_builder(n, planes,
+    lines) makes the Kuhn cube mesh (default: the library's mhdarcy.cube_mesh); this module
+    needs nothing else from the package, so a CPU-only caller can load it by file path and
+    pass its own builder of the same mesh."""
+    if mesh_builder is None:
+        from .mesh import cube_mesh as mesh_builder
+    cube_mesh = mesh_builder
     seed = 1234 + cfg if seed is None else seed
     rng = np.random.default_rng(seed)
     if cfg == 1:

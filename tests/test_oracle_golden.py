@@ -6,6 +6,7 @@ pressures of the reference's VTK outputs, solved with the reference's default to
 (r_tol 1e-7), so agreement is expected at that level.  t06 also has analytic answers."""
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import oracle as O
 import topology as T
@@ -311,3 +312,71 @@ def test_cpu_pcg_matches_direct():
     import scipy.sparse.linalg as spla
     lam = spla.spsolve(S.tocsc(), r)
     assert np.abs(x - lam).max() < 1e-9
+
+
+def _dense_iluk(A, pattern, k):
+    """Level-of-fill ILU(k) on a dense copy, restated independently of orc_iluk.c (Saad,
+    algorithm 10.5): levels start at 0 on the pattern of A (inf elsewhere); row i is
+    eliminated with every finished row j < i whose entry (i, j) has level <= k, which updates
+    all (i, m) and gives them the level min(lev_im, lev_ij + lev_jm + 1); at the end of the
+    row, entries above level k are dropped."""
+    n = A.shape[0]
+    W = A.copy()
+    lev = np.where(pattern, 0, np.inf)
+    for i in range(n):
+        for j in range(i):
+            if lev[i, j] > k:
+                continue
+            W[i, j] /= W[j, j]
+            m = np.arange(j + 1, n)
+            m = m[lev[j, m] <= k]
+            W[i, m] -= W[i, j] * W[j, m]
+            lev[i, m] = np.minimum(lev[i, m], lev[i, j] + lev[j, m] + 1)
+        drop = lev[i] > k
+        lev[i, drop] = np.inf
+        W[i, drop] = 0.0
+    return W, lev <= k
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_cpu_iluk_matches_dense_restatement(k):
+    """ILU(k) of the CPU baseline (the reference's PETSc preconditioner is ILU(3)): pattern and
+    factors equal a dense restatement of the level-of-fill rule on a small fractured system."""
+    import cases as OC
+    P, mesh, coeffs, topo, bc = OC.problem(1, n=3)
+    S, r = O.schur2(P)
+    F = O.iluk(S, k, raw=True)
+    Sc = S.tocoo()
+    spat = np.zeros(S.shape, bool)
+    spat[Sc.row, Sc.col] = True
+    W, pat = _dense_iluk(S.toarray(), spat, k)
+    Fd = F.toarray()
+    got_pat = np.zeros_like(pat)
+    Fc = F.tocoo()
+    got_pat[Fc.row, Fc.col] = True
+    assert np.array_equal(got_pat, pat)
+    assert np.abs(Fd - np.where(pat, W, 0.0)).max() <= 1e-12 * np.abs(W).max()
+
+
+def test_cpu_iluk_pcg():
+    """ILU(0) through orc_iluk equals orc_ilu0; more levels need fewer iterations; enough
+    levels give the exact LU, and PCG converges in one iteration."""
+    import cases as OC
+    P, mesh, coeffs, topo, bc = OC.problem(1, n=6)
+    S, r = O.schur2(P)
+    L0, U0 = O.ilu0(S)
+    Lk, Uk = O.iluk(S, 0)
+    assert abs(L0 - Lk).max() == 0.0 and abs(U0 - Uk).max() == 0.0
+    its = []
+    for k in (0, 1, 3):
+        x, it, res, tf, fill = O.pcg_iluk(S, r, k=k, rtol=1e-10)
+        assert it > 0 and res <= 1e-10 * 1.01
+        its.append(it)
+        if k == 0:
+            assert fill == 1.0 and it == O.pcg_ilu0(S, r, rtol=1e-10)[1]
+    assert its[0] > its[1] > its[2]
+    Lf, Uf = O.iluk(S, 10 ** 6)
+    A = S.toarray()
+    assert np.abs((Lf @ Uf).toarray() - A).max() <= 1e-13 * np.abs(A).max()
+    x, it, res, tf, fill = O.pcg_iluk(S, r, k=10 ** 6, rtol=1e-10)
+    assert it <= 1

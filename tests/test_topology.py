@@ -101,3 +101,48 @@ def test_gmsh_reader_round_trip(tmp_path):
     m2 = mhdarcy.read_gmsh(str(path))
     assert np.array_equal(m2.el_nodes, mesh.el_nodes) and np.array_equal(m2.bc_nodes, mesh.bc_nodes)
     assert np.allclose(m2.nodes, mesh.nodes, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("name", ["t01", "t02", "t03", "t05_robin", "t06_32", "t06_21", "t08", "t10_mh", "t13", "t14"])
+def test_oracle_c_topology_matches_python_restatement(name):
+    """The oracle's C topology (used by the CPU arm of the benchmark, which loads no product
+    code) equals the pure-Python restatement on every fixture, explicit boundary elements
+    included."""
+    import cases as OC
+    z, mesh = load_fixture(name)
+    ref = T.build(mesh)
+    t = OC.topology(mesh)
+    assert t["n_edges"] == ref["n_edges"]
+    for k in KEYS:
+        assert np.array_equal(t[k], ref[k]), k
+
+
+@pytest.mark.parametrize("cfg,n,seed", [(1, 6, None), (2, 8, None), (3, None, 77), (4, 6, None), (5, 16, None)])
+def test_oracle_cases_match_library_cases(cfg, n, seed):
+    """The CPU arm's numpy Kuhn cube and C topology give the library's mesh, coefficients and
+    topology element for element (the two benchmark arms solve identical inputs)."""
+    import cases as OC
+    from mhdarcy.cases import make_case
+    m1, c1 = make_case(cfg, seed=seed, n=n)
+    m2, c2 = OC.make_case(cfg, seed=seed, n=n)
+    assert np.array_equal(m1.nodes, m2.nodes)
+    assert np.array_equal(m1.el_dim, m2.el_dim) and np.array_equal(m1.el_nodes, m2.el_nodes)
+    assert sorted(c1) == sorted(c2)
+    for k in c1:
+        assert np.array_equal(c1[k], c2[k]), k
+    t2 = OC.topology(m2)
+    with mhdarcy.MHSystem(m1) as s:
+        t1 = s.topology()
+        assert s.n_edges == t2["n_edges"]
+    for k in KEYS:
+        assert np.array_equal(t1[k], t2[k]), k
+
+
+def test_oracle_c_topology_rejects_boundary_on_bulk_element():
+    import cases as OC
+    z, mesh = load_fixture("t06_32")
+    tri = np.nonzero(mesh.el_dim == 2)[0][0]
+    bad = mhdarcy.Mesh(mesh.nodes, mesh.el_dim, mesh.el_nodes, np.array([2], np.int32),
+                       mesh.el_nodes[tri:tri + 1].copy())
+    with pytest.raises(ValueError):
+        OC.topology(bad)
