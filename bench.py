@@ -1,22 +1,33 @@
 #!/usr/bin/env python
 """Benchmark: steady MH Darcy solves/s to relative residual 1e-10 on one B200.
 
-Workload (default): the n=64 fractured Kuhn cube — 1,572,864 tetrahedra, the 8,192 fracture
-triangles of the z=0.5 plane (delta=1e-3, K=1e-3), a 64-segment 1D channel along x at
-y=z=0.5 (delta=1e-4, K=1e-2), log10 K ~ N(-6, 1.5) Gaussian-correlated with correlation
-length 0.1, Dirichlet p=1 at x=0 / p=0 at x=1.  Synthetic, seeded (no public dataset).
+Workload (default, --config 5): the n=96 fractured Kuhn cube -- 5,308,416 tetrahedra, six
+axis-aligned fracture planes at seeded grid positions (their triangles: cross-section 1e-3,
+log10 K ~ U(-4,-2) per plane) and four 1D channels along grid lines inside fracture planes
+(cross-section 1e-4, K = 1e-2); matrix log10 K ~ N(-7, 2) Gaussian-correlated with correlation
+length 0.05, clipped to 1e-9..1e-2; Dirichlet p=1 at x=0 / p=0 at x=1.  10,950,146 edge
+unknowns.  Synthetic and seeded: there is no public dataset for this path.  --config 1..4 select
+the other workloads (2: the n=64 cube with one fracture and one channel).
 
 A step is one full solve: local MH assembly + both Schur eliminations (K1), the Krylov solve
 of the edge system to FP64 true relative residual <= 1e-10 (Jacobi-scaled and unscaled), and
 back-substitution of element pressures and side fluxes (K4), with mesh, coefficients and
-boundary data resident in HBM.  `e2e` times the same step through the public API with host
-buffers: coefficients and boundary data copied in from pinned memory every step and the full
-MH solution copied back.
+boundary data resident in HBM.  Methods (--methods): pcg64 (plain FP64 Jacobi-PCG, the
+baseline), amg (aggregation-multigrid-preconditioned flexible CG, FP32/FP16 inner iteration,
+FP64 residual replacements), fcg (the same with the learned smoother, trained first on a
+smaller system of the same family), ir32, cheb.  `value` is the fastest converged method;
+every method's row, its speed-up over pcg64 and its flux and pressure errors (at r_tol 1e-10
+and 1e-12, against a solve to 1e-14) are in the line.  `e2e` times the fastest method through
+the public API with host buffers: coefficients and boundary data copied in from pinned memory
+every step and the full MH solution copied back.
 
---impl reference times the CPU path (the FP64 C restatement of the reference in oracle/,
-OpenMP over all host threads, Jacobi-preconditioned CG; --cpu-precond ilu0 selects ILU(0), the
-zero-fill member of the reference's PETSc ILU) on a bounded sample of the same workload.
-Multi-GPU (torchrun): independent replicas, one per GPU, no data-path collective.
+--impl reference times the CPU path: the FP64 C restatement of the reference in oracle/ (OpenMP
+over all host threads; Jacobi-preconditioned CG, or --cpu-precond ilu3 for the reference's own
+ILU(3)), on the same workload built by the oracle alone (numpy mesh, C topology; no GPU
+library).  Complete solves when they fit the time budget, else bounded samples projected with
+the iteration count of a complete CPU solve recorded by oracle/cpu_full_solves.py.
+Multi-GPU (torchrun): independent replicas, one per GPU, no data-path collective (--config 3:
+one fixed batch sharded over the ranks).
 """
 import argparse
 import json
@@ -31,22 +42,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "svn-export_b200"))
 
 METRIC = "MH Darcy solves/s to 1e-10 residual: learned+FP32 vs plain FP64 PCG, 1 B200"
+R_TOL = 1e-10
 WORKLOADS = {
     1: "n=16 fractured Kuhn cube: 24,576 tets + 512 fracture triangles + 16 channel segments, log10 K ~ N(-6,1)",
-    3: "batch of uneven fractured cubes (n in {8,12,16,24,32}, one z=0.5 fracture each), log10 K ~ N(-6,1) "
-       "correlated (length 0.05..0.2), all instances in one launch sequence",
     2: "n=64 fractured Kuhn cube: 1,572,864 tets + 8,192 fracture triangles + 64 channel segments, "
        "log10 K ~ N(-6,1.5) correlated (length 0.1)",
+    3: "batch of uneven fractured cubes (n in {8,12,16,24,32}, one z=0.5 fracture each), log10 K ~ N(-6,1) "
+       "correlated (length 0.05..0.2), all instances in one launch sequence",
     4: "n=48 fractured Kuhn cube: 663,552 tets + 4,608 fracture triangles, log10 K ~ N(-6,1)",
     5: "n=96 cube: 5,308,416 tets, 6 fracture planes, 4 channels, log10 K ~ N(-7,2) correlated (0.05)",
 }
-# Jacobi-PCG iterations to 1e-10 (same algorithm and stopping rule on CPU and GPU), measured on
-# a B200 with the FP64 path of this bench (seeded inputs, so deterministic); used to scale the
-# CPU per-iteration sample of --impl reference to a full solve.
-JACOBI_PCG_ITERS = {1: 1630, 2: 4785}
-# ILU(0)-PCG iterations to 1e-10 under the same stopping rule, measured with the CPU restatement
-# (oracle/, 8 host threads, seeded inputs); the projection count of --cpu-precond ilu0.
-ILU0_PCG_ITERS = {1: 168, 2: 1509}
+# solver ids of mh_darcy.h (MH_SOLVER_*) and per-method options
+METHOD_IDS = {"pcg64": 0, "ir32": 1, "cheb": 2, "fcg": 3, "amg": 4}
+SOLVE_KW = {"amg": lambda a: {"inner_rtol": a.amg_inner_rtol}, "fcg": lambda a: {"inner_rtol": a.amg_inner_rtol}}
 
 
 def parse():
@@ -55,26 +63,30 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=2, choices=sorted(WORKLOADS))
-    ap.add_argument("--methods", default="pcg64,ir32,amg",
+    ap.add_argument("--config", type=int, default=5, choices=sorted(WORKLOADS))
+    ap.add_argument("--methods", default="pcg64,amg,fcg",
                     help="comma list of pcg64, ir32, amg (multigrid FCG), cheb (Chebyshev-Jacobi FCG), "
-                         "fcg (learned FCG)")
+                         "fcg (multigrid FCG with the learned smoother)")
     ap.add_argument("--amg-inner-rtol", type=float, default=1e-3,
-                    help="FP32 residual reduction between FP64 replacements in the AMG solve")
+                    help="FP32 residual reduction between FP64 replacements in the multigrid solves")
     ap.add_argument("--train-n", type=int, default=24, help="cube size of the system the network trains on")
     ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the flux/pressure error block")
+    ap.add_argument("--pcg-accuracy", action="store_true", help="also time pcg64 at r_tol 1e-12 in the error block")
+    ap.add_argument("--extra-config", type=int, default=2, help="second workload timed with fewer steps (0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-iters", type=int, default=200)
-    ap.add_argument("--cpu-precond", choices=["jacobi", "ilu0"], default="jacobi",
-                    help="preconditioner of the CPU baseline's CG: Jacobi (threaded throughout; the faster "
-                         "CPU solve on multi-core hosts at the benchmark sizes) or ILU(0) (the zero-fill "
-                         "member of the reference's PETSc ILU, sequential triangular solves; used where its "
-                         "iteration count is recorded)")
+    ap.add_argument("--cpu-precond", choices=["jacobi", "ilu0", "ilu3"], default="jacobi",
+                    help="preconditioner of the CPU path's CG: Jacobi (threaded throughout; the faster CPU solve on "
+                         "multi-core hosts at the benchmark sizes) or ILU(k) (the reference's PETSc solver uses "
+                         "ILU(3); sequential triangular solves)")
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0, help="CPU work of the cpu_baseline sample")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="CPU work of all warm-up and timed steps of --impl reference")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-setup-timing", action="store_true",
                     help="skip the host setup timing (gmsh read and handle creation at 56k elements)")
-    ap.add_argument("--instances", type=int, default=256, help="batch size of --config 3")
+    ap.add_argument("--instances", type=int, default=256, help="batch size of --config 3 (over all ranks)")
     ap.add_argument("--accuracy", action="store_true",
                     help="flux and pressure errors of AMG and FP64 PCG solves at r_tol 1e-10 and 1e-12 against "
                          "an AMG solve driven to r_tol 1e-14 (full-size systems have no direct solve)")
@@ -437,26 +449,109 @@ def setup_timing_isolated(n=21, reps=3, timeout_s=300):
         return {"error": "%s: %s" % (type(e).__name__, e)}
 
 
+# ---------------------------------------------------------------- shared config ---------
+def workload_config(cfg, n_edges, schur_nnz, mh_size, elements):
+    """The `config` object of both benchmark arms: the workload and its sizes only (the
+    method each arm runs is reported beside it)."""
+    return {"workload": "cfg%d: %s" % (cfg, WORKLOADS[cfg]), "n_edges": int(n_edges), "schur_nnz": int(schur_nnz),
+            "mh_size": int(mh_size), "elements": int(elements), "r_tol": R_TOL,
+            "l2": "inputs larger than L2 (edge matrix %.0f MB in FP64 CSR)" % (schur_nnz * 12 / 1e6)}
+
+
+def method_dtype(name, amg_half):
+    """Arithmetic types a method computes in (FP64 true residual and updates in all)."""
+    if name == "pcg64":
+        return "f64"
+    if name == "amg":
+        return "f64+f32+f16" if amg_half else "f64+f32"
+    if name == "fcg":
+        return "f64+f32+f16+bf16" if amg_half else "f64+f32+bf16"
+    return "f64+f32"
+
+
 # ---------------------------------------------------------------- ours ------------------
+def timed_solves(system, stream, method, k, warmup, kw, barrier, r_tol=R_TOL):
+    """warmup untimed and k timed steps (assembly + solve + back-substitution) on the handle's
+    stream; returns (ms per step on the device, stats of the last step, launches)."""
+    import torch
+    for _ in range(warmup):
+        system.assemble()
+        system.solve(method=method, r_tol=r_tol, **kw)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    l0 = system.kernel_launches()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(k):
+        system.assemble()
+        stats.append(system.solve(method=method, r_tol=r_tol, **kw))
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    barrier()
+    return ev0.elapsed_time(ev1) / k, stats, system.kernel_launches() - l0
+
+
+def run_extra_config(a, cfg, methods, barrier):
+    """A second workload (cfg2 by default) timed with fewer steps, reported under `extra`."""
+    import torch
+
+    import mhdarcy
+    from mhdarcy.cases import dirichlet_x_bc, make_case
+    stream = torch.cuda.Stream()
+    mesh, coeffs = make_case(cfg)
+    out = {}
+    with mhdarcy.MHSystem(mesh) as s:
+        s.set_stream(stream.cuda_stream)
+        bc, _ = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        sz = s.sizes
+        for name in methods:
+            kw = {"inner_rtol": a.amg_inner_rtol} if name == "amg" else {}
+            ms, stats, _ = timed_solves(s, stream, METHOD_IDS[name], 5, 3, kw, barrier)
+            out[name] = {"ms_per_solve": round(ms, 3), "solves_per_s": round(1e3 / ms, 3),
+                         "iterations": stats[-1]["iterations"], "converged": stats[-1]["status"] in (0, 2)}
+        return {"config": workload_config(cfg, sz.n_edges, sz.schur_nnz, sz.mh_size, sz.n_elements),
+                "steps": 5, "warmup": 3, "methods": out}
+
+
+def train_network(a, rank, system, cfg):
+    """Trains the learned preconditioner once on a smaller system of the same family (the
+    network depends on local matrix features only, so it transfers) and loads its weights
+    into `system`."""
+    import mhdarcy
+    from mhdarcy.cases import dirichlet_x_bc, make_case
+    tmesh, tcoeffs = make_case(cfg if cfg != 3 else 1, seed=4321 + rank, n=a.train_n)
+    with mhdarcy.MHSystem(tmesh) as tsys:
+        tbc, _ = dirichlet_x_bc(tsys.topology(), tmesh)
+        tsys.set_coeffs(**tcoeffs)
+        tsys.set_bc(tbc["bc_type"], tbc["pressure"])
+        tsys.assemble()
+        training = tsys.learned_train(n_pairs=12, epochs=a.train_epochs, lr=2e-3)
+        training["train_edges"] = tsys.n_edges
+        system.set_learned_weights(tsys.learned_weights())
+    return training
+
+
 def run_ours(a, rank, world):
     import numpy as np
     import torch
 
     import mhdarcy
-    from mhdarcy.cases import dirichlet_x_bc, make_case
-
     from mhdarcy import parallel
+    from mhdarcy.cases import dirichlet_x_bc, make_case
 
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    # one process per GPU, each with its own realisations: no collective on the data path,
-    # only the barrier and the max over ranks that time the run
+    # one process per GPU: independent replicas (or, for a batch, each rank's own share of the
+    # instances); no collective on the data path, only the barrier and the max over ranks
     rank, world, dist = parallel.init("nccl", timeout_s=300) if world > 1 else (rank, world, None)
     stream = torch.cuda.Stream()
     if a.config == 3:
-        # uneven batch: n in {8,12,16,24,32}, one z-plane fracture each, correlation 0.05..0.2
-        import numpy as np
-        parts = [make_case(3, seed=parallel.case_seed(3, rank, i)) for i in range(a.instances)]
+        # one fixed batch of a.instances uneven instances, sharded contiguously over the ranks
+        lo, hi = parallel.shard(a.instances, rank, world)
+        parts = [make_case(3, seed=parallel.case_seed(3, 0, i)) for i in range(lo, hi)]
         system = mhdarcy.MHSystem.batch([m for m, _ in parts])
         mesh = system.mesh
         coeffs = {k: np.concatenate([c[k] for _, c in parts]) for k in parts[0][1]}
@@ -482,66 +577,61 @@ def run_ours(a, rank, world):
     def max_over_ranks(x):
         return parallel.max_over_ranks(x, dist, device="cuda")
 
-    methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32, "cheb": mhdarcy.MH_SOLVER_CHEB,
-               "fcg": mhdarcy.MH_SOLVER_FCG_LEARNED, "amg": mhdarcy.MH_SOLVER_AMG}
-    solve_kw = {"amg": {"inner_rtol": a.amg_inner_rtol}}
+    names = [m for m in a.methods.split(",") if m]
     results = {}
-    training = None
-    if "fcg" in a.methods.split(","):
-        # the network is trained once, on a smaller system of the same family, and reused
-        tmesh, tcoeffs = make_case(a.config if a.config != 3 else 1, seed=4321 + rank, n=a.train_n)
-        with mhdarcy.MHSystem(tmesh) as tsys:
-            tbc, _ = dirichlet_x_bc(tsys.topology(), tmesh)
-            tsys.set_coeffs(**tcoeffs)
-            tsys.set_bc(tbc["bc_type"], tbc["pressure"])
-            tsys.assemble()
-            training = tsys.learned_train(n_pairs=12, epochs=a.train_epochs, lr=2e-3)
-            training["train_edges"] = tsys.n_edges
-            system.set_learned_weights(tsys.learned_weights())
+    training = train_network(a, rank, system, a.config) if "fcg" in names else None
     clocks = ClockSampler(local) if not a.no_clocks else None
-    for name in a.methods.split(","):
-        m = methods[name]
-        for _ in range(a.warmup):
-            system.assemble()
-            st = system.solve(method=m, r_tol=1e-10, **solve_kw.get(name, {}))
-        barrier()
+    for name in names:
+        m = METHOD_IDS[name]
+        kw = SOLVE_KW.get(name, lambda a: {})(a)
         if clocks and not results:
+            barrier()
             clocks.start()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stats = []
-        l0 = system.kernel_launches()
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-        for _ in range(a.steps):
-            system.assemble()
-            stats.append(system.solve(method=m, r_tol=1e-10, **solve_kw.get(name, {})))
-        with torch.cuda.stream(stream):
-            ev1.record(stream)
-        barrier()
-        ms = max_over_ranks(ev0.elapsed_time(ev1))
-        launches = system.kernel_launches() - l0
+        ms, stats, launches = timed_solves(system, stream, m, a.steps, a.warmup, kw, barrier)
+        ms = max_over_ranks(ms)
         ok = all(s["status"] in (0, mhdarcy.MH_FELL_BACK) for s in stats)
-        # the same steps again with every Krylov kernel timed by in-graph CUDA events (for the
+        # one more step with every Krylov kernel timed by in-graph CUDA events (for the
         # roofline; the events and per-graph read-backs add overhead, so not used for `value`)
-        prof = []
-        for _ in range(a.steps):
-            system.assemble()
-            prof.append(system.solve(method=m, r_tol=1e-10, profile_kernels=True, **solve_kw.get(name, {})))
-        barrier()
-        results[name] = {"ms_per_solve": ms / a.steps, "solves_per_s": world * per_step * a.steps / (ms / 1e3),
+        system.assemble()
+        prof = [system.solve(method=m, r_tol=R_TOL, profile_kernels=True, **kw)]
+        results[name] = {"ms_per_solve": ms, "solves_per_s": world * per_step / (ms / 1e3),
                          "iterations": stats[-1]["iterations"], "outer": stats[-1]["outer_iterations"],
                          "rel_residual": stats[-1]["rel_residual"],
                          "rel_residual_unscaled": stats[-1]["rel_residual_unscaled"], "converged": ok,
                          "ms_assembly": stats[-1]["ms_assembly"], "ms_backsub": stats[-1]["ms_backsub"],
-                         "ms_precond_setup": stats[-1]["ms_setup"],
-                         "stats": prof, "launches": launches,
-                         "ms_per_solve_profiled": statistics.mean(p["ms_solve"] + p["ms_backsub"] for p in prof),
-                         "fell_back": stats[-1]["fell_back"]}
+                         "ms_precond_setup": stats[-1]["ms_setup"], "stats": prof, "launches": launches,
+                         "dtype": method_dtype(name, AMG_VALUE_BYTES == 2), "fell_back": stats[-1]["fell_back"]}
         if name == "fcg":
             results[name]["training"] = training
     clock_info = clocks.stop() if clocks else None
     best = max((r for r in results if results[r]["converged"]), key=lambda r: results[r]["solves_per_s"])
     rb = results[best]
+
+    # accuracy: side fluxes and element pressures of every method's solve at r_tol 1e-10 and
+    # 1e-12 against an AMG solve driven to 1e-14 (a full-size system has no direct solve); the
+    # 1e-12 solve is timed too (the tolerance that meets a flux error of 1e-8 on these systems)
+    accuracy = None
+    if a.config != 3 and not a.no_accuracy:
+        accuracy = {}
+        st = system.solve(method=mhdarcy.MH_SOLVER_AMG, r_tol=1e-14, max_it=20000, inner_rtol=a.amg_inner_rtol)
+        ref = system.solution()
+        ns, ne = sz.n_sides, sz.n_elements
+        accuracy["reference"] = {"method": "amg", "r_tol": 1e-14, "iterations": st["iterations"],
+                                 "rel_residual": st["rel_residual"],
+                                 "rel_residual_unscaled": st["rel_residual_unscaled"]}
+        fmax, pmax = np.abs(ref[:ns]).max(), np.abs(ref[ns:ns + ne]).max()
+        for name in names:
+            kw = SOLVE_KW.get(name, lambda a: {})(a)
+            for rt in (R_TOL, 1e-12):
+                if rt != R_TOL and name == "pcg64" and not a.pcg_accuracy:
+                    continue
+                ms, stats, _ = timed_solves(system, stream, METHOD_IDS[name], 1, 0, kw, barrier, r_tol=rt)
+                sol = system.solution()
+                accuracy["%s@%g" % (name, rt)] = {
+                    "ms_per_solve": round(ms, 3), "iterations": stats[-1]["iterations"],
+                    "status": stats[-1]["status"],
+                    "flux_err": float(np.abs(sol[:ns] - ref[:ns]).max() / fmax),
+                    "pressure_err": float(np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max() / pmax)}
 
     # end to end through the public API with host buffers
     ne = sz.n_elements
@@ -552,21 +642,22 @@ def run_ours(a, rank, world):
     import ctypes as C
 
     from mhdarcy import _lib
-    for _ in range(max(1, a.warmup - 1)):
+    kwb = SOLVE_KW.get(best, lambda a: {})(a)
+
+    def e2e_step():
         system.set_coeffs(**hc)
         system.set_bc(hbt, hbp)
         system.assemble()
-        system.solve(method=methods[best], r_tol=1e-10, **solve_kw.get(best, {}))
+        system.solve(method=METHOD_IDS[best], r_tol=R_TOL, **kwb)
         _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
+    for _ in range(max(1, a.warmup - 1)):
+        e2e_step()
     barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         ev0.record(stream)
     for _ in range(a.steps):
-        system.set_coeffs(**hc)
-        system.set_bc(hbt, hbp)
-        system.assemble()
-        system.solve(method=methods[best], r_tol=1e-10, **solve_kw.get(best, {}))
-        _lib.check(_lib.lib.mh_get_solution(system.h, _lib.ptr(hsol, C.c_double), len(hsol)), system.h)
+        e2e_step()
     with torch.cuda.stream(stream):
         ev1.record(stream)
     barrier()
@@ -575,7 +666,7 @@ def run_ours(a, rank, world):
     h2d = sum(v.nbytes for v in hc.values()) + hbt.nbytes + hbp.nbytes
     d2h = 8 * sz.mh_size
     peaks = load_json(os.path.join(ROOT, "MEASURED_PEAKS.json"))
-    # Krylov kernels timed in-graph (PCG64 / IR32); the flexible-CG graphs carry no events
+    # Krylov kernels timed in-graph: the best method's, else the fastest timed one's
     timed = [r for r in results if any(st["kernel_count"][k] for st in results[r]["stats"] for k in range(5))]
     rstats = rb["stats"] if best in timed else (results[max(timed, key=lambda r: results[r]["solves_per_s"])]["stats"]
                                                  if timed else [])
@@ -583,118 +674,173 @@ def run_ours(a, rank, world):
     out = {
         "metric": METRIC, "value": round(rb["solves_per_s"], 4), "unit": "solves/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(rb["ms_per_solve"], 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if best == "pcg64" else "f32+f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": rb["dtype"],
         "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
-        "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": best,
-                   "instances_per_step": per_step,
-                   "n_edges": N, "schur_nnz": Z, "mh_size": sz.mh_size, "elements": ne,
-                   "r_tol": 1e-10, "l2": "inputs larger than L2 (edge matrix %.0f MB)" % (sz.sell_slots * 24 / 1e6),
-                   "parallelism": "replicas" if world > 1 else "single GPU", "autotune": tune},
+        "config": workload_config(a.config, N, Z, sz.mh_size, ne),
+        "method": best, "instances_per_step": per_step,
+        "parallelism": ("batch sharded over ranks" if a.config == 3 else "replicas") if world > 1 else "single GPU",
+        "autotune": tune,
         "e2e": {"value": round(world * per_step * a.steps / (ms_e2e / 1e3), 4), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roof,
         "gpu_launches": int(rb["launches"]),
         "methods": {k: {kk: vv for kk, vv in v.items() if kk != "stats"} for k, v in results.items()},
+        "speedup_vs_pcg64": ({k: round(v["solves_per_s"] / results["pcg64"]["solves_per_s"], 3)
+                              for k, v in results.items()} if "pcg64" in results else None),
+        "accuracy": accuracy,
         "dofs_per_s": round(rb["solves_per_s"] / per_step * sz.mh_size, 1),
         "clocks": clock_info,
     }
-    if "pcg64" in results:
-        JACOBI_PCG_ITERS[a.config] = results["pcg64"]["iterations"]
     out["postprocess"] = element_flux_timing(system, stream, sz, mesh)
     system.close()
+    if a.extra_config and world == 1 and a.extra_config != a.config:
+        out["extra"] = {"cfg%d" % a.extra_config: run_extra_config(a, a.extra_config, ["pcg64", "amg"], barrier)}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    return out, (mesh, coeffs, bc, topo, N)
+    return out
 
 
 # ------------------------------------------------------------ CPU path ------------------
-def cpu_sample(a, mesh=None, coeffs=None, bc=None, topo=None, n_edges=None, pcg_iters=None):
-    """Times the CPU restatement (oracle/, all host threads) on a bounded sample of the workload:
-    the threaded element-local double-Schur assembly, `cpu_sample_iters` Jacobi-PCG iterations and
-    the threaded back-substitution, projected to a full solve with the Jacobi-PCG iteration count
-    of this system (same algorithm and stopping rule as the GPU FP64 path).  With --cpu-precond
-    ilu0 (for workloads whose ILU(0) count is recorded) the sample is the ILU(0) factorisation
-    and ILU(0)-PCG iterations (threaded SpMV and vector updates, sequential triangular solves),
-    projected with the ILU(0)-PCG count."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
+def cpu_full_record(cfg, precond):
+    """Iterations of a complete CPU solve of this configuration to r_tol 1e-10 with this
+    preconditioner, measured by the CPU restatement itself (oracle/cpu_full_solves.py, which
+    appends every run to oracle/cpu_full_solves.jsonl); None when not recorded."""
+    rec = None
+    try:
+        with open(os.path.join(ROOT, "oracle", "cpu_full_solves.jsonl")) as f:
+            for line in f:
+                d = json.loads(line)
+                if d.get("config") == cfg and d.get("precond") == precond and d.get("r_tol") == R_TOL \
+                        and d.get("iterations", -1) > 0:
+                    rec = d
+    except OSError:
+        pass
+    return rec
 
-    import oracle as O
-    if mesh is None:
-        import mhdarcy
-        from mhdarcy.cases import dirichlet_x_bc, make_case
-        mesh, coeffs = make_case(a.config)
-        with mhdarcy.MHSystem(mesh) as s:
-            topo = s.topology()
-            n_edges = s.n_edges
-        bc, _ = dirichlet_x_bc(topo, mesh)
-    P = O.Problem(mesh, topo, n_edges, conductivity=coeffs["conductivity"], cross_section=coeffs["cross_section"],
-                  storativity=coeffs.get("storativity", 1.0), bc_type=bc["bc_type"], bc_pressure=bc["pressure"])
-    S, r = O.schur2(P)                      # pattern (setup, untimed)
-    S.sort_indices()
-    rp = np.ascontiguousarray(S.indptr, np.int32)
-    col = np.ascontiguousarray(S.indices, np.int32)
-    val = np.zeros(len(col))
-    rhs = np.zeros(n_edges)
-    t0 = time.perf_counter()
-    O.schur2_csr_into(P, rp, col, val, rhs)
-    t_asm = time.perf_counter() - t0
-    S.data[:] = val
-    k = a.cpu_sample_iters
-    ilu = a.cpu_precond == "ilu0" and a.config in ILU0_PCG_ITERS
-    t0 = time.perf_counter()
-    if ilu:
-        x, it, res, t_factor = O.pcg_ilu0(S, rhs, rtol=1e-30, max_it=k)
-        t_iter = (time.perf_counter() - t0 - t_factor) / k
-    else:
+
+class CpuProblem:
+    """The workload built by the oracle alone (numpy mesh, C topology, C assembly): nothing of
+    the GPU library is loaded.  The edge system's pattern is set-up work (not timed)."""
+
+    def __init__(self, cfg):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
+
+        import cases as OC
+        import oracle as O
+        self.O = O
+        self.cfg = cfg
+        self.P, mesh, _, _, _ = OC.problem(cfg)
+        S, _ = O.schur2(self.P)
+        self.rp = np.ascontiguousarray(S.indptr, np.int32)
+        self.col = np.ascontiguousarray(S.indices, np.int32)
+        self.nnz = len(self.col)
+        self.val = np.zeros(self.nnz)
+        self.rhs = np.zeros(self.P.n_edges)
+        del S
+
+    def config(self):
+        P = self.P
+        return workload_config(self.cfg, P.n_edges, self.nnz, P.mh_size, P.n_el)
+
+    def step(self, precond, iters):
+        """One step: the threaded double-Schur assembly, `iters` iterations of preconditioned CG
+        (None: to convergence at r_tol), and the back-substitution, each host-timed."""
+        import scipy.sparse as sp
+        O, P = self.O, self.P
+        t0 = time.perf_counter()
+        O.schur2_csr_into(P, self.rp, self.col, self.val, self.rhs)
+        t_asm = time.perf_counter() - t0
+        S = sp.csr_matrix((self.val, self.col, self.rp), shape=(P.n_edges, P.n_edges))
+        rtol, max_it = (R_TOL, 200000) if iters is None else (1e-30, iters)
+        t0 = time.perf_counter()
         t_factor = 0.0
-        x, it, res = O.pcg_jacobi(S, rhs, rtol=1e-30, max_it=k)
-        t_iter = (time.perf_counter() - t0) / k
-    t0 = time.perf_counter()
-    O.resolve(P, x)
-    t_res = time.perf_counter() - t0
-    iters = ILU0_PCG_ITERS[a.config] if ilu else (pcg_iters or JACOBI_PCG_ITERS.get(a.config))
-    t_solve = t_asm + t_factor + t_iter * iters + t_res if iters else None
-    name = "ILU(0)-PCG" if ilu else "Jacobi-PCG"
-    return {"t_asm": t_asm, "t_factor": t_factor, "t_iter": t_iter, "t_res": t_res, "iters": iters,
-            "t_solve": t_solve, "cores": O.num_threads(), "method": ("ilu0" if ilu else "jacobi") + "-pcg64 (CPU)",
-            "sample": "cfg%d full mesh: threaded double-Schur assembly + %s%d %s iterations + "
-                      "back-substitution, projected to %s iterations" % (
-                          a.config, "ILU(0) factorisation + " if ilu else "", k, name, iters)}
+        if precond == "jacobi":
+            x, it, res = O.pcg_jacobi(S, self.rhs, rtol=rtol, max_it=max_it)
+        else:
+            x, it, res, t_factor, _ = O.pcg_iluk(S, self.rhs, k=int(precond[3:]), rtol=rtol, max_it=max_it)
+        t_cg = time.perf_counter() - t0 - t_factor
+        t0 = time.perf_counter()
+        O.resolve(P, x)
+        t_res = time.perf_counter() - t0
+        done = max_it if iters is not None else it
+        return {"t_asm": t_asm, "t_factor": t_factor, "t_iter": t_cg / max(1, done), "t_res": t_res,
+                "iterations": done, "converged": iters is None and it > 0, "t_step": t_asm + t_factor + t_cg + t_res}
 
 
-def cpu_baseline_entry(a, ctx, pcg_iters):
-    """The `cpu_baseline` object of the bench line: the CPU restatement timed on the workload of
-    the GPU run (ctx = mesh, coefficients, boundary data, topology, edge count)."""
-    mesh, coeffs, bc, topo, N = ctx
-    cb = cpu_sample(a, mesh, coeffs, bc, topo, N, pcg_iters)
-    return {"value": round(1.0 / cb["t_solve"], 6) if cb["t_solve"] else None, "unit": "solves/s",
-            "cores": cb["cores"], "kind": "port", "sample": cb["sample"],
-            "detail": {k: cb[k] for k in ("method", "t_asm", "t_factor", "t_iter", "t_res", "iters")}}
+def cpu_runs(cp, precond, steps, warmup, budget_s):
+    """Times the CPU path: complete solves when (warmup + steps) of them fit the time budget,
+    else bounded samples (assembly, a number of CG iterations sized to the budget, and the
+    back-substitution) whose per-iteration time is projected to the iteration count a
+    complete CPU solve of this configuration needed (cpu_full_record).  Returns the measured
+    steps and the solves/s, with how it was obtained."""
+    probe = cp.step(precond, 10)
+    rec = cpu_full_record(cp.cfg, precond)
+    per_step = budget_s / max(1, steps + warmup)
+    full_est = probe["t_asm"] + probe["t_res"] + probe["t_iter"] * (rec["iterations"] if rec else 1e9)
+    complete = rec is None or full_est <= per_step
+    if complete:
+        iters = None
+    else:
+        iters = max(10, int((per_step - probe["t_asm"] - probe["t_res"]) / max(probe["t_iter"], 1e-9)))
+        iters = min(iters, rec["iterations"])
+    for _ in range(warmup):
+        cp.step(precond, iters)
+    runs = [cp.step(precond, iters) for _ in range(steps)]
+    t_step = statistics.median(r["t_step"] for r in runs)
+    if complete:
+        value, how = 1.0 / t_step, "complete solves to r_tol 1e-10 (%d iterations)" % runs[-1]["iterations"]
+        n_full = runs[-1]["iterations"]
+    else:
+        n_full = rec["iterations"]
+        t_full = statistics.median(r["t_asm"] + r["t_res"] for r in runs) + \
+            statistics.median(r["t_iter"] for r in runs) * n_full
+        value = 1.0 / t_full
+        how = ("projected: each step times the assembly, %d CG iterations and the back-substitution; the "
+               "per-iteration time is multiplied by the %d iterations a complete CPU solve of this workload "
+               "needed (oracle/cpu_full_solves.jsonl, measured by the CPU code itself)" % (iters, n_full))
+    return {"value": value, "t_step_ms": t_step * 1e3, "complete": complete, "how": how, "runs": runs,
+            "iterations_full": n_full, "sample_iterations": iters}
+
+
+def cpu_baseline_entry(a, cp):
+    """The `cpu_baseline` object of the bench line: the CPU path on all host threads (a bounded
+    sample of about 20 s) and on one thread (per-iteration time from a short sample)."""
+    O = cp.O
+    r = cpu_runs(cp, a.cpu_precond, 1, 0, a.cpu_budget_s)
+    cores = O.num_threads()
+    O.set_threads(1)
+    try:
+        one = cp.step(a.cpu_precond, 10)
+    finally:
+        O.set_threads(cores)
+    n_full = r["iterations_full"]
+    one_value = 1.0 / (one["t_asm"] + one["t_res"] + one["t_iter"] * n_full) if n_full else None
+    return {"value": round(r["value"], 6), "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": "cfg%d full mesh, %s-preconditioned CG (oracle/, OpenMP): %s" % (cp.cfg, a.cpu_precond, r["how"]),
+            "one_core": {"value": round(one_value, 6) if one_value else None, "unit": "solves/s", "cores": 1,
+                         "t_iter_s": one["t_iter"], "t_asm_s": one["t_asm"], "t_backsub_s": one["t_res"]},
+            "detail": {k: r["runs"][-1][k] for k in ("t_asm", "t_factor", "t_iter", "t_res")}}
 
 
 def run_reference(a):
+    """The reference arm: the CPU restatement of the reference path (oracle/), all host
+    threads, on this run's workload; rank 0 only (other ranks exit without work)."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return None
-    samples = []
-    for _ in range(a.warmup):
-        cpu_sample(a)
-    for _ in range(a.steps):
-        samples.append(cpu_sample(a))
-    t = statistics.median(s["t_solve"] for s in samples) if samples[0]["t_solve"] else None
-    v = round(1.0 / t, 6) if t else None
-    s0 = samples[0]
+    cp = CpuProblem(a.config)
+    r = cpu_runs(cp, a.cpu_precond, a.steps, a.warmup, a.ref_budget_s)
+    v = round(r["value"], 6)
+    cores = cp.O.num_threads()
     return {"metric": METRIC, "impl": "reference", "value": v, "unit": "solves/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(t * 1e3, 3) if t else None,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(r["t_step_ms"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
-            "config": {"workload": "cfg%d: %s" % (a.config, WORKLOADS[a.config]), "method": s0["method"],
-                       "r_tol": 1e-10},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": s0["cores"], "kind": "port",
-                             "sample": s0["sample"]},
+            "config": cp.config(), "method": "%s-pcg64 (CPU, oracle/)" % a.cpu_precond,
+            "projected": not r["complete"],
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": r["how"]},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -715,10 +861,10 @@ def main():
         if rank == 0:
             run_unsteady(a, rank, world)
         return
-    out, ctx = run_ours(a, rank, world)
+    out = run_ours(a, rank, world)
     if rank == 0:
         if not a.no_cpu_baseline and world == 1 and a.config != 3:
-            out["cpu_baseline"] = cpu_baseline_entry(a, ctx, out["methods"].get("pcg64", {}).get("iterations"))
+            out["cpu_baseline"] = cpu_baseline_entry(a, CpuProblem(a.config))
         if world == 1 and not a.no_setup_timing:
             out["setup"] = setup_timing_isolated()
         print(json.dumps(out))

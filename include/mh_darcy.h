@@ -417,6 +417,24 @@ int mh_amg_info(const mh_handle *h, int32_t *n_levels, int64_t *rows, int64_t *s
 int mh_amg_level(const mh_handle *h, int32_t level, int64_t *n, int64_t *nnz, int32_t *agg, float *weight,
                  int32_t *row_ptr, int32_t *col, float *val);
 
+/* ---- a general symmetric positive definite system (the LinSys seam) ------------------- */
+/* The solvers of mh_solve on a sparse SPD system the caller assembles itself, as Flow123d's
+ * LinSys hands a system to PETSc's KSP (src/la/linsys.hh:63-222, solve_system in
+ * src/la/solve.cc:175-209): for example the schur2 complement that SchurComplement::form_schur
+ * builds (src/la/schur.cc:566-611), or any other SPD system of the reference.  C++ callers use
+ * it through LinSys_CUDA (include/linsys_cuda.hh).
+ * mh_csr_create: n rows, CSR pattern row_ptr [n+1], col [row_ptr[n]] with the columns of every
+ * row sorted and unique and the diagonal present (MH_ERR_INVALID otherwise).  Without a device
+ * the handle is created (the layout is host work) and compute calls return MH_ERR_CUDA.
+ * mh_csr_set_values: val [row_ptr[n]] in CSR order and rhs [n]; every diagonal value must be
+ * > 0.  Then mh_solve (any MH_SOLVER_* method, the same convergence test on the FP64 true
+ * residual) and mh_csr_get_solution (x [n]).  The mesh-based calls (mh_set_coeffs, mh_set_bc,
+ * mh_assemble, mh_unsteady_*) return MH_ERR_STATE on such a handle; mh_get_sizes reports n as
+ * n_edges and the pattern's nonzeros as schur_nnz. */
+int mh_csr_create(int64_t n, const int32_t *row_ptr, const int32_t *col, mh_handle **out);
+int mh_csr_set_values(mh_handle *h, const double *val, const double *rhs);
+int mh_csr_get_solution(const mh_handle *h, double *x, int64_t n);
+
 /* ---- residual check without device allocation --------------------------------------- */
 /* No counterpart in the reference: Flow123d leaves this check to PETSc's KSP monitor.
  * For callers that cannot call cudaMalloc at the point where they need to check a solution:

@@ -1022,6 +1022,16 @@ int orc_pcg_ilu0(int64_t n, const int32_t *rp, const int32_t *col, const double 
     return (rr > tol2 || rdr > tol2s) ? -1 : it;
 }
 
+/* OpenMP threads of the following oracle calls (the CPU baseline's 1-core figure). */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    extern void omp_set_num_threads(int);
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     extern int omp_get_max_threads(void);

@@ -59,6 +59,8 @@ def _load():
     L.orc_local_matrix.restype = C.c_int
     L.orc_local_matrix.argtypes = [f64p, i32p, i32p, C.c_int64, f64p, C.c_double, C.c_double, f64p, f64p, f64p]
     L.orc_num_threads.restype = C.c_int
+    L.orc_set_threads.restype = None
+    L.orc_set_threads.argtypes = [C.c_int]
     L.orc_topology.restype = C.c_int
     L.orc_topology.argtypes = [C.c_int64, C.c_int64, i32p, i32p, C.c_int64, i32p, i32p] + [i32p] * 8 + \
         [C.POINTER(C.c_int64)]
@@ -185,6 +187,29 @@ def schur2(P):
     S.sum_duplicates()
     S.sort_indices()
     return S, rhs
+
+
+def schur2_element_blocks(P):
+    """The element-local blocks of the second Schur complement in element order, as
+    SchurComplement would hand them to LinSys::mat_set_values: (rows, vals) per element with
+    rows the element's local edges and vals the m x m block; and the summed rhs."""
+    m = _local_sizes(P)
+    cap = int(np.sum(m ** 2)) + 16
+    I = np.zeros(cap, np.int32)
+    J = np.zeros(cap, np.int32)
+    V = np.zeros(cap)
+    rhs = np.zeros(P.n_edges)
+    s = P.struct()
+    k = lib.orc_schur2_coo(C.byref(s), _ptr(I, C.c_int32), _ptr(J, C.c_int32), _ptr(V, C.c_double), cap,
+                           _ptr(rhs, C.c_double))
+    if k != int(np.sum(m ** 2)):
+        raise RuntimeError(f"orc_schur2_coo failed ({k})")
+    blocks, o = [], 0
+    for me in m:
+        me = int(me)
+        blocks.append((I[o:o + me * me:me].copy(), V[o:o + me * me].reshape(me, me).copy()))
+        o += me * me
+    return blocks, rhs
 
 
 def schur2_csr_into(P, row_ptr, col, val, rhs):
@@ -355,3 +380,8 @@ def local_matrix(mesh, e, conductivity=1.0, cross_section=1.0, anisotropy=None):
 
 def num_threads():
     return lib.orc_num_threads()
+
+
+def set_threads(n):
+    """OpenMP threads of the following oracle calls."""
+    lib.orc_set_threads(int(n))

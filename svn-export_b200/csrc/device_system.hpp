@@ -106,11 +106,10 @@ cudaError_t launch_backsub(const ElemData &d, const DevAssembly &a, const DevSys
 // out[3 e + k], k = x, y, z.
 cudaError_t launch_element_flux(const ElemData &d, const DevAssembly &a, const double *sol, double *out,
                                 cudaStream_t s);
-// Pressure at every node from the element and side pressures of sol (postprocess.cu); dsum and
-// cnt are scratch of n_nodes entries.
-cudaError_t launch_node_pressure(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_nodes,
-                                 int64_t n_sides, int64_t n_el, double *dsum, int32_t *cnt, double *out,
-                                 cudaStream_t s);
+// Pressure at every node from the element and side pressures of sol (postprocess.cu): one
+// thread per node over its elements, inc_start [n_nodes+1] / inc_el (ascending element ids).
+cudaError_t launch_node_pressure(const ElemData &d, const int32_t *inc_start, const int32_t *inc_el, int64_t n_nodes,
+                                 const double *sol, int64_t n_sides, int64_t n_el, double *out, cudaStream_t s);
 // Convection matrix of the explicit transport (transport.cu).  The pattern is built on the host
 // once per mesh: per row, slots sorted by column, each with its kind and the side indices its
 // value reads (edge: own side a, other side b; VB: the higher-dimensional side a).
@@ -126,11 +125,21 @@ struct TransportPattern {
 cudaError_t launch_transport_matrix(const ElemData &d, const TransportPattern &p, const double *porosity,
                                     const double *sol, double *val, cudaStream_t s);
 
-// Water balance per region (postprocess.cu): bdr_out [3 n_bdr_reg] total, outflow, inflow of
-// the boundary side fluxes; src_out [n_el_reg] the sources.  Region indices are device arrays.
-cudaError_t launch_water_balance(const ElemData &d, const DevAssembly &a, const double *sol, int64_t n_sides,
-                                 const int32_t *bdr_region, int32_t n_bdr_reg, const int32_t *el_region,
-                                 int32_t n_el_reg, double *bdr_out, double *src_out, cudaStream_t s);
+// Water balance per region (postprocess.cu).  Items grouped by region (ascending within a
+// region) and cut into chunks: *_chunk_begin [n_chunks+1] into *_items, *_region_chunk
+// [n_reg+1] into the chunks.  Device arrays, built on the host for each call.
+struct BalanceLists {
+    const int32_t *bdr_items = nullptr, *src_items = nullptr;           // side / element ids
+    const int64_t *bdr_chunk_begin = nullptr, *src_chunk_begin = nullptr;
+    const int64_t *bdr_region_chunk = nullptr, *src_region_chunk = nullptr;
+    int64_t n_bdr_chunks = 0, n_src_chunks = 0;
+    int32_t n_bdr_reg = 0, n_src_reg = 0;
+};
+// bdr_out [3 n_bdr_reg] total, outflow, inflow of the boundary side fluxes; src_out
+// [n_src_reg] the sources; partial holds 3 n_bdr_chunks + n_src_chunks values.
+cudaError_t launch_water_balance(const ElemData &d, const double *sol, const BalanceLists &L, double *partial,
+                                 double *bdr_out, double *src_out, cudaStream_t s);
+constexpr int64_t kBalanceChunkItems = 8192;
 
 // x = lambda * dsq (initial guess in scaled space; padding rows 0).
 cudaError_t launch_scale_in(const DevSystem &sys, const double *lambda, cudaStream_t s);

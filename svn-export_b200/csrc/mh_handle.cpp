@@ -53,11 +53,13 @@ struct mh_handle {
     mh::DevAssembly as{};
     double *sol = nullptr, *sol_prev = nullptr;
     double *d_elflux = nullptr;         // element flux vectors for mh_get_element_flux (3 n_el)
-    double *d_node_sum = nullptr, *d_node_p = nullptr;  // node pressures: distance sums, result
-    int32_t *d_node_cnt = nullptr;
-    int32_t *d_bdr_region = nullptr, *d_el_region = nullptr;  // water balance inputs
-    double *d_balance = nullptr;        // water balance sums (capacity in balance_cap)
-    int64_t balance_cap = 0;
+    double *d_node_p = nullptr;                                // node pressures
+    int32_t *d_node_inc_start = nullptr, *d_node_inc = nullptr;  // node -> elements (ascending)
+    // water balance: items grouped by region and their chunks (built per call, capacities kept)
+    int32_t *d_bal_items = nullptr;
+    int64_t *d_bal_index = nullptr;     // chunk begins and region-chunk offsets of both kinds
+    double *d_balance = nullptr;        // chunk partials, then the per-region sums
+    int64_t bal_items_cap = 0, bal_index_cap = 0, balance_cap = 0;
     // convection matrix of the transport: pattern (built once), host copies of its CSR
     // structure, device values and porosity
     bool tr_built = false;
@@ -66,6 +68,9 @@ struct mh_handle {
     double *d_tr_val = nullptr, *d_tr_por = nullptr;
     double *d_aniso = nullptr;
     bool coeffs_set = false, bc_set = false, assembled = false, solved = false;
+    bool general = false;               // a general SPD system given in CSR form (no mesh)
+    std::vector<double> gen_slot_val;   // its values in SELL slot order (host staging)
+    std::vector<double> gen_rhs;
     bool rhs_stale = false;             // boundary values changed since the last assembly
     int time_mode = 0;
     double dt = 0.0;
@@ -1401,6 +1406,82 @@ int mh_create_batch(const mh_mesh_desc *meshes, int32_t n_inst, mh_handle **out)
     return MH_OK;
 }
 
+int mh_csr_create(int64_t n, const int32_t *row_ptr, const int32_t *col, mh_handle **out) {
+    if (!out || n <= 0 || n > INT32_MAX || !row_ptr || !col) return MH_ERR_INVALID;
+    *out = nullptr;
+    auto *h = new (std::nothrow) mh_handle();
+    if (!h) return MH_ERR_NOMEM;
+    h->general = true;
+    // no mesh: n edges, no sides, elements, boundary objects or neighbours
+    h->topo.el_side_start.assign(1, 0);
+    h->topo.el_ngh_start.assign(1, 0);
+    h->topo.edge_side_start.assign(n + 1, 0);
+    int rpt = 1;
+    const int targets[2] = {mh::krylov_target_blocks(rpt, 64), mh::krylov_target_blocks(rpt, 32)};
+    int rc = mh::build_host_system_csr(n, row_ptr, col, rpt, targets, h->hs, &h->err);
+    if (!rc) {
+        h->inst_iters.assign(1, 0);
+        h->inst_status.assign(1, 0);
+        h->inst_rel.assign(1, 0.0);
+        rc = device_setup(h);
+    }
+    if (rc) {
+        mh_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return MH_OK;
+}
+
+int mh_csr_set_values(mh_handle *h, const double *val, const double *rhs) {
+    if (!h || !h->general || !val || !rhs) return MH_ERR_INVALID;
+    const mh::HostSystem &hs = h->hs;
+    const int64_t n = h->topo.n_edges(), nnz = hs.nnz;
+    if (!check_finite(val, nnz) || !check_finite(rhs, n)) {
+        h->err = "non-finite matrix or right-hand side value";
+        return MH_ERR_NONFINITE;
+    }
+    h->gen_slot_val.assign(hs.n_slots, 0.0);
+    for (int64_t k = 0; k < nnz; ++k) h->gen_slot_val[hs.csr_slot[k]] = val[k];
+    for (int64_t r = 0; r < hs.n_rows; ++r) {
+        const double d = r < n ? h->gen_slot_val[hs.diag_slot[r]] : 1.0;
+        if (!(d > 0.0)) {
+            h->err = "row " + std::to_string(r) + " has a diagonal entry <= 0: not a positive definite system";
+            return MH_ERR_INVALID;
+        }
+        if (r >= n) h->gen_slot_val[hs.diag_slot[r]] = 1.0;  // padding rows: unit diagonal
+    }
+    h->gen_rhs.assign(hs.n_rows, 0.0);
+    std::copy(rhs, rhs + n, h->gen_rhs.begin());
+    int rc = need_device(h);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->sys.val_raw, h->gen_slot_val.data(), hs.n_slots * sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaMemcpyAsync(h->sys.b, h->gen_rhs.data(), hs.n_rows * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(mh::launch_scale(h->sys, 1, h->stream));
+    h->n_launch += 3;
+    CK(cudaStreamSynchronize(h->stream));
+    h->assembled = true;
+    h->rhs_stale = false;
+    h->solved = false;
+    h->matrix_epoch += 1;
+    return MH_OK;
+}
+
+int mh_csr_get_solution(const mh_handle *hc, double *x, int64_t n) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    if (!h || !h->general || !x || n < h->topo.n_edges()) return MH_ERR_INVALID;
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->solved) {
+        h->err = "mh_solve must come before mh_csr_get_solution";
+        return MH_ERR_STATE;
+    }
+    CK(cudaMemcpyAsync(x, h->sol, h->topo.n_edges() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
 void mh_destroy(mh_handle *h) {
     if (!h) return;
     if (h->device) cudaDeviceSynchronize();
@@ -1464,6 +1545,10 @@ int mh_get_topology(const mh_handle *h, int32_t *el_side_start, int32_t *side_ed
 int mh_set_coeffs(mh_handle *h, const mh_coeffs *c) {
     int rc = need_device(h);
     if (rc) return rc;
+    if (h->general) {
+        h->err = "the handle holds a general system (mh_csr_create): it has no mesh data";
+        return MH_ERR_STATE;
+    }
     if (!c) return MH_ERR_INVALID;
     const int64_t n = h->mesh.n_el;
     const double *arrs[6] = {c->conductivity, c->cross_section, c->sigma, c->water_source_density, c->storativity,
@@ -1506,6 +1591,10 @@ int mh_set_coeffs(mh_handle *h, const mh_coeffs *c) {
 int mh_set_bc(mh_handle *h, const mh_bc *bc) {
     int rc = need_device(h);
     if (rc) return rc;
+    if (h->general) {
+        h->err = "the handle holds a general system (mh_csr_create): it has no mesh data";
+        return MH_ERR_STATE;
+    }
     if (!bc) return MH_ERR_INVALID;
     const int64_t n = h->topo.n_bdr();
     if (bc->type)
@@ -1545,6 +1634,10 @@ int mh_set_bc(mh_handle *h, const mh_bc *bc) {
 int mh_assemble(mh_handle *h) {
     int rc = need_device(h);
     if (rc) return rc;
+    if (h->general) {
+        h->err = "the handle holds a general system (mh_csr_create): it has no mesh data";
+        return MH_ERR_STATE;
+    }
     if (!h->coeffs_set || !h->bc_set) {
         h->err = "mh_set_coeffs and mh_set_bc must come before mh_assemble";
         return MH_ERR_STATE;
@@ -1624,23 +1717,51 @@ int mh_get_node_pressure(const mh_handle *hc, double *out, int64_t len) {
     mh_handle *h = const_cast<mh_handle *>(hc);
     int rc = need_device(h);
     if (rc) return rc;
-    const int64_t nn = h->mesh.n_nodes;
+    const int64_t nn = h->mesh.n_nodes, ne = h->mesh.n_el;
     if (!out || len < nn) return MH_ERR_INVALID;
     if (!h->solved) {
         h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the node pressures";
         return MH_ERR_STATE;
     }
     if (!h->d_node_p) {
-        h->d_node_sum = dalloc<double>(h, std::max<int64_t>(nn, 1));
+        // node -> element incidence (elements ascending), once per mesh
+        std::vector<int32_t> start(nn + 1, 0), inc;
+        for (int64_t e = 0; e < ne; ++e)
+            for (int32_t k = 0; k <= h->mesh.dim[e]; ++k) start[h->mesh.nodes[4 * e + k] + 1]++;
+        for (int64_t v = 0; v < nn; ++v) start[v + 1] += start[v];
+        inc.resize(start[nn]);
+        std::vector<int32_t> fill(start.begin(), start.end() - 1);
+        for (int64_t e = 0; e < ne; ++e)
+            for (int32_t k = 0; k <= h->mesh.dim[e]; ++k) inc[fill[h->mesh.nodes[4 * e + k]]++] = (int32_t)e;
+        if ((rc = upload(h, h->d_node_inc_start, start)) || (rc = upload(h, h->d_node_inc, inc))) return rc;
         h->d_node_p = dalloc<double>(h, std::max<int64_t>(nn, 1));
-        h->d_node_cnt = dalloc<int32_t>(h, std::max<int64_t>(nn, 1));
-        if (!h->d_node_sum || !h->d_node_p || !h->d_node_cnt) return MH_ERR_NOMEM;
+        if (!h->d_node_p) return MH_ERR_NOMEM;
     }
-    CK(mh::launch_node_pressure(h->ed, h->as, h->sol, nn, h->topo.n_sides(), h->mesh.n_el, h->d_node_sum,
-                                h->d_node_cnt, h->d_node_p, h->stream));
+    CK(mh::launch_node_pressure(h->ed, h->d_node_inc_start, h->d_node_inc, nn, h->sol, h->topo.n_sides(), ne,
+                                h->d_node_p, h->stream));
     CK(cudaMemcpyAsync(out, h->d_node_p, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return MH_OK;
+}
+
+// Items of one kind grouped by region (ascending within a region), cut into chunks of at most
+// kBalanceChunkItems: items, chunk begins [n_chunks+1] and region-chunk offsets [n_reg+1].
+static void group_by_region(const std::vector<int32_t> &item_region, const std::vector<int32_t> &item_id,
+                            int32_t n_reg, std::vector<int32_t> &items, std::vector<int64_t> &chunk_begin,
+                            std::vector<int64_t> &region_chunk) {
+    std::vector<int64_t> off(n_reg + 1, 0);
+    for (int32_t r : item_region) off[r + 1]++;
+    for (int32_t r = 0; r < n_reg; ++r) off[r + 1] += off[r];
+    items.assign(item_id.size(), 0);
+    std::vector<int64_t> fill(off.begin(), off.end() - 1);
+    for (size_t i = 0; i < item_id.size(); ++i) items[fill[item_region[i]]++] = item_id[i];
+    chunk_begin.assign(1, 0);
+    region_chunk.assign(1, 0);
+    for (int32_t r = 0; r < n_reg; ++r) {
+        for (int64_t b = off[r]; b < off[r + 1]; b += mh::kBalanceChunkItems)
+            chunk_begin.push_back(std::min(off[r + 1], b + mh::kBalanceChunkItems));
+        region_chunk.push_back((int64_t)chunk_begin.size() - 1);
+    }
 }
 
 int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_bdr_regions,
@@ -1648,7 +1769,7 @@ int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_b
     mh_handle *h = const_cast<mh_handle *>(hc);
     int rc = need_device(h);
     if (rc) return rc;
-    const int64_t nb = h->topo.n_bdr(), ne = h->mesh.n_el;
+    const int64_t nb = h->topo.n_bdr(), ne = h->mesh.n_el, ns = h->topo.n_sides();
     if (!bdr_region || !el_region || !bdr_out || !src_out || n_bdr_regions < 1 || n_el_regions < 1)
         return MH_ERR_INVALID;
     for (int64_t b = 0; b < nb; ++b)
@@ -1665,23 +1786,58 @@ int mh_water_balance(const mh_handle *hc, const int32_t *bdr_region, int32_t n_b
         h->err = "no solution of the current coefficients: mh_solve or mh_unsteady_step must come before the water balance";
         return MH_ERR_STATE;
     }
-    if (!h->d_el_region) {
-        h->d_bdr_region = dalloc<int32_t>(h, std::max<int64_t>(nb, 1));
-        h->d_el_region = dalloc<int32_t>(h, std::max<int64_t>(ne, 1));
-        if (!h->d_bdr_region || !h->d_el_region) return MH_ERR_NOMEM;
+    // boundary sides (ascending) and elements, grouped by region
+    std::vector<int32_t> reg, ids, bitems, sitems;
+    std::vector<int64_t> bchunk, breg, schunk, sreg;
+    for (int64_t sd = 0; sd < ns; ++sd) {
+        const int32_t b = h->topo.side_bdr[sd];
+        if (b < 0) continue;
+        reg.push_back(bdr_region[b]);
+        ids.push_back((int32_t)sd);
     }
-    const int64_t need = 3 * (int64_t)n_bdr_regions + n_el_regions;
+    group_by_region(reg, ids, n_bdr_regions, bitems, bchunk, breg);
+    reg.assign(el_region, el_region + ne);
+    ids.resize(ne);
+    for (int64_t e = 0; e < ne; ++e) ids[e] = (int32_t)e;
+    group_by_region(reg, ids, n_el_regions, sitems, schunk, sreg);
+    const int64_t n_items = (int64_t)bitems.size() + (int64_t)sitems.size();
+    const int64_t n_index = (int64_t)(bchunk.size() + breg.size() + schunk.size() + sreg.size());
+    const int64_t nbc = (int64_t)bchunk.size() - 1, nsc = (int64_t)schunk.size() - 1;
+    const int64_t need = 3 * nbc + nsc + 3 * (int64_t)n_bdr_regions + n_el_regions;
+    if (n_items > h->bal_items_cap) {
+        if (!(h->d_bal_items = dalloc<int32_t>(h, n_items))) return MH_ERR_NOMEM;
+        h->bal_items_cap = n_items;
+    }
+    if (n_index > h->bal_index_cap) {
+        if (!(h->d_bal_index = dalloc<int64_t>(h, n_index))) return MH_ERR_NOMEM;
+        h->bal_index_cap = n_index;
+    }
     if (need > h->balance_cap) {
-        h->d_balance = dalloc<double>(h, need);
-        if (!h->d_balance) return MH_ERR_NOMEM;
+        if (!(h->d_balance = dalloc<double>(h, need))) return MH_ERR_NOMEM;
         h->balance_cap = need;
     }
-    if (nb > 0)
-        CK(cudaMemcpyAsync(h->d_bdr_region, bdr_region, nb * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d_el_region, el_region, ne * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
-    double *bo = h->d_balance, *so = h->d_balance + 3 * (int64_t)n_bdr_regions;
-    CK(mh::launch_water_balance(h->ed, h->as, h->sol, h->topo.n_sides(), h->d_bdr_region, n_bdr_regions,
-                                h->d_el_region, n_el_regions, bo, so, h->stream));
+    std::vector<int32_t> hitems(bitems);
+    hitems.insert(hitems.end(), sitems.begin(), sitems.end());
+    std::vector<int64_t> hindex(bchunk);
+    hindex.insert(hindex.end(), breg.begin(), breg.end());
+    hindex.insert(hindex.end(), schunk.begin(), schunk.end());
+    hindex.insert(hindex.end(), sreg.begin(), sreg.end());
+    if (n_items > 0)
+        CK(cudaMemcpyAsync(h->d_bal_items, hitems.data(), n_items * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_bal_index, hindex.data(), n_index * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    mh::BalanceLists L;
+    L.bdr_items = h->d_bal_items;
+    L.src_items = h->d_bal_items + bitems.size();
+    L.bdr_chunk_begin = h->d_bal_index;
+    L.bdr_region_chunk = L.bdr_chunk_begin + bchunk.size();
+    L.src_chunk_begin = L.bdr_region_chunk + breg.size();
+    L.src_region_chunk = L.src_chunk_begin + schunk.size();
+    L.n_bdr_chunks = nbc;
+    L.n_src_chunks = nsc;
+    L.n_bdr_reg = n_bdr_regions;
+    L.n_src_reg = n_el_regions;
+    double *bo = h->d_balance + 3 * nbc + nsc, *so = bo + 3 * (int64_t)n_bdr_regions;
+    CK(mh::launch_water_balance(h->ed, h->sol, L, h->d_balance, bo, so, h->stream));
     CK(cudaMemcpyAsync(bdr_out, bo, 3 * (size_t)n_bdr_regions * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(src_out, so, (size_t)n_el_regions * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));

@@ -310,4 +310,90 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     return MH_OK;
 }
 
+int build_host_system_csr(int64_t n, const int32_t *row_ptr, const int32_t *col, int rows_per_thread,
+                          const int target_blocks[2], HostSystem &hs, std::string *err) {
+    hs = HostSystem();
+    if (n <= 0 || !row_ptr || !col || row_ptr[0] != 0) {
+        if (err) *err = "empty system or invalid row pointers";
+        return MH_ERR_INVALID;
+    }
+    for (int64_t r = 0; r < n; ++r) {
+        bool diag = false;
+        if (row_ptr[r + 1] < row_ptr[r]) {
+            if (err) *err = "row pointers decrease";
+            return MH_ERR_INVALID;
+        }
+        for (int32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            if (col[k] < 0 || col[k] >= n || (k > row_ptr[r] && col[k] <= col[k - 1])) {
+                char msg[160];
+                snprintf(msg, sizeof msg, "row %lld: columns out of range, unsorted or repeated", (long long)r);
+                if (err) *err = msg;
+                return MH_ERR_INVALID;
+            }
+            diag |= col[k] == r;
+        }
+        if (!diag) {
+            char msg[160];
+            snprintf(msg, sizeof msg, "row %lld has no diagonal entry", (long long)r);
+            if (err) *err = msg;
+            return MH_ERR_INVALID;
+        }
+    }
+    hs.inst_el = {0, 0};
+    hs.inst_edge = {0, n};
+    const int64_t pad = ((n + kPadRows - 1) / kPadRows) * kPadRows;
+    hs.inst_row = {0, pad};
+    hs.n_rows = pad;
+    hs.n_slices = pad / kSliceRowsHost;
+    hs.edge_row.resize(n);
+    hs.row_edge.assign(pad, -1);
+    for (int64_t g = 0; g < n; ++g) {
+        hs.edge_row[g] = (int32_t)g;
+        hs.row_edge[g] = (int32_t)g;
+    }
+    set_launch_shape(hs, rows_per_thread, target_blocks);
+    hs.row_ptr.assign(pad + 1, 0);
+    for (int64_t r = 0; r < pad; ++r) hs.row_ptr[r + 1] = hs.row_ptr[r] + (r < n ? row_ptr[r + 1] - row_ptr[r] : 1);
+    hs.row_col.resize(hs.row_ptr[pad]);
+    for (int64_t r = 0; r < pad; ++r) {
+        if (r < n)
+            std::copy(col + row_ptr[r], col + row_ptr[r + 1], hs.row_col.begin() + hs.row_ptr[r]);
+        else
+            hs.row_col[hs.row_ptr[r]] = (int32_t)r;  // padding rows: a unit diagonal
+    }
+    hs.nnz = row_ptr[n];
+    hs.slice_off.assign(hs.n_slices + 1, 0);
+    for (int64_t sl = 0; sl < hs.n_slices; ++sl) {
+        int64_t w = 0;
+        for (int l = 0; l < kSliceRowsHost; ++l) {
+            const int64_t r = sl * kSliceRowsHost + l;
+            w = std::max(w, hs.row_ptr[r + 1] - hs.row_ptr[r]);
+        }
+        hs.slice_off[sl + 1] = hs.slice_off[sl] + w * kSliceRowsHost;
+    }
+    hs.n_slots = hs.slice_off[hs.n_slices];
+    if (hs.n_slots > INT32_MAX) {
+        if (err) *err = "system too large for 32-bit slot indices";
+        return MH_ERR_INVALID;
+    }
+    hs.sell_col.resize(hs.n_slots);
+    hs.diag_slot.resize(pad);
+    hs.csr_slot.resize(hs.nnz);
+    for (int64_t r = 0; r < pad; ++r) {
+        const int64_t sl = r / kSliceRowsHost, lane = r % kSliceRowsHost;
+        const int64_t off = hs.slice_off[sl], w = (hs.slice_off[sl + 1] - off) / kSliceRowsHost;
+        const int64_t len = hs.row_ptr[r + 1] - hs.row_ptr[r];
+        for (int64_t j = 0; j < w; ++j) {
+            const int64_t slot = off + j * kSliceRowsHost + lane;
+            const int32_t c = j < len ? hs.row_col[hs.row_ptr[r] + j] : (int32_t)r;
+            hs.sell_col[slot] = c;
+            if (j < len && c == r) hs.diag_slot[r] = (int32_t)slot;
+            if (j < len && r < n) hs.csr_slot[hs.row_ptr[r] + j] = (int32_t)slot;
+        }
+    }
+    hs.slot_cstart.assign(hs.n_slots + 1, 0);
+    hs.row_cstart.assign(pad + 1, 0);
+    return MH_OK;
+}
+
 }  // namespace mh

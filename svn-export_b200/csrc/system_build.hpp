@@ -37,6 +37,7 @@ struct HostSystem {
     std::vector<int32_t> slot_cstart, slot_cidx;
     std::vector<int32_t> row_cstart, row_cidx;
     std::vector<int32_t> dim_list[4];
+    std::vector<int32_t> csr_slot;       // general systems: SELL slot of every CSR entry
 };
 
 // Local edge list of element e: own side edges then VB-neighbour edges.
@@ -44,6 +45,13 @@ int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out);
 
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
                       int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err);
+
+// Layout of a general sparse system given by its CSR pattern (n rows, columns sorted and
+// unique in every row, each row holding its diagonal): one instance, rows = unknowns, padded
+// to kPadRows, SELL-C-sigma as for the edge system, and csr_slot mapping the CSR entries to
+// slots.  No element contributions.
+int build_host_system_csr(int64_t n, const int32_t *row_ptr, const int32_t *col, int rows_per_thread,
+                          const int target_blocks[2], HostSystem &hs, std::string *err);
 
 // Splits every instance's tiles into contiguous runs, one run per block, with about
 // target_blocks blocks in total (at least one per instance) in proportion to instance size.

@@ -24,19 +24,55 @@ def test_bench_setup_timing():
 
 
 def test_bench_cpu_baseline_entry():
-    """bench.py's cpu_baseline object (the CPU restatement on the GPU run's workload) for both
-    preconditioners, on a small cube."""
+    """bench.py's cpu_baseline object (the CPU restatement on the workload, all threads and one
+    thread) for Jacobi and ILU(3) CG, on cfg1 (complete solves fit the budget)."""
     bench = load_bench()
-    from mhdarcy.cases import dirichlet_x_bc, make_case
-    mesh, coeffs = make_case(1, n=6)
+    cp = bench.CpuProblem(1)
+    for pre in ("jacobi", "ilu3"):
+        a = SimpleNamespace(config=1, cpu_precond=pre, cpu_budget_s=20.0)
+        e = bench.cpu_baseline_entry(a, cp)
+        assert e["value"] > 0 and e["cores"] >= 1 and e["kind"] == "port"
+        assert e["one_core"]["cores"] == 1 and e["one_core"]["value"] > 0
+        assert "complete solves" in e["sample"]
+
+
+def test_bench_reference_arm_complete_and_projected(monkeypatch):
+    """The reference arm on cfg1: complete solves when they fit the budget; with a recorded
+    complete-solve iteration count and a small budget, bounded samples projected with it.
+    Its config equals the GPU arm's for the same workload (sizes from the library)."""
+    bench = load_bench()
+    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=60.0, gpus=1)
+    out = bench.run_reference(a)
+    assert out["impl"] == "reference" and out["value"] > 0 and out["projected"] is False
+    assert out["e2e"]["value"] == out["value"] and out["cpu_baseline"]["kind"] == "port"
+    assert out["ms_per_step"] > 0 and out["steps"] == 2 and out["warmup"] == 1
+    from mhdarcy.cases import make_case
+    mesh, _ = make_case(1)
     with mhdarcy.MHSystem(mesh) as s:
-        topo, n_edges = s.topology(), s.n_edges
-    bc, _ = dirichlet_x_bc(topo, mesh)
-    for pre, iters in (("jacobi", 50), ("ilu0", 10)):
-        a = SimpleNamespace(config=1, cpu_sample_iters=5, cpu_precond=pre)
-        e = bench.cpu_baseline_entry(a, (mesh, coeffs, bc, topo, n_edges), iters if pre == "jacobi" else None)
-        assert e["value"] > 0 and e["detail"]["method"].startswith(pre)
-        assert e["detail"]["iters"] == (iters if pre == "jacobi" else bench.ILU0_PCG_ITERS[1])
+        z = s.sizes
+        assert out["config"] == bench.workload_config(1, z.n_edges, z.schur_nnz, z.mh_size, z.n_elements)
+    monkeypatch.setattr(bench, "cpu_full_record", lambda cfg, pre: {"iterations": 1630})
+    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=0.05, gpus=1)
+    out2 = bench.run_reference(a)
+    assert out2["projected"] is True and "projected" in out2["cpu_baseline"]["sample"]
+    # the projection of a 1630-iteration solve lands near the measured complete solve
+    assert 0.2 < out2["value"] / out["value"] < 5.0
+
+
+def test_bench_reference_arm_loads_no_product_library():
+    """The reference arm builds and solves the workload with the oracle alone: the GPU
+    library's shared object is never loaded into its process."""
+    import subprocess
+    import sys
+    code = ("import sys, json; sys.path.insert(0, %r); import bench; from types import SimpleNamespace as N; "
+            "o = bench.run_reference(N(config=1, cpu_precond='jacobi', steps=1, warmup=0, ref_budget_s=30.0, gpus=1)); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'v': o['value'], 'lib': 'libmhdarcy' in maps, 'orc': 'libmhoracle' in maps}))" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    import json
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["v"] > 0 and d["orc"] and not d["lib"]
 
 
 def test_bench_setup_timing_isolated():

@@ -1,0 +1,92 @@
+"""Parity of the CUDA path with the CPU oracle at the benchmark sizes, and of the plain FP64
+solve at the 1e-10 level.
+
+  * K1 (the assembled edge system and rhs) at the full size of the two steady benchmark
+    workloads (cfg2: 3.2M edges; cfg5: 10.9M edges): entrywise |S_gpu - S_orc|_ij <= 1e-14
+    sqrt(S_ii S_jj), the rhs likewise; K4 (back-substitution of the GPU's edge pressures):
+    1e-12 relative to the largest flux and pressure.
+  * FP64 Jacobi-PCG: the GPU iterate after k iterations equals the oracle's CPU Jacobi-PCG
+    iterate after the same k iterations (same algorithm, same start) within 1e-10 relative,
+    for edge pressures and, through the back-substitution, for fluxes and element pressures.
+  * A converged FP64 solve (r_tol 1e-14) matches the FP64 direct solve of the full
+    saddle-point system within 1e-10 relative on the reference's test problems.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+import mhdarcy
+import oracle as O
+from helpers import cube_bc, fixture_bc, fixture_coeffs, load_fixture, oracle_problem
+from mhdarcy import _lib
+from mhdarcy.cases import dirichlet_x_bc, make_case
+from test_gpu_parity import assert_schur_parity
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("cfg", [2, 5])
+def test_k1_k4_at_benchmark_size(gpu, cfg):
+    mesh, coeffs = make_case(cfg)
+    with mhdarcy.MHSystem(mesh) as s:
+        bc, _ = dirichlet_x_bc(s.topology(), mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        assert_schur_parity(s, P)
+        st = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+        assert st["status"] in (0, _lib.MH_FELL_BACK), st
+        sol = s.solution()
+        ns, ne = s.n_sides, s.n_elements
+        ref = O.resolve(P, sol[ns + ne:])
+        assert np.abs(sol[:ns] - ref[:ns]).max() <= 1e-12 * np.abs(ref[:ns]).max()
+        assert np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max() <= 1e-12 * np.abs(ref[ns:ns + ne]).max()
+
+
+@pytest.mark.parametrize("k", [10, 50, 200])
+def test_pcg64_iterate_matches_oracle_iterate(gpu, k):
+    """Jacobi-PCG on S (CPU) and CG on D^-1/2 S D^-1/2 (GPU) produce the same iterates in exact
+    arithmetic; after k iterations from zero they agree to 1e-10 relative in FP64."""
+    mesh, coeffs = make_case(1)
+    with mhdarcy.MHSystem(mesh) as s:
+        bc = cube_bc(s, mesh)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc["pressure"])
+        s.assemble()
+        P = oracle_problem(mesh, s.topology(), s.n_edges, coeffs, bc)
+        S, r = O.schur2(P)
+        x_cpu, it, _ = O.pcg_jacobi(S, r, rtol=1e-300, max_it=k)
+        assert it == -1  # ran exactly k iterations
+        st = s.solve(method=_lib.MH_SOLVER_PCG64, r_tol=1e-300, max_it=k)
+        assert st["status"] == _lib.MH_NOT_CONVERGED and st["iterations"] == k, st
+        sol = s.solution()
+        ns, ne = s.n_sides, s.n_elements
+        lam = sol[ns + ne:]
+        assert np.abs(lam - x_cpu).max() <= 1e-10 * np.abs(x_cpu).max(), np.abs(lam - x_cpu).max()
+        ref = O.resolve(P, x_cpu)
+        assert np.abs(sol[:ns] - ref[:ns]).max() <= 1e-10 * np.abs(ref[:ns]).max()
+        assert np.abs(sol[ns:ns + ne] - ref[ns:ns + ne]).max() <= 1e-10 * np.abs(ref[ns:ns + ne]).max()
+
+
+@pytest.mark.parametrize("name", ["t01", "t05_dirichlet", "t05_neumann", "t05_robin", "t06_32", "t06_21", "t08"])
+def test_fp64_solution_within_1e10_of_direct(gpu, name):
+    """Pressures, fluxes and edge pressures of the plain FP64 solve against the FP64 direct
+    solve of the full saddle-point system: 1e-10 relative (to the largest value of each part)."""
+    z, mesh = load_fixture(name)
+    with mhdarcy.MHSystem(mesh) as s:
+        topo = s.topology()
+        coeffs = fixture_coeffs(z)
+        bc = fixture_bc(z, topo)
+        s.set_coeffs(**coeffs)
+        s.set_bc(bc["bc_type"], bc.get("pressure"), bc.get("flux"), bc.get("robin_sigma"))
+        s.assemble()
+        st = s.solve(method=_lib.MH_SOLVER_PCG64, r_tol=1e-14)
+        assert st["status"] == 0, st
+        sol = s.solution()
+        ref = O.solve_mh_direct(oracle_problem(mesh, topo, s.n_edges, coeffs, bc))
+        ns, ne = s.n_sides, s.n_elements
+        for part in (slice(0, ns), slice(ns, ns + ne), slice(ns + ne, len(ref))):
+            scale = np.abs(ref[part]).max()
+            if scale > 0:
+                assert np.abs(sol[part] - ref[part]).max() <= 1e-10 * scale, (part, np.abs(sol[part] - ref[part]).max() / scale)
