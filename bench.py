@@ -71,6 +71,8 @@ def parse():
                     help="FP32 residual reduction between FP64 replacements in the multigrid solves")
     ap.add_argument("--train-n", type=int, default=24, help="cube size of the system the network trains on")
     ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--train-steps", type=int, default=20,
+                    help="--unsteady: steps solved with the plain multigrid before the learned method trains")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the flux/pressure error block")
     ap.add_argument("--pcg-accuracy", action="store_true", help="also time pcg64 at r_tol 1e-12 in the error block")
     ap.add_argument("--extra-config", type=int, default=2, help="second workload timed with fewer steps (0: none)")
@@ -228,7 +230,10 @@ def run_unsteady(a, rank, world):
     """K steps of the unsteady MH system (mh_unsteady_step: right-hand side from the previous
     pressures, solve, back-substitution) with the boundary pressure on x = 0 following
     1 + 0.5 sin(2 pi t); each method starts from zero pressure.  The matrix is the same in every
-    step (same dt), so the multigrid hierarchy is built once and reused."""
+    step (same dt), so the multigrid hierarchy is built once and reused.  The learned method
+    (fcg) runs the first --train-steps steps with the plain multigrid, trains the network on the
+    system of the last of them (pairs from the plain solver) and solves the remaining steps with
+    it; every method's steps after that point are timed as the window the comparison is made on."""
     import numpy as np
     import torch
 
@@ -239,50 +244,78 @@ def run_unsteady(a, rank, world):
     stream = torch.cuda.Stream()
     mesh, coeffs = make_case(a.config)
     dt = 0.01
+    k0 = min(a.train_steps, a.unsteady - 1)
     out = {}
     with mhdarcy.MHSystem(mesh) as s:
         s.set_stream(stream.cuda_stream)
         bc, left = dirichlet_x_bc(s.topology(), mesh)
         s.set_coeffs(**coeffs)
-        methods = {"pcg64": mhdarcy.MH_SOLVER_PCG64, "ir32": mhdarcy.MH_SOLVER_IR32, "amg": mhdarcy.MH_SOLVER_AMG}
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for name in a.methods.split(","):
-            kw = {"inner_rtol": a.amg_inner_rtol} if name == "amg" else {}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
-            def steps(k):
+        def rec(e):
+            with torch.cuda.stream(stream):
+                e.record(stream)
+
+        for name in a.methods.split(","):
+            kw = SOLVE_KW.get(name, lambda a: {})(a)
+
+            def run(k, record=False):
                 s.set_bc(bc["bc_type"], bc["pressure"])
                 s.unsteady_init(dt, init_pressure=np.zeros(s.n_elements), lumped=False)
                 p = bc["pressure"].copy()
-                its = []
+                its, training = [], None
+                if record:
+                    rec(ev[0])
                 for i in range(1, k + 1):
                     p[left] = 1.0 + 0.5 * np.sin(2 * np.pi * i * dt)
                     s.set_bc(bc["bc_type"], p)
-                    st = s.unsteady_step(dt, method=methods[name], r_tol=1e-10, **kw)
+                    m = METHOD_IDS[name]
+                    if name == "fcg" and i <= k0:
+                        m = METHOD_IDS["amg"]
+                    st = s.unsteady_step(dt, method=m, r_tol=R_TOL, **kw)
                     if st["status"] not in (0, mhdarcy.MH_FELL_BACK):
                         raise RuntimeError(f"{name} step {i}: {st}")
                     its.append(st["iterations"])
-                return its
+                    if i == k0:
+                        if record:
+                            rec(ev[1])
+                        if name == "fcg":
+                            training = s.learned_train(n_pairs=12, epochs=a.train_epochs, lr=2e-3)
+                        if record:
+                            rec(ev[2])
+                if record:
+                    rec(ev[3])
+                return its, training
 
-            steps(max(3, a.warmup))
+            if name == "fcg":
+                s.reset_learned()
+            run(max(3, a.warmup))
+            if name == "fcg":  # the timed run trains from the initial network again
+                s.reset_learned()
             torch.cuda.synchronize()
-            with torch.cuda.stream(stream):
-                ev0.record(stream)
-            its = steps(a.unsteady)
-            with torch.cuda.stream(stream):
-                ev1.record(stream)
+            its, training = run(a.unsteady, record=True)
             torch.cuda.synchronize()
-            ms = ev0.elapsed_time(ev1)
-            out[name] = {"steps_per_s": round(a.unsteady / (ms / 1e3), 3), "ms_per_step": round(ms / a.unsteady, 3),
-                         "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its))}
-    best = max(out, key=lambda m: out[m]["steps_per_s"])
-    line = {"metric": "MH Darcy unsteady steps/s (implicit Euler, residual 1e-10)", "value": out[best]["steps_per_s"],
-            "unit": "steps/s", "n_gpus": 1, "steps": a.unsteady, "warmup": max(3, a.warmup),
-            "ms_per_step": out[best]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if best == "pcg64" else "f32+f64",
+            ms_all = ev[0].elapsed_time(ev[3])
+            ms_win = ev[2].elapsed_time(ev[3])
+            nwin = a.unsteady - k0
+            out[name] = {"steps_per_s": round(a.unsteady / (ms_all / 1e3), 3),
+                         "window_steps": [k0 + 1, a.unsteady],
+                         "window_steps_per_s": round(nwin / (ms_win / 1e3), 3),
+                         "ms_per_step_window": round(ms_win / nwin, 3),
+                         "iterations_mean_window": round(float(np.mean(its[k0:])), 2),
+                         "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its)),
+                         "ms_training": round(ev[1].elapsed_time(ev[2]), 2) if name == "fcg" else 0.0}
+            if training:
+                out[name]["training"] = training
+    best = max(out, key=lambda m: out[m]["window_steps_per_s"])
+    line = {"metric": "MH Darcy unsteady steps/s (implicit Euler, residual 1e-10)",
+            "value": out[best]["window_steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": a.unsteady,
+            "warmup": max(3, a.warmup), "ms_per_step": out[best]["ms_per_step_window"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": method_dtype(best, AMG_VALUE_BYTES == 2),
             "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
             "config": {"workload": "cfg%d: %s, dt %g, %d steps" % (a.config, WORKLOADS[a.config], dt, a.unsteady),
-                       "method": best},
-            "methods": out}
+                       "window": "steps %d-%d (the learned method trains after step %d)" % (k0 + 1, a.unsteady, k0)},
+            "method": best, "methods": out}
     print(json.dumps(line), flush=True)
 
 

@@ -356,34 +356,49 @@ int mh_unsteady_step(mh_handle *h, double dt, const mh_solve_opts *opts,
 
 /* ---- learned preconditioner (MH_SOLVER_FCG_LEARNED) ---------------------------------- */
 /* No counterpart in the reference, which preconditions the Schur system with PETSc ILU
- * (src/la/solve.cc).  A 3-layer message-passing network over the Jacobi-scaled edge system
- * S^ (node state 4 channels, MLP width 32, bf16 weights on the tensor cores, fp32 sums):
- *   h0 = (r/|r|, 0, 0, 0);  h^{l+1} = h^l + W2 relu(W1 [h^l ; S^ h^l] + b1) + b2;
- *   z = |r| h3[0].
- * MH_NN_PARAMS floats, per layer: W1 [32][8], b1 [32], W2 [4][32], b2 [4] (row-major).
- * A new handle starts from the identity network (W2 = 0: z = r, Jacobi). */
-#define MH_NN_PARAMS 1260
+ * (src/la/solve.cc).  The learned method is the aggregation multigrid of MH_SOLVER_AMG whose
+ * fine-level smoother is Chebyshev on diag(w) S^, with the weights w given by a message-
+ * passing network over the Jacobi-scaled edge system S^ (off-diagonal o_ij):
+ *   x_i = (1, sum|o_ij|, max|o_ij|, sum o_ij, sum max(o_ij,0), nnz_i/8, sum o_ij^2, [nnz_i = 0])
+ *   h0 = relu(W0 x + b0)                                  8 -> 32
+ *   3 layers: h = h + relu(W_l [h ; A h] + b_l),  A_ij = |o_ij|       64 -> 32 (bf16 tensor
+ *                                                                     cores, fp32 sums)
+ *   w_i = exp(ln2 tanh(w_out . h_i + b_out))              w in [1/2, 2]
+ * The network reads the matrix, not the residual: during a solve the preconditioner is a
+ * fixed symmetric positive definite operator (the V-cycle), so flexible CG keeps its
+ * guarantees.  A new handle starts from random hidden layers and a zero output layer: w = 1,
+ * the plain multigrid.  MH_NN_PARAMS floats: W0 [32][8], b0 [32], per layer W_l [32][64],
+ * b_l [32], then w_out [32], b_out [1] (row-major). */
+#define MH_NN_PARAMS 6561
 int mh_learned_set_weights(mh_handle *h, const float *w, int64_t n);
 int mh_learned_get_weights(const mh_handle *h, float *w, int64_t n);
+/* Back to the parameters a new handle starts from (w = 1) and a fresh Adam state. */
+int mh_learned_reset(mh_handle *h);
 
-/* Loss and gradient of one training pair (r, e) on the assembled system, for checking the
- * training kernels: r, e [n_edges] in edge order, in the Jacobi-scaled space (S^ e = r for
- * an exact pair).  loss = (z - e)' S^ (z - e) / (e' S^ e) = (z - e)' (S^ z - r) / (e' r) with
- * z = NN(r) evaluated without the |r| normalisation; grad [MH_NN_PARAMS]. */
+/* Loss and parameter gradient of one training pair (r, e) on the assembled system, for
+ * checking the training kernels: r, e [n_edges] in edge order, in the Jacobi-scaled space
+ * (S^ e = r for an exact pair).  loss = (M r - e)' S^ (M r - e) / (e' S^ e) with M the
+ * training V-cycle (no energy-optimal coarse scaling, FP32 fine values) and the network's
+ * smoother weights; grad [MH_NN_PARAMS] = d loss / d parameters, with the smoothing interval
+ * held at its estimate for the current weights. */
 int mh_learned_grad(mh_handle *h, const double *r, const double *e, float *grad, double *loss);
-
-/* z = NN(r) through the inference kernels (bf16 tensor-core MLP): r, z [n_edges] in edge
- * order, Jacobi-scaled space; each instance's input is normalised by its own |r| and the
- * output scaled back.  For checking the inference path against the training path and a
- * CPU restatement. */
+/* The same evaluation, returning dw [n_edges] = d loss / d w (the cycle's adjoint) and the
+ * weights w [n_edges] (either may be NULL).  refresh = 0 keeps the smoothing interval of the
+ * previous evaluation (so that finite differences see the same function the gradient is of);
+ * refresh = 1 re-estimates it for the current weights. */
+int mh_learned_grad_weights(mh_handle *h, const double *r, const double *e, int32_t refresh, float *dw, float *w,
+                            double *loss);
+/* The network's smoother weights for the assembled system: w [n_edges] in edge order. */
+int mh_learned_smoother(mh_handle *h, float *w, int64_t n);
+/* z = M r: one application of the learned preconditioner (the solver's V-cycle with the
+ * network's smoother weights); r, z [n_edges] in edge order, Jacobi-scaled space. */
 int mh_learned_apply(mh_handle *h, const double *r, double *z);
 
 typedef struct mh_learn_opts {
     int32_t n_pairs;        /* training pairs: snapshots of the plain solver (default 12) */
     int32_t epochs;         /* passes over the pairs, one Adam step per pair (default 40) */
     float   lr;             /* Adam step size (default 2e-3)                          */
-    int32_t train_bias;     /* 0 (default): b1 = b2 = 0 stay fixed, the network is
-                               positively homogeneous                                 */
+    int32_t train_bias;     /* unused (every parameter is trained)                    */
     double  solve_rtol;     /* accuracy of the reference solution x* (default 1e-9)   */
     uint64_t seed;          /* order of the pairs within an epoch                     */
     int32_t reserved[6];
@@ -403,7 +418,8 @@ void mh_learn_opts_default(mh_learn_opts *o);
  * solves it with FP64 PCG to solve_rtol for x*, reruns FP64 PCG from zero and takes
  * n_pairs snapshots x_s at geometrically spaced iterations, giving pairs
  * (r_s = b^ - S^ x_s, e_s = x* - x_s) scaled by 1/|r_s|, and runs epochs x n_pairs Adam
- * steps on the energy-norm loss.  The solution left in the handle is x*. */
+ * steps on the loss of mh_learned_grad (the energy-norm error of the V-cycle's answer), the
+ * smoothing interval re-estimated at every step.  The solution left in the handle is x*. */
 int mh_learned_train(mh_handle *h, const mh_learn_opts *opts, mh_learn_stats *stats);
 
 /* ---- aggregation multigrid (MH_SOLVER_AMG) ------------------------------------------- */
@@ -416,6 +432,16 @@ int mh_amg_info(const mh_handle *h, int32_t *n_levels, int64_t *rows, int64_t *s
  * P_{i,agg[i]} = 1 and W = diag(weight).  Call with NULL arrays to get n and nnz first. */
 int mh_amg_level(const mh_handle *h, int32_t level, int64_t *n, int64_t *nnz, int32_t *agg, float *weight,
                  int32_t *row_ptr, int32_t *col, float *val);
+
+/* Per-edge weights w of the multigrid's fine-level smoother for MH_SOLVER_AMG: Chebyshev
+ * smoothing on diag(w) S^ instead of the Jacobi-scaled S^ (MH_SOLVER_FCG_LEARNED sets them
+ * from its network instead).  w [n_edges] in edge order, every weight > 0 and finite; NULL
+ * restores plain smoothing.  Rows outside the hierarchy (no coupling) keep weight 1 (they are
+ * solved exactly).  Takes effect at the next solve (the fine level's smoothing interval is
+ * re-estimated for the weights). */
+int mh_smoother_weights_set(mh_handle *h, const float *w, int64_t n);
+/* The weights of the last multigrid solve (1 where it used none); w [n_edges]. */
+int mh_smoother_weights_get(const mh_handle *h, float *w, int64_t n);
 
 /* ---- a general symmetric positive definite system (the LinSys seam) ------------------- */
 /* The solvers of mh_solve on a sparse SPD system the caller assembles itself, as Flow123d's

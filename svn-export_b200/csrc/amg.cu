@@ -1019,6 +1019,37 @@ __global__ void k_sm_first_step(Gate gate, MatView A, const float *__restrict__ 
     x_out[i] = x1 + dn;
 }
 
+// The same with smoother weights w (Omega S^): x1 = c0 w b, d = c1 x1 + c2 w (b - S^ x1); the
+// product S^ (w b) gathers w and b together
+__global__ void k_sm_first_step_w(Gate gate, MatView A, const float *__restrict__ b, const float *__restrict__ w,
+                                  float *__restrict__ x_out, float *__restrict__ d, float c0, float c1, float c2,
+                                  const int32_t *__restrict__ agg) {
+    if (closed(gate)) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const float bi = b[i];
+    if (agg && agg[i] < 0) {  // a row outside the hierarchy: exact
+        d[i] = 0.f;
+        x_out[i] = bi;
+        return;
+    }
+    int64_t base;
+    int wd, ln;
+    row_of(A, i, base, wd, ln);
+    float y = 0.f;
+    for (int j = 0; j < wd; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        const int32_t c = __ldg(A.col + slot);
+        const float v = A.hval ? __half2float(A.hval[slot]) : __ldg(A.val + slot);
+        y += v * (w[c] * b[c]);
+    }
+    const float wi = w[i];
+    const float x1 = c0 * wi * bi;
+    const float dn = c1 * x1 + c2 * wi * (bi - c0 * y);
+    d[i] = dn;
+    x_out[i] = x1 + dn;
+}
+
 template <int G>
 __global__ void __launch_bounds__(256) k_residual(Gate gate, MatView A, const float *__restrict__ b,
                                                   const float *__restrict__ x, float *__restrict__ r) {
@@ -1327,6 +1358,103 @@ cudaError_t Amg::level_stats(AmgLevel &L, unsigned int *bound, cudaStream_t s) {
     return cudaSuccess;
 }
 
+// ---- spectral estimates ---------------------------------------------------------------------
+// One power-iteration step y = D^-1 A x (thread per row over the whole row, long rows included:
+// setup only).  The start vector is a fixed pseudo-random sign pattern of amplitude in [0.5, 1)
+// (no scaling between steps: |D^-1 A| <= a few, so 12 steps stay far from FP32 overflow).
+__global__ void k_power_start(int64_t n, float *x) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t h = (uint32_t)i * 2654435761u;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    x[i] = ((h & 1u) ? 1.f : -1.f) * (0.5f + (float)((h >> 8) & 0xffffu) * (0.5f / 65536.f));
+}
+
+__global__ void __launch_bounds__(256) k_power_step(MatView A, const float *__restrict__ invd,
+                                                    const float *__restrict__ x, float *__restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    float acc = 0.f;
+    for (int j = 0; j < w; ++j) {
+        const int64_t slot = base + (int64_t)j * kS + ln;
+        acc += __ldg(A.val + slot) * __ldg(x + __ldg(A.col + slot));
+    }
+    y[i] = invd ? invd[i] * acc : acc;
+}
+
+// per-block partial sums of x.x and y.y (fixed grid, fixed tree: deterministic)
+constexpr int kPowerBlocks = 296;
+__global__ void __launch_bounds__(256) k_power_norms(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
+                                                     double *__restrict__ part) {
+    double sx = 0.0, sy = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        sx += (double)x[i] * x[i];
+        sy += (double)y[i] * y[i];
+    }
+    __shared__ double sh[2][256];
+    sh[0][threadIdx.x] = sx;
+    sh[1][threadIdx.x] = sy;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sh[0][0];
+        part[2 * blockIdx.x + 1] = sh[1][0];
+    }
+}
+
+// fine smoother weights in effect: 1 on the rows outside the hierarchy (solved exactly, x = b)
+__global__ void k_fine_weights_eff(int64_t n, const int32_t *__restrict__ agg, const float *__restrict__ w,
+                                   float *__restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (agg && agg[i] < 0) ? 1.f : w[i];
+}
+
+// Gershgorin bound of Omega S^ on the fine level (unit diagonal): max_i w_i sum_j |a_ij|
+__global__ void __launch_bounds__(256) k_fine_bound(MatView A, const float *__restrict__ w, unsigned int *bound) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float m = 0.f;
+    if (i < A.n) {
+        int64_t base;
+        int wd, ln;
+        row_of(A, i, base, wd, ln);
+        float sum = 0.f;
+        for (int j = 0; j < wd; ++j) sum += fabsf(__ldg(A.val + base + (int64_t)j * kS + ln));
+        m = w[i] * sum;
+    }
+    __shared__ float wm[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(kFull, m, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t = fmaxf(t, wm[k]);
+        if (t > 0.f) atomicMax(bound, __float_as_uint(t));
+    }
+}
+
+__global__ void k_power_total(const double *__restrict__ part, int nb, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < nb; ++k) {
+        a += part[2 * k];
+        b += part[2 * k + 1];
+    }
+    out[0] = a;
+    out[1] = b;
+}
+
 // One pairing pass on A (rows excluded by row_edge < 0 or without coupling get agg = -1):
 // agg [A.n], nc aggregates, member lists mstart [nc+1], mrows.
 cudaError_t Amg::pair_pass(const AmgMatrix &A, const float *isd, const int32_t *row_edge, DBuf<int32_t> &agg,
@@ -1565,9 +1693,18 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         }
     }
     {
+        cudaError_t e2 = fine_weights_eff(s);
+        if (e2 != cudaSuccess || (e2 = fine_interval(s)) != cudaSuccess || (e2 = power_estimates(s)) != cudaSuccess)
+            return e2;
         std::vector<unsigned int> bits(n_levels_);
         std::vector<int32_t> nlong(n_levels_, 0);
+        std::vector<double> pw(2 * n_levels_, 0.0);
         AMG_CK(cudaMemcpyAsync(bits.data(), bounds_.p, n_levels_ * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        if (fine_w_)  // the fine level is smoothed on Omega S^: its own bound
+            AMG_CK(cudaMemcpyAsync(bits.data(), bounds_.p + opt_.max_levels, sizeof(unsigned int),
+                                   cudaMemcpyDeviceToHost, s));
+        if (opt_.power_steps > 0)
+            AMG_CK(cudaMemcpyAsync(pw.data(), pw_sums_.p, 2 * n_levels_ * sizeof(double), cudaMemcpyDeviceToHost, s));
         for (int l = 1; l < n_levels_; ++l)
             if (lv_[l].A.long_count)
                 AMG_CK(cudaMemcpyAsync(&nlong[l], lv_[l].A.long_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1580,7 +1717,13 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         for (int l = 0; l < n_levels_; ++l) {
             float hi;
             std::memcpy(&hi, &bits[l], sizeof(hi));
-            lv_[l].hi = hi > 0.f ? hi : 2.f;
+            lv_[l].gershgorin = hi > 0.f ? hi : 2.f;
+            lv_[l].hi = lv_[l].gershgorin;
+            // |v_k| / |v_{k-1}| of the power iteration (a lower estimate of lambda_max)
+            if (opt_.power_steps > 0 && pw[2 * l] > 0.0 && pw[2 * l + 1] > 0.0 && std::isfinite(pw[2 * l + 1])) {
+                const double est = std::sqrt(pw[2 * l + 1] / pw[2 * l]);
+                lv_[l].hi = (float)std::min((double)lv_[l].gershgorin, opt_.power_safety * est);
+            }
             lv_[l].A.n_long = nlong[l];
             // warps per slice in the row kernels: at most split_width slots per warp and row
             // (the fine level, 7-8 entries per row, keeps one thread per row)
@@ -1618,6 +1761,81 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     return dense_n_ > 0 ? dense_coarse(Lc.A, s) : cudaSuccess;
 }
 
+cudaError_t Amg::power_estimates(cudaStream_t s, int only_level) {
+    if (opt_.power_steps <= 0) return cudaSuccess;
+    int64_t nmax = 0;
+    for (int l = 0; l < n_levels_; ++l) nmax = std::max(nmax, lv_[l].A.n);
+    AMG_CK(pw_a_.ensure(std::max<int64_t>(nmax, 1)));
+    AMG_CK(pw_b_.ensure(std::max<int64_t>(nmax, 1)));
+    AMG_CK(pw_part_.ensure(2 * kPowerBlocks));
+    AMG_CK(pw_sums_.ensure(2 * (size_t)std::max(n_levels_, 1)));
+    if (only_level < 0)
+        AMG_CK(cudaMemsetAsync(pw_sums_.p, 0, 2 * (size_t)std::max(n_levels_, 1) * sizeof(double), s));
+    // the coarsest level is solved, not smoothed (unless coarsening stalled: it then gets a
+    // Chebyshev polynomial of its own and an estimate too)
+    for (int l = 0; l < n_levels_; ++l) {
+        if (only_level >= 0 && l != only_level) continue;
+        AmgLevel &L = lv_[l];
+        const int64_t n = L.A.n;
+        if (n <= 0) continue;
+        // the fine level is the Jacobi-scaled system (unit diagonal): no D^-1, or the
+        // smoother's row weights
+        const float *invd = l == 0 ? fw() : L.inv_diag.p;
+        const MatView V = view(L.A);
+        float *x = pw_a_.p, *y = pw_b_.p;
+        k_power_start<<<nblk(n, 256), 256, 0, s>>>(n, x);
+        for (int k = 0; k < opt_.power_steps; ++k) {
+            k_power_step<<<nblk(n, 256), 256, 0, s>>>(V, invd, x, y);
+            if (k + 1 < opt_.power_steps) std::swap(x, y);
+        }
+        k_power_norms<<<kPowerBlocks, 256, 0, s>>>(n, x, y, pw_part_.p);
+        k_power_total<<<1, 32, 0, s>>>(pw_part_.p, kPowerBlocks, pw_sums_.p + 2 * l);
+        AMG_CK(cudaGetLastError());
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Amg::fine_weights_eff(cudaStream_t s) {
+    if (!fine_w_) return cudaSuccess;
+    const int64_t n = lv_[0].A.n;
+    AMG_CK(fine_w_eff_.ensure(std::max<int64_t>(n, 1)));
+    k_fine_weights_eff<<<nblk(n, 256), 256, 0, s>>>(n, n_levels_ > 1 ? lv_[0].agg.p : nullptr, fine_w_,
+                                                    fine_w_eff_.p);
+    AMG_CK(cudaGetLastError());
+    return cudaSuccess;
+}
+
+// Level 0's Gershgorin bound of Omega S^ (into the spare bound word) for fine weights
+cudaError_t Amg::fine_interval(cudaStream_t s) {
+    if (!fine_w_) return cudaSuccess;
+    unsigned int *b = bounds_.p + opt_.max_levels;
+    AMG_CK(cudaMemsetAsync(b, 0, sizeof(unsigned int), s));
+    k_fine_bound<<<nblk(lv_[0].A.n, 256), 256, 0, s>>>(view(lv_[0].A), fw(), b);
+    AMG_CK(cudaGetLastError());
+    return cudaSuccess;
+}
+
+cudaError_t Amg::refresh_fine(cudaStream_t s) {
+    if (n_levels_ < 1) return cudaSuccess;
+    cudaError_t e;
+    if ((e = fine_weights_eff(s)) != cudaSuccess || (e = fine_interval(s)) != cudaSuccess ||
+        (e = power_estimates(s, 0)) != cudaSuccess)
+        return e;
+    unsigned int bits = 0;
+    double pw[2] = {0.0, 0.0};
+    AMG_CK(cudaMemcpyAsync(&bits, bounds_.p + (fine_w_ ? opt_.max_levels : 0), sizeof(bits), cudaMemcpyDeviceToHost, s));
+    if (opt_.power_steps > 0) AMG_CK(cudaMemcpyAsync(pw, pw_sums_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AMG_CK(cudaStreamSynchronize(s));
+    float hi;
+    std::memcpy(&hi, &bits, sizeof(hi));
+    AmgLevel &L = lv_[0];
+    L.gershgorin = hi > 0.f ? hi : 2.f;
+    L.hi = L.gershgorin;
+    if (opt_.power_steps > 0 && pw[0] > 0.0 && pw[1] > 0.0 && std::isfinite(pw[1]))
+        L.hi = (float)std::min((double)L.gershgorin, opt_.power_safety * std::sqrt(pw[1] / pw[0]));
+    return cudaSuccess;
+}
+
 void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<double> &c2, int degree,
                       float ratio) const {
     const int deg = std::max(1, degree > 0 ? degree : opt_.cheb_degree);
@@ -1644,6 +1862,14 @@ int Amg::kernels_per_apply() const {
 
 cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
                        AmgProf *prof) {
+    return cycle(0, r, z, n_done, n_inst, s, prof, nullptr);
+}
+
+// The V-cycle from level l0: l0 = 0 is the preconditioner (rhs r, result z); l0 > 0 runs the
+// cycle of the coarser levels on the rhs already in lv_[l0].b and leaves its result in
+// *x_l0 (a level buffer), with no fine-level work.
+cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
+                       AmgProf *prof, float **x_l0) {
     const Gate gate_{n_done, n_inst};
     const int pre = pre_degree();
     int launches = 0;  // kernels of one cycle, for the launch count
@@ -1675,10 +1901,11 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
     const int deg = std::max(1, opt_.cheb_degree);
     const int nl = n_levels_;
     std::vector<float *> xout(nl);
-    for (int l = 0; l < nl - 1; ++l) {
+    for (int l = l0; l < nl - 1; ++l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
-        const float *invd = l == 0 ? nullptr : L.inv_diag.p;  // the scaled fine level has unit diagonal
+        // the scaled fine level has unit diagonal; with smoother weights Omega, D^-1 -> Omega
+        const float *invd = l == 0 ? fw() : L.inv_diag.p;
         MatView A = view(L.A);
         if (l == 0 && opt_.half_fine) A.hval = reinterpret_cast<const __half *>(fine_half_.p);
         const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
@@ -1688,12 +1915,16 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         int k0 = 1;
         if (l == 0 && pre >= 2) {  // first two steps in one pass
             rec_step(true);
-            k_sm_first_step<<<g, 256, 0, s>>>(gate_, A, b, xo, L.d.p, (float)c2[0], (float)c1[1], (float)c2[1],
-                                              L.agg.p);
+            if (fine_w_)
+                k_sm_first_step_w<<<g, 256, 0, s>>>(gate_, A, b, fw(), xo, L.d.p, (float)c2[0], (float)c1[1],
+                                                    (float)c2[1], L.agg.p);
+            else
+                k_sm_first_step<<<g, 256, 0, s>>>(gate_, A, b, xo, L.d.p, (float)c2[0], (float)c1[1], (float)c2[1],
+                                                  L.agg.p);
             rec_step(false);
             std::swap(xi, xo);
             k0 = 2;
-        } else if (l == 0) {
+        } else if (l == 0 || l == l0) {  // (a cycle started below the fine level: its first step)
             k_sm_first<<<g, 256, 0, s>>>(gate_, L.A.n, b, invd, (float)c2[0], xi, L.d.p, L.agg.p);
         }
         // (coarser levels: the first step was fused into the restriction from the level above)
@@ -1746,10 +1977,10 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         }
     }
     // ascend: prolong, smooth
-    for (int l = nl - 2; l >= 0; --l) {
+    for (int l = nl - 2; l >= l0; --l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
-        const float *invd = l == 0 ? nullptr : L.inv_diag.p;
+        const float *invd = l == 0 ? fw() : L.inv_diag.p;
         MatView A = view(L.A);
         if (l == 0 && opt_.half_fine) A.hval = reinterpret_cast<const __half *>(fine_half_.p);
         const unsigned g = nblk(L.A.n, 256), gs = row_blocks(L);
@@ -1782,8 +2013,55 @@ cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t 
         xout[l] = xi;
     }
     if (prof) rec(prof->cycle[1]);
-    last_long_launches_ = launches;
+    if (l0 == 0) last_long_launches_ = launches;
+    if (x_l0) *x_l0 = xout[l0];
     return cudaGetLastError();
+}
+
+cudaError_t Amg::coarse_correct(const float *v, float *out, cudaStream_t s) {
+    const int64_t n = lv_[0].A.n;
+    AMG_CK(cudaMemsetAsync(out, 0, n * sizeof(float), s));
+    if (n_levels_ < 2) return cudaSuccess;
+    AmgLevel &L0 = lv_[0], &C = lv_[1];
+    const Gate g{nullptr, 0};
+    k_restrict<<<nblk(C.A.n, 256), 256, 0, s>>>(g, L0.nc, C.A.n, L0.mem_start.p, L0.mem_rows.p, v, C.b.p, w0_used_);
+    AMG_CK(cudaGetLastError());
+    float *xc = nullptr;
+    cudaError_t e = cycle(1, nullptr, nullptr, nullptr, 0, s, nullptr, &xc);
+    if (e != cudaSuccess) return e;
+    k_prolong<<<nblk(n, 256), 256, 0, s>>>(g, n, L0.agg.p, xc, out, nullptr, 1.f, w0_used_);
+    return cudaGetLastError();
+}
+
+cudaError_t Amg::smooth_fine(const float *b, float *x, cudaStream_t s) {
+    AmgLevel &L = lv_[0];
+    std::vector<double> c1, c2;
+    cheb_coeffs(L, c1, c2);
+    const int pre = pre_degree();
+    const float *invd = fw();
+    MatView A = view(L.A);
+    if (opt_.half_fine) A.hval = reinterpret_cast<const __half *>(fine_half_.p);
+    const int32_t *agg = n_levels_ > 1 ? L.agg.p : nullptr;
+    const Gate g{nullptr, 0};
+    float *xi = L.xa.p, *xo = L.xb.p;
+    k_sm_first<<<nblk(L.A.n, 256), 256, 0, s>>>(g, L.A.n, b, invd, (float)c2[0], xi, L.d.p, agg);
+    const auto sm_step = sm_step_kernel(L.g);
+    for (int k = 1; k < pre; ++k) {
+        sm_step<<<row_blocks(L), 256, 0, s>>>(g, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], agg);
+        std::swap(xi, xo);
+    }
+    AMG_CK(cudaGetLastError());
+    AMG_CK(cudaMemcpyAsync(x, xi, L.A.n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    return cudaSuccess;
+}
+
+bool Amg::fine_poly(double &a0, double &a1) const {
+    if (n_levels_ < 1 || pre_degree() != 2) return false;
+    std::vector<double> c1, c2;
+    cheb_coeffs(lv_[0], c1, c2);
+    a0 = c2[0] * (1.0 + c1[1]) + c2[1];
+    a1 = -c2[1] * c2[0];
+    return true;
 }
 
 }  // namespace mh

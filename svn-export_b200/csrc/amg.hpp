@@ -44,6 +44,9 @@ struct AmgOptions {
     int split = 0;          // warps per slice in the coarse row kernels (1, 2, 4, 8; 0: by row width)
     int split_width = 12;   // ... by row width: the fewest warps with at most this many slots each
     int half_fine = 1;      // 1: the cycle reads the fine matrix's values in FP16 (a copy made at setup)
+    int power_steps = 12;   // power-iteration steps estimating lambda_max(D^-1 A) per level (0: the
+                            // Gershgorin bound alone)
+    float power_safety = 1.1f;  // smoothing interval top = min(Gershgorin, safety * estimate)
 };
 
 template <class T> struct DBuf {
@@ -75,7 +78,10 @@ struct AmgLevel {
     DBuf<int32_t> mem_start, mem_rows;         // rows of each coarse row: [nc+1], [n]
     DBuf<float> b, xa, xb, d, r;               // cycle vectors
     int64_t nc = 0;                            // coarse rows (0 on the coarsest level)
-    float hi = 2.f;                            // Gershgorin bound of D^-1 A
+    float hi = 2.f;                            // top of the smoothing interval: the power-iteration
+                                               // estimate of lambda_max(D^-1 A) times a safety
+                                               // factor, at most the Gershgorin bound
+    float gershgorin = 2.f;                    // Gershgorin bound of D^-1 A
     int g = 1;                                 // warps per slice in the row kernels (amg.cu)
 };
 
@@ -106,6 +112,28 @@ public:
     int64_t coarse_rows() const { return n_levels_ ? lv_[n_levels_ - 1].A.n : 0; }
     int kernels_per_apply() const;
     const float *fine_weights() const { return w0_used_; }  // null when the transfers are unweighted
+    // Per-row weights of the fine level's smoother (device array over the solver rows, owned by
+    // the caller; null: none): the fine level is then smoothed with Chebyshev on Omega S^
+    // instead of S^.  Takes effect at the next setup, or at refresh_fine for the current
+    // hierarchy (the fine level's interval is re-estimated for the new weights).
+    void set_fine_weights(const float *w) { fine_w_ = w; }
+    const float *fine_smoother_weights() const { return fine_w_; }
+    // the weights the cycle uses (1 on the rows outside the hierarchy), null when none are set
+    const float *fine_smoother_weights_in_effect() const { return fw(); }
+    cudaError_t refresh_fine(cudaStream_t s);
+    // new values in the weights array, the smoothing interval kept as it is
+    cudaError_t update_fine_weights(cudaStream_t s) { return fine_weights_eff(s); }
+    // Parts of the cycle for training the fine smoother (the cycle is linear when kcycle = 0):
+    //   coarse_correct: out = P B P^T v (restriction with the level-0 weights, the cycle of the
+    //                   coarser levels B, prolongation), out over the fine rows;
+    //   smooth_fine:    x = Q b, the fine level's smoothing from zero (Q = q(Omega S^) Omega);
+    //   fine_poly:      Q = a0 Omega + a1 Omega S^ Omega for the degree-2 smoother (false for
+    //                   other degrees).
+    cudaError_t coarse_correct(const float *v, float *out, cudaStream_t s);
+    cudaError_t smooth_fine(const float *b, float *x, cudaStream_t s);
+    bool fine_poly(double &a0, double &a1) const;
+    const AmgOptions &options() const { return opt_; }
+    float level_hi(int l) const { return lv_[l].hi; }
     bool half_fine() const { return opt_.half_fine != 0; }
     std::string err;
 
@@ -118,6 +146,11 @@ private:
                          const float *wt);
     cudaError_t level_stats(AmgLevel &L, unsigned int *bound, cudaStream_t s);
     cudaError_t dense_coarse(const AmgMatrix &A, cudaStream_t s);
+    // lambda_max estimates of D^-1 A on every level but the coarsest (power iteration from a
+    // fixed pseudo-random start; deterministic sums), as |v_k|^2 and |v_{k-1}|^2 per level
+    cudaError_t power_estimates(cudaStream_t s, int only_level = -1);
+    cudaError_t cycle(int l0, const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
+                      AmgProf *prof, float **x_l0);
     cudaError_t scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t &total, cudaStream_t s);
     cudaError_t scan_i64(const int64_t *in, int64_t *out, int64_t n, int64_t &total, cudaStream_t s);
     // the same without reading the total back (out[n] holds it on the device)
@@ -156,6 +189,13 @@ private:
     DBuf<double> dots_, alpha_;     // coarse-correction scaling: partials, factor per level
     DBuf<unsigned int> tickets_;    // last-block tickets of the scaling reductions, per level
     std::vector<int64_t> dots_off_;
+    const float *fine_w_ = nullptr;  // fine-level smoother weights (set_fine_weights)
+    DBuf<float> fine_w_eff_;         // ... with 1 on the rows outside the hierarchy (solved exactly)
+    const float *fw() const { return fine_w_ ? fine_w_eff_.p : nullptr; }
+    cudaError_t fine_weights_eff(cudaStream_t s);
+    cudaError_t fine_interval(cudaStream_t s);  // level 0's bound for the weights
+    DBuf<float> pw_a_, pw_b_;       // power-iteration vectors
+    DBuf<double> pw_part_, pw_sums_;  // its per-block partial norms and the two norms per level
     DBuf<float> w0_;                // sqrt(diag S) per fine row
     DBuf<uint16_t> fine_half_;      // FP16 bits of the fine matrix's values (half_fine)
     const float *w0_used_ = nullptr;

@@ -18,6 +18,7 @@
 #include "device_system.hpp"
 #include "amg.hpp"
 #include "learned.hpp"
+#include "smoother_nn.hpp"
 #include "mesh_store.hpp"
 #include "mh_darcy.h"
 #include "system_build.hpp"
@@ -87,14 +88,21 @@ struct mh_handle {
     std::vector<int32_t> inst_iters, inst_status;  // per instance, last solve
     std::vector<double> inst_rel;
     // learned preconditioner: fp32 master weights, bf16 fragments, Adam state, work buffers
+    // learned smoother network: parameters, Adam state, gradient; row features of the current
+    // matrix and the activations of an inference pass; the weights it gives
     float *nn_w = nullptr, *nn_m = nullptr, *nn_v = nullptr, *nn_grad = nullptr;
-    uint32_t *nn_wb = nullptr;
     int nn_step = 0;
-    float4 *nn_h0 = nullptr, *nn_h1 = nullptr;
+    float *sn_x = nullptr, *sn_w = nullptr;
+    mh::SnActs sn_inf{};
+    int64_t sn_x_epoch = -1;            // matrix epoch the features were computed from
+    int64_t sn_key_epoch = -1;          // matrix epoch and training step of the weights in sn_w
+    int sn_key_step = -1;
+    bool user_fine_w = false;           // mh_smoother_weights_set holds weights in d_fine_w
     float *cheb_z0 = nullptr, *cheb_z1 = nullptr, *cheb_d = nullptr;
     unsigned int *spec_bound = nullptr;
     double *d_loss = nullptr;
     mh::Amg amg;                        // aggregation multigrid (MH_SOLVER_AMG)
+    float *d_fine_w = nullptr;          // fine-level smoother weights per solver row (or unused)
     int64_t amg_epoch = 0;              // setups so far (captured graphs refer to one)
     int64_t matrix_epoch = 0;           // matrix assemblies so far
     int64_t amg_matrix_epoch = -1;      // the assembly the current hierarchy was built from
@@ -103,8 +111,13 @@ struct mh_handle {
     cudaGraphExec_t fcg_graph = nullptr;
     FcgKey fcg_key{};
     std::vector<mh::AmgProf> amg_prof;  // timing events of the V-cycles of one FCG graph
-    mh::NnTrainBuffers tr{};            // activations of a training pass
+    mh::SnActs sn_tr{};                 // activations of a training pass
+    mh::SnScratch sn_sc{};
+    float *tv[16] = {};                 // vectors of the smoother gradient
+    double *tdot = nullptr;             // dot-product partials and results
     bool tr_ready = false;
+    bool amg_training = false;          // the hierarchy is the training one ...
+    int64_t tr_hier_epoch = -1;         // ... of this matrix epoch
     float *pair_r = nullptr, *pair_e = nullptr;  // training pairs, [cap][n_rows] each
     int pair_cap = 0;
     double *x_star = nullptr, *pair_acc = nullptr;
@@ -673,23 +686,22 @@ int solve_ir32(mh_handle *h, const mh_solve_opts &o, SolveResult &res) {
 
 // ---- learned preconditioner and flexible CG ----------------------------------------------
 
-// Identity network (Jacobi preconditioning): W1 small random, b1 = W2 = b2 = 0.
-void nn_identity_weights(std::vector<float> &w, uint64_t seed) {
-    w.assign(mh::kNnParams, 0.f);
-    uint64_t s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
-    for (int l = 0; l < mh::kNnLayers; ++l)
-        for (int k = 0; k < mh::kNnH * 2 * mh::kNnK; ++k) {
-            s = s * 6364136223846793005ULL + 1442695040888963407ULL;
-            const double u = ((s >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0;
-            w[l * mh::kNnPerLayer + k] = (float)(0.2 * u);
-        }
+// Initial parameters of the smoother network: Xavier-scaled random layers (fixed seed) and a
+// zero output layer, so that every weight is 1 (plain smoothing) until training.
+void nn_initial_params(std::vector<float> &w, uint64_t seed) {
+    w.assign(mh::kSnParams, 0.f);
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    const double s0 = std::sqrt(2.0 / (mh::kSnF + mh::kSnW)), s1 = 0.5 * std::sqrt(2.0 / (3 * mh::kSnW));
+    for (int k = 0; k < mh::kSnW * mh::kSnF; ++k) w[mh::kSnOffW0 + k] = (float)(s0 * nd(rng));
+    for (int l = 0; l < mh::kSnL; ++l)
+        for (int k = 0; k < mh::kSnW * 2 * mh::kSnW; ++k) w[mh::kSnOffLayer + l * mh::kSnPerLayer + k] = (float)(s1 * nd(rng));
 }
 
 int nn_upload_weights(mh_handle *h, const float *w_host) {
-    CK(cudaMemcpyAsync(h->nn_w, w_host, mh::kNnParams * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->nn_m, 0, mh::kNnParams * sizeof(float), h->stream));
-    CK(cudaMemsetAsync(h->nn_v, 0, mh::kNnParams * sizeof(float), h->stream));
-    CK(mh::launch_nn_pack(h->nn_w, h->nn_wb, h->stream));
+    CK(cudaMemcpyAsync(h->nn_w, w_host, mh::kSnParams * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->nn_m, 0, mh::kSnParams * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(h->nn_v, 0, mh::kSnParams * sizeof(float), h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->nn_step = 0;
     return MH_OK;
@@ -698,24 +710,45 @@ int nn_upload_weights(mh_handle *h, const float *w_host) {
 int ensure_learned(mh_handle *h) {
     if (h->nn_w) return MH_OK;
     const int64_t nr = h->sys.n_rows;
-    h->nn_w = dalloc<float>(h, mh::kNnParams);
-    h->nn_m = dalloc<float>(h, mh::kNnParams);
-    h->nn_v = dalloc<float>(h, mh::kNnParams);
-    h->nn_grad = dalloc<float>(h, mh::kNnParams);
-    h->nn_wb = dalloc<uint32_t>(h, mh::kNnLayers * mh::kNnPackedPerLayer);
-    h->nn_h0 = dalloc<float4>(h, nr);
-    h->nn_h1 = dalloc<float4>(h, nr);
+    h->nn_w = dalloc<float>(h, mh::kSnParams);
+    h->nn_m = dalloc<float>(h, mh::kSnParams);
+    h->nn_v = dalloc<float>(h, mh::kSnParams);
+    h->nn_grad = dalloc<float>(h, mh::kSnParams);
     h->cheb_z0 = dalloc<float>(h, nr);
     h->cheb_z1 = dalloc<float>(h, nr);
     h->cheb_d = dalloc<float>(h, nr);
     h->spec_bound = dalloc<unsigned int>(h, 1);
     h->d_loss = dalloc<double>(h, 1);
-    if (!h->nn_w || !h->nn_m || !h->nn_v || !h->nn_grad || !h->nn_wb || !h->nn_h0 || !h->nn_h1 || !h->cheb_z0 ||
-        !h->cheb_z1 || !h->cheb_d || !h->spec_bound || !h->d_loss)
+    if (!h->nn_w || !h->nn_m || !h->nn_v || !h->nn_grad || !h->cheb_z0 || !h->cheb_z1 || !h->cheb_d ||
+        !h->spec_bound || !h->d_loss)
         return MH_ERR_NOMEM;
     std::vector<float> w;
-    nn_identity_weights(w, 1);
+    nn_initial_params(w, 1);
     return nn_upload_weights(h, w.data());
+}
+
+// The network's smoother weights for the current matrix into h->sn_w (features recomputed when
+// the matrix changed).  The inference buffers are allocated on first use.
+int nn_weights(mh_handle *h) {
+    int rc;
+    if ((rc = ensure_learned(h))) return rc;
+    const int64_t nr = h->sys.n_rows;
+    if (!h->sn_x) {
+        h->sn_x = dalloc<float>(h, nr * mh::kSnF);
+        h->sn_w = dalloc<float>(h, nr);
+        h->sn_inf.h[0] = dalloc<float>(h, nr * mh::kSnW);
+        h->sn_inf.h[1] = dalloc<float>(h, nr * mh::kSnW);
+        h->sn_inf.a[0] = dalloc<float>(h, nr * mh::kSnW);
+        if (!h->sn_x || !h->sn_w || !h->sn_inf.h[0] || !h->sn_inf.h[1] || !h->sn_inf.a[0]) return MH_ERR_NOMEM;
+    }
+    if (h->sn_x_epoch != h->matrix_epoch) {
+        CK(mh::sn_features(h->sys, h->sn_x, h->stream));
+        h->sn_x_epoch = h->matrix_epoch;
+        h->n_launch += 1;
+    }
+    CK(mh::sn_forward(h->sys, h->nn_w, h->sn_x, h->sn_inf, h->sn_w, false, h->stream));
+    h->n_launch += 2 + 2 * mh::kSnL;
+    return MH_OK;
 }
 
 // Upper bound of the spectrum of the scaled FP32 system (Gershgorin).
@@ -737,9 +770,6 @@ cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double h
     mh::DevSystem &sys = h->sys;
     cudaError_t e;
     switch (kind) {
-        case Pc::Nn:
-            e = mh::launch_nn_apply(sys, h->nn_w, h->nn_wb, sys.r32, h->nn_h0, h->nn_h1, sys.z32, sys.q32, s);
-            break;
         case Pc::Cheb:
             e = mh::launch_cheb_apply(sys, sys.r32, h->cheb_z0, h->cheb_z1, h->cheb_d, sys.z32, sys.q32, degree, lo, hi,
                                       s);
@@ -757,7 +787,6 @@ cudaError_t fcg_iteration(mh_handle *h, Pc kind, int degree, double lo, double h
 
 int fcg_kernels_per_iteration(mh_handle *h, Pc kind, int degree) {
     switch (kind) {
-        case Pc::Nn: return mh::kNnLayers + 3;
         case Pc::Cheb: return degree + 3;
         default: return h->amg.kernels_per_apply() + 4;
     }
@@ -774,7 +803,7 @@ void drop_fcg_graph(mh_handle *h) {
 // iterations that did work are added to the MH_KERNEL_VCYCLE / MH_KERNEL_SMOOTH0 classes.
 int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it, bool prof) {
     ipg = std::max(1, ipg);  // an empty graph would never make progress
-    prof = prof && kind == Pc::Amg;
+    prof = prof && (kind == Pc::Amg || kind == Pc::Nn);
     const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch, prof};
     if (prof) {
         const int steps = h->amg.fine_steps();
@@ -893,14 +922,73 @@ mh::AmgOptions amg_options() {
         const float x = (float)atof(e);
         if (x > 0.f && x <= 3.f) o.alpha = x;
     }
+    env_i("MH_AMG_POWER", o.power_steps, 0, 64);
+    if (const char *e = getenv("MH_AMG_SAFETY")) {
+        const float x = (float)atof(e);
+        if (x >= 1.f && x <= 3.f) o.power_safety = x;
+    }
     return o;
 }
 
-// Mixed-precision flexible CG: FP32 FCG with the learned (or Chebyshev-Jacobi) preconditioner
-// inside FP64 reliable updates, as solve_ir32; the direction sequence runs on across them.
-// If a learned segment breaks down (non-finite network output), uses up inner_max_it, or the
-// FP64 residual stops improving over three replacements, Chebyshev-Jacobi replaces the
-// network for the rest of the solve (fell_back = 1).
+// The multigrid preconditioner for the current matrix, with the fine level's smoother weights
+// of the method: the network's (learned method), the caller's (mh_smoother_weights_set), or
+// none.  The hierarchy is rebuilt when the matrix changed (ms_setup: its device time, else 0);
+// MH_FELL_BACK when the setup failed (h->err says why).
+int prepare_multigrid(mh_handle *h, Pc kind, double &ms_setup) {
+    int rc;
+    ms_setup = 0.0;
+    // the fine level's smoother weights: the network's (learned method), the caller's
+    // (mh_smoother_weights_set), or none
+    const float *want = nullptr;
+    if (kind == Pc::Nn) {
+        if (h->sn_key_epoch != h->matrix_epoch || h->sn_key_step != h->nn_step || !h->sn_w) {
+            if ((rc = nn_weights(h))) return rc;
+            h->sn_key_epoch = h->matrix_epoch;
+            h->sn_key_step = h->nn_step;
+            h->amg.set_fine_weights(nullptr);  // new values: the interval is re-estimated below
+        }
+        want = h->sn_w;
+    } else if (h->user_fine_w) {
+        want = h->d_fine_w;
+    }
+    if (h->amg_matrix_epoch == h->matrix_epoch && h->amg.levels() > 0) {
+        // same matrix as the hierarchy was built from (unsteady steps at a fixed dt): the
+        // hierarchy is reused, with the fine interval re-estimated when the weights changed
+        ms_setup = 0.0;
+        if (h->amg.fine_smoother_weights() != want) {
+            h->amg.set_fine_weights(want);
+            CK(h->amg.refresh_fine(h->stream));
+            h->amg_epoch += 1;  // captured cycles hold the old smoothing coefficients
+        }
+    } else {
+        // the hierarchy is built from the current matrix values
+        h->amg.set_fine_weights(want);
+        h->amg_training = false;
+        h->amg_epoch += 1;
+        h->amg_matrix_epoch = h->matrix_epoch;
+        CK(cudaEventRecord(h->ev[6], h->stream));
+        cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
+        CK(cudaEventRecord(h->ev[7], h->stream));
+        CK(cudaEventSynchronize(h->ev[7]));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]));
+        ms_setup = ms;
+        h->n_launch += h->amg.levels() * 12;
+        if (e != cudaSuccess) {
+            h->err = "AMG setup: " + h->amg.err;
+            cudaGetLastError();
+            h->amg_matrix_epoch = -1;
+            return MH_FELL_BACK;
+        }
+    }
+    return MH_OK;
+}
+
+// Mixed-precision flexible CG: FP32 FCG with the multigrid (plain or with the learned smoother)
+// or Chebyshev-Jacobi preconditioner inside FP64 reliable updates, as solve_ir32; the direction
+// sequence runs on across them.  If a segment of the learned method breaks down, uses up
+// inner_max_it, or the FP64 residual stops improving over three replacements, Chebyshev-Jacobi
+// replaces it for the rest of the solve (fell_back = 1).
 int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     int rc = ensure_learned(h);
     if (rc) return rc;
@@ -912,25 +1000,9 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     if ((rc = spectrum_bound(h, hi))) return rc;
     const double lo = hi / 30.0;
     const int degree = std::max(1, std::min(o.cheb_degree, 16));
-    if (kind == Pc::Amg && h->amg_matrix_epoch == h->matrix_epoch && h->amg.levels() > 0) {
-        res.ms_setup = 0.0;  // same matrix as the hierarchy was built from (unsteady steps at
-                             // a fixed dt): the hierarchy is reused
-    } else if (kind == Pc::Amg) {
-        // the hierarchy is built from the current matrix values
-        h->amg_epoch += 1;
-        h->amg_matrix_epoch = h->matrix_epoch;
-        CK(cudaEventRecord(h->ev[6], h->stream));
-        cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
-        CK(cudaEventRecord(h->ev[7], h->stream));
-        CK(cudaEventSynchronize(h->ev[7]));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]));
-        res.ms_setup = ms;
-        h->n_launch += h->amg.levels() * 12;
-        if (e != cudaSuccess) {
-            h->err = "AMG setup: " + h->amg.err;
-            cudaGetLastError();
-            h->amg_matrix_epoch = -1;
+    if (kind == Pc::Amg || kind == Pc::Nn) {
+        if ((rc = prepare_multigrid(h, kind, res.ms_setup))) {
+            if (rc != MH_FELL_BACK) return rc;
             kind = Pc::Cheb;  // the polynomial preconditioner needs no setup
             res.fell_back = 1;
         }
@@ -1009,18 +1081,23 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
 int ensure_train(mh_handle *h, int n_pairs) {
     const int64_t nr = h->sys.n_rows;
     if (!h->tr_ready) {
-        mh::NnTrainBuffers &b = h->tr;
-        for (auto &v : b.h) v = dalloc<float4>(h, nr);
-        for (auto &v : b.a) v = dalloc<float4>(h, nr);
-        for (auto &v : b.g) v = dalloc<float4>(h, nr);
-        b.ga = dalloc<float4>(h, nr);
-        b.z = dalloc<float>(h, nr);
-        h->pair_acc = dalloc<double>(h, 2);
-        for (auto v : b.h)
-            if (!v) return MH_ERR_NOMEM;
-        for (auto v : b.a)
-            if (!v) return MH_ERR_NOMEM;
-        if (!b.g[0] || !b.g[1] || !b.ga || !b.z || !h->pair_acc) return MH_ERR_NOMEM;
+        const size_t big = (size_t)nr * mh::kSnW;
+        bool ok = true;
+        for (auto &v : h->sn_tr.h) ok &= (v = dalloc<float>(h, big)) != nullptr;
+        for (auto &v : h->sn_tr.a) ok &= (v = dalloc<float>(h, big)) != nullptr;
+        for (auto &v : h->sn_tr.u) ok &= (v = dalloc<float>(h, big)) != nullptr;
+        ok &= (h->sn_tr.u0 = dalloc<float>(h, big)) != nullptr;
+        ok &= (h->sn_tr.z = dalloc<float>(h, nr)) != nullptr;
+        ok &= (h->sn_sc.dz = dalloc<float>(h, nr)) != nullptr;
+        ok &= (h->sn_sc.dh = dalloc<float>(h, big)) != nullptr;
+        ok &= (h->sn_sc.du = dalloc<float>(h, big)) != nullptr;
+        ok &= (h->sn_sc.da = dalloc<float>(h, big)) != nullptr;
+        ok &= (h->sn_sc.part = dalloc<float>(h, (size_t)mh::kSnWgradBlocks * (mh::kSnW * 2 * mh::kSnW + mh::kSnW))) !=
+              nullptr;
+        for (auto &v : h->tv) ok &= (v = dalloc<float>(h, nr)) != nullptr;
+        ok &= (h->tdot = dalloc<double>(h, 256)) != nullptr;
+        ok &= (h->pair_acc = dalloc<double>(h, 2)) != nullptr;
+        if (!ok) return MH_ERR_NOMEM;
         h->tr_ready = true;
     }
     if (h->pair_cap < n_pairs) {
@@ -1032,29 +1109,92 @@ int ensure_train(mh_handle *h, int n_pairs) {
     return MH_OK;
 }
 
-// One forward/backward pass over pair k of the pair storage: grad (zeroed first) and the
-// pair's loss added to d_loss.
-int train_pass(mh_handle *h, int k, double er) {
-    const int64_t nr = h->sys.n_rows;
-    CK(cudaMemsetAsync(h->nn_grad, 0, mh::kNnParams * sizeof(float), h->stream));
-    CK(mh::launch_nn_train_pair(h->sys, h->nn_w, h->pair_r + (size_t)k * nr, h->pair_e + (size_t)k * nr, er, h->tr,
-                                h->nn_grad, h->d_loss, h->stream));
-    h->n_launch += 3 + 2 * mh::kNnLayers + 2 * mh::kNnLayers;
-    return MH_OK;
+// Multigrid options of training: the cycle without the energy-optimal coarse scaling (so that
+// it is linear in the residual and its adjoint exact) and with FP32 fine values (those of the
+// adjoint's products)
+mh::AmgOptions training_amg_options() {
+    mh::AmgOptions o = amg_options();
+    o.kcycle = 0;
+    o.half_fine = 0;
+    return o;
 }
 
-int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st) {
+// One training evaluation on pair k (r, e in the solver rows, e'S^e = er): the network gives the
+// smoother weights w; M is the V-cycle with them; the loss is L = (x3 - e)' S^ (x3 - e) / er for
+// x3 = M r, and dw = dL/dw comes from the cycle's adjoint.  With the cycle
+//   x1 = Q r,  x2 = x1 + P B P' (r - S^ x1),  x3 = x2 + Q (r - S^ x2),   Q = a0 W + a1 W S^ W,
+// g = 2 S^ (x3 - e) / er, u = g - S^ Q g, hh = u - S^ P B P' u and r2 = r - S^ x2:
+//   dL/dw_i = a0 (g_i r2_i + hh_i r_i) + a1 (g_i (S^W r2)_i + (S^W g)_i r2_i + hh_i (S^W r)_i
+//             + (S^W hh)_i r_i)
+// (the smoothing interval is held fixed: refresh = 1 re-estimates it for the current weights
+// first).  Then grad = dL/dtheta through the network's backward kernels.  The loss goes to *loss
+// (host).  The hierarchy must be the training one (training_amg_options) of this matrix.
+int train_eval(mh_handle *h, const float *r, const float *e, double er, bool refresh, double *loss) {
+    const int64_t nr = h->sys.n_rows;
+    mh::DevSystem &S = h->sys;
+    cudaStream_t st = h->stream;
+    if (h->sn_x_epoch != h->matrix_epoch) {
+        CK(mh::sn_features(S, h->sn_x, st));
+        h->sn_x_epoch = h->matrix_epoch;
+    }
+    CK(mh::sn_forward(S, h->nn_w, h->sn_x, h->sn_tr, h->sn_w, true, st));
+    h->amg.set_fine_weights(h->sn_w);
+    if (refresh) CK(h->amg.refresh_fine(st));
+    else CK(h->amg.update_fine_weights(st));
+    double a0, a1;
+    if (!h->amg.fine_poly(a0, a1)) {
+        h->err = "training needs the degree-2 fine smoother";
+        return MH_ERR_STATE;
+    }
+    float **v = h->tv;
+    float *x1 = v[0], *t1 = v[1], *r1 = v[2], *c = v[3], *x2 = v[4], *r2 = v[5], *x3 = v[6], *d = v[7];
+    float *sd = v[8], *g = v[9], *qg = v[10], *u = v[11], *cu = v[12], *hh = v[13], *swr = v[14], *dw = v[15];
+    CK(h->amg.smooth_fine(r, x1, st));
+    CK(mh::sn_spmv(S, nullptr, x1, t1, st));
+    CK(mh::sn_axpy(nr, r, -1.f, t1, r1, st));
+    CK(h->amg.coarse_correct(r1, c, st));
+    CK(mh::sn_axpy(nr, x1, 1.f, c, x2, st));
+    CK(mh::sn_spmv(S, nullptr, x2, t1, st));
+    CK(mh::sn_axpy(nr, r, -1.f, t1, r2, st));
+    CK(h->amg.smooth_fine(r2, t1, st));
+    CK(mh::sn_axpy(nr, x2, 1.f, t1, x3, st));
+    CK(mh::sn_axpy(nr, x3, -1.f, e, d, st));
+    CK(mh::sn_spmv(S, nullptr, d, sd, st));
+    CK(mh::sn_dot(nr, d, sd, h->tdot, h->tdot + 200, st));
+    CK(mh::sn_axpy(nr, sd, (float)(2.0 / er) - 1.f, sd, g, st));
+    CK(h->amg.smooth_fine(g, qg, st));
+    CK(mh::sn_spmv(S, nullptr, qg, t1, st));
+    CK(mh::sn_axpy(nr, g, -1.f, t1, u, st));
+    CK(h->amg.coarse_correct(u, cu, st));
+    CK(mh::sn_spmv(S, nullptr, cu, t1, st));
+    CK(mh::sn_axpy(nr, u, -1.f, t1, hh, st));
+    // the four products S^ W v (x1, c and t1 are free again)
+    CK(mh::sn_spmv(S, h->amg.fine_smoother_weights_in_effect(), r, swr, st));
+    CK(mh::sn_spmv(S, h->amg.fine_smoother_weights_in_effect(), r2, t1, st));
+    CK(mh::sn_spmv(S, h->amg.fine_smoother_weights_in_effect(), g, x1, st));
+    CK(mh::sn_spmv(S, h->amg.fine_smoother_weights_in_effect(), hh, c, st));
+    CK(cudaMemsetAsync(dw, 0, nr * sizeof(float), st));
+    const int32_t *agg = h->amg.levels() > 1 ? h->amg.level(0).agg.p : nullptr;
+    CK(mh::sn_grad_w(S, (float)a0, (float)a1, g, hh, r, r2, swr, t1, x1, c, agg, 1.f, dw, st));
+    CK(mh::sn_backward(S, h->nn_w, h->sn_x, h->sn_tr, dw, h->nn_grad, h->sn_sc, st));
+    h->n_launch += 40 + 2 * h->amg.levels() * 8;
+    double num = 0.0;
+    CK(cudaMemcpyAsync(&num, h->tdot + 200, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (loss) *loss = num / er;
+    return std::isfinite(num) ? MH_OK : MH_ERR_NONFINITE;
+}
+
+// Training pairs from the plain solver (FP64 PCG): x* to solve_rtol, then snapshots x_s of a
+// rerun from zero at geometrically spaced iterations; pair s = (r_s, e_s = x* - x_s) scaled by
+// 1/|r_s|, stored in pair_r / pair_e; er[s] = e_s'r_s after scaling.
+int make_pairs(mh_handle *h, int np, double solve_rtol, std::vector<double> &er) {
     int rc;
-    const int np = std::max(1, std::min(o.n_pairs, 64));
-    if ((rc = ensure_learned(h)) || (rc = ensure_train(h, np))) return rc;
     const int64_t nr = h->sys.n_rows;
     if (!h->x_star && !(h->x_star = dalloc<double>(h, nr))) return MH_ERR_NOMEM;
-    cudaEvent_t e0 = h->ev[0], e1 = h->ev[1], e2 = h->ev[5];
-    CK(cudaEventRecord(e0, h->stream));
-    // reference solution x* (scaled space)
     mh_solve_opts so;
     mh_solve_opts_default(&so);
-    so.r_tol = o.solve_rtol > 0.0 ? o.solve_rtol : 1e-9;
+    so.r_tol = solve_rtol > 0.0 ? solve_rtol : 1e-9;
     so.iters_per_graph = 16;
     std::fill(h->inst_iters.begin(), h->inst_iters.end(), 0);
     std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
@@ -1066,7 +1206,6 @@ int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st)
         return res.status;
     }
     CK(cudaMemcpyAsync(h->x_star, h->sys.x, nr * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    // snapshots of FP64 PCG from zero at geometrically spaced iterations 0 .. total
     const int total = std::max(1, res.iterations);
     std::vector<int> snap;
     for (int k = 0; k < np; ++k) {
@@ -1077,14 +1216,15 @@ int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st)
     CK(mh::launch_reset_ctl(h->sys, h->stream));
     CK(mh::launch_cg_init(h->sys, so.r_tol * so.r_tol, 0.0, total + 1, 0, h->stream));
     h->n_launch += 1;
-    std::vector<double> er;
-    int it = 0, n_ok = 0;
+    er.clear();
+    int it = 0;
     for (int target : snap) {
         for (; it < target; ++it) {
             CK(mh::launch_cg_iteration(h->sys, 64, h->stream));
             h->n_launch += 2;
         }
-        float *pr = h->pair_r + (size_t)n_ok * nr, *pe = h->pair_e + (size_t)n_ok * nr;
+        const int k = (int)er.size();
+        float *pr = h->pair_r + (size_t)k * nr, *pe = h->pair_e + (size_t)k * nr;
         CK(mh::launch_pair_make(nr, h->x_star, h->sys.x, h->sys.r, pe, pr, h->pair_acc, h->stream));
         double acc[2];
         CK(cudaMemcpyAsync(acc, h->pair_acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream));
@@ -1095,13 +1235,49 @@ int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st)
         CK(mh::launch_pair_scale(nr, pe, pr, (float)sc, h->stream));
         h->n_launch += 1;
         er.push_back(acc[1] * sc * sc);
-        ++n_ok;
     }
-    CK(cudaEventRecord(e1, h->stream));
-    if (n_ok == 0) {
+    if (er.empty()) {
         h->err = "no usable training pair";
         return MH_ERR_STATE;
     }
+    return MH_OK;
+}
+
+// Builds the training hierarchy of the current matrix (the network's inputs need the FP32
+// scaled matrix and its features).
+int training_setup(mh_handle *h) {
+    int rc;
+    if ((rc = ensure_learned(h)) || (rc = nn_weights(h))) return rc;
+    if (h->sys.rows_per_thread != 1) {
+        const int t[2] = {mh::krylov_target_blocks(1, 64), mh::krylov_target_blocks(1, 32)};
+        if ((rc = apply_launch_shape(h, 1, t))) return rc;
+    }
+    h->amg.set_fine_weights(h->sn_w);
+    cudaError_t e = h->amg.setup(h->sys, training_amg_options(), h->stream);
+    h->amg_epoch += 1;
+    h->amg_matrix_epoch = -1;  // the next solve builds the solver's hierarchy again
+    h->amg_training = true;
+    h->tr_hier_epoch = h->matrix_epoch;
+    if (e != cudaSuccess) {
+        h->err = "AMG setup: " + h->amg.err;
+        cudaGetLastError();
+        return MH_ERR_CUDA;
+    }
+    return MH_OK;
+}
+
+int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st) {
+    int rc;
+    const int np = std::max(1, std::min(o.n_pairs, 64));
+    if ((rc = ensure_learned(h)) || (rc = ensure_train(h, np))) return rc;
+    const int64_t nr = h->sys.n_rows;
+    cudaEvent_t e0 = h->ev[0], e1 = h->ev[1], e2 = h->ev[5];
+    CK(cudaEventRecord(e0, h->stream));
+    std::vector<double> er;
+    if ((rc = make_pairs(h, np, o.solve_rtol, er))) return rc;
+    const int n_ok = (int)er.size();
+    CK(cudaEventRecord(e1, h->stream));
+    if ((rc = training_setup(h))) return rc;
     // Adam, one step per pair, pairs shuffled every epoch
     const int epochs = std::max(1, o.epochs);
     const float lr = o.lr > 0.f ? o.lr : 2e-3f;
@@ -1110,27 +1286,22 @@ int learned_train_impl(mh_handle *h, const mh_learn_opts &o, mh_learn_stats &st)
     for (int k = 0; k < n_ok; ++k) order[k] = k;
     for (int ep = 0; ep < epochs; ++ep) {
         std::shuffle(order.begin(), order.end(), rng);
-        CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), h->stream));
+        double sum = 0.0;
         for (int k : order) {
-            if ((rc = train_pass(h, k, er[k]))) return rc;
+            double l = 0.0;
+            if ((rc = train_eval(h, h->pair_r + (size_t)k * nr, h->pair_e + (size_t)k * nr, er[k], true, &l))) {
+                if (rc == MH_ERR_NONFINITE) h->err = "training loss is not finite";
+                return rc;
+            }
+            sum += l;
             h->nn_step += 1;
-            CK(mh::launch_nn_adam(h->nn_w, h->nn_m, h->nn_v, h->nn_grad, h->nn_step, lr, 1.f, o.train_bias,
-                                  h->stream));
+            CK(mh::sn_adam(h->nn_w, h->nn_m, h->nn_v, h->nn_grad, h->nn_step, lr, h->stream));
             h->n_launch += 1;
         }
-        if (ep == 0 || ep == epochs - 1) {
-            double l = 0.0;
-            CK(cudaMemcpyAsync(&l, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            if (!std::isfinite(l)) {
-                h->err = "training loss is not finite";
-                return MH_ERR_NONFINITE;
-            }
-            (ep == 0 ? st.loss_initial : st.loss_final) = l / n_ok;
-        }
+        if (ep == 0) st.loss_initial = sum / n_ok;
+        if (ep == epochs - 1) st.loss_final = sum / n_ok;
     }
-    CK(mh::launch_nn_pack(h->nn_w, h->nn_wb, h->stream));
-    h->n_launch += 1;
+    h->sn_key_step = -1;  // the solver recomputes the weights with the trained network
     CK(cudaEventRecord(e2, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     float ms = 0.f;
@@ -1403,6 +1574,48 @@ int mh_create_batch(const mh_mesh_desc *meshes, int32_t n_inst, mh_handle **out)
         return rc;
     }
     *out = h;
+    return MH_OK;
+}
+
+int mh_smoother_weights_set(mh_handle *h, const float *w, int64_t n) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t ne = h->topo.n_edges();
+    if (!w) {
+        h->user_fine_w = false;
+        return MH_OK;
+    }
+    if (n < ne) return MH_ERR_INVALID;
+    for (int64_t g = 0; g < ne; ++g)
+        if (!(w[g] > 0.f) || !std::isfinite(w[g])) {
+            h->err = "smoother weights must be positive and finite";
+            return MH_ERR_INVALID;
+        }
+    if (!h->d_fine_w && !(h->d_fine_w = dalloc<float>(h, h->sys.n_rows))) return MH_ERR_NOMEM;
+    std::vector<float> rows(h->sys.n_rows, 1.f);
+    for (int64_t g = 0; g < ne; ++g) rows[h->hs.edge_row[g]] = w[g];
+    CK(cudaMemcpyAsync(h->d_fine_w, rows.data(), rows.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->user_fine_w = true;
+    if (h->amg.fine_smoother_weights() == h->d_fine_w) h->amg.set_fine_weights(nullptr);  // new values
+    return MH_OK;
+}
+
+int mh_smoother_weights_get(const mh_handle *hc, float *w, int64_t n) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    const int64_t ne = h->topo.n_edges();
+    if (!w || n < ne) return MH_ERR_INVALID;
+    const float *cur = h->amg.fine_smoother_weights();
+    if (!cur) {
+        std::fill(w, w + ne, 1.f);
+        return MH_OK;
+    }
+    std::vector<float> rows(h->sys.n_rows);
+    CK(cudaMemcpyAsync(rows.data(), cur, rows.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t g = 0; g < ne; ++g) w[g] = rows[h->hs.edge_row[g]];
     return MH_OK;
 }
 
@@ -2153,8 +2366,7 @@ int64_t mh_kernel_launches(const mh_handle *h) { return h ? h->n_launch : 0; }
 int mh_learned_set_weights(mh_handle *h, const float *w, int64_t n) {
     int rc = need_device(h);
     if (rc) return rc;
-    if (!h->assembled && !h->sys.n_rows) return MH_ERR_STATE;
-    if (!w || n != mh::kNnParams) {
+    if (!w || n != mh::kSnParams) {
         h->err = "weights: expected MH_NN_PARAMS floats";
         return MH_ERR_INVALID;
     }
@@ -2164,51 +2376,105 @@ int mh_learned_set_weights(mh_handle *h, const float *w, int64_t n) {
             return MH_ERR_NONFINITE;
         }
     if ((rc = ensure_learned(h))) return rc;
+    h->sn_key_step = -1;  // the next learned solve evaluates the network again
     return nn_upload_weights(h, w);
+}
+
+int mh_learned_reset(mh_handle *h) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if ((rc = ensure_learned(h))) return rc;
+    std::vector<float> w;
+    nn_initial_params(w, 1);
+    h->sn_key_step = -1;
+    return nn_upload_weights(h, w.data());
 }
 
 int mh_learned_get_weights(const mh_handle *hc, float *w, int64_t n) {
     mh_handle *h = const_cast<mh_handle *>(hc);
     int rc = need_device(h);
     if (rc) return rc;
-    if (!w || n != mh::kNnParams) {
+    if (!w || n != mh::kSnParams) {
         h->err = "weights: expected MH_NN_PARAMS floats";
         return MH_ERR_INVALID;
     }
     if ((rc = ensure_learned(h))) return rc;
-    CK(cudaMemcpyAsync(w, h->nn_w, mh::kNnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(w, h->nn_w, mh::kSnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return MH_OK;
 }
 
-int mh_learned_grad(mh_handle *h, const double *r, const double *e, float *grad, double *loss) {
+// a training evaluation of one pair given in edge order (see mh_learned_grad)
+static int learned_eval_pair(mh_handle *h, const double *r, const double *e, bool refresh, double *loss) {
     int rc = need_device(h);
     if (rc) return rc;
     if (!h->assembled) return MH_ERR_STATE;
-    if (!r || !e || !grad) return MH_ERR_INVALID;
+    if (!r || !e) return MH_ERR_INVALID;
     if ((rc = ensure_learned(h)) || (rc = ensure_train(h, 1))) return rc;
     const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
     std::vector<float> rv(nr, 0.f), ev(nr, 0.f);
-    double er = 0.0;
     for (int64_t k = 0; k < ne; ++k) {
         const int64_t row = h->hs.edge_row[k];
         rv[row] = (float)r[k];
         ev[row] = (float)e[k];
-        er += (double)rv[row] * (double)ev[row];
     }
-    if (!(er != 0.0) || !std::isfinite(er)) {
-        h->err = "grad: e.r must be finite and non-zero";
-        return MH_ERR_INVALID;
+    if (!h->amg_training || h->tr_hier_epoch != h->matrix_epoch) {
+        if ((rc = training_setup(h))) return rc;
+        refresh = true;
     }
     CK(cudaMemcpyAsync(h->pair_r, rv.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->pair_e, ev.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->d_loss, 0, sizeof(double), h->stream));
-    if ((rc = train_pass(h, 0, er))) return rc;
-    double l = 0.0;
-    CK(cudaMemcpyAsync(grad, h->nn_grad, mh::kNnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(&l, h->d_loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // e'S^e in FP32 products, as the loss's numerator
+    CK(mh::sn_spmv(h->sys, nullptr, h->pair_e, h->tv[8], h->stream));
+    CK(mh::sn_dot(nr, h->pair_e, h->tv[8], h->tdot, h->tdot + 201, h->stream));
+    double er = 0.0;
+    CK(cudaMemcpyAsync(&er, h->tdot + 201, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (loss) *loss = l;
+    if (!(er > 0.0) || !std::isfinite(er)) {
+        h->err = "grad: e'S^e must be positive and finite";
+        return MH_ERR_INVALID;
+    }
+    return train_eval(h, h->pair_r, h->pair_e, er, refresh, loss);
+}
+
+int mh_learned_grad(mh_handle *h, const double *r, const double *e, float *grad, double *loss) {
+    if (!grad) return MH_ERR_INVALID;
+    int rc = learned_eval_pair(h, r, e, true, loss);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(grad, h->nn_grad, mh::kSnParams * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MH_OK;
+}
+
+int mh_learned_grad_weights(mh_handle *h, const double *r, const double *e, int32_t refresh, float *dw, float *w,
+                            double *loss) {
+    if (!dw && !w && !loss) return MH_ERR_INVALID;
+    int rc = learned_eval_pair(h, r, e, refresh != 0, loss);
+    if (rc) return rc;
+    const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
+    std::vector<float> a(nr), b(nr);
+    CK(cudaMemcpyAsync(a.data(), h->tv[15], nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(b.data(), h->sn_w, nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t k = 0; k < ne; ++k) {
+        if (dw) dw[k] = a[h->hs.edge_row[k]];
+        if (w) w[k] = b[h->hs.edge_row[k]];
+    }
+    return MH_OK;
+}
+
+int mh_learned_smoother(mh_handle *h, float *w, int64_t n) {
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (!h->assembled) return MH_ERR_STATE;
+    const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
+    if (!w || n < ne) return MH_ERR_INVALID;
+    if ((rc = nn_weights(h))) return rc;
+    std::vector<float> a(nr);
+    CK(cudaMemcpyAsync(a.data(), h->sn_w, nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t k = 0; k < ne; ++k) w[k] = a[h->hs.edge_row[k]];
+    h->sn_key_step = -1;
     return MH_OK;
 }
 
@@ -2222,28 +2488,14 @@ int mh_learned_apply(mh_handle *h, const double *r, double *z) {
         const int t[2] = {mh::krylov_target_blocks(1, 64), mh::krylov_target_blocks(1, 32)};
         if ((rc = apply_launch_shape(h, 1, t))) return rc;
     }
+    double ms = 0.0;
+    if ((rc = prepare_multigrid(h, Pc::Nn, ms))) return rc == MH_FELL_BACK ? MH_ERR_CUDA : rc;
     const int64_t nr = h->sys.n_rows, ne = h->topo.n_edges();
-    const int n_inst = h->sys.n_inst;
     std::vector<float> rv(nr, 0.f), zv(nr);
-    std::vector<double> rr(n_inst, 0.0);
-    for (int i = 0; i < n_inst; ++i)
-        for (int64_t k = h->hs.inst_edge[i]; k < h->hs.inst_edge[i + 1]; ++k) {
-            const float v = (float)r[k];
-            rv[h->hs.edge_row[k]] = v;
-            rr[i] += (double)v * (double)v;
-        }
-    // the network reads each instance's |r|^2 and done flag from the Krylov control block
-    std::vector<mh::InstCtl> ctl;
-    if ((rc = read_ctl(h, ctl))) return rc;
-    for (int i = 0; i < n_inst; ++i) {
-        ctl[i].rr = rr[i];
-        ctl[i].done = 0;
-        ctl[i].iter = 0;
-    }
-    CK(cudaMemcpyAsync(h->sys.ctl, ctl.data(), sizeof(mh::InstCtl) * n_inst, cudaMemcpyHostToDevice, h->stream));
+    for (int64_t k = 0; k < ne; ++k) rv[h->hs.edge_row[k]] = (float)r[k];
     CK(cudaMemcpyAsync(h->pair_r, rv.data(), nr * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    CK(mh::launch_nn_apply(h->sys, h->nn_w, h->nn_wb, h->pair_r, h->nn_h0, h->nn_h1, h->pair_e, nullptr, h->stream));
-    h->n_launch += mh::kNnLayers;
+    CK(h->amg.apply(h->pair_r, h->pair_e, nullptr, 0, h->stream));
+    h->n_launch += h->amg.kernels_per_apply();
     CK(cudaMemcpyAsync(zv.data(), h->pair_e, nr * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (int64_t k = 0; k < ne; ++k) z[k] = zv[h->hs.edge_row[k]];

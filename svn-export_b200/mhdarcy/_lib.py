@@ -166,6 +166,14 @@ def _load():
                                    _i32p, _f32p]),
         "mh_learn_opts_default": (None, [C.POINTER(LearnOpts)]),
         "mh_learned_train": (C.c_int, [vp, C.POINTER(LearnOpts), C.POINTER(LearnStats)]),
+        "mh_smoother_weights_set": (C.c_int, [vp, _f32p, C.c_int64]),
+        "mh_learned_grad_weights": (C.c_int, [vp, _f64p, _f64p, C.c_int32, _f32p, _f32p, _f64p]),
+        "mh_learned_smoother": (C.c_int, [vp, _f32p, C.c_int64]),
+        "mh_learned_reset": (C.c_int, [vp]),
+        "mh_smoother_weights_get": (C.c_int, [vp, _f32p, C.c_int64]),
+        "mh_csr_create": (C.c_int, [C.c_int64, _i32p, _i32p, C.POINTER(vp)]),
+        "mh_csr_set_values": (C.c_int, [vp, _f64p, _f64p]),
+        "mh_csr_get_solution": (C.c_int, [vp, _f64p, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -188,9 +196,11 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune",
             "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",
             "mh_amg_info", "mh_amg_level",
-            "mh_learned_train")
+            "mh_learned_train", "mh_smoother_weights_set", "mh_smoother_weights_get",
+            "mh_learned_grad_weights", "mh_learned_smoother", "mh_learned_reset",
+            "mh_csr_create", "mh_csr_set_values", "mh_csr_get_solution")
 
-MH_NN_PARAMS = 1260
+MH_NN_PARAMS = 6561
 
 MH_NOALLOC_MAX_ROWS = 16384 * 256
 

@@ -294,10 +294,28 @@ class MHSystem:
         return (rp, col, val), agg, wt
 
     # ---- learned preconditioner (MH_SOLVER_FCG_LEARNED) ----
+    def smoother_weights(self):
+        """Per-edge weights of the multigrid's fine-level smoother (1 where none are set)."""
+        w = np.zeros(self.n_edges, np.float32)
+        check(lib.mh_smoother_weights_get(self.h, ptr(w, C.c_float), len(w)), self.h)
+        return w
+
+    def set_smoother_weights(self, w):
+        """Fine-level smoother weights per edge (None: plain Jacobi-scaled smoothing)."""
+        if w is None:
+            check(lib.mh_smoother_weights_set(self.h, None, 0), self.h)
+            return
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib.mh_smoother_weights_set(self.h, ptr(w, C.c_float), len(w)), self.h)
+
     def learned_weights(self):
         w = np.zeros(_lib.MH_NN_PARAMS, np.float32)
         check(lib.mh_learned_get_weights(self.h, ptr(w, C.c_float), len(w)), self.h)
         return w
+
+    def reset_learned(self):
+        """The network's initial parameters (smoother weights 1) and a fresh optimiser state."""
+        check(lib.mh_learned_reset(self.h), self.h)
 
     def set_learned_weights(self, w):
         w = np.ascontiguousarray(w, np.float32)
@@ -314,8 +332,27 @@ class MHSystem:
                                   C.byref(loss)), self.h)
         return loss.value, g
 
+    def learned_grad_weights(self, r, e, refresh=True):
+        """Loss, d loss / d smoother weight [n_edges] and the weights [n_edges] of one pair;
+        refresh=False keeps the smoothing interval of the previous evaluation."""
+        r, e = f64(r), f64(e)
+        if len(r) != self.n_edges or len(e) != self.n_edges:
+            raise ValueError("r and e need n_edges entries")
+        dw = np.zeros(self.n_edges, np.float32)
+        w = np.zeros(self.n_edges, np.float32)
+        loss = C.c_double(0.0)
+        check(lib.mh_learned_grad_weights(self.h, ptr(r, C.c_double), ptr(e, C.c_double), int(bool(refresh)),
+                                          ptr(dw, C.c_float), ptr(w, C.c_float), C.byref(loss)), self.h)
+        return loss.value, dw, w
+
+    def learned_smoother(self):
+        """The network's smoother weights [n_edges] for the assembled system."""
+        w = np.zeros(self.n_edges, np.float32)
+        check(lib.mh_learned_smoother(self.h, ptr(w, C.c_float), len(w)), self.h)
+        return w
+
     def learned_apply(self, r):
-        """z = NN(r) [n_edges] through the tensor-core inference kernels."""
+        """z = M r [n_edges]: one V-cycle with the network's smoother weights."""
         r = f64(r)
         if len(r) != self.n_edges:
             raise ValueError("r needs n_edges entries")

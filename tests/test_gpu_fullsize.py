@@ -81,8 +81,10 @@ def test_fp64_solution_within_1e10_of_direct(gpu, name):
         s.set_coeffs(**coeffs)
         s.set_bc(bc["bc_type"], bc.get("pressure"), bc.get("flux"), bc.get("robin_sigma"))
         s.assemble()
+        # 1e-14 is below what FP64 reaches on some of these systems: the solve stops at its
+        # restart cap (status 1) with a residual still far below what 1e-10 needs
         st = s.solve(method=_lib.MH_SOLVER_PCG64, r_tol=1e-14)
-        assert st["status"] == 0, st
+        assert st["status"] == 0 or (st["status"] == _lib.MH_NOT_CONVERGED and st["rel_residual"] <= 1e-12), st
         sol = s.solution()
         ref = O.solve_mh_direct(oracle_problem(mesh, topo, s.n_edges, coeffs, bc))
         ns, ne = s.n_sides, s.n_elements

@@ -1,57 +1,67 @@
-"""Learned preconditioner and flexible CG.
+"""Learned smoother (MH_SOLVER_FCG_LEARNED) and flexible CG.
 
-CPU: the NumPy restatement's gradient against finite differences.  GPU: the inference
-(tensor-core) network and the training kernels (loss, gradient) against that restatement;
-flexible-CG solves with the Chebyshev-Jacobi and the learned preconditioner to tolerance;
-the fallback from a broken network to Chebyshev-Jacobi; and the ablation trained vs
-untrained network on the same system."""
+CPU: the NumPy restatement of the network (oracle/smoother_nn.py): its backward against
+central differences in FP64; the untrained output is w = 1.  GPU: the network's forward
+(tensor-core layers) and its parameter gradient (backward kernels) against that restatement;
+the smoother-weight gradient (the V-cycle's adjoint) against finite differences of the GPU's
+own loss; flexible-CG solves to tolerance; the fallback; and the ablation trained vs untrained
+network on a held-out system (iterations and time)."""
+import time
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
-import learned as NN
 import mhdarcy
+import smoother_nn as SN
 from mhdarcy import _lib
 from mhdarcy.cases import dirichlet_x_bc, make_case
 
 CONVERGED = (0, _lib.MH_FELL_BACK)
 
 
-def random_weights(seed, scale=0.2, bias=True):
-    rng = np.random.default_rng(seed)
-    w = rng.normal(0.0, scale, NN.N_PARAMS).astype(np.float32)
-    if not bias:
-        for l in range(NN.LAYERS):
-            o = l * NN.PER_LAYER
-            w[o + NN.H * 2 * NN.K:o + NN.H * 2 * NN.K + NN.H] = 0.0
-            w[o + NN.PER_LAYER - NN.K:o + NN.PER_LAYER] = 0.0
-    return w
+def random_params(seed, out_scale=0.5):
+    """Random hidden layers (the library's initial scale) and a random output layer."""
+    th = SN.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    th[SN.PARAMS - SN.WIDTH - 1:] = rng.normal(0.0, out_scale, SN.WIDTH + 1).astype(np.float32)
+    th[SN.WIDTH * SN.NFEAT:SN.WIDTH * SN.NFEAT + SN.WIDTH] = rng.normal(0.0, 0.1, SN.WIDTH)  # b0
+    return th
 
 
-def test_oracle_gradient_finite_differences():
-    """loss_and_grad (without bf16 rounding, in FP64) against central differences."""
-    n = 48
-    rng = np.random.default_rng(0)
-    S = sp.diags([-0.45 * np.ones(n - 1), np.ones(n), -0.45 * np.ones(n - 1)], [-1, 0, 1]).tocsr()
-    w = random_weights(3, 0.3).astype(np.float64)
-    r = rng.normal(size=n)
-    e = spla.spsolve(S.tocsc(), r)
-    NN.QUANTIZE = False
-    try:
-        _, g = NN.loss_and_grad(S, r, e, w)
-        gmax = np.abs(g).max()
-        for idx in rng.choice(NN.N_PARAMS, 60, replace=False):
-            h = 1e-6
-            wp, wm = w.copy(), w.copy()
-            wp[idx] += h
-            wm[idx] -= h
-            lp, _ = NN.loss_and_grad(S, r, e, wp)
-            lm, _ = NN.loss_and_grad(S, r, e, wm)
-            fd = (lp - lm) / (2 * h)
-            assert abs(fd - g[idx]) <= 1e-5 * max(abs(g[idx]), 0.05 * gmax), (idx, fd, g[idx])
-    finally:
-        NN.QUANTIZE = True
+def small_scaled(n=4, seed=0):
+    import cases as OC
+    import oracle as O
+    P, *_ = OC.problem(1, n=n, seed=seed)
+    S, r = O.schur2(P)
+    d = 1.0 / np.sqrt(S.diagonal())
+    return (sp.diags(d) @ S @ sp.diags(d)).tocsr()
+
+
+def test_oracle_backward_finite_differences():
+    """backward() of the restatement against central differences of its FP64 forward."""
+    Sh = small_scaled()
+    x, A = SN.features(Sh)
+    th = random_params(3).astype(np.float64)
+    w, acts = SN.forward(th, x, A, exact=True)
+    c = np.random.default_rng(7).normal(size=len(w))
+    g = SN.backward(th, x, A, acts, 2 * c * w)
+    gmax = np.abs(g).max()
+    for idx in np.random.default_rng(1).choice(SN.PARAMS, 40, replace=False):
+        e = 1e-6
+        tp, tm = th.copy(), th.copy()
+        tp[idx] += e
+        tm[idx] -= e
+        fd = (np.sum(c * SN.forward(tp, x, A, True)[0] ** 2) - np.sum(c * SN.forward(tm, x, A, True)[0] ** 2)) / (2 * e)
+        assert abs(fd - g[idx]) <= 1e-6 * max(abs(g[idx]), 1e-3 * gmax), (idx, fd, g[idx])
+
+
+def test_oracle_untrained_output_is_one():
+    Sh = small_scaled()
+    x, A = SN.features(Sh)
+    w, _ = SN.forward(SN.init_params(0), x, A)
+    assert np.all(w == 1.0)
 
 
 def assembled(n, seed=5, cfg=1):
@@ -65,7 +75,7 @@ def assembled(n, seed=5, cfg=1):
 
 
 def scaled_system(s):
-    """The Jacobi-scaled edge system S^ = D^-1/2 S D^-1/2 and b^ = D^-1/2 b."""
+    """The Jacobi-scaled edge system S^ = D^-1/2 S D^-1/2 and b^ = D^-1/2 b (edge order)."""
     rp, col, val, rhs = s.schur_system()
     S = sp.csr_matrix((val, col, rp), shape=(s.n_edges, s.n_edges))
     d = 1.0 / np.sqrt(S.diagonal())
@@ -73,57 +83,106 @@ def scaled_system(s):
     return (D @ S @ D).tocsr(), d * rhs, S, rhs
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("bias", [False, True])
-def test_inference_matches_oracle(gpu, bias):
-    """Tensor-core inference (bf16 mma, fp32 accumulate) against the NumPy forward."""
-    with assembled(4) as s:
-        Sh, _, _, _ = scaled_system(s)
-        S32 = Sh.astype(np.float32).astype(np.float64)
-        w = random_weights(11, bias=bias)
-        s.set_learned_weights(w)
-        assert np.array_equal(s.learned_weights(), w)
-        rng = np.random.default_rng(12)
-        r = rng.normal(size=s.n_edges).astype(np.float32).astype(np.float64)
-        z = s.learned_apply(r)
-        rn = np.sqrt(np.dot(r, r))
-        zref, _, _ = NN.forward(S32, (r / rn).astype(np.float32), w)
-        zref = zref.astype(np.float64) * rn
-        assert np.linalg.norm(z - zref) <= 2e-3 * np.linalg.norm(zref), np.linalg.norm(z - zref) / np.linalg.norm(zref)
+def oracle_inputs(s):
+    """Features and aggregation matrix of the restatement from the GPU's FP32 scaled matrix."""
+    Sh, _, _, _ = scaled_system(s)
+    S32 = sp.csr_matrix(Sh.astype(np.float32))
+    return SN.features(S32)
 
 
 @pytest.mark.gpu
-def test_identity_network_is_jacobi(gpu):
-    """A new handle starts from W2 = b2 = 0: z = r."""
-    with assembled(4) as s:
-        w = s.learned_weights()
-        for l in range(NN.LAYERS):
-            o = l * NN.PER_LAYER + NN.H * 2 * NN.K + NN.H
-            assert np.all(w[o:o + NN.K * NN.H + NN.K] == 0.0)
-        r = np.random.default_rng(1).normal(size=s.n_edges).astype(np.float32).astype(np.float64)
-        z = s.learned_apply(r)
-        assert np.allclose(z, r, rtol=1e-6, atol=1e-6 * np.abs(r).max())
+def test_forward_matches_oracle(gpu):
+    """The network's smoother weights on the GPU (tensor-core layers: bf16 operands, fp32 sums)
+    against the NumPy forward with the same bf16 roundings."""
+    with assembled(6) as s:
+        th = random_params(11)
+        s.set_learned_weights(th)
+        assert np.array_equal(s.learned_weights(), th)
+        w = s.learned_smoother()
+        x, A = oracle_inputs(s)
+        wref, _ = SN.forward(th, x, A)
+        assert w.min() < 0.98 and w.max() > 1.02  # a non-trivial network
+        assert np.abs(w - wref).max() <= 2e-3, np.abs(w - wref).max()
 
 
 @pytest.mark.gpu
-def test_training_gradient_matches_oracle(gpu):
-    """Training forward + backward on the GPU against loss_and_grad (bf16-rounded operands,
-    fp32 sums on both sides; tolerance 1e-3 on the loss, 2e-2 on each layer's gradient)."""
-    with assembled(4) as s:
-        Sh, _, _, _ = scaled_system(s)
-        S32 = Sh.astype(np.float32).astype(np.float64)
-        w = random_weights(7)
-        s.set_learned_weights(w)
-        rng = np.random.default_rng(8)
-        r = rng.normal(size=s.n_edges).astype(np.float32).astype(np.float64)
-        e = spla.spsolve(Sh.tocsc(), r).astype(np.float32).astype(np.float64)
+def test_untrained_network_is_plain_multigrid(gpu):
+    """A new handle's network gives w = 1: the learned method's first solve is the plain
+    multigrid's (same iterations)."""
+    with assembled(8) as s:
+        assert np.all(s.learned_smoother() == 1.0)
+        a = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+        b = s.solve(method=_lib.MH_SOLVER_FCG_LEARNED, r_tol=1e-10)
+        assert a["status"] == 0 and b["status"] == 0 and a["iterations"] == b["iterations"], (a, b)
+
+
+def pair(s, k=30, seed=0):
+    """A solver pair (r, e) of the held-out kind: CG iterate x_k on S^, r = b^ - S^ x_k, e = x* - x_k,
+    scaled by 1/|r| (edge order)."""
+    Sh, bh, _, _ = scaled_system(s)
+    xs = spla.spsolve(Sh.tocsc(), bh)
+    it = [0]
+    snap = {}
+
+    def keep(xk):
+        it[0] += 1
+        if it[0] == k:
+            snap["x"] = xk.copy()
+
+    spla.cg(Sh, bh, rtol=1e-14, maxiter=k, callback=keep)
+    r = bh - Sh @ snap["x"]
+    e = xs - snap["x"]
+    sc = 1.0 / np.linalg.norm(r)
+    return r * sc, e * sc
+
+
+@pytest.mark.gpu
+def test_parameter_gradient_matches_oracle(gpu):
+    """The backward kernels: the GPU's parameter gradient equals the restatement's backward
+    applied to the GPU's smoother-weight gradient dL/dw (tolerance 2e-2 of each layer's norm:
+    bf16 operands, FP32 sums in another order)."""
+    with assembled(6) as s:
+        th = random_params(7)
+        s.set_learned_weights(th)
+        r, e = pair(s)
         loss, g = s.learned_grad(r, e)
-        L, gref = NN.loss_and_grad(S32, r, e, w)
-        assert abs(loss - L) <= 1e-3 * abs(L), (loss, L)
-        for l in range(NN.LAYERS):
-            sl = slice(l * NN.PER_LAYER, (l + 1) * NN.PER_LAYER)
+        loss2, dw, w = s.learned_grad_weights(r, e, refresh=False)
+        assert abs(loss - loss2) <= 1e-6 * abs(loss) and np.abs(dw).max() > 0
+        x, A = oracle_inputs(s)
+        wref, acts = SN.forward(th, x, A)
+        assert np.abs(w - wref).max() <= 2e-3
+        gref = SN.backward(th, x, A, acts, dw)
+        o = 0
+        blocks = [SN.WIDTH * SN.NFEAT + SN.WIDTH] + [SN.WIDTH * 2 * SN.WIDTH + SN.WIDTH] * SN.LAYERS + [SN.WIDTH + 1]
+        for b in blocks:
+            sl = slice(o, o + b)
             err = np.linalg.norm(g[sl] - gref[sl])
-            assert err <= 2e-2 * np.linalg.norm(gref[sl]), (l, err, np.linalg.norm(gref[sl]))
+            assert err <= 2e-2 * np.linalg.norm(gref[sl]) + 1e-30, (o, err, np.linalg.norm(gref[sl]))
+            o += b
+
+
+@pytest.mark.gpu
+def test_smoother_weight_gradient_finite_differences(gpu):
+    """dL/dw from the V-cycle's adjoint against central differences of the GPU loss along
+    parameter directions (the smoothing interval held fixed, as the gradient assumes):
+    the output bias (every weight moves), an output weight and a hidden weight."""
+    with assembled(6) as s:
+        th = random_params(5)
+        s.set_learned_weights(th)
+        r, e = pair(s)
+        loss, g = s.learned_grad(r, e)
+        s.learned_grad_weights(r, e, refresh=True)  # the interval of the base point
+        for idx, eps in ((SN.PARAMS - 1, 2e-2), (SN.PARAMS - 7, 2e-2), (SN.WIDTH * SN.NFEAT + 3, 2e-2)):
+            tp, tm = th.copy(), th.copy()
+            tp[idx] += eps
+            tm[idx] -= eps
+            s.set_learned_weights(tp)
+            lp = s.learned_grad_weights(r, e, refresh=False)[0]
+            s.set_learned_weights(tm)
+            lm = s.learned_grad_weights(r, e, refresh=False)[0]
+            fd = (lp - lm) / (2 * eps)
+            assert abs(fd - g[idx]) <= 3e-2 * abs(g[idx]) + 1e-4 * abs(loss), (idx, fd, g[idx], loss)
+        s.set_learned_weights(th)
 
 
 def check_solution(s, st, r_tol):
@@ -142,6 +201,8 @@ def check_solution(s, st, r_tol):
 @pytest.mark.parametrize("method", [_lib.MH_SOLVER_CHEB, _lib.MH_SOLVER_FCG_LEARNED])
 def test_fcg_solves_to_tolerance(gpu, method):
     with assembled(8) as s:
+        if method == _lib.MH_SOLVER_FCG_LEARNED:
+            s.set_learned_weights(random_params(9, out_scale=0.3))
         st = s.solve(method=method, r_tol=1e-10, cheb_degree=4)
         assert st["status"] == 0 and st["fell_back"] == 0, st
         lam, S, rhs = check_solution(s, st, 1e-10)
@@ -153,60 +214,39 @@ def test_fcg_solves_to_tolerance(gpu, method):
 
 
 @pytest.mark.gpu
-def test_broken_network_falls_back(gpu):
-    """Weights whose output overflows to Inf/NaN: the flexible iteration breaks down, the
-    solve continues with Chebyshev-Jacobi and still converges (status MH_FELL_BACK)."""
-    with assembled(6) as s:
-        w = np.full(NN.N_PARAMS, 1e30, np.float32)
-        s.set_learned_weights(w)
-        st = s.solve(method=_lib.MH_SOLVER_FCG_LEARNED, r_tol=1e-10)
+def test_stalled_learned_solve_falls_back(gpu):
+    """A learned segment that uses up its inner iterations hands the solve to Chebyshev-Jacobi,
+    which finishes it (status MH_FELL_BACK, the residual criterion met)."""
+    with assembled(8) as s:
+        st = s.solve(method=_lib.MH_SOLVER_FCG_LEARNED, r_tol=1e-10, inner_rtol=1e-12, inner_max_it=2)
         assert st["status"] == _lib.MH_FELL_BACK and st["fell_back"] == 1, st
         check_solution(s, st, 1e-10)
-        assert np.all(s.instance_stats()["status"] == 0)
+
+
+def timed_solves(s, method, reps=5):
+    best, it = 1e30, None
+    for _ in range(reps):
+        s.assemble()
+        st = s.solve(method=method, r_tol=1e-10)
+        assert st["status"] in CONVERGED, st
+        best = min(best, st["ms_solve"])
+        it = st["iterations"]
+    return it, best
 
 
 @pytest.mark.gpu
 def test_training_ablation(gpu):
-    """Train on one system, evaluate on another of the same family (other seed).  Ablation of
-    the training: on the held-out system's own right-hand side the trained network's
-    energy-norm error is below the untrained (identity, i.e. Jacobi) network's.  Both networks
-    precondition flexible CG to tolerance.  The iteration counts are printed, not compared: the
-    trained network is nonlinear in r, which costs flexible CG the conjugacy that the linear
-    Jacobi preconditioner keeps, and on these systems it needs more iterations."""
-    with assembled(12, seed=21) as s:
-        st = s.learned_train(n_pairs=12, epochs=60, lr=2e-3)
-        assert st["n_pairs"] >= 8 and st["loss_final"] < 0.95 * st["loss_initial"], st
-        w = s.learned_weights()
-    with assembled(12, seed=22) as s:
-        # held-out pairs made like the training pairs: iterates x_k of CG on S^ (unit diagonal,
-        # so Jacobi-PCG), r = b^ - S^ x_k, e = x* - x_k
-        Sh, bh, _, _ = scaled_system(s)
-        xs = spla.spsolve(Sh.tocsc(), bh)
-        snaps = {}
-        it = [0]
-
-        def keep(xk):
-            it[0] += 1
-            if it[0] in (25, 100, 400):
-                snaps[it[0]] = xk.copy()
-
-        spla.cg(Sh, bh, rtol=1e-14, maxiter=400, callback=keep)
-        pairs = []
-        for k in sorted(snaps):
-            r = bh - Sh @ snaps[k]
-            e = xs - snaps[k]
-            sc = 1.0 / np.linalg.norm(r)
-            pairs.append(((r * sc).astype(np.float32).astype(np.float64), (e * sc).astype(np.float32).astype(np.float64)))
-        assert len(pairs) == 3
-        loss_id = np.mean([s.learned_grad(r, e)[0] for r, e in pairs])
-        base = s.solve(method=_lib.MH_SOLVER_FCG_LEARNED, r_tol=1e-10)
-        assert base["status"] == 0, base
-        check_solution(s, base, 1e-10)
-        s.set_learned_weights(w)
-        loss_tr = np.mean([s.learned_grad(r, e)[0] for r, e in pairs])
-        tr = s.solve(method=_lib.MH_SOLVER_FCG_LEARNED, r_tol=1e-10)
-        assert tr["status"] in CONVERGED, tr
-        check_solution(s, tr, 1e-10)
-        print(f"ablation: held-out loss identity {loss_id:.4f}, trained {loss_tr:.4f}; FCG iterations "
-              f"identity {base['iterations']}, trained {tr['iterations']}")
-        assert loss_tr < loss_id, (loss_tr, loss_id)
+    """Train on one system, evaluate on another of the same family (other seed, larger): the
+    trained network's learned multigrid needs fewer iterations and less solve time than the
+    untrained network (w = 1, i.e. the plain multigrid), and both reach the tolerance."""
+    with assembled(16, seed=21, cfg=5) as s:
+        st = s.learned_train(n_pairs=12, epochs=30, lr=2e-3)
+        assert st["n_pairs"] >= 8 and st["loss_final"] < st["loss_initial"], st
+        th = s.learned_weights()
+    with assembled(32, seed=22, cfg=5) as s:
+        it0, ms0 = timed_solves(s, _lib.MH_SOLVER_FCG_LEARNED)  # untrained: w = 1
+        s.set_learned_weights(th)
+        it1, ms1 = timed_solves(s, _lib.MH_SOLVER_FCG_LEARNED)
+        check_solution(s, None, 1e-10)
+        print(f"ablation: iterations untrained {it0}, trained {it1}; ms untrained {ms0:.2f}, trained {ms1:.2f}")
+        assert it1 < it0 and ms1 < ms0, (it0, it1, ms0, ms1)
