@@ -339,6 +339,33 @@ int mh_get_instance_offsets(const mh_handle *h, int64_t *el_off, int64_t *side_o
  * residual, status (0 converged, 1 not converged, < 0 breakdown).  Arrays of n_inst. */
 int mh_get_instance_stats(const mh_handle *h, int32_t *iterations, double *rel_residual, int32_t *status);
 
+/* ---- mortar coupling of non-matching 1D and 2D elements ---------------------------------- */
+/* The reference couples a 1D element to 2D elements that do not share its nodes through the
+ * intersections read from its neighbouring file (Mesh::read_intersections, src/mesh/mesh.cc:
+ * 703-755) with mortar_method P0 (coupling_P0_mortar_assembly, src/flow/darcy_flow_mh.cc:
+ * 698-799) or P1 (mh_abstract_assembly_intersection, :815-937), with the coefficient
+ * mortar_sigma.  Intersection k: the 1D master element master[k], the 2D slave element
+ * slave[k] (element indices), and its two points X, Y given by their local coordinates on the
+ * master, master_t[2k] and [2k+1] (0 and 1 at the line's nodes 0 and 1), and on the slave,
+ * slave_xy[4k], [4k+1] for X and [4k+2], [4k+3] for Y (t0, t1 with nodes 0, 1, 2 at (0,0),
+ * (1,0), (0,1)), as in the file's intersection points. */
+#define MH_MORTAR_NONE 0
+#define MH_MORTAR_P0   1
+#define MH_MORTAR_P1   2
+typedef struct mh_mortar_desc {
+    int32_t        method;    /* MH_MORTAR_*                                               */
+    double         sigma;     /* mortar_sigma                                              */
+    int64_t        n;         /* intersections                                             */
+    const int32_t *master;    /* [n]                                                       */
+    const int32_t *slave;     /* [n]                                                       */
+    const double  *master_t;  /* [2n]                                                      */
+    const double  *slave_xy;  /* [4n]                                                      */
+} mh_mortar_desc;
+/* mh_create with the mortar blocks of the intersections added to the edge system at every
+ * assembly (their pattern is part of the layout).  MH_ERR_INVALID for a pair that is not
+ * (1D master, 2D slave) or an index out of range. */
+int mh_create_mortar(const mh_mesh_desc *mesh, const mh_mortar_desc *mortar, mh_handle **out);
+
 /* Autotuner: times `iterations` FP64 and FP32 CG iterations on the assembled system for
  * every launch shape (rows per thread R in {1, 2, 4}, blocks per SM from the occupancy of
  * that R's SpMV kernels) and keeps the fastest.  Writes the chosen R and the FP32 and FP64

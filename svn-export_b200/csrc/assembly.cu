@@ -200,10 +200,19 @@ cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mod
     return cudaGetLastError();
 }
 
+// constant additions (mortar coupling): one thread per slot, each slot once
+__global__ void k_add_slots(int64_t n, const int32_t *__restrict__ slot, const double *__restrict__ v,
+                            double *__restrict__ val) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) val[slot[k]] += v[k];
+}
+
 cudaError_t launch_gather(const DevAssembly &a, const DevSystem &sys, int mode, cudaStream_t s) {
     k1_gather<<<blocks_for(sys.n_rows, 256), 256, 0, s>>>(sys.n_rows, sys.slice_off, sys.row_edge, a.slot_cstart,
                                                            a.slot_cidx, a.blk, a.row_cstart, a.row_cidx, a.rhs_loc,
                                                            sys.val_raw, sys.b, mode);
+    if ((mode & 1) && a.n_add > 0)
+        k_add_slots<<<blocks_for(a.n_add, 256), 256, 0, s>>>(a.n_add, a.add_slot, a.add_val, sys.val_raw);
     return cudaGetLastError();
 }
 

@@ -94,6 +94,9 @@ struct DevAssembly {
     int32_t *dim_list[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t dim_count[4] = {0, 0, 0, 0};
     int32_t *status = nullptr;       // bit 0: singular local matrix, bit 1: non-finite value
+    int64_t n_add = 0;               // constant additions to the edge system (mortar terms)
+    int32_t *add_slot = nullptr;
+    double *add_val = nullptr;
 };
 
 // ---- launchers (assembly.cu) ----

@@ -237,6 +237,8 @@ int device_setup(mh_handle *h) {
         a.dim_count[dd] = (int64_t)hs.dim_list[dd].size();
         if ((rc = upload(h, a.dim_list[dd], hs.dim_list[dd]))) return rc;
     }
+    a.n_add = (int64_t)hs.add_slot.size();
+    if (a.n_add > 0 && ((rc = upload(h, a.add_slot, hs.add_slot)) || (rc = upload(h, a.add_val, hs.add_val)))) return rc;
     a.blk = dalloc<double>(h, hs.n_blk);
     a.rhs_loc = dalloc<double>(h, hs.n_rhs_loc);
     a.status = dalloc<int32_t>(h, 1);
@@ -1508,7 +1510,7 @@ void append_mesh(mh::MeshData &m, const mh_mesh_desc *md) {
 
 // Topology, edge-system layout and device set-up for a mesh whose instances own the element
 // ranges inst_el (one instance: {0, n_el}).
-int create_impl(mh_handle *h, const std::vector<int64_t> &inst) {
+int create_impl(mh_handle *h, const std::vector<int64_t> &inst, const mh_mortar_desc *mortar = nullptr) {
     mh::MeshData &m = h->mesh;
     if (!check_finite(m.xyz.data(), (int64_t)m.xyz.size())) return MH_ERR_NONFINITE;
     int rc = mh::build_topology(m, h->topo, &h->err);
@@ -1528,7 +1530,9 @@ int create_impl(mh_handle *h, const std::vector<int64_t> &inst) {
         if (v == 1 || v == 2 || v == 4) rpt = v;
     }
     const int targets[2] = {mh::krylov_target_blocks(rpt, 64), mh::krylov_target_blocks(rpt, 32)};
-    rc = mh::build_host_system(m, h->topo, inst, rpt, targets, h->hs, &h->err);
+    mh::ExtraBlocks extra;
+    if (mortar && (rc = mh::mortar_blocks(m, h->topo, *mortar, extra, &h->err))) return rc;
+    rc = mh::build_host_system(m, h->topo, inst, rpt, targets, h->hs, &h->err, extra.edges.empty() ? nullptr : &extra);
     if (rc) return rc;
     const int n_inst = (int)inst.size() - 1;
     h->inst_iters.assign(n_inst, 0);
@@ -1548,6 +1552,21 @@ int mh_create(const mh_mesh_desc *md, mh_handle **out) {
     if (!h) return MH_ERR_NOMEM;
     append_mesh(h->mesh, md);
     int rc = create_impl(h, {0, h->mesh.n_el});
+    if (rc) {
+        mh_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return MH_OK;
+}
+
+int mh_create_mortar(const mh_mesh_desc *md, const mh_mortar_desc *mortar, mh_handle **out) {
+    if (!out || !desc_valid(md) || !mortar) return MH_ERR_INVALID;
+    *out = nullptr;
+    auto *h = new (std::nothrow) mh_handle();
+    if (!h) return MH_ERR_NOMEM;
+    append_mesh(h->mesh, md);
+    int rc = create_impl(h, {0, h->mesh.n_el}, mortar);
     if (rc) {
         mh_destroy(h);
         return rc;

@@ -53,7 +53,8 @@ void set_launch_shape(HostSystem &hs, int rows_per_thread, const int target_bloc
 }
 
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
-                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err) {
+                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err,
+                      const ExtraBlocks *extra) {
     char msg[256];
     hs = HostSystem();
     hs.inst_el = inst_el;
@@ -163,6 +164,9 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
     }
     for (int64_t r = 0; r < hs.n_rows; ++r)
         if (hs.row_edge[r] < 0) cnt[r + 1] += 1;
+    if (extra)
+        for (const auto &g : extra->edges)
+            for (int32_t a : g) cnt[hs.edge_row[a] + 1] += (int64_t)g.size();
     for (int64_t r = 0; r < hs.n_rows; ++r) cnt[r + 1] += cnt[r];
     std::vector<int32_t> raw(cnt[hs.n_rows]);
     {
@@ -184,6 +188,12 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
         }
         for (int64_t r = 0; r < hs.n_rows; ++r)
             if (hs.row_edge[r] < 0) raw[fill[r]++] = (int32_t)r;
+        if (extra)
+            for (const auto &g : extra->edges)
+                for (int32_t a : g) {
+                    const int64_t ra = hs.edge_row[a];
+                    for (int32_t b : g) raw[fill[ra]++] = hs.edge_row[b];
+                }
     }
     hs.row_ptr.assign(hs.n_rows + 1, 0);
     std::vector<int64_t> len(hs.n_rows);
@@ -233,6 +243,26 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
         int64_t j = std::lower_bound(b, e, c) - b;
         return hs.slice_off[r / kSliceRowsHost] + j * kSliceRowsHost + r % kSliceRowsHost;
     };
+
+    // the extra blocks' values summed per slot in group order (the host does it once)
+    if (extra) {
+        std::vector<std::pair<int32_t, double>> sv;
+        for (size_t k = 0; k < extra->edges.size(); ++k) {
+            const auto &g = extra->edges[k];
+            const size_t q = g.size();
+            for (size_t a = 0; a < q; ++a)
+                for (size_t b = 0; b < q; ++b)
+                    sv.push_back({(int32_t)slot_of(hs.edge_row[g[a]], hs.edge_row[g[b]]), extra->vals[k][a * q + b]});
+        }
+        std::stable_sort(sv.begin(), sv.end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+        for (const auto &e : sv) {
+            if (hs.add_slot.empty() || hs.add_slot.back() != e.first) {
+                hs.add_slot.push_back(e.first);
+                hs.add_val.push_back(0.0);
+            }
+            hs.add_val.back() += e.second;
+        }
+    }
 
     // contributions: element blocks -> slots, element rhs -> rows, in element order (the
     // device sums each slot's contributions in list order).  The slot of every block entry

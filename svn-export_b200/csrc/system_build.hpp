@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "mh_darcy.h"
 #include "topology.hpp"
 
 namespace mh {
@@ -38,13 +39,25 @@ struct HostSystem {
     std::vector<int32_t> row_cstart, row_cidx;
     std::vector<int32_t> dim_list[4];
     std::vector<int32_t> csr_slot;       // general systems: SELL slot of every CSR entry
+    // constant additions to the edge system (mortar coupling): slots and summed values
+    std::vector<int32_t> add_slot;
+    std::vector<double> add_val;
+};
+
+// Constant couplings added to the edge system besides the element blocks (the mortar terms of
+// non-matching lower-dimensional elements): each group is a set of edges that are coupled
+// pairwise, with the dense |group| x |group| block of values (row-major) to add.
+struct ExtraBlocks {
+    std::vector<std::vector<int32_t>> edges;
+    std::vector<std::vector<double>> vals;
 };
 
 // Local edge list of element e: own side edges then VB-neighbour edges.
 int local_edges(const MeshData &m, const Topology &t, int64_t e, int32_t *out);
 
 int build_host_system(const MeshData &m, const Topology &t, const std::vector<int64_t> &inst_el,
-                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err);
+                      int rows_per_thread, const int target_blocks[2], HostSystem &hs, std::string *err,
+                      const ExtraBlocks *extra = nullptr);
 
 // Layout of a general sparse system given by its CSR pattern (n rows, columns sorted and
 // unique in every row, each row holding its diagonal): one instance, rows = unknowns, padded
@@ -52,6 +65,9 @@ int build_host_system(const MeshData &m, const Topology &t, const std::vector<in
 // slots.  No element contributions.
 int build_host_system_csr(int64_t n, const int32_t *row_ptr, const int32_t *col, int rows_per_thread,
                           const int target_blocks[2], HostSystem &hs, std::string *err);
+
+// The mortar blocks of mh_create_mortar's intersections (mortar.cpp).
+int mortar_blocks(const MeshData &m, const Topology &t, const mh_mortar_desc &d, ExtraBlocks &out, std::string *err);
 
 // Splits every instance's tiles into contiguous runs, one run per block, with about
 // target_blocks blocks in total (at least one per instance) in proportion to instance size.

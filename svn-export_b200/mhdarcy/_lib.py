@@ -46,6 +46,11 @@ class MeshDesc(C.Structure):
                 ("bc_dim", _i32p), ("bc_nodes", _i32p)]
 
 
+class MortarDesc(C.Structure):
+    _fields_ = [("method", C.c_int32), ("sigma", C.c_double), ("n", C.c_int64), ("master", _i32p), ("slave", _i32p),
+                ("master_t", _f64p), ("slave_xy", _f64p)]
+
+
 class GmshInfo(C.Structure):
     _fields_ = [("node_id", _i64p), ("el_id", _i64p), ("el_region", _i32p), ("el_partition", _i32p),
                 ("bc_id", _i64p), ("bc_region", _i32p), ("n_regions", C.c_int32), ("region_id", _i32p),
@@ -172,6 +177,7 @@ def _load():
         "mh_learned_reset": (C.c_int, [vp]),
         "mh_smoother_weights_get": (C.c_int, [vp, _f32p, C.c_int64]),
         "mh_csr_create": (C.c_int, [C.c_int64, _i32p, _i32p, C.POINTER(vp)]),
+        "mh_create_mortar": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(MortarDesc), C.POINTER(vp)]),
         "mh_csr_set_values": (C.c_int, [vp, _f64p, _f64p]),
         "mh_csr_get_solution": (C.c_int, [vp, _f64p, C.c_int64]),
     }
@@ -198,11 +204,12 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_amg_info", "mh_amg_level",
             "mh_learned_train", "mh_smoother_weights_set", "mh_smoother_weights_get",
             "mh_learned_grad_weights", "mh_learned_smoother", "mh_learned_reset",
-            "mh_csr_create", "mh_csr_set_values", "mh_csr_get_solution")
+            "mh_csr_create", "mh_csr_set_values", "mh_csr_get_solution", "mh_create_mortar")
 
 MH_NN_PARAMS = 6561
 
 MH_NOALLOC_MAX_ROWS = 16384 * 256
+MH_MORTAR_NONE, MH_MORTAR_P0, MH_MORTAR_P1 = 0, 1, 2
 
 
 def ptr(a, ctype):

@@ -36,12 +36,19 @@ class MHSystem:
     """One mixed-hybrid Darcy system on the GPU (an mh_handle), or a batch of independent
     systems (see :meth:`batch`) solved together with per-instance convergence."""
 
-    def __init__(self, mesh, _batch=None):
+    def __init__(self, mesh, _batch=None, mortar=None):
+        """mortar: (method, sigma, master, slave, master_t, slave_xy) of mh_create_mortar
+        (see mhdarcy.mortar.plane_intersections), or None."""
         self.mesh = mesh
         h = C.c_void_p()
         if _batch is None:
             d = mesh.desc()
-            check(lib.mh_create(C.byref(d), C.byref(h)))
+            if mortar is None:
+                check(lib.mh_create(C.byref(d), C.byref(h)))
+            else:
+                from .mortar import mortar_desc
+                md, keep = mortar_desc(*mortar)
+                check(lib.mh_create_mortar(C.byref(d), C.byref(md), C.byref(h)))
             self.n_instances = 1
         else:
             descs = (_lib.MeshDesc * len(_batch))(*[m.desc() for m in _batch])
