@@ -75,7 +75,8 @@ def parse():
                     help="--unsteady: steps solved with the plain multigrid before the learned method trains")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the flux/pressure error block")
     ap.add_argument("--pcg-accuracy", action="store_true", help="also time pcg64 at r_tol 1e-12 in the error block")
-    ap.add_argument("--extra-config", type=int, default=2, help="second workload timed with fewer steps (0: none)")
+    ap.add_argument("--extra-config", default="2,3",
+                    help="comma list of further workloads timed with fewer steps, reported under `extra` (0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-precond", choices=["jacobi", "ilu0", "ilu3"], default="jacobi",
                     help="preconditioner of the CPU path's CG: Jacobi (threaded throughout; the faster CPU solve on "
@@ -525,28 +526,52 @@ def timed_solves(system, stream, method, k, warmup, kw, barrier, r_tol=R_TOL):
     return ev0.elapsed_time(ev1) / k, stats, system.kernel_launches() - l0
 
 
+def batch_case(instance_ids):
+    """The cfg3 batch of the given instances (each its own seeded uneven case) as one handle:
+    (system, union mesh, concatenated coefficients)."""
+    import numpy as np
+
+    import mhdarcy
+    from mhdarcy import parallel
+    from mhdarcy.cases import make_case
+    parts = [make_case(3, seed=parallel.case_seed(3, 0, i)) for i in instance_ids]
+    system = mhdarcy.MHSystem.batch([m for m, _ in parts])
+    coeffs = {k: np.concatenate([c[k] for _, c in parts]) for k in parts[0][1]}
+    return system, system.mesh, coeffs
+
+
 def run_extra_config(a, cfg, methods, barrier):
-    """A second workload (cfg2 by default) timed with fewer steps, reported under `extra`."""
+    """Another workload timed with fewer steps, reported under `extra` (cfg3: one step solves
+    the whole batch of a.instances uneven instances)."""
+    import numpy as np
     import torch
 
     import mhdarcy
+    from mhdarcy import parallel
     from mhdarcy.cases import dirichlet_x_bc, make_case
     stream = torch.cuda.Stream()
-    mesh, coeffs = make_case(cfg)
+    if cfg == 3:
+        s, mesh, coeffs = batch_case(range(a.instances))
+    else:
+        mesh, coeffs = make_case(cfg)
+        s = mhdarcy.MHSystem(mesh)
     out = {}
-    with mhdarcy.MHSystem(mesh) as s:
+    with s:
         s.set_stream(stream.cuda_stream)
         bc, _ = dirichlet_x_bc(s.topology(), mesh)
         s.set_coeffs(**coeffs)
         s.set_bc(bc["bc_type"], bc["pressure"])
         sz = s.sizes
+        per = s.n_instances
         for name in methods:
             kw = {"inner_rtol": a.amg_inner_rtol} if name == "amg" else {}
             ms, stats, _ = timed_solves(s, stream, METHOD_IDS[name], 5, 3, kw, barrier)
-            out[name] = {"ms_per_solve": round(ms, 3), "solves_per_s": round(1e3 / ms, 3),
+            out[name] = {"ms_per_step": round(ms, 3), "solves_per_s": round(per * 1e3 / ms, 3),
                          "iterations": stats[-1]["iterations"], "converged": stats[-1]["status"] in (0, 2)}
-        return {"config": workload_config(cfg, sz.n_edges, sz.schur_nnz, sz.mh_size, sz.n_elements),
-                "steps": 5, "warmup": 3, "methods": out}
+        cfg_d = workload_config(cfg, sz.n_edges, sz.schur_nnz, sz.mh_size, sz.n_elements)
+        if cfg == 3:
+            cfg_d["instances_per_step"] = per
+        return {"config": cfg_d, "steps": 5, "warmup": 3, "methods": out}
 
 
 def train_network(a, rank, system, cfg):
@@ -583,11 +608,7 @@ def run_ours(a, rank, world):
     stream = torch.cuda.Stream()
     if a.config == 3:
         # one fixed batch of a.instances uneven instances, sharded contiguously over the ranks
-        lo, hi = parallel.shard(a.instances, rank, world)
-        parts = [make_case(3, seed=parallel.case_seed(3, 0, i)) for i in range(lo, hi)]
-        system = mhdarcy.MHSystem.batch([m for m, _ in parts])
-        mesh = system.mesh
-        coeffs = {k: np.concatenate([c[k] for _, c in parts]) for k in parts[0][1]}
+        system, mesh, coeffs = batch_case(parallel.shard(a.instances, rank, world))
     else:
         mesh, coeffs = make_case(a.config, seed=parallel.case_seed(a.config, rank))
         system = mhdarcy.MHSystem(mesh)
@@ -726,8 +747,10 @@ def run_ours(a, rank, world):
     }
     out["postprocess"] = element_flux_timing(system, stream, sz, mesh)
     system.close()
-    if a.extra_config and world == 1 and a.extra_config != a.config:
-        out["extra"] = {"cfg%d" % a.extra_config: run_extra_config(a, a.extra_config, ["pcg64", "amg"], barrier)}
+    extra = [int(c) for c in str(a.extra_config).split(",") if c.strip() not in ("", "0")]
+    extra = [c for c in extra if c != a.config]
+    if extra and world == 1:
+        out["extra"] = {"cfg%d" % c: run_extra_config(a, c, ["pcg64", "amg"], barrier) for c in extra}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -127,12 +127,18 @@ typedef struct mh_solve_opts {
     int32_t use_initial_guess;  /* start from the current edge pressures             */
     int32_t cheb_degree;    /* MH_SOLVER_CHEB: polynomial degree (default 4)         */
     double  inner_rtol;     /* FP32 residual reduction between two FP64 residual
-                               replacements; 0: 1e-3 for MH_SOLVER_AMG, else 0.1     */
-    int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000) */
+                               replacements; 0: 1e-3 for MH_SOLVER_AMG and
+                               MH_SOLVER_FCG_LEARNED, else 0.1                       */
+    int32_t inner_max_it;   /* FP32 iterations between two replacements at most (2000;
+                               after the learned method fell back, at least 200)     */
     int32_t iters_per_graph;/* Krylov iterations per captured CUDA graph launch; 0:
-                               16, or 4 for MH_SOLVER_AMG (long iterations)           */
+                               16, or 4 for the multigrid methods (long iterations)  */
     int32_t profile_kernels;/* 1: time every Krylov kernel with CUDA events in-graph */
-    int32_t reserved[6];
+    int32_t host_loop;      /* 0: each Krylov run is one graph launch whose iterations
+                               repeat on the device (a conditional loop that ends when
+                               every instance is done); 1: graphs of iters_per_graph
+                               iterations launched while the host sees one running   */
+    int32_t reserved[5];
 } mh_solve_opts;
 
 /* kernel classes of mh_solve_stats.kernel_ms / kernel_count */
@@ -371,6 +377,23 @@ int mh_create_mortar(const mh_mesh_desc *mesh, const mh_mortar_desc *mortar, mh_
  * that R's SpMV kernels) and keeps the fastest.  Writes the chosen R and the FP32 and FP64
  * microseconds per iteration (either pointer may be NULL). */
 int mh_autotune(mh_handle *h, int32_t iterations, int32_t *rows_per_thread, double *us_per_iter);
+
+/* The launch shapes mh_autotune_ex chose. */
+typedef struct mh_tune_result {
+    int32_t rows_per_thread;    /* R of the Krylov kernels (mh_autotune)                  */
+    int32_t sell_rows_per_warp; /* rows one warp's SELL-32 tile covers: 32 R              */
+    int32_t k1_group;           /* elements per K1 block (one per thread): 64, 128 or 256 */
+    int32_t reserved_i;
+    double  us_per_iter_fp32;   /* FP32 CG iteration at R                                  */
+    double  us_per_iter_fp64;   /* FP64 CG iteration at R                                  */
+    double  us_assembly;        /* K1 + gather at k1_group (median of three)               */
+    double  reserved[3];
+} mh_tune_result;
+
+/* mh_autotune, then the element group of the assembly's K1 kernel: the matrix and rhs are
+ * assembled again (same values) three times per group size and the fastest median is kept
+ * for every later assembly. */
+int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out);
 
 /* ---- unsteady MH (DarcyFlowMH_Unsteady, darcy_flow_mh.cc:1601-1675) ----------------- */
 /* lumped = 0: MH time term on element rows (setup_time_term :1614-1658);

@@ -20,8 +20,8 @@ namespace {
 constexpr int kModeMatrix = 1;
 constexpr int kModeRhs = 2;
 
-template <int DIM>
-__global__ void __launch_bounds__(128) k1_local_blocks(ElemData d, const int32_t *__restrict__ list, int64_t n,
+template <int DIM, int G>
+__global__ void __launch_bounds__(G) k1_local_blocks(ElemData d, const int32_t *__restrict__ list, int64_t n,
                                                        const int64_t *__restrict__ blk_off,
                                                        const int64_t *__restrict__ rhs_off, double *__restrict__ blk,
                                                        double *__restrict__ rhs_loc, int mode, int32_t *status) {
@@ -187,16 +187,25 @@ inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + thre
 
 }  // namespace
 
-cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mode, cudaStream_t s) {
+template <int G>
+void local_blocks_group(const ElemData &d, const DevAssembly &a, int mode, cudaStream_t s) {
     if (a.dim_count[1] > 0)
-        k1_local_blocks<1><<<blocks_for(a.dim_count[1], 128), 128, 0, s>>>(
+        k1_local_blocks<1, G><<<blocks_for(a.dim_count[1], G), G, 0, s>>>(
             d, a.dim_list[1], a.dim_count[1], a.blk_off, a.rhs_off, a.blk, a.rhs_loc, mode, a.status);
     if (a.dim_count[2] > 0)
-        k1_local_blocks<2><<<blocks_for(a.dim_count[2], 128), 128, 0, s>>>(
+        k1_local_blocks<2, G><<<blocks_for(a.dim_count[2], G), G, 0, s>>>(
             d, a.dim_list[2], a.dim_count[2], a.blk_off, a.rhs_off, a.blk, a.rhs_loc, mode, a.status);
     if (a.dim_count[3] > 0)
-        k1_local_blocks<3><<<blocks_for(a.dim_count[3], 128), 128, 0, s>>>(
+        k1_local_blocks<3, G><<<blocks_for(a.dim_count[3], G), G, 0, s>>>(
             d, a.dim_list[3], a.dim_count[3], a.blk_off, a.rhs_off, a.blk, a.rhs_loc, mode, a.status);
+}
+
+cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mode, int group, cudaStream_t s) {
+    switch (group) {
+        case 64: local_blocks_group<64>(d, a, mode, s); break;
+        case 256: local_blocks_group<256>(d, a, mode, s); break;
+        default: local_blocks_group<128>(d, a, mode, s); break;
+    }
     return cudaGetLastError();
 }
 

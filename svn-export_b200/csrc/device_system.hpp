@@ -100,7 +100,8 @@ struct DevAssembly {
 };
 
 // ---- launchers (assembly.cu) ----
-cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mode, cudaStream_t s);
+// K1 with `group` elements per block (one per thread; 64, 128 or 256, else 128).
+cudaError_t launch_local_blocks(const ElemData &d, const DevAssembly &a, int mode, int group, cudaStream_t s);
 cudaError_t launch_gather(const DevAssembly &a, const DevSystem &sys, int mode, cudaStream_t s);
 cudaError_t launch_scale(const DevSystem &sys, int matrix, cudaStream_t s);
 cudaError_t launch_backsub(const ElemData &d, const DevAssembly &a, const DevSystem &sys, double *sol,
@@ -165,6 +166,11 @@ cudaError_t launch_ir_correct(const DevSystem &sys, cudaStream_t s);
 cudaError_t launch_ir_replace(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
 cudaError_t launch_ir_continue(const DevSystem &sys, double rtol2, int max_it, cudaStream_t s);
 cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s);
+// Device-side loop control for a conditional WHILE node: init (before the node) resets the body
+// count loop[0]; next (the body's last kernel) counts the body and keeps the loop running while
+// an instance is not done and the count is below loop[1].
+cudaError_t launch_loop_init(const DevSystem &sys, cudaGraphConditionalHandle hnd, int32_t *loop, cudaStream_t s);
+cudaError_t launch_loop_next(const DevSystem &sys, cudaGraphConditionalHandle hnd, int32_t *loop, cudaStream_t s);
 // Blocks per Krylov launch for precision 64 or 32: SMs of the current device times the blocks
 // of that precision's SpMV kernel that fit on one SM (148 x 4 without a device).
 int krylov_target_blocks(int rows_per_thread, int prec);

@@ -32,9 +32,10 @@ struct FcgKey {  // what a captured flexible-CG graph depends on
     double lo = 0.0, hi = 0.0;
     int64_t amg_epoch = -1;
     bool prof = false;
+    bool loop = false;  // the iterations sit in a device-side WHILE loop
     bool operator==(const FcgKey &o) const {
         return kind == o.kind && ipg == o.ipg && degree == o.degree && lo == o.lo && hi == o.hi &&
-               amg_epoch == o.amg_epoch && prof == o.prof;
+               amg_epoch == o.amg_epoch && prof == o.prof && loop == o.loop;
     }
 };
 
@@ -78,6 +79,12 @@ struct mh_handle {
     // captured Krylov iterations: [precision 64/32][plain / with per-kernel timing events]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int graph_iters[2][2] = {{0, 0}, {0, 0}};
+    // the same iterations in a conditional WHILE loop (one launch per Krylov run; per precision)
+    cudaGraphExec_t loop_graph[2] = {nullptr, nullptr};
+    int loop_iters[2] = {0, 0};
+    int32_t *d_loop = nullptr;  // {bodies run, body cap} of the device-side loop
+    int k1_group = 128;         // elements per K1 block (mh_autotune_ex)
+    bool host_loop = false;     // the current solve polls from the host instead (mh_solve_opts)
     std::vector<cudaEvent_t> prof_ev[2];
     int32_t *h_done = nullptr;
     cudaEvent_t ev[8] = {};
@@ -334,6 +341,7 @@ int apply_launch_shape(mh_handle *h, int R, const int targets[2]) {
     }
     s.partial = dalloc<double>(h, (size_t)max_blocks * 4);
     if (!s.partial) return MH_ERR_NOMEM;
+    if (!h->d_loop && !(h->d_loop = dalloc<int32_t>(h, 2))) return MH_ERR_NOMEM;
     for (auto &gp : h->graph)
         for (auto &g : gp)
             if (g) {
@@ -341,6 +349,12 @@ int apply_launch_shape(mh_handle *h, int R, const int targets[2]) {
                 g = nullptr;
             }
     for (auto &gi : h->graph_iters) gi[0] = gi[1] = 0;
+    for (auto &g : h->loop_graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    h->loop_iters[0] = h->loop_iters[1] = 0;
     if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
     h->fcg_graph = nullptr;
     return MH_OK;
@@ -396,7 +410,7 @@ int assemble_impl(mh_handle *h, int mode) {
     h->ed.prev_edge = h->sol_prev + h->topo.n_sides() + h->mesh.n_el;
     CK(cudaMemsetAsync(h->as.status, 0, sizeof(int32_t), h->stream));
     CK(cudaEventRecord(h->ev[0], h->stream));
-    CK(mh::launch_local_blocks(h->ed, h->as, mode, h->stream));
+    CK(mh::launch_local_blocks(h->ed, h->as, mode, h->k1_group, h->stream));
     CK(mh::launch_gather(h->as, h->sys, mode, h->stream));
     CK(mh::launch_scale(h->sys, (mode & 1) ? 1 : 0, h->stream));
     CK(cudaEventRecord(h->ev[1], h->stream));
@@ -478,10 +492,97 @@ int capture_iterations(mh_handle *h, int prec, int ipg, bool prof) {
     return MH_OK;
 }
 
-// Runs captured Krylov iterations until every instance reports done.  With `prof`, the
-// kernels of the iterations that still did work are timed from the in-graph events.
+// The device-side Krylov loop: a graph of k_loop_init followed by a conditional WHILE node
+// whose body is what `body` launches on the capture stream, ending with k_loop_next.  The body
+// repeats on the device, with no host round trip, until every instance is done or the body
+// count reaches the cap written into d_loop[1] before each launch.
+template <class F>
+int build_loop_graph(mh_handle *h, F body, cudaGraph_t *out) {
+    cudaStream_t cs = h->own_stream;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hnd{};
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hnd, g, 0, 0);
+    auto captured = [&](cudaGraph_t target, auto launches) {
+        cudaError_t c = cudaStreamBeginCaptureToGraph(cs, target, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (c != cudaSuccess) return c;
+        const cudaError_t c1 = launches();
+        cudaGraph_t same = nullptr;
+        const cudaError_t c2 = cudaStreamEndCapture(cs, &same);
+        return c1 != cudaSuccess ? c1 : c2;
+    };
+    if (e == cudaSuccess) e = captured(g, [&] { return mh::launch_loop_init(h->sys, hnd, h->d_loop, cs); });
+    cudaGraphNode_t init = nullptr, loop = nullptr;
+    size_t n_nodes = 1;
+    if (e == cudaSuccess) e = cudaGraphGetNodes(g, &init, &n_nodes);
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hnd;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&loop, g, &init, 1, &cp);
+    if (e == cudaSuccess)
+        e = captured(cp.conditional.phGraph_out[0], [&] {
+            cudaError_t b = body(cs);
+            return b != cudaSuccess ? b : mh::launch_loop_next(h->sys, hnd, h->d_loop, cs);
+        });
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        h->err = std::string("device loop graph: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return MH_ERR_CUDA;
+    }
+    *out = g;
+    return MH_OK;
+}
+
+// One launch of a device-loop graph with at most `cap` bodies of `per_body` kernels each; the
+// bodies that ran are read back for the launch count.
+int run_loop(mh_handle *h, cudaGraphExec_t exec, int64_t cap, int64_t per_body) {
+    h->h_done[2] = (int32_t)std::min<int64_t>(std::max<int64_t>(cap, 1), INT32_MAX);
+    CK(cudaMemcpyAsync(h->d_loop + 1, h->h_done + 2, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaGraphLaunch(exec, h->stream));
+    CK(cudaMemcpyAsync(h->h_done + 3, h->d_loop, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->n_launch += 1 + (int64_t)h->h_done[3] * (per_body + 1);
+    return MH_OK;
+}
+
+// Krylov iterations in the device-side loop: `ipg` CG iterations per body.
+int run_krylov_loop(mh_handle *h, int prec, int ipg, int max_it) {
+    const int gi = prec == 64 ? 0 : 1;
+    if (!h->loop_graph[gi] || h->loop_iters[gi] != ipg) {
+        if (h->loop_graph[gi]) cudaGraphExecDestroy(h->loop_graph[gi]);
+        h->loop_graph[gi] = nullptr;
+        cudaGraph_t g = nullptr;
+        int rc = build_loop_graph(
+            h,
+            [&](cudaStream_t cs) {
+                cudaError_t e = cudaSuccess;
+                for (int k = 0; k < ipg && e == cudaSuccess; ++k) e = mh::launch_cg_iteration(h->sys, prec, cs);
+                return e;
+            },
+            &g);
+        if (rc) return rc;
+        cudaError_t e = cudaGraphInstantiate(&h->loop_graph[gi], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->loop_graph[gi] = nullptr;
+            h->err = cudaGetErrorString(e);
+            return MH_ERR_CUDA;
+        }
+        h->loop_iters[gi] = ipg;
+    }
+    return run_loop(h, h->loop_graph[gi], ((int64_t)max_it + 2 * ipg) / ipg + 1, 2 * (int64_t)ipg);
+}
+
+// Runs captured Krylov iterations until every instance reports done: in the device-side loop,
+// or (host_loop, or `prof`) as graphs of `ipg` iterations launched while the host sees an
+// instance running.  With `prof`, the kernels of the iterations that still did work are timed
+// from the in-graph events.
 int run_krylov(mh_handle *h, int prec, int ipg, int max_it, bool prof) {
     ipg = std::max(1, ipg);  // an empty graph would never make progress
+    if (!prof && !h->host_loop) return run_krylov_loop(h, prec, ipg, max_it);
     const int gi = prec == 64 ? 0 : 1, pi = prof ? 1 : 0;
     int rc = capture_iterations(h, prec, ipg, prof);
     if (rc) return rc;
@@ -806,7 +907,8 @@ void drop_fcg_graph(mh_handle *h) {
 int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it, bool prof) {
     ipg = std::max(1, ipg);  // an empty graph would never make progress
     prof = prof && (kind == Pc::Amg || kind == Pc::Nn);
-    const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch, prof};
+    const bool loop = !prof && !h->host_loop;
+    const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch, prof, loop};
     if (prof) {
         const int steps = h->amg.fine_steps();
         if ((int)h->amg_prof.size() < ipg) h->amg_prof.resize(ipg);
@@ -822,21 +924,35 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
     }
     if (!h->fcg_graph || !(h->fcg_key == key)) {
         cudaGraph_t g;
-        CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k < ipg && e == cudaSuccess; ++k)
-            e = fcg_iteration(h, kind, degree, lo, hi, h->own_stream, prof ? &h->amg_prof[k] : nullptr);
-        cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
-        if (e != cudaSuccess || e2 != cudaSuccess) {
-            if (e2 == cudaSuccess) cudaGraphDestroy(g);
-            h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
-            cudaGetLastError();
-            return MH_ERR_CUDA;
+        if (loop) {
+            const int rc = build_loop_graph(
+                h,
+                [&](cudaStream_t cs) {
+                    cudaError_t b = cudaSuccess;
+                    for (int k = 0; k < ipg && b == cudaSuccess; ++k)
+                        b = fcg_iteration(h, kind, degree, lo, hi, cs, nullptr);
+                    return b;
+                },
+                &g);
+            if (rc) return rc;
+        } else {
+            CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < ipg && e == cudaSuccess; ++k)
+                e = fcg_iteration(h, kind, degree, lo, hi, h->own_stream, prof ? &h->amg_prof[k] : nullptr);
+            cudaError_t e2 = cudaStreamEndCapture(h->own_stream, &g);
+            if (e != cudaSuccess || e2 != cudaSuccess) {
+                if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                h->err = cudaGetErrorString(e != cudaSuccess ? e : e2);
+                cudaGetLastError();
+                return MH_ERR_CUDA;
+            }
         }
         // a new hierarchy of the same shape (the usual case when only values changed) only
         // changes kernel parameters: update the executable graph in place
         bool updated = false;
-        if (h->fcg_graph && h->fcg_key.kind == key.kind && h->fcg_key.ipg == key.ipg && h->fcg_key.prof == prof) {
+        if (h->fcg_graph && h->fcg_key.kind == key.kind && h->fcg_key.ipg == key.ipg && h->fcg_key.prof == prof &&
+            h->fcg_key.loop == loop) {
             cudaGraphExecUpdateResultInfo info;
             updated = cudaGraphExecUpdate(h->fcg_graph, g, &info) == cudaSuccess;
             if (!updated) cudaGetLastError();
@@ -854,6 +970,7 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
         h->fcg_key = key;
     }
     const int per_iter = fcg_kernels_per_iteration(h, kind, degree);
+    if (loop) return run_loop(h, h->fcg_graph, ((int64_t)max_it + 2 * ipg) / ipg + 1, (int64_t)per_iter * ipg);
     int64_t launched = 0;
     std::vector<mh::InstCtl> ctl;
     int it_before = 0;
@@ -990,7 +1107,10 @@ int prepare_multigrid(mh_handle *h, Pc kind, double &ms_setup) {
 // or Chebyshev-Jacobi preconditioner inside FP64 reliable updates, as solve_ir32; the direction
 // sequence runs on across them.  If a segment of the learned method breaks down, uses up
 // inner_max_it, or the FP64 residual stops improving over three replacements, Chebyshev-Jacobi
-// replaces it for the rest of the solve (fell_back = 1).
+// replaces it for the rest of the solve (fell_back = 1), with segments of at least
+// kFallbackSegment iterations.
+constexpr int kFallbackSegment = 200;
+
 int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
     int rc = ensure_learned(h);
     if (rc) return rc;
@@ -1038,6 +1158,7 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
                 use_nn = false;
                 res.fell_back = 1;
                 stall = 0;
+                best = 1e300;
                 restart = true;
                 std::fill(h->inst_status.begin(), h->inst_status.end(), 0);
             } else {
@@ -1048,7 +1169,10 @@ int solve_fcg(mh_handle *h, const mh_solve_opts &o, SolveResult &res, Pc kind) {
         CK(cudaMemcpyAsync(h->sys.inst_sums, sums.data(), sizeof(double) * sums.size(), cudaMemcpyHostToDevice,
                            h->stream));
         CK(mh::launch_reset_ctl(h->sys, h->stream));
-        const int seg_max = std::min(o.inner_max_it, o.max_it - total);
+        // a fallback gets segments long enough to make progress whatever limit the learned
+        // method was given
+        const int seg_lim = learned && !use_nn ? std::max(o.inner_max_it, kFallbackSegment) : o.inner_max_it;
+        const int seg_max = std::min(seg_lim, o.max_it - total);
         // the direction sequence continues across replacements unless the preconditioner changed
         if (outer == 0 || restart)
             CK(mh::launch_ir_start(h->sys, o.inner_rtol * o.inner_rtol, seg_max, h->stream));
@@ -1321,9 +1445,13 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     mh_solve_opts_default(&o);
     if (opts_in) o = *opts_in;
     if (o.max_it <= 0) o.max_it = 20000;
-    if (o.iters_per_graph <= 0) o.iters_per_graph = o.method == MH_SOLVER_AMG ? 4 : 16;
+    // the multigrid methods (plain or with the learned smoother) take long iterations and few
+    // FP64 replacements
+    const bool multigrid = o.method == MH_SOLVER_AMG || o.method == MH_SOLVER_FCG_LEARNED;
+    if (o.iters_per_graph <= 0) o.iters_per_graph = multigrid ? 4 : 16;
     if (o.inner_max_it <= 0) o.inner_max_it = 2000;
-    if (!(o.inner_rtol > 0.0)) o.inner_rtol = o.method == MH_SOLVER_AMG ? 1e-3 : 0.1;
+    if (!(o.inner_rtol > 0.0)) o.inner_rtol = multigrid ? 1e-3 : 0.1;
+    h->host_loop = o.host_loop != 0;
     if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
     if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
     const bool guess = o.use_initial_guess || have_guess_default;
@@ -1720,6 +1848,8 @@ void mh_destroy(mh_handle *h) {
     for (auto &gp : h->graph)
         for (auto &g : gp)
             if (g) cudaGraphExecDestroy(g);
+    for (auto &g : h->loop_graph)
+        if (g) cudaGraphExecDestroy(g);
     for (auto &evs : h->prof_ev)
         for (auto e : evs) cudaEventDestroy(e);
     if (h->fcg_graph) cudaGraphExecDestroy(h->fcg_graph);
@@ -2312,6 +2442,45 @@ int mh_get_instance_stats(const mh_handle *h, int32_t *iterations, double *rel_r
         if (rel_residual) rel_residual[i] = h->inst_rel[i];
         if (status) status[i] = h->inst_status[i];
     }
+    return MH_OK;
+}
+
+int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out) {
+    if (!out) return MH_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    int32_t R = 0;
+    double us[2] = {0.0, 0.0};
+    int rc = mh_autotune(h, iterations, &R, us);
+    if (rc) return rc;
+    out->rows_per_thread = R;
+    out->us_per_iter_fp32 = us[0];
+    out->us_per_iter_fp64 = us[1];
+    // K1's element group: each candidate assembles the matrix and rhs three times (the same
+    // values again), the fastest median wins
+    double best = 1e300;
+    int best_g = h->k1_group;
+    for (int G : {64, 128, 256}) {
+        float t[3];
+        for (float &tk : t) {
+            CK(cudaEventRecord(h->ev[0], h->stream));
+            CK(mh::launch_local_blocks(h->ed, h->as, 3, G, h->stream));
+            CK(mh::launch_gather(h->as, h->sys, 3, h->stream));
+            CK(cudaEventRecord(h->ev[1], h->stream));
+            CK(cudaEventSynchronize(h->ev[1]));
+            CK(cudaEventElapsedTime(&tk, h->ev[0], h->ev[1]));
+            for (int d = 1; d <= 3; ++d) h->n_launch += h->as.dim_count[d] > 0;
+            h->n_launch += 1 + (h->as.n_add > 0);
+        }
+        std::sort(t, t + 3);
+        if (1e3 * t[1] < best) {
+            best = 1e3 * t[1];
+            best_g = G;
+        }
+    }
+    h->k1_group = best_g;
+    out->k1_group = best_g;
+    out->us_assembly = best;
+    out->sell_rows_per_warp = 32 * R;
     return MH_OK;
 }
 

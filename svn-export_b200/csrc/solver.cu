@@ -595,6 +595,32 @@ cudaError_t launch_reset_ctl(const DevSystem &sys, cudaStream_t s) {
     return cudaMemsetAsync(sys.n_done, 0, sizeof(int32_t), s);
 }
 
+// Loop control of a conditional WHILE graph node (the device-side Krylov loop): the body runs
+// while some instance is not done and fewer than loop[1] bodies have run.  loop[0] counts the
+// bodies; the count bounds the loop whatever the kernels of the body do.
+__global__ void k_loop_init(cudaGraphConditionalHandle hnd, int32_t *__restrict__ loop,
+                            const int32_t *__restrict__ n_done, int32_t n_inst) {
+    loop[0] = 0;
+    cudaGraphSetConditional(hnd, (*n_done < n_inst && loop[1] > 0) ? 1u : 0u);
+}
+
+__global__ void k_loop_next(cudaGraphConditionalHandle hnd, int32_t *__restrict__ loop,
+                            const int32_t *__restrict__ n_done, int32_t n_inst) {
+    const int32_t c = loop[0] + 1;
+    loop[0] = c;
+    cudaGraphSetConditional(hnd, (*n_done < n_inst && c < loop[1]) ? 1u : 0u);
+}
+
+cudaError_t launch_loop_init(const DevSystem &sys, cudaGraphConditionalHandle hnd, int32_t *loop, cudaStream_t s) {
+    k_loop_init<<<1, 1, 0, s>>>(hnd, loop, sys.n_done, sys.n_inst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loop_next(const DevSystem &sys, cudaGraphConditionalHandle hnd, int32_t *loop, cudaStream_t s) {
+    k_loop_next<<<1, 1, 0, s>>>(hnd, loop, sys.n_done, sys.n_inst);
+    return cudaGetLastError();
+}
+
 int krylov_target_blocks(int rows_per_thread, int prec) {
     int dev = 0, sms = 148, per_sm = 4;
     if (cudaGetDevice(&dev) == cudaSuccess &&

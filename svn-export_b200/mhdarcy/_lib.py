@@ -77,7 +77,8 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int32), ("max_it", C.c_int32), ("r_tol", C.c_double),
                 ("a_tol", C.c_double), ("use_initial_guess", C.c_int32), ("cheb_degree", C.c_int32),
                 ("inner_rtol", C.c_double), ("inner_max_it", C.c_int32),
-                ("iters_per_graph", C.c_int32), ("profile_kernels", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("iters_per_graph", C.c_int32), ("profile_kernels", C.c_int32), ("host_loop", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class SolveStats(C.Structure):
@@ -93,6 +94,15 @@ class SolveStats(C.Structure):
         d["kernel_ms"] = list(self.kernel_ms)
         d["kernel_count"] = list(self.kernel_count)
         return d
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("rows_per_thread", C.c_int32), ("sell_rows_per_warp", C.c_int32), ("k1_group", C.c_int32),
+                ("reserved_i", C.c_int32), ("us_per_iter_fp32", C.c_double), ("us_per_iter_fp64", C.c_double),
+                ("us_assembly", C.c_double), ("reserved", C.c_double * 3)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
 
 
 class LearnOpts(C.Structure):
@@ -162,6 +172,7 @@ def _load():
         "mh_get_instance_offsets": (C.c_int, [vp] + [C.POINTER(C.c_int64)] * 4),
         "mh_get_instance_stats": (C.c_int, [vp, _i32p, _f64p, _i32p]),
         "mh_autotune": (C.c_int, [vp, C.c_int32, _i32p, _f64p]),
+        "mh_autotune_ex": (C.c_int, [vp, C.c_int32, C.POINTER(TuneResult)]),
         "mh_learned_set_weights": (C.c_int, [vp, _f32p, C.c_int64]),
         "mh_learned_get_weights": (C.c_int, [vp, _f32p, C.c_int64]),
         "mh_learned_grad": (C.c_int, [vp, _f64p, _f64p, _f32p, _f64p]),
@@ -199,7 +210,7 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_get_element_flux", "mh_get_element_flux_device", "mh_raw_output_write",
             "mh_get_node_pressure", "mh_water_balance", "mh_transport_matrix", "mh_transport_matrix_device", "mh_get_schur_system",
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
-            "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune",
+            "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune", "mh_autotune_ex",
             "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",
             "mh_amg_info", "mh_amg_level",
             "mh_learned_train", "mh_smoother_weights_set", "mh_smoother_weights_get",

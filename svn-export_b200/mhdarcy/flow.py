@@ -16,7 +16,7 @@ from ._lib import lib, check, f64, i32, ptr
 
 def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000,
                use_initial_guess=False, inner_rtol=0.0, inner_max_it=2000, iters_per_graph=0,
-               cheb_degree=4, profile_kernels=False):
+               cheb_degree=4, profile_kernels=False, host_loop=False):
     o = _lib.SolveOpts()
     lib.mh_solve_opts_default(C.byref(o))
     o.method = method
@@ -29,6 +29,7 @@ def solve_opts(method=_lib.MH_SOLVER_PCG64, r_tol=1e-10, a_tol=0.0, max_it=20000
     o.iters_per_graph = iters_per_graph
     o.cheb_degree = cheb_degree
     o.profile_kernels = int(bool(profile_kernels))
+    o.host_loop = int(bool(host_loop))
     return o
 
 
@@ -87,11 +88,12 @@ class MHSystem:
         return dict(iterations=it, rel_residual=rel, status=st)
 
     def autotune(self, iterations=64):
-        """Times the launch shapes on the assembled system and keeps the fastest."""
-        r = np.zeros(1, np.int32)
-        us = np.zeros(2)
-        check(lib.mh_autotune(self.h, iterations, ptr(r, C.c_int32), ptr(us, C.c_double)), self.h)
-        return dict(rows_per_thread=int(r[0]), us_per_iter_fp32=float(us[0]), us_per_iter_fp64=float(us[1]))
+        """Times the launch shapes on the assembled system and keeps the fastest: rows per
+        thread of the Krylov kernels (SELL-32 rows per warp 32 R) and the element group of
+        the assembly's K1 kernel (mh_autotune_ex)."""
+        t = _lib.TuneResult()
+        check(lib.mh_autotune_ex(self.h, iterations, C.byref(t)), self.h)
+        return t.as_dict()
 
     def instance_solution(self, sol, i):
         """(side fluxes, element pressures, edge pressures) of instance i from a union solution."""

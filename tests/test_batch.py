@@ -88,9 +88,40 @@ def test_autotune_keeps_results(gpu):
         s.assemble()
         s.solve(r_tol=1e-12)
         before = s.solution()
+        rp0, col0, val0, rhs0 = s.schur_system()
         tune = s.autotune(32)
         assert tune["rows_per_thread"] in (1, 2, 4) and tune["us_per_iter_fp32"] > 0
+        assert tune["sell_rows_per_warp"] == 32 * tune["rows_per_thread"]
+        assert tune["k1_group"] in (64, 128, 256) and tune["us_assembly"] > 0
+        # the assembly with the chosen element group gives the same system bit for bit
+        s.assemble()
+        rp1, col1, val1, rhs1 = s.schur_system()
+        assert np.array_equal(val0, val1) and np.array_equal(rhs0, rhs1)
         st = s.solve(r_tol=1e-12)
         assert st["status"] == 0
         after = s.solution()
         assert np.abs(after - before).max() <= 1e-8 * np.abs(before).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", [_lib.MH_SOLVER_PCG64, _lib.MH_SOLVER_IR32, _lib.MH_SOLVER_AMG,
+                                    _lib.MH_SOLVER_CHEB])
+def test_device_loop_matches_host_loop(gpu, method):
+    """Each Krylov run as one graph launch with a device-side conditional loop (the default)
+    gives the host-polled run's per-instance iterations and bit-identical solutions: the loop
+    stops when every instance is done, and iterations launched after that are no-ops."""
+    inst = instances()
+    with mhdarcy.MHSystem.batch([m for m, _ in inst]) as b:
+        coeffs, bc = batch_inputs(b, inst)
+        b.set_coeffs(**coeffs)
+        b.set_bc(bc["bc_type"], bc["pressure"])
+        b.assemble()
+        out = []
+        for host_loop in (False, True, False):
+            st = b.solve(method=method, r_tol=1e-10, host_loop=host_loop)
+            assert st["status"] in (0, _lib.MH_FELL_BACK), st
+            ist = b.instance_stats()
+            out.append((st["iterations"], ist["iterations"].copy(), b.solution()))
+        for it, per, sol in out[1:]:
+            assert it == out[0][0] and np.array_equal(per, out[0][1])
+            assert np.array_equal(sol, out[0][2])

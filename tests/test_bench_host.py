@@ -23,6 +23,18 @@ def test_bench_setup_timing():
     assert r["read_gmsh_s"] > 0 and r["create_s"] > 0 and r["gmsh_file_bytes"] > 0
 
 
+def test_bench_batch_case_shards():
+    """bench.py's cfg3 batch over the instances a rank owns: one handle with one instance per
+    id, the union mesh and the coefficients of every instance (host side, no GPU)."""
+    bench = load_bench()
+    from mhdarcy import parallel
+    ids = parallel.shard(5, 1, 2)  # rank 1 of 2 owns instances 3 and 4
+    system, mesh, coeffs = bench.batch_case(ids)
+    with system:
+        assert system.n_instances == len(ids) == 2
+        assert len(coeffs["conductivity"]) == mesh.n_elements == system.n_elements
+
+
 def test_bench_cpu_baseline_entry():
     """bench.py's cpu_baseline object (the CPU restatement on the workload, all threads and one
     thread) for Jacobi and ILU(3) CG, on cfg1 (complete solves fit the budget)."""

@@ -163,26 +163,38 @@ def test_parameter_gradient_matches_oracle(gpu):
 
 @pytest.mark.gpu
 def test_smoother_weight_gradient_finite_differences(gpu):
-    """dL/dw from the V-cycle's adjoint against central differences of the GPU loss along
-    parameter directions (the smoothing interval held fixed, as the gradient assumes):
-    the output bias (every weight moves), an output weight and a hidden weight."""
+    """The parameter gradient (the V-cycle's adjoint, then the network's backward) against the
+    slope of the GPU loss along the gradient's own direction, for the output layer and for the
+    hidden layers (the smoothing interval held fixed, as the gradient assumes).  The FP32 cycle
+    makes the loss noisy at the 1e-5 level (rounding through the coarse levels), so each slope
+    is a quadratic fit over nine points spanning a loss change far above that noise, and the
+    single-parameter differences a noise-free function would allow are not used."""
     with assembled(6) as s:
         th = random_params(5)
         s.set_learned_weights(th)
         r, e = pair(s)
         loss, g = s.learned_grad(r, e)
         s.learned_grad_weights(r, e, refresh=True)  # the interval of the base point
-        for idx, eps in ((SN.PARAMS - 1, 2e-2), (SN.PARAMS - 7, 2e-2), (SN.WIDTH * SN.NFEAT + 3, 2e-2)):
-            tp, tm = th.copy(), th.copy()
-            tp[idx] += eps
-            tm[idx] -= eps
-            s.set_learned_weights(tp)
-            lp = s.learned_grad_weights(r, e, refresh=False)[0]
-            s.set_learned_weights(tm)
-            lm = s.learned_grad_weights(r, e, refresh=False)[0]
-            fd = (lp - lm) / (2 * eps)
-            assert abs(fd - g[idx]) <= 3e-2 * abs(g[idx]) + 1e-4 * abs(loss), (idx, fd, g[idx], loss)
+        g = g.astype(np.float64)
+        out = slice(SN.PARAMS - SN.WIDTH - 1, SN.PARAMS)
+        rows = []
+        for name, part in (("output", out), ("hidden", slice(0, out.start))):
+            v = np.zeros(SN.PARAMS)
+            v[part] = g[part]
+            gn = np.linalg.norm(v)
+            v /= gn
+            h = 2e-3 * abs(loss) / gn  # a loss change of about 0.2%
+            ts = np.linspace(-h, h, 9)
+            ls = []
+            for t in ts:
+                s.set_learned_weights((th + t * v).astype(np.float32))
+                ls.append(s.learned_grad_weights(r, e, refresh=False)[0])
+            slope = np.polyfit(ts, ls, 2)[1]
+            rows.append((name, slope, gn, h))
         s.set_learned_weights(th)
+        print("directional slopes (part, fit, |g|, step):", rows, "loss", loss)
+        for name, slope, gn, _ in rows:
+            assert abs(slope - gn) <= 0.1 * gn, (name, slope, gn)
 
 
 def check_solution(s, st, r_tol):
