@@ -657,6 +657,19 @@ def run_ours(a, rank, world):
                          "dtype": method_dtype(name, AMG_VALUE_BYTES == 2), "fell_back": stats[-1]["fell_back"]}
         if name == "fcg":
             results[name]["training"] = training
+        if name == "pcg64":
+            # the whole Krylov solve against HBM: per iteration one FP64 SpMV (8 + 4 bytes per
+            # slot, the row pointers, x read and q written) and 11 FP64 vector streams (p, x, r
+            # updates and the Jacobi step), counted once each; assembly and back-substitution
+            # left out (their own kernels, about 0.1% of the time)
+            N, Z = sz.n_edges, sz.schur_nnz
+            b_iter = Z * 12 + 4 * (N + 1) + 16 * N + 88 * N
+            t_k = stats[-1]["ms_solve"] / 1e3
+            gbs = stats[-1]["iterations"] * b_iter / t_k / 1e9
+            pk = (load_json(os.path.join(ROOT, "MEASURED_PEAKS.json")) or {}).get("hbm_gbs") or 6650.0
+            results[name]["hbm_per_solve"] = {
+                "algorithmic_bytes_per_iteration": int(b_iter), "ms_krylov": round(1e3 * t_k, 3),
+                "achieved_gbs": round(gbs, 1), "peak_gbs": pk, "frac": round(gbs / pk, 4)}
     clock_info = clocks.stop() if clocks else None
     best = max((r for r in results if results[r]["converged"]), key=lambda r: results[r]["solves_per_s"])
     rb = results[best]

@@ -476,6 +476,11 @@ int mh_learned_train(mh_handle *h, const mh_learn_opts *opts, mh_learn_stats *st
 /* No counterpart in the reference (PETSc ILU there).  The hierarchy of the last AMG solve:
  * number of levels, real rows and SELL slots per level (arrays of cap entries). */
 int mh_amg_info(const mh_handle *h, int32_t *n_levels, int64_t *rows, int64_t *slots, int32_t cap);
+/* The coarse tail of that hierarchy's V-cycle: the first level of the levels (below the fine
+ * one, each of at most MH_AMG_TAIL rows; the environment variable, default 0: off) that run
+ * as one thread-block cluster launch, and the cluster's CTAs; 0 and 0 when every level runs
+ * its own kernels. */
+int mh_amg_tail(const mh_handle *h, int32_t *level, int32_t *cluster_ctas);
 /* One level of that hierarchy in CSR without zero entries (level 0 = the FP32 Jacobi-scaled
  * edge system in padded solver-row order), its aggregation agg [n] (coarse row of each row,
  * -1: none; not on the last level) and transfer weights [n]: level l+1 is P^T W A_l W P with

@@ -5,9 +5,12 @@
 #include <cmath>
 #include <cstring>
 
+#include <cooperative_groups.h>
 #include <cuda_fp16.h>
 
 #include "amg.hpp"
+
+namespace cg = cooperative_groups;
 
 namespace mh {
 
@@ -34,6 +37,7 @@ template struct DBuf<float>;
 template struct DBuf<double>;
 template struct DBuf<unsigned int>;
 template struct DBuf<uint16_t>;
+template struct DBuf<unsigned char>;
 
 namespace {
 
@@ -1099,7 +1103,7 @@ __global__ void k_prolong(Gate gate, int64_t n, const int32_t *__restrict__ agg,
 // One block per long row (kLongRow): y = (A x)_i by a block reduction, then the epilogue of
 // the thread-per-row kernel it stands in for.  MODE 0: Chebyshev step (k_sm_step), 1: residual
 // (k_residual), 2: the row's terms x_i b_i and x_i (A x)_i of the coarse-correction scaling
-// (k_coarse_dots), written to long_part[2k], [2k+1].
+// (k_coarse_dots), written to long_part[2k], [2k+1], 3: power step D^-1 A x (k_power_step).
 template <int MODE>
 __global__ void __launch_bounds__(256) k_long_rows(Gate gate, MatView A, const int32_t *__restrict__ rows,
                                                    const float *__restrict__ b, const float *__restrict__ invd,
@@ -1131,6 +1135,8 @@ __global__ void __launch_bounds__(256) k_long_rows(Gate gate, MatView A, const i
         out[i] = x_in[i] + dn;
     } else if (MODE == 1) {
         out[i] = b[i] - y;
+    } else if (MODE == 3) {
+        out[i] = invd ? invd[i] * y : y;
     } else {
         long_part[2 * blockIdx.x] = (double)x_in[i] * (double)b[i];
         long_part[2 * blockIdx.x + 1] = (double)x_in[i] * (double)y;
@@ -1219,6 +1225,318 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
         const double num = red[0][0], den = red[1][0];
         *alpha = (den > 0.0 && num > 0.0 && isfinite(num / den)) ? num / den : 1.0;
         *ticket = 0u;
+    }
+}
+
+// ---- the coarse tail of the V-cycle in one cluster launch -----------------------------------
+// The levels below a few thousand rows are latency-bound: each of their kernels does a
+// microsecond of work and costs a launch.  One thread-block cluster runs all of them: the host
+// compiles the tail's part of the cycle into a list of phases (the operations, pointers and
+// coefficients the per-level kernels would get), and the cluster executes the list with a
+// cluster barrier after each phase.  Every phase keeps the per-level kernels' work split and
+// summation order (rows in 32-row slices with G warps each, the 256-thread groups of the long
+// rows and of the scaling's partial sums), so the tail gives the same bits as the separate
+// launches.  Vectors written by one phase are read by later ones through L2 (ld.global.cg);
+// the matrices through the read-only path.
+constexpr int kTailThreads = 1024, kTailWarps = kTailThreads / 32;
+constexpr int kTailGroups = kTailThreads / 256;  // 256-thread groups per CTA
+
+enum TailOp : int32_t {
+    kTailStep = 0,           // Chebyshev step (k_sm_step + k_long_rows<0>)
+    kTailResid = 1,          // residual (k_residual + k_long_rows<1>)
+    kTailRestrict = 2,       // restriction (k_restrict)
+    kTailRestrictFirst = 3,  // restriction and the coarse level's first step (k_restrict_first)
+    kTailFirst = 4,          // first step from zero (k_sm_first)
+    kTailDense = 5,          // dense coarsest solve (k_dense_gemv)
+    kTailDots = 6,           // coarse-correction scaling (k_long_rows<2> + k_coarse_dots)
+    kTailProlong = 7         // prolongation (k_prolong)
+};
+
+struct TailLevel {
+    MatView A;
+    const float *invd;
+    const int32_t *agg;       // coarse row of each row of this level, -1: none
+    const int32_t *ms, *mr;   // rows of each coarse row (restriction from this level)
+    const int32_t *longrows;  // rows longer than kLongRow
+    int64_t nc;               // coarse rows (restriction from this level)
+    int32_t n_long, g;
+};
+
+struct TailPhase {
+    int32_t op, level;   // level: index into the level table (Restrict*: the fine side)
+    int32_t next;        // Restrict*: the coarse side's index
+    int32_t use_alpha;   // Prolong: scale by *alpha (the last Dots), else by alpha_fixed
+    const float *b;      // Step, Resid, First, Dense, Dots: the level's rhs
+    const float *x_in;   // Step, Resid, Dots: x; Prolong: the coarse level's x; Restrict*: r
+    float *x_out;        // Step: new x; Resid: r; First, Dense: x; Prolong: x (+=); Restrict*: b_c
+    float *d;            // Step, First: d; RestrictFirst: the coarse level's d
+    float *x2;           // RestrictFirst: the coarse level's x
+    const float *dense;  // Dense: the inverse (n x n)
+    double *alpha;       // Dots: written; Prolong: read
+    float c1, c2, alpha_fixed;
+    int32_t dense_n;
+};
+
+__device__ __forceinline__ float tail_part(const MatView &A, int64_t i, int g, int G, const float *__restrict__ x) {
+    int64_t base;
+    int w, ln;
+    row_of(A, i, base, w, ln);
+    constexpr int kB = 8;
+    float y = 0.f;
+    for (int j0 = g; j0 < w; j0 += kB * G) {
+        int32_t c[kB];
+        float v[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            const int j = j0 + k * G;
+            const int64_t slot = base + (int64_t)j * kS + ln;
+            c[k] = j < w ? __ldg(A.col + slot) : 0;
+            v[k] = j < w ? __ldg(A.val + slot) : 0.f;
+        }
+        float gx[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) gx[k] = j0 + k * G < w ? __ldcg(x + c[k]) : 0.f;
+#pragma unroll
+        for (int k = 0; k < kB; ++k) y += v[k] * gx[k];
+    }
+    return y;
+}
+
+// Step, Resid or Dots over the regular rows of a level: rounds of 32 warps per CTA, warp gw of
+// the cluster-wide virtual grid taking slice gw / G, part g = gw % G (split_row's mapping);
+// Dots leaves its per-256-thread-group partials (k_coarse_dots' blocks) in part.
+__device__ void tail_rows(const TailPhase &p, const TailLevel &L, int cta, int n_cta, double *__restrict__ part,
+                          float (*sh)[32], double (*shd)[kTailWarps]) {
+    const MatView &A = L.A;
+    const int G = L.g, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t warps_all = (int64_t)n_cta * kTailWarps;
+    const int64_t tasks = A.n / kS * G;  // warps of the per-level launch (split_blocks * 8, rounded up)
+    const int64_t n_vb = (tasks + 7) / 8;
+    for (int64_t r0 = 0; r0 < n_vb * 8; r0 += warps_all) {
+        const int64_t gw = r0 + (int64_t)cta * kTailWarps + warp;
+        const int64_t i = (gw / G) * kS + lane;
+        const int g = (int)(gw % G);
+        const bool outside = p.op == kTailStep && i < A.n && L.agg && L.agg[i] < 0;
+        const bool live = i < A.n && !outside && !is_long(A, i);
+        float y = live ? tail_part(A, i, g, G, p.x_in) : 0.f;
+        if (G > 1) {
+            sh[warp][lane] = y;
+            __syncthreads();
+            float t = 0.f;
+            if (warp % G == 0)
+                for (int k = 0; k < G; ++k) t += sh[warp + k][lane];
+            y = t;
+            __syncthreads();
+        }
+        if (p.op == kTailDots) {
+            double xb = 0.0, xax = 0.0;
+            if (g == 0 && live) {
+                const double xi = (double)__ldcg(p.x_in + i);
+                xb = xi * (double)__ldcg(p.b + i);
+                xax = xi * (double)y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                xb += __shfl_xor_sync(kFull, xb, o);
+                xax += __shfl_xor_sync(kFull, xax, o);
+            }
+            if (lane == 0) {
+                shd[0][warp] = xb;
+                shd[1][warp] = xax;
+            }
+            __syncthreads();
+            if (threadIdx.x < kTailWarps / 8) {  // one thread per group of 8 warps
+                const int64_t vb = (r0 + (int64_t)cta * kTailWarps) / 8 + threadIdx.x;
+                double a = 0.0, c = 0.0;
+                for (int w = 0; w < 8; ++w) {
+                    a += shd[0][threadIdx.x * 8 + w];
+                    c += shd[1][threadIdx.x * 8 + w];
+                }
+                if (vb < n_vb) {
+                    __stcg(part + 2 * vb, a);
+                    __stcg(part + 2 * vb + 1, c);
+                }
+            }
+            __syncthreads();
+            continue;
+        }
+        if (g != 0 || i >= A.n) continue;
+        if (p.op == kTailResid) {
+            if (live) p.x_out[i] = __ldcg(p.b + i) - y;
+            continue;
+        }
+        const float di = L.invd ? __ldg(L.invd + i) : 1.f;
+        if (outside) {
+            p.d[i] = 0.f;
+            p.x_out[i] = di * __ldcg(p.b + i);
+            continue;
+        }
+        if (!live) continue;
+        const float rr = __ldcg(p.b + i) - y;
+        const float dn = (p.c1 != 0.f ? p.c1 * __ldcg(p.d + i) : 0.f) + p.c2 * di * rr;
+        p.d[i] = dn;
+        p.x_out[i] = __ldcg(p.x_in + i) + dn;
+    }
+}
+
+// the long rows of a level: 256-thread groups, one row each (k_long_rows' block); Dots leaves
+// the rows' terms in long_part
+__device__ void tail_long(const TailPhase &p, const TailLevel &L, int cta, int n_cta, double *__restrict__ long_part,
+                          float (*red)[8]) {
+    if (L.n_long <= 0) return;
+    const MatView &A = L.A;
+    const int grp = threadIdx.x >> 8, t = threadIdx.x & 255;
+    const int n_grp = n_cta * kTailGroups;
+    for (int k0 = 0; k0 < L.n_long; k0 += n_grp) {
+        const int k = k0 + cta * kTailGroups + grp;
+        float y = 0.f;
+        int64_t i = 0;
+        if (k < L.n_long) {
+            i = __ldg(L.longrows + k);
+            int64_t base;
+            int w, ln;
+            row_of(A, i, base, w, ln);
+            for (int j = t; j < w; j += 256) {
+                const int64_t slot = base + (int64_t)j * kS + ln;
+                y += __ldg(A.val + slot) * __ldcg(p.x_in + __ldg(A.col + slot));
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(kFull, y, o);
+        if ((t & 31) == 0) red[grp][t >> 5] = y;
+        __syncthreads();
+        if (t == 0 && k < L.n_long) {
+            y = 0.f;
+            for (int q = 0; q < 8; ++q) y += red[grp][q];
+            if (p.op == kTailStep) {
+                const float di = L.invd ? __ldg(L.invd + i) : 1.f;
+                const float dn = (p.c1 != 0.f ? p.c1 * __ldcg(p.d + i) : 0.f) + p.c2 * di * (__ldcg(p.b + i) - y);
+                p.d[i] = dn;
+                p.x_out[i] = __ldcg(p.x_in + i) + dn;
+            } else if (p.op == kTailResid) {
+                p.x_out[i] = __ldcg(p.b + i) - y;
+            } else {
+                const double xi = (double)__ldcg(p.x_in + i);
+                __stcg(long_part + 2 * k, xi * (double)__ldcg(p.b + i));
+                __stcg(long_part + 2 * k + 1, xi * (double)y);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kTailThreads, 1)
+    k_tail(Gate gate, const TailPhase *__restrict__ prog, int n_phases, const TailLevel *__restrict__ levels,
+           double *__restrict__ scratch, int64_t long_off) {
+    if (closed(gate)) return;  // the same for every CTA: nothing else writes n_done meanwhile
+    cg::cluster_group cluster = cg::this_cluster();
+    const int cta = (int)cluster.block_rank(), n_cta = (int)cluster.num_blocks();
+    __shared__ float sh[kTailWarps][32];
+    __shared__ double shd[2][kTailWarps];
+    __shared__ float red[kTailGroups][8];
+    __shared__ double tree[2][256];
+    const int64_t tid = (int64_t)cta * kTailThreads + threadIdx.x, n_thr = (int64_t)n_cta * kTailThreads;
+    for (int ph = 0; ph < n_phases; ++ph) {
+        const TailPhase &p = prog[ph];
+        const TailLevel &L = levels[p.level];
+        switch (p.op) {
+            case kTailStep:
+            case kTailResid:
+                tail_rows(p, L, cta, n_cta, scratch, sh, shd);
+                tail_long(p, L, cta, n_cta, scratch + long_off, red);
+                break;
+            case kTailDots: {
+                tail_rows(p, L, cta, n_cta, scratch, sh, shd);
+                tail_long(p, L, cta, n_cta, scratch + long_off, red);
+                cluster.sync();
+                // the factor from the partials in k_coarse_dots' order, by the first CTA
+                if (cta == 0) {
+                    const int64_t n_vb = (L.A.n / kS * L.g + 7) / 8;
+                    double a = 0.0, c = 0.0;
+                    if (threadIdx.x < 256) {
+                        for (int64_t k = threadIdx.x; k < n_vb; k += 256) {
+                            a += __ldcg(scratch + 2 * k);
+                            c += __ldcg(scratch + 2 * k + 1);
+                        }
+                        for (int k = threadIdx.x; k < L.n_long; k += 256) {
+                            a += __ldcg(scratch + long_off + 2 * k);
+                            c += __ldcg(scratch + long_off + 2 * k + 1);
+                        }
+                        tree[0][threadIdx.x] = a;
+                        tree[1][threadIdx.x] = c;
+                    }
+                    __syncthreads();
+                    for (int st = 128; st > 0; st >>= 1) {
+                        if ((int)threadIdx.x < st) {
+                            tree[0][threadIdx.x] += tree[0][threadIdx.x + st];
+                            tree[1][threadIdx.x] += tree[1][threadIdx.x + st];
+                        }
+                        __syncthreads();
+                    }
+                    if (threadIdx.x == 0) {
+                        const double num = tree[0][0], den = tree[1][0];
+                        __stcg(p.alpha, (den > 0.0 && num > 0.0 && isfinite(num / den)) ? num / den : 1.0);
+                    }
+                }
+                break;
+            }
+            case kTailRestrict:
+            case kTailRestrictFirst: {
+                const TailLevel &C = levels[p.next];
+                const int64_t nc_pad = C.A.n;
+                for (int64_t I = tid; I < nc_pad; I += n_thr) {
+                    float s = 0.f;
+                    if (I < L.nc)
+                        for (int32_t k = __ldg(L.ms + I); k < __ldg(L.ms + I + 1); ++k)
+                            s += 1.f * __ldcg(p.x_in + __ldg(L.mr + k));
+                    p.x_out[I] = s;
+                    if (p.op == kTailRestrictFirst) {
+                        const bool exact = __ldg(C.agg + I) < 0;
+                        const float v = (exact ? 1.f : p.c2) * __ldg(C.invd + I) * s;
+                        p.d[I] = exact ? 0.f : v;
+                        p.x2[I] = v;
+                    }
+                }
+                break;
+            }
+            case kTailFirst:
+                for (int64_t i = tid; i < L.A.n; i += n_thr) {
+                    const float di = L.invd ? __ldg(L.invd + i) : 1.f;
+                    if (L.agg && __ldg(L.agg + i) < 0) {
+                        p.d[i] = 0.f;
+                        p.x_out[i] = di * __ldcg(p.b + i);
+                        continue;
+                    }
+                    const float v = p.c2 * di * __ldcg(p.b + i);
+                    p.d[i] = v;
+                    p.x_out[i] = v;
+                }
+                break;
+            case kTailDense: {
+                const int64_t n = p.dense_n, n_pad = L.A.n;
+                const int lane = threadIdx.x & 31;
+                for (int64_t i = tid >> 5; i < n_pad; i += n_thr >> 5) {
+                    float s = 0.f;
+                    if (i < n)
+                        for (int64_t j = lane; j < n; j += 32) s += __ldg(p.dense + i * n + j) * __ldcg(p.b + j);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+                    if (lane == 0) p.x_out[i] = s;
+                }
+                break;
+            }
+            case kTailProlong: {
+                const float al = p.use_alpha ? (float)__ldcg(p.alpha) : p.alpha_fixed;
+                for (int64_t i = tid; i < L.A.n; i += n_thr) {
+                    const int32_t a = __ldg(L.agg + i);
+                    if (a >= 0) p.x_out[i] = __ldcg(p.x_out + i) + al * 1.f * __ldcg(p.x_in + a);
+                }
+                break;
+            }
+            default:
+                break;
+        }
+        cluster.sync();
     }
 }
 
@@ -1316,6 +1634,11 @@ void Amg::release() {
     isd_.release();
     dense_inv_.release();
     bound_.release();
+    tail_prog_.release();
+    tail_levels_.release();
+    tail_scratch_.release();
+    tail_level_ = tail_phases_ = tail_regular_ = 0;
+    tail_out_ = nullptr;
     if (h_flag_) cudaFreeHost(h_flag_);
     h_flag_ = nullptr;
 }
@@ -1372,18 +1695,17 @@ __global__ void k_power_start(int64_t n, float *x) {
     x[i] = ((h & 1u) ? 1.f : -1.f) * (0.5f + (float)((h >> 8) & 0xffffu) * (0.5f / 65536.f));
 }
 
+// y = D^-1 A x with the cycle's row kernels' split (G warps per slice, eight loads in flight);
+// the long rows are left to k_long_rows<3>
+template <int G>
 __global__ void __launch_bounds__(256) k_power_step(MatView A, const float *__restrict__ invd,
                                                     const float *__restrict__ x, float *__restrict__ y) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
-    int64_t base;
-    int w, ln;
-    row_of(A, i, base, w, ln);
-    float acc = 0.f;
-    for (int j = 0; j < w; ++j) {
-        const int64_t slot = base + (int64_t)j * kS + ln;
-        acc += __ldg(A.val + slot) * __ldg(x + __ldg(A.col + slot));
-    }
+    int64_t i;
+    int g;
+    split_row<G>(i, g);
+    const bool live = i < A.n && !is_long(A, i);
+    const float acc = split_sum<G>(live ? split_part<G>(A, i, g, x) : 0.f);
+    if (g != 0 || !live) return;
     y[i] = invd ? invd[i] * acc : acc;
 }
 
@@ -1694,8 +2016,9 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     }
     {
         cudaError_t e2 = fine_weights_eff(s);
-        if (e2 != cudaSuccess || (e2 = fine_interval(s)) != cudaSuccess || (e2 = power_estimates(s)) != cudaSuccess)
-            return e2;
+        if (e2 != cudaSuccess || (e2 = fine_interval(s)) != cudaSuccess) return e2;
+        // the bounds, the long-row counts and the overflow flag first: the power iteration's
+        // row kernels need each level's split and long rows
         std::vector<unsigned int> bits(n_levels_);
         std::vector<int32_t> nlong(n_levels_, 0);
         std::vector<double> pw(2 * n_levels_, 0.0);
@@ -1703,8 +2026,6 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         if (fine_w_)  // the fine level is smoothed on Omega S^: its own bound
             AMG_CK(cudaMemcpyAsync(bits.data(), bounds_.p + opt_.max_levels, sizeof(unsigned int),
                                    cudaMemcpyDeviceToHost, s));
-        if (opt_.power_steps > 0)
-            AMG_CK(cudaMemcpyAsync(pw.data(), pw_sums_.p, 2 * n_levels_ * sizeof(double), cudaMemcpyDeviceToHost, s));
         for (int l = 1; l < n_levels_; ++l)
             if (lv_[l].A.long_count)
                 AMG_CK(cudaMemcpyAsync(&nlong[l], lv_[l].A.long_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1713,6 +2034,17 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         if (*h_flag_) {
             err = "Galerkin row wider than the gather buffer";
             return cudaErrorInvalidValue;
+        }
+        for (int l = 0; l < n_levels_; ++l) {
+            lv_[l].A.n_long = nlong[l];
+            // warps per slice in the row kernels: at most split_width slots per warp and row
+            // (the fine level, 7-8 entries per row, keeps one thread per row)
+            lv_[l].g = split_of(lv_[l].A, opt_.split, opt_.split_width);
+        }
+        if ((e2 = power_estimates(s)) != cudaSuccess) return e2;
+        if (opt_.power_steps > 0) {
+            AMG_CK(cudaMemcpyAsync(pw.data(), pw_sums_.p, 2 * n_levels_ * sizeof(double), cudaMemcpyDeviceToHost, s));
+            AMG_CK(cudaStreamSynchronize(s));
         }
         for (int l = 0; l < n_levels_; ++l) {
             float hi;
@@ -1724,10 +2056,6 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
                 const double est = std::sqrt(pw[2 * l + 1] / pw[2 * l]);
                 lv_[l].hi = (float)std::min((double)lv_[l].gershgorin, opt_.power_safety * est);
             }
-            lv_[l].A.n_long = nlong[l];
-            // warps per slice in the row kernels: at most split_width slots per warp and row
-            // (the fine level, 7-8 entries per row, keeps one thread per row)
-            lv_[l].g = split_of(lv_[l].A, opt_.split, opt_.split_width);
         }
     }
     const AmgLevel &Lc = lv_[n_levels_ - 1];
@@ -1758,7 +2086,8 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     AMG_CK(alpha_.ensure(n_levels_ + 1));
     AMG_CK(tickets_.ensure(n_levels_ + 1));
     AMG_CK(cudaMemsetAsync(tickets_.p, 0, (n_levels_ + 1) * sizeof(unsigned int), s));
-    return dense_n_ > 0 ? dense_coarse(Lc.A, s) : cudaSuccess;
+    if (dense_n_ > 0) AMG_CK(dense_coarse(Lc.A, s));
+    return build_tail(s);
 }
 
 cudaError_t Amg::power_estimates(cudaStream_t s, int only_level) {
@@ -1785,7 +2114,16 @@ cudaError_t Amg::power_estimates(cudaStream_t s, int only_level) {
         float *x = pw_a_.p, *y = pw_b_.p;
         k_power_start<<<nblk(n, 256), 256, 0, s>>>(n, x);
         for (int k = 0; k < opt_.power_steps; ++k) {
-            k_power_step<<<nblk(n, 256), 256, 0, s>>>(V, invd, x, y);
+            const unsigned gs = row_blocks(L);
+            switch (L.g >= 8 ? 8 : L.g >= 4 ? 4 : L.g >= 2 ? 2 : 1) {
+                case 8: k_power_step<8><<<gs, 256, 0, s>>>(V, invd, x, y); break;
+                case 4: k_power_step<4><<<gs, 256, 0, s>>>(V, invd, x, y); break;
+                case 2: k_power_step<2><<<gs, 256, 0, s>>>(V, invd, x, y); break;
+                default: k_power_step<1><<<gs, 256, 0, s>>>(V, invd, x, y); break;
+            }
+            if (L.A.n_long > 0)
+                k_long_rows<3><<<(unsigned)L.A.n_long, 256, 0, s>>>(Gate{nullptr, 0}, V, L.A.longrows, nullptr, invd,
+                                                                    x, y, nullptr, 0.f, 0.f, nullptr);
             if (k + 1 < opt_.power_steps) std::swap(x, y);
         }
         k_power_norms<<<kPowerBlocks, 256, 0, s>>>(n, x, y, pw_part_.p);
@@ -1857,7 +2195,215 @@ int Amg::kernels_per_apply() const {
     const int coarse = dense_n_ > 0 ? 1 : kCoarseDegree;
     return last_long_launches_ + (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) -
            (n_levels_ > 1 && pre >= 2 ? 1 : 0) +
-           (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0);
+           (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0) -
+           (tail_phases_ > 0 ? tail_regular_ - 1 : 0);
+}
+
+// Compiles the cycle's part on levels tail_level_ .. coarsest (for the cycle from level 0) into
+// the phase list k_tail runs: the same operations, buffers and coefficients, in the order
+// cycle() launches them, with level tail_level_'s first step left to the restriction above it
+// and the scaling of level tail_level_ - 1's coarse correction as the last phase.
+cudaError_t Amg::build_tail(cudaStream_t s) {
+    tail_level_ = tail_phases_ = tail_regular_ = 0;
+    tail_out_ = nullptr;
+    const int nl = n_levels_;
+    if (opt_.tail_rows <= 0 || nl < 3) return cudaSuccess;
+    int t = nl - 1;
+    while (t - 1 >= 1 && lv_[t - 1].A.n <= opt_.tail_rows) --t;
+    if (t > nl - 2) return cudaSuccess;  // only the coarsest solve would move: nothing to gain
+    // the cluster: 16 CTAs where the device schedules them, else 8
+    if (tail_cluster_ == 0) {
+        cudaFuncSetAttribute(k_tail, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaGetLastError();
+        for (int cl : {16, 8}) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cl);
+            cfg.blockDim = dim3(kTailThreads);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = cl;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, k_tail, &cfg) == cudaSuccess && n > 0) {
+                tail_cluster_ = cl;
+                break;
+            }
+            cudaGetLastError();
+        }
+        if (tail_cluster_ == 0) tail_cluster_ = -1;  // clusters unavailable: no tail
+    }
+    if (tail_cluster_ < 0) return cudaSuccess;
+    std::vector<TailLevel> tl(nl);
+    for (int l = t; l < nl; ++l) {
+        const AmgLevel &L = lv_[l];
+        TailLevel &q = tl[l];
+        q.A = view(L.A);
+        q.invd = L.inv_diag.p;
+        q.agg = L.agg.p;
+        q.ms = l + 1 < nl ? L.mem_start.p : nullptr;
+        q.mr = l + 1 < nl ? L.mem_rows.p : nullptr;
+        q.longrows = L.A.longrows;
+        q.nc = l + 1 < nl ? L.nc : 0;
+        q.n_long = (int32_t)L.A.n_long;
+        q.g = L.g;
+    }
+    std::vector<TailPhase> ph;
+    int64_t max_vb = 1, max_long = 1;
+    auto phase = [&](int32_t op, int level) {
+        TailPhase p = {};
+        p.op = op;
+        p.level = level;
+        p.alpha_fixed = opt_.alpha;
+        tail_regular_ += 1;
+        return p;
+    };
+    auto dots = [&](int lc, const float *x, double *alpha) {
+        TailPhase p = phase(kTailDots, lc);
+        p.x_in = x;
+        p.b = lv_[lc].b.p;
+        p.alpha = alpha;
+        ph.push_back(p);
+        max_vb = std::max<int64_t>(max_vb, (lv_[lc].A.n / kS * lv_[lc].g + 7) / 8);
+        max_long = std::max<int64_t>(max_long, lv_[lc].A.n_long);
+    };
+    std::vector<double> c1, c2;
+    std::vector<float *> xout(nl, nullptr);
+    const int pre = pre_degree(), deg = std::max(1, opt_.cheb_degree);
+    // descend (level t's first step: the restriction from level t - 1)
+    for (int l = t; l < nl - 1; ++l) {
+        AmgLevel &L = lv_[l];
+        cheb_coeffs(L, c1, c2);
+        float *xi = L.xa.p, *xo = L.xb.p;
+        for (int k = 1; k < pre; ++k) {
+            TailPhase p = phase(kTailStep, l);
+            p.b = L.b.p;
+            p.x_in = xi;
+            p.x_out = xo;
+            p.d = L.d.p;
+            p.c1 = (float)c1[k];
+            p.c2 = (float)c2[k];
+            ph.push_back(p);
+            std::swap(xi, xo);
+        }
+        xout[l] = xi;
+        TailPhase r = phase(kTailResid, l);
+        r.b = L.b.p;
+        r.x_in = xi;
+        r.x_out = L.r.p;
+        ph.push_back(r);
+        AmgLevel &C = lv_[l + 1];
+        TailPhase q = phase(l + 2 < nl ? kTailRestrictFirst : kTailRestrict, l);
+        q.next = l + 1;
+        q.x_in = L.r.p;
+        q.x_out = C.b.p;
+        if (l + 2 < nl) {
+            std::vector<double> cc1, cc2;
+            cheb_coeffs(C, cc1, cc2);
+            q.c2 = (float)cc2[0];
+            q.d = C.d.p;
+            q.x2 = C.xa.p;
+        }
+        ph.push_back(q);
+    }
+    // coarsest
+    {
+        AmgLevel &Lc = lv_[nl - 1];
+        if (dense_n_ > 0) {
+            TailPhase p = phase(kTailDense, nl - 1);
+            p.b = Lc.b.p;
+            p.x_out = Lc.xa.p;
+            p.dense = dense_inv_.p;
+            p.dense_n = (int32_t)dense_n_;
+            ph.push_back(p);
+            xout[nl - 1] = Lc.xa.p;
+        } else {
+            cheb_coeffs(Lc, c1, c2, kCoarseDegree, kCoarseRatio);
+            float *xi = Lc.xa.p, *xo = Lc.xb.p;
+            TailPhase f = phase(kTailFirst, nl - 1);
+            f.b = Lc.b.p;
+            f.x_out = xi;
+            f.d = Lc.d.p;
+            f.c2 = (float)c2[0];
+            ph.push_back(f);
+            for (int k = 1; k < kCoarseDegree; ++k) {
+                TailPhase p = phase(kTailStep, nl - 1);
+                p.b = Lc.b.p;
+                p.x_in = xi;
+                p.x_out = xo;
+                p.d = Lc.d.p;
+                p.c1 = (float)c1[k];
+                p.c2 = (float)c2[k];
+                ph.push_back(p);
+                float *xk = xo;
+                xo = xi;
+                xi = xk;
+            }
+            xout[nl - 1] = xi;
+        }
+    }
+    // ascend
+    auto kcycle_at = [&](int l) { return opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0); };
+    for (int l = nl - 2; l >= t; --l) {
+        AmgLevel &L = lv_[l];
+        cheb_coeffs(L, c1, c2);
+        float *xi = xout[l];
+        TailPhase pr = phase(kTailProlong, l);
+        if (kcycle_at(l)) {
+            dots(l + 1, xout[l + 1], alpha_.p + l);
+            pr.use_alpha = 1;
+            pr.alpha = alpha_.p + l;
+        }
+        pr.x_in = xout[l + 1];
+        pr.x_out = xi;
+        ph.push_back(pr);
+        float *other = xi == L.xa.p ? L.xb.p : L.xa.p;
+        for (int k = 0; k < deg; ++k) {
+            TailPhase p = phase(kTailStep, l);
+            p.b = L.b.p;
+            p.x_in = xi;
+            p.x_out = other;
+            p.d = L.d.p;
+            p.c1 = k == 0 ? 0.f : (float)c1[k];
+            p.c2 = (float)c2[k];
+            ph.push_back(p);
+            float *xo = other;
+            other = xi;
+            xi = xo;
+        }
+        xout[l] = xi;
+    }
+    if (kcycle_at(t - 1)) dots(t, xout[t], alpha_.p + (t - 1));
+    AMG_CK(tail_prog_.ensure(ph.size() * sizeof(TailPhase)));
+    AMG_CK(tail_levels_.ensure(tl.size() * sizeof(TailLevel)));
+    AMG_CK(tail_scratch_.ensure(2 * (size_t)(max_vb + max_long)));
+    AMG_CK(cudaMemcpyAsync(tail_prog_.p, ph.data(), ph.size() * sizeof(TailPhase), cudaMemcpyHostToDevice, s));
+    AMG_CK(cudaMemcpyAsync(tail_levels_.p, tl.data(), tl.size() * sizeof(TailLevel), cudaMemcpyHostToDevice, s));
+    AMG_CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    tail_long_off_ = 2 * max_vb;
+    tail_level_ = t;
+    tail_phases_ = (int)ph.size();
+    tail_out_ = xout[t];
+    return cudaSuccess;
+}
+
+cudaError_t Amg::launch_tail(const int32_t *n_done, int32_t n_inst, cudaStream_t s) const {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tail_cluster_);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = tail_cluster_;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const Gate gate{n_done, n_inst};
+    return cudaLaunchKernelEx(&cfg, k_tail, gate, reinterpret_cast<const TailPhase *>(tail_prog_.p), tail_phases_,
+                              reinterpret_cast<const TailLevel *>(tail_levels_.p), tail_scratch_.p, tail_long_off_);
 }
 
 cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
@@ -1901,7 +2447,9 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
     const int deg = std::max(1, opt_.cheb_degree);
     const int nl = n_levels_;
     std::vector<float *> xout(nl);
-    for (int l = l0; l < nl - 1; ++l) {
+    // the levels from tail_level_ down run as one cluster launch (the cycle from level 0 only)
+    const bool use_tail = tail_phases_ > 0 && tail_level_ > l0;
+    for (int l = l0; l < (use_tail ? tail_level_ : nl - 1); ++l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
         // the scaled fine level has unit diagonal; with smoother weights Omega, D^-1 -> Omega
@@ -1952,7 +2500,10 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
     }
     // coarsest: dense inverse, or (when coarsening stalled above the dense limit) a Chebyshev
     // polynomial of degree kCoarseDegree on a wide interval
-    {
+    if (use_tail) {
+        AMG_CK(launch_tail(n_done, n_inst, s));
+        xout[tail_level_] = tail_out_;
+    } else {
         AmgLevel &Lc = lv_[nl - 1];
         const float *b = nl == 1 ? r : Lc.b.p;
         if (dense_n_ > 0) {
@@ -1977,7 +2528,7 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         }
     }
     // ascend: prolong, smooth
-    for (int l = nl - 2; l >= l0; --l) {
+    for (int l = use_tail ? tail_level_ - 1 : nl - 2; l >= l0; --l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
         const float *invd = l == 0 ? fw() : L.inv_diag.p;
@@ -1989,7 +2540,10 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         float *xi = xout[l];
         const double *al = nullptr;
         // (a dense coarsest correction is exact: its optimal scaling is 1)
-        if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0)) {
+        if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0) && use_tail &&
+            l == tail_level_ - 1) {
+            al = alpha_.p + l;  // the tail's last phase
+        } else if (opt_.kcycle && l < opt_.kcycle_levels && (l + 2 < nl || dense_n_ == 0)) {
             AmgLevel &C = lv_[l + 1];
             double *lp = dots_long_.p + dots_long_off_[l];
             long_rows(C.A, 2, C.b.p, nullptr, xout[l + 1], nullptr, nullptr, 0.f, 0.f, lp);

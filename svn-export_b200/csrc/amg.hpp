@@ -47,6 +47,8 @@ struct AmgOptions {
     int power_steps = 12;   // power-iteration steps estimating lambda_max(D^-1 A) per level (0: the
                             // Gershgorin bound alone)
     float power_safety = 1.1f;  // smoothing interval top = min(Gershgorin, safety * estimate)
+    int tail_rows = 0;      // levels (below the fine one) from which every level has at most this
+                            // many rows run in one cluster launch (0: every level on its own)
 };
 
 template <class T> struct DBuf {
@@ -110,6 +112,9 @@ public:
     int levels() const { return n_levels_; }
     const AmgLevel &level(int l) const { return lv_[l]; }
     int64_t coarse_rows() const { return n_levels_ ? lv_[n_levels_ - 1].A.n : 0; }
+    // the first level of the coarse tail run as one cluster launch (0: none) and its CTAs
+    int tail_level() const { return tail_phases_ > 0 ? tail_level_ : 0; }
+    int tail_cluster() const { return tail_cluster_; }
     int kernels_per_apply() const;
     const float *fine_weights() const { return w0_used_; }  // null when the transfers are unweighted
     // Per-row weights of the fine level's smoother (device array over the solver rows, owned by
@@ -198,6 +203,18 @@ private:
     DBuf<double> pw_part_, pw_sums_;  // its per-block partial norms and the two norms per level
     DBuf<float> w0_;                // sqrt(diag S) per fine row
     DBuf<uint16_t> fine_half_;      // FP16 bits of the fine matrix's values (half_fine)
+    // the coarse tail: levels tail_level_ .. coarsest of the cycle from level 0 as one cluster
+    // launch running a list of phases (amg.cu, k_tail)
+    cudaError_t build_tail(cudaStream_t s);
+    cudaError_t launch_tail(const int32_t *n_done, int32_t n_inst, cudaStream_t s) const;
+    int tail_level_ = 0;            // 0: no tail
+    int tail_cluster_ = 0;          // CTAs of the cluster
+    int tail_phases_ = 0;
+    int tail_regular_ = 0;          // row kernels (not long-row ones) the tail stands in for
+    float *tail_out_ = nullptr;     // the tail's result: x of level tail_level_
+    int64_t tail_long_off_ = 0;     // long-row terms' offset in the scratch
+    DBuf<unsigned char> tail_prog_, tail_levels_;
+    DBuf<double> tail_scratch_;
     const float *w0_used_ = nullptr;
     int64_t dense_n_ = 0;
     int32_t *h_flag_ = nullptr;

@@ -311,7 +311,8 @@ int device_setup(mh_handle *h) {
     const int64_t msize = t.n_sides() + m.n_el + t.n_edges();
     h->sol = dalloc<double>(h, msize);
     h->sol_prev = dalloc<double>(h, msize);
-    if (!h->sol || !h->sol_prev) return MH_ERR_NOMEM;
+    h->d_loop = dalloc<int32_t>(h, 2);
+    if (!h->sol || !h->sol_prev || !h->d_loop) return MH_ERR_NOMEM;
     CK(cudaMemset(h->sol, 0, msize * sizeof(double)));
     CK(cudaMemset(h->sol_prev, 0, msize * sizeof(double)));
     h->device = true;
@@ -341,7 +342,6 @@ int apply_launch_shape(mh_handle *h, int R, const int targets[2]) {
     }
     s.partial = dalloc<double>(h, (size_t)max_blocks * 4);
     if (!s.partial) return MH_ERR_NOMEM;
-    if (!h->d_loop && !(h->d_loop = dalloc<int32_t>(h, 2))) return MH_ERR_NOMEM;
     for (auto &gp : h->graph)
         for (auto &g : gp)
             if (g) {
@@ -1042,6 +1042,7 @@ mh::AmgOptions amg_options() {
         if (x > 0.f && x <= 3.f) o.alpha = x;
     }
     env_i("MH_AMG_POWER", o.power_steps, 0, 64);
+    env_i("MH_AMG_TAIL", o.tail_rows, 0, 1 << 22);
     if (const char *e = getenv("MH_AMG_SAFETY")) {
         const float x = (float)atof(e);
         if (x >= 1.f && x <= 3.f) o.power_safety = x;
@@ -1451,7 +1452,10 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
     if (o.iters_per_graph <= 0) o.iters_per_graph = multigrid ? 4 : 16;
     if (o.inner_max_it <= 0) o.inner_max_it = 2000;
     if (!(o.inner_rtol > 0.0)) o.inner_rtol = multigrid ? 1e-3 : 0.1;
-    h->host_loop = o.host_loop != 0;
+    // MH_HOST_LOOP=1 makes the host-polled loop the default (profilers cannot see the kernels
+    // inside a graph with conditional nodes)
+    const char *hl = getenv("MH_HOST_LOOP");
+    h->host_loop = o.host_loop != 0 || (hl && hl[0] == '1');
     if (!(o.r_tol >= 0.0)) o.r_tol = 1e-10;
     if (!(o.a_tol >= 0.0)) o.a_tol = 0.0;
     const bool guess = o.use_initial_guess || have_guess_default;
@@ -2701,6 +2705,15 @@ int mh_amg_info(const mh_handle *hc, int32_t *n_levels, int64_t *rows, int64_t *
         if (rows) rows[l] = real;
         if (slots) slots[l] = a.level(l).A.slots;
     }
+    return MH_OK;
+}
+
+int mh_amg_tail(const mh_handle *hc, int32_t *level, int32_t *cluster_ctas) {
+    mh_handle *h = const_cast<mh_handle *>(hc);
+    int rc = need_device(h);
+    if (rc) return rc;
+    if (level) *level = h->amg.tail_level();
+    if (cluster_ctas) *cluster_ctas = h->amg.tail_level() > 0 ? h->amg.tail_cluster() : 0;
     return MH_OK;
 }
 

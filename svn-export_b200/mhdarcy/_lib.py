@@ -178,6 +178,7 @@ def _load():
         "mh_learned_grad": (C.c_int, [vp, _f64p, _f64p, _f32p, _f64p]),
         "mh_learned_apply": (C.c_int, [vp, _f64p, _f64p]),
         "mh_amg_info": (C.c_int, [vp, _i32p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]),
+        "mh_amg_tail": (C.c_int, [vp, _i32p, _i32p]),
         "mh_amg_level": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _i32p, _f32p, _i32p,
                                    _i32p, _f32p]),
         "mh_learn_opts_default": (None, [C.POINTER(LearnOpts)]),
@@ -212,7 +213,7 @@ EXPORTED = ("mh_version", "mh_status_string", "mh_device_available", "mh_last_er
             "mh_solve_opts_default", "mh_unsteady_init", "mh_unsteady_step", "mh_csr_residual_noalloc",
             "mh_create_batch", "mh_get_instance_offsets", "mh_get_instance_stats", "mh_autotune", "mh_autotune_ex",
             "mh_learned_set_weights", "mh_learned_get_weights", "mh_learned_grad", "mh_learned_apply", "mh_learn_opts_default",
-            "mh_amg_info", "mh_amg_level",
+            "mh_amg_info", "mh_amg_tail", "mh_amg_level",
             "mh_learned_train", "mh_smoother_weights_set", "mh_smoother_weights_get",
             "mh_learned_grad_weights", "mh_learned_smoother", "mh_learned_reset",
             "mh_csr_create", "mh_csr_set_values", "mh_csr_get_solution", "mh_create_mortar")

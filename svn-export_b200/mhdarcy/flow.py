@@ -289,6 +289,13 @@ class MHSystem:
         n = int(nl[0])
         return dict(levels=n, rows=rows[:n].tolist(), slots=slots[:n].tolist())
 
+    def amg_tail(self):
+        """The coarse tail of the last AMG hierarchy's V-cycle: its first level and the CTAs of
+        the cluster that runs it (0, 0: none)."""
+        lv, cl = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        check(lib.mh_amg_tail(self.h, ptr(lv, C.c_int32), ptr(cl, C.c_int32)), self.h)
+        return dict(level=int(lv[0]), cluster=int(cl[0]))
+
     def amg_level(self, level):
         """((row_ptr, col, val), agg, weight) of level `level` of the last AMG hierarchy."""
         n, nnz = C.c_int64(0), C.c_int64(0)
