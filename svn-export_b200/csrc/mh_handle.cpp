@@ -1043,6 +1043,7 @@ mh::AmgOptions amg_options() {
     }
     env_i("MH_AMG_POWER", o.power_steps, 0, 64);
     env_i("MH_AMG_TAIL", o.tail_rows, 0, 1 << 22);
+    env_i("MH_AMG_LEVELS", o.max_levels, 2, 20);
     if (const char *e = getenv("MH_AMG_SAFETY")) {
         const float x = (float)atof(e);
         if (x >= 1.f && x <= 3.f) o.power_safety = x;

@@ -49,11 +49,14 @@ def test_bench_cpu_baseline_entry():
 
 
 def test_bench_reference_arm_complete_and_projected(monkeypatch):
-    """The reference arm on cfg1: complete solves when they fit the budget; with a recorded
-    complete-solve iteration count and a small budget, bounded samples projected with it.
-    Its config equals the GPU arm's for the same workload (sizes from the library)."""
+    """The reference arm on cfg1: complete solves when they fit the budget; when only one fits
+    its cap, that one complete solve (steps 1, warm-up 0, the requested counts beside them); with
+    no cap and a small budget, bounded samples projected with the recorded complete-solve
+    iteration count.  Its config equals the GPU arm's for the same workload (sizes from the
+    library)."""
     bench = load_bench()
-    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=60.0, gpus=1)
+    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=60.0, gpus=1,
+                        ref_single_cap_s=400.0)
     out = bench.run_reference(a)
     assert out["impl"] == "reference" and out["value"] > 0 and out["projected"] is False
     assert out["e2e"]["value"] == out["value"] and out["cpu_baseline"]["kind"] == "port"
@@ -64,7 +67,14 @@ def test_bench_reference_arm_complete_and_projected(monkeypatch):
         z = s.sizes
         assert out["config"] == bench.workload_config(1, z.n_edges, z.schur_nnz, z.mh_size, z.n_elements)
     monkeypatch.setattr(bench, "cpu_full_record", lambda cfg, pre: {"iterations": 1630})
-    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=0.05, gpus=1)
+    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=0.05, gpus=1,
+                        ref_single_cap_s=400.0)
+    one = bench.run_reference(a)
+    assert one["projected"] is False and one["steps"] == 1 and one["warmup"] == 0
+    assert one["steps_requested"] == 2 and "one complete solve" in one["cpu_baseline"]["sample"]
+    assert abs(one["value"] - 1e3 / one["ms_per_step"]) <= 1e-3 * one["value"]
+    a = SimpleNamespace(config=1, cpu_precond="jacobi", steps=2, warmup=1, ref_budget_s=0.05, gpus=1,
+                        ref_single_cap_s=0.0)
     out2 = bench.run_reference(a)
     assert out2["projected"] is True and "projected" in out2["cpu_baseline"]["sample"]
     # the projection of a 1630-iteration solve lands near the measured complete solve
@@ -77,7 +87,8 @@ def test_bench_reference_arm_loads_no_product_library():
     import subprocess
     import sys
     code = ("import sys, json; sys.path.insert(0, %r); import bench; from types import SimpleNamespace as N; "
-            "o = bench.run_reference(N(config=1, cpu_precond='jacobi', steps=1, warmup=0, ref_budget_s=30.0, gpus=1)); "
+            "o = bench.run_reference(N(config=1, cpu_precond='jacobi', steps=1, warmup=0, ref_budget_s=30.0, gpus=1, "
+            "ref_single_cap_s=400.0)); "
             "maps = open('/proc/self/maps').read(); "
             "print(json.dumps({'v': o['value'], 'lib': 'libmhdarcy' in maps, 'orc': 'libmhoracle' in maps}))" % ROOT)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
