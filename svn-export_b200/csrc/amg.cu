@@ -778,8 +778,6 @@ __global__ void k_slice_width(int64_t n_slices, int64_t nc, const int32_t *rowle
 // into shared memory, inverted, and written out as FP32.  flag = 1 on a non-positive or
 // non-finite pivot.
 constexpr int kDenseMax = 160;  // n^2 doubles + n factors fit in 227 KB of shared memory
-constexpr int kCoarseDegree = 12;     // Chebyshev degree of a smoothed (not inverted) coarsest level
-constexpr float kCoarseRatio = 50.f;  // ... on [hi / 50, hi]
 
 __global__ void __launch_bounds__(1024) k_dense_inverse(MatView A, int n, float *inv, int32_t *flag) {
     extern __shared__ double sm[];
@@ -1941,6 +1939,7 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
     AMG_CK(cudaGetLastError());
     const float *w0 = opt_.weighted ? w0_.p : nullptr;
     cudaError_t e;
+    int poor_run = 0;  // consecutive coarsenings that kept more than half of the rows
     for (int l = 0;; ++l) {
         AmgLevel &L = lv_[l];
         AmgLevel &C = lv_[l + 1 < (int)lv_.size() ? l + 1 : l];
@@ -2013,6 +2012,12 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         if ((double)L.nc > 0.85 * (double)n_real) {  // coarsening stalls: stop one level later
             opt_.max_levels = std::min(opt_.max_levels, l + 2);
         }
+        // slow coarsening (hub-dominated levels keep more than half their rows, level after
+        // level): once the next level is small, it becomes the coarsest, smoothed by the
+        // coarse polynomial, instead of many more levels of a few kernels each
+        poor_run = 2 * L.nc > n_real ? poor_run + 1 : 0;
+        if (opt_.stall_rows > 0 && poor_run >= 2 && L.nc <= opt_.stall_rows)
+            opt_.max_levels = std::min(opt_.max_levels, l + 2);
     }
     {
         cudaError_t e2 = fine_weights_eff(s);
@@ -2192,7 +2197,7 @@ void Amg::cheb_coeffs(const AmgLevel &L, std::vector<double> &c1, std::vector<do
 
 int Amg::kernels_per_apply() const {
     const int deg = std::max(1, opt_.cheb_degree), pre = pre_degree();
-    const int coarse = dense_n_ > 0 ? 1 : kCoarseDegree;
+    const int coarse = dense_n_ > 0 ? 1 : std::max(1, opt_.coarse_degree);
     return last_long_launches_ + (n_levels_ - 1) * (pre + deg + 3) + coarse - std::max(0, n_levels_ - 2) -
            (n_levels_ > 1 && pre >= 2 ? 1 : 0) +
            (opt_.kcycle ? std::min(opt_.kcycle_levels, std::max(0, n_levels_ - (dense_n_ > 0 ? 2 : 1))) : 0) -
@@ -2320,7 +2325,7 @@ cudaError_t Amg::build_tail(cudaStream_t s) {
             ph.push_back(p);
             xout[nl - 1] = Lc.xa.p;
         } else {
-            cheb_coeffs(Lc, c1, c2, kCoarseDegree, kCoarseRatio);
+            cheb_coeffs(Lc, c1, c2, std::max(1, opt_.coarse_degree), opt_.coarse_ratio);
             float *xi = Lc.xa.p, *xo = Lc.xb.p;
             TailPhase f = phase(kTailFirst, nl - 1);
             f.b = Lc.b.p;
@@ -2328,7 +2333,7 @@ cudaError_t Amg::build_tail(cudaStream_t s) {
             f.d = Lc.d.p;
             f.c2 = (float)c2[0];
             ph.push_back(f);
-            for (int k = 1; k < kCoarseDegree; ++k) {
+            for (int k = 1; k < std::max(1, opt_.coarse_degree); ++k) {
                 TailPhase p = phase(kTailStep, nl - 1);
                 p.b = Lc.b.p;
                 p.x_in = xi;
@@ -2499,7 +2504,7 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         }
     }
     // coarsest: dense inverse, or (when coarsening stalled above the dense limit) a Chebyshev
-    // polynomial of degree kCoarseDegree on a wide interval
+    // polynomial of degree coarse_degree on a wide interval
     if (use_tail) {
         AMG_CK(launch_tail(n_done, n_inst, s));
         xout[tail_level_] = tail_out_;
@@ -2513,11 +2518,12 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         } else {
             const unsigned g = nblk(Lc.A.n, 256), gs = row_blocks(Lc);
             const auto sm_step = sm_step_kernel(Lc.g);
-            cheb_coeffs(Lc, c1, c2, kCoarseDegree, kCoarseRatio);
+            cheb_coeffs(Lc, c1, c2, std::max(1, opt_.coarse_degree), opt_.coarse_ratio);
             float *xi = Lc.xa.p, *xo = Lc.xb.p;
             k_sm_first<<<g, 256, 0, s>>>(gate_, Lc.A.n, b, Lc.inv_diag.p, (float)c2[0], xi, Lc.d.p, Lc.agg.p);
-            for (int k = 1; k < kCoarseDegree; ++k) {
-                float *xk = (nl == 1 && k == kCoarseDegree - 1) ? z : xo;
+            const int cdeg = std::max(1, opt_.coarse_degree);
+            for (int k = 1; k < cdeg; ++k) {
+                float *xk = (nl == 1 && k == cdeg - 1) ? z : xo;
                 sm_step<<<gs, 256, 0, s>>>(gate_, view(Lc.A), b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k],
                                            (float)c2[k], Lc.agg.p);
                 long_rows(Lc.A, 0, b, Lc.inv_diag.p, xi, xk, Lc.d.p, (float)c1[k], (float)c2[k], nullptr);

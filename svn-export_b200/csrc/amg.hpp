@@ -37,7 +37,7 @@ struct AmgOptions {
     int pre_degree = 0;     // pre_degree > 0 sets a different number of steps before it)
     float cheb_ratio = 4.f; // smoothing interval [hi / ratio, hi]
     int kcycle = 1;         // 1: scale each coarse correction by its energy-optimal factor
-    int kcycle_levels = 64; // ... on the corrections of the first kcycle_levels levels
+    int kcycle_levels = 6;  // ... on the corrections of the first kcycle_levels levels
     float alpha = 1.f;      // fixed scaling of the coarse corrections when kcycle = 0
     int weighted = 1;       // level-0 transfers weighted by sqrt(diag S) (near-null vector)
     int mix_coarse = 1;     // coarse levels may pair along positive couplings (weakly preferred)
@@ -47,6 +47,10 @@ struct AmgOptions {
     int power_steps = 12;   // power-iteration steps estimating lambda_max(D^-1 A) per level (0: the
                             // Gershgorin bound alone)
     float power_safety = 1.1f;  // smoothing interval top = min(Gershgorin, safety * estimate)
+    int coarse_degree = 12;     // Chebyshev degree of a smoothed (not inverted) coarsest level
+    float coarse_ratio = 50.f;  // ... on [hi / coarse_ratio, hi]
+    int stall_rows = 32768; // after two coarsenings in a row that kept more than half of the rows, a
+                            // next level of at most this many rows is the coarsest (0: off)
     int tail_rows = 0;      // levels (below the fine one) from which every level has at most this
                             // many rows run in one cluster launch (0: every level on its own)
 };

@@ -1044,6 +1044,12 @@ mh::AmgOptions amg_options() {
     env_i("MH_AMG_POWER", o.power_steps, 0, 64);
     env_i("MH_AMG_TAIL", o.tail_rows, 0, 1 << 22);
     env_i("MH_AMG_LEVELS", o.max_levels, 2, 20);
+    env_i("MH_AMG_CDEG", o.coarse_degree, 1, 64);
+    env_i("MH_AMG_STALL", o.stall_rows, 0, 1 << 24);
+    if (const char *e = getenv("MH_AMG_CRATIO")) {
+        const float x = (float)atof(e);
+        if (x >= 2.f && x <= 1000.f) o.coarse_ratio = x;
+    }
     if (const char *e = getenv("MH_AMG_SAFETY")) {
         const float x = (float)atof(e);
         if (x >= 1.f && x <= 3.f) o.power_safety = x;
