@@ -1226,6 +1226,185 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
     }
 }
 
+// ---- fine-level smoothing with the matrix streamed by TMA bulk copies ----------------------
+// The fine level's row kernels are one long stream of SELL slots (column index and FP16 value,
+// 6 bytes a slot) plus gathers of x[col] that mostly hit L2.  In the thread-per-row kernels each
+// warp waits for its slots from DRAM before it can issue its gathers, and the kernel runs at
+// load latency (about 0.6 of the copy bandwidth).  Here a CTA streams tiles of 8 slices
+// (256 rows) through a ring of NST shared-memory stages with 1D bulk copies (cp.async.bulk,
+// completion counted on an mbarrier), so the DRAM stream runs NST - 1 tiles ahead of the warps, which read their slots from shared memory and only wait on the
+// gathers.  The row arithmetic and its summation order are those of k_sm_first_step, k_sm_step<1>
+// and k_residual<1> (bit-identical results).  Every wait is bounded: a stage that does not
+// complete in kFineSpin polls sets *err, and the CTA waits (bounded again) for its copies in
+// flight before it returns.
+constexpr int kFineTileSlices = 8;
+constexpr int kFineSpin = 1 << 22;
+
+enum FineMode : int { kFineFirst = 0, kFineStep = 1, kFineResid = 2 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait on a phase of an mbarrier: false when it did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (int k = 0; k < kFineSpin; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// global -> shared bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct FineTma {
+    const int64_t *off;  // slice offsets (slots)
+    const int32_t *col;
+    const __half *hval;
+    int64_t n, n_slices, n_tiles;
+    int32_t stage_slots;  // slots one stage holds (the widest tile, rounded up to 64)
+};
+
+template <int MODE, int NST>
+__global__ void __launch_bounds__(256) k_fine_tma(Gate gate, FineTma F, const float *__restrict__ b,
+                                                  const float *__restrict__ invd, const float *__restrict__ x_in,
+                                                  float *__restrict__ x_out, float *__restrict__ d, float c0, float c1,
+                                                  float c2, const int32_t *__restrict__ agg, int32_t *err) {
+    if (closed(gate)) return;
+    extern __shared__ __align__(128) unsigned char fsm[];
+    __shared__ __align__(8) uint64_t bar[NST];
+    int s_bad = 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t col_bytes = (size_t)F.stage_slots * 4, stage_bytes = (size_t)F.stage_slots * 6;
+    auto stage_col = [&](int k) { return reinterpret_cast<int32_t *>(fsm + k * stage_bytes); };
+    auto stage_val = [&](int k) { return reinterpret_cast<__half *>(fsm + k * stage_bytes + col_bytes); };
+    // tiles of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
+    const int64_t my_tiles = F.n_tiles > blockIdx.x ? (F.n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    auto issue = [&](int64_t k) {  // copy this CTA's tile k into stage k % NST
+        const int64_t t = blockIdx.x + k * gridDim.x;
+        const int64_t s0 = t * kFineTileSlices, s1 = min(s0 + kFineTileSlices, F.n_slices);
+        const int64_t a = F.off[s0], z = F.off[s1];
+        const uint32_t slots = (uint32_t)(z - a);
+        const int st = (int)(k % NST);
+        mbar_expect_tx(&bar[st], slots * 6u);
+        bulk_g2s(stage_col(st), F.col + a, slots * 4u, &bar[st]);
+        bulk_g2s(stage_val(st), F.hval + a, slots * 2u, &bar[st]);
+    };
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NST; ++k) mbar_init(&bar[k], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int64_t k = 0; k < (my_tiles < NST ? my_tiles : (int64_t)NST); ++k) issue(k);
+    int64_t done = 0;  // tiles whose stage completed (for the drain on an error)
+    for (int64_t k = 0; k < my_tiles; ++k) {
+        const int st = (int)(k % NST);
+        const uint32_t parity = (uint32_t)((k / NST) & 1);
+        // every thread observes the stage's completed phase itself (bounded)
+        if (!__syncthreads_and(mbar_wait(&bar[st], parity))) {
+            s_bad = 1;
+            break;
+        }
+        done = k + 1;
+        const int64_t t = blockIdx.x + k * gridDim.x;
+        const int64_t s = t * kFineTileSlices + warp;
+        if (s < F.n_slices) {
+            const int64_t a0 = F.off[t * kFineTileSlices];
+            const int64_t base = F.off[s];
+            const int w = (int)((F.off[s + 1] - base) / kS);
+            const int32_t *cs = stage_col(st) + (base - a0) + lane;
+            const __half *vs = stage_val(st) + (base - a0) + lane;
+            const int64_t i = s * kS + lane;
+            const float *xg = MODE == kFineFirst ? b : x_in;
+            constexpr int kB = 8;
+            int32_t c[kB];
+            float v[kB];
+#pragma unroll
+            for (int q = 0; q < kB; ++q) {
+                c[q] = q < w ? cs[q * kS] : 0;
+                v[q] = q < w ? __half2float(vs[q * kS]) : 0.f;
+            }
+            float g[kB];
+#pragma unroll
+            for (int q = 0; q < kB; ++q) g[q] = q < w ? xg[c[q]] : 0.f;
+            float y = 0.f;
+#pragma unroll
+            for (int q = 0; q < kB; ++q) y += v[q] * g[q];
+            for (int j = kB; j < w; ++j) y += __half2float(vs[j * kS]) * xg[cs[j * kS]];
+            if (i < F.n) {
+                if (MODE == kFineResid) {
+                    x_out[i] = b[i] - y;
+                } else if (MODE == kFineFirst) {
+                    const float bi = b[i];
+                    if (agg && agg[i] < 0) {
+                        d[i] = 0.f;
+                        x_out[i] = bi;
+                    } else {
+                        const float x1 = c0 * bi;
+                        const float r = bi - c0 * y;
+                        const float dn = c1 * x1 + c2 * r;
+                        d[i] = dn;
+                        x_out[i] = x1 + dn;
+                    }
+                } else {
+                    const float di = invd ? invd[i] : 1.f;
+                    if (agg && agg[i] < 0) {
+                        d[i] = 0.f;
+                        x_out[i] = di * b[i];
+                    } else {
+                        const float r = b[i] - y;
+                        const float dn = (c1 != 0.f ? c1 * d[i] : 0.f) + c2 * di * r;
+                        d[i] = dn;
+                        x_out[i] = x_in[i] + dn;
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the stage is free again
+        if (threadIdx.x == 0 && k + NST < my_tiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + NST);
+        }
+    }
+    if (s_bad && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // let the copies this CTA still has in flight land before the CTA leaves
+        for (int64_t k = done; k < (my_tiles < done + NST ? my_tiles : done + NST); ++k)
+            mbar_wait(&bar[k % NST], (uint32_t)((k / NST) & 1));
+    }
+}
+
+// widest tile of the fine level (slots), for the stage size
+__global__ void k_fine_tile_max(const int64_t *__restrict__ off, int64_t n_slices, int64_t n_tiles,
+                                unsigned int *mx) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    const int64_t s0 = t * kFineTileSlices, s1 = min(s0 + kFineTileSlices, n_slices);
+    atomicMax(mx, (unsigned int)(off[s1] - off[s0]));
+}
+
 // ---- the coarse tail of the V-cycle in one cluster launch -----------------------------------
 // The levels below a few thousand rows are latency-bound: each of their kernels does a
 // microsecond of work and costs a launch.  One thread-block cluster runs all of them: the host
@@ -1634,6 +1813,9 @@ void Amg::release() {
     bound_.release();
     tail_prog_.release();
     tail_levels_.release();
+    tile_max_.release();
+    tma_err_.release();
+    fine_tma_ = false;
     tail_scratch_.release();
     tail_level_ = tail_phases_ = tail_regular_ = 0;
     tail_out_ = nullptr;
@@ -1932,6 +2114,14 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
         k_to_half<<<nblk(sys.n_slots, 256), 256, 0, s>>>(sys.n_slots, sys.val32, fine_half_.p);
         AMG_CK(cudaGetLastError());
     }
+    fine_tma_ = false;
+    const int64_t fine_tiles = (sys.n_slices + kFineTileSlices - 1) / kFineTileSlices;
+    if (opt_.fine_tma && opt_.half_fine && fine_tiles > 0) {  // the widest tile, read with the bounds
+        AMG_CK(tile_max_.ensure(1));
+        AMG_CK(cudaMemsetAsync(tile_max_.p, 0, sizeof(unsigned int), s));
+        k_fine_tile_max<<<nblk(fine_tiles, 256), 256, 0, s>>>(sys.slice_off, sys.n_slices, fine_tiles, tile_max_.p);
+        AMG_CK(cudaGetLastError());
+    }
     // level-0 weights: the near-null vector of the scaled system S^ = D^-1/2 S D^-1/2 is
     // D^1/2 1 (constants are near-null for S), so the level-0 transfers carry sqrt(diag S)
     AMG_CK(w0_.ensure(sys.n_rows));
@@ -2035,11 +2225,15 @@ cudaError_t Amg::setup(const DevSystem &sys, const AmgOptions &o, cudaStream_t s
             if (lv_[l].A.long_count)
                 AMG_CK(cudaMemcpyAsync(&nlong[l], lv_[l].A.long_count, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         AMG_CK(cudaMemcpyAsync(h_flag_, flag_.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        unsigned int widest = 0;
+        if (opt_.fine_tma && opt_.half_fine && fine_tiles > 0)
+            AMG_CK(cudaMemcpyAsync(&widest, tile_max_.p, sizeof(widest), cudaMemcpyDeviceToHost, s));
         AMG_CK(cudaStreamSynchronize(s));
         if (*h_flag_) {
             err = "Galerkin row wider than the gather buffer";
             return cudaErrorInvalidValue;
         }
+        if (widest > 0) AMG_CK(prepare_fine_tma(widest, s));
         for (int l = 0; l < n_levels_; ++l) {
             lv_[l].A.n_long = nlong[l];
             // warps per slice in the row kernels: at most split_width slots per warp and row
@@ -2411,6 +2605,65 @@ cudaError_t Amg::launch_tail(const int32_t *n_done, int32_t n_inst, cudaStream_t
                               reinterpret_cast<const TailLevel *>(tail_levels_.p), tail_scratch_.p, tail_long_off_);
 }
 
+// Stage size and grid of the fine level's TMA-staged kernels for the widest tile: the ring of
+// fine_stages_ stages must fit 100 KB of shared memory, else the per-thread kernels stay in use.
+cudaError_t Amg::prepare_fine_tma(unsigned int widest, cudaStream_t s) {
+    fine_tma_ = false;
+    const AmgMatrix &A = lv_[0].A;
+    const int64_t stage_slots = ((int64_t)widest + 63) / 64 * 64;
+    fine_stages_ = opt_.fine_tma_stages >= 3 ? 4 : 2;
+    const size_t smem = (size_t)fine_stages_ * (size_t)stage_slots * 6;
+    if (stage_slots <= 0 || smem > 100 * 1024 || A.n_slices <= 0) return cudaSuccess;
+    for (auto f : {k_fine_tma<kFineFirst, 2>, k_fine_tma<kFineStep, 2>, k_fine_tma<kFineResid, 2>,
+                   k_fine_tma<kFineFirst, 4>, k_fine_tma<kFineStep, 4>, k_fine_tma<kFineResid, 4>})
+        AMG_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    AMG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, fine_stages_ == 4 ? k_fine_tma<kFineStep, 4> : k_fine_tma<kFineStep, 2>, 256, smem));
+    AMG_CK(cudaGetDevice(&dev));
+    AMG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return cudaSuccess;
+    const int64_t tiles = (A.n_slices + kFineTileSlices - 1) / kFineTileSlices;
+    fine_stage_slots_ = (int32_t)stage_slots;
+    fine_tma_grid_ = (int)std::min<int64_t>(tiles, (int64_t)per_sm * sms);
+    AMG_CK(tma_err_.ensure(1));
+    AMG_CK(cudaMemsetAsync(tma_err_.p, 0, sizeof(int32_t), s));
+    fine_tma_ = true;
+    return cudaSuccess;
+}
+
+template <int MODE>
+void Amg::launch_fine(const int32_t *n_done, int32_t n_inst, const float *b, const float *invd, const float *x_in,
+                      float *x_out, float *d, float c0, float c1, float c2, cudaStream_t s) const {
+    const AmgMatrix &A = lv_[0].A;
+    FineTma F;
+    F.off = A.slice_off;
+    F.col = A.col;
+    F.hval = reinterpret_cast<const __half *>(fine_half_.p);
+    F.n = A.n;
+    F.n_slices = A.n_slices;
+    F.n_tiles = (A.n_slices + kFineTileSlices - 1) / kFineTileSlices;
+    F.stage_slots = fine_stage_slots_;
+    const size_t smem = (size_t)fine_stages_ * (size_t)fine_stage_slots_ * 6;
+    const int32_t *agg = n_levels_ > 1 ? lv_[0].agg.p : nullptr;
+    if (fine_stages_ == 4)
+        k_fine_tma<MODE, 4><<<fine_tma_grid_, 256, smem, s>>>(Gate{n_done, n_inst}, F, b, invd, x_in, x_out, d, c0, c1,
+                                                              c2, agg, tma_err_.p);
+    else
+        k_fine_tma<MODE, 2><<<fine_tma_grid_, 256, smem, s>>>(Gate{n_done, n_inst}, F, b, invd, x_in, x_out, d, c0, c1,
+                                                              c2, agg, tma_err_.p);
+}
+
+bool Amg::fine_tma_failed(cudaStream_t s) {
+    if (!fine_tma_) return false;
+    int32_t e = 0;
+    if (cudaMemcpyAsync(&e, tma_err_.p, sizeof(e), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return true;
+    if (e) cudaMemsetAsync(tma_err_.p, 0, sizeof(int32_t), s);
+    return e != 0;
+}
+
 cudaError_t Amg::apply(const float *r, float *z, const int32_t *n_done, int32_t n_inst, cudaStream_t s,
                        AmgProf *prof) {
     return cycle(0, r, z, n_done, n_inst, s, prof, nullptr);
@@ -2454,6 +2707,8 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
     std::vector<float *> xout(nl);
     // the levels from tail_level_ down run as one cluster launch (the cycle from level 0 only)
     const bool use_tail = tail_phases_ > 0 && tail_level_ > l0;
+    // the fine level's kernels stream its FP16 matrix through shared memory (k_fine_tma)
+    const bool tma0 = fine_tma_ && opt_.half_fine && l0 == 0;
     for (int l = l0; l < (use_tail ? tail_level_ : nl - 1); ++l) {
         AmgLevel &L = lv_[l];
         const float *b = l == 0 ? r : L.b.p;
@@ -2471,6 +2726,9 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
             if (fine_w_)
                 k_sm_first_step_w<<<g, 256, 0, s>>>(gate_, A, b, fw(), xo, L.d.p, (float)c2[0], (float)c1[1],
                                                     (float)c2[1], L.agg.p);
+            else if (tma0)
+                launch_fine<kFineFirst>(n_done, n_inst, b, nullptr, nullptr, xo, L.d.p, (float)c2[0], (float)c1[1],
+                                        (float)c2[1], s);
             else
                 k_sm_first_step<<<g, 256, 0, s>>>(gate_, A, b, xo, L.d.p, (float)c2[0], (float)c1[1], (float)c2[1],
                                                   L.agg.p);
@@ -2483,13 +2741,19 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         // (coarser levels: the first step was fused into the restriction from the level above)
         for (int k = k0; k < pre; ++k) {
             if (l == 0) rec_step(true);
-            sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
+            if (l == 0 && tma0)
+                launch_fine<kFineStep>(n_done, n_inst, b, invd, xi, xo, L.d.p, 0.f, (float)c1[k], (float)c2[k], s);
+            else
+                sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], L.agg.p);
             long_rows(L.A, 0, b, invd, xi, xo, L.d.p, (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             std::swap(xi, xo);
         }
         xout[l] = xi;
-        residual_kernel(L.g)<<<gs, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
+        if (l == 0 && tma0)
+            launch_fine<kFineResid>(n_done, n_inst, b, nullptr, xi, L.r.p, nullptr, 0.f, 0.f, 0.f, s);
+        else
+            residual_kernel(L.g)<<<gs, 256, 0, s>>>(gate_, A, b, xi, L.r.p);
         long_rows(L.A, 1, b, nullptr, xi, L.r.p, nullptr, 0.f, 0.f, nullptr);
         AmgLevel &C = lv_[l + 1];
         const float *wt = l == 0 ? w0_used_ : nullptr;
@@ -2563,8 +2827,12 @@ cudaError_t Amg::cycle(int l0, const float *r, float *z, const int32_t *n_done, 
         for (int k = 0; k < deg; ++k) {
             float *xo = (l == 0 && k == deg - 1) ? z : other;
             if (l == 0) rec_step(true);
-            sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k],
-                                       L.agg.p);
+            if (l == 0 && tma0)
+                launch_fine<kFineStep>(n_done, n_inst, b, invd, xi, xo, L.d.p, 0.f, k == 0 ? 0.f : (float)c1[k],
+                                       (float)c2[k], s);
+            else
+                sm_step<<<gs, 256, 0, s>>>(gate_, A, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k],
+                                           (float)c2[k], L.agg.p);
             long_rows(L.A, 0, b, invd, xi, xo, L.d.p, k == 0 ? 0.f : (float)c1[k], (float)c2[k], nullptr);
             if (l == 0) rec_step(false);
             other = xi;

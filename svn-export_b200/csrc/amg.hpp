@@ -51,6 +51,9 @@ struct AmgOptions {
     float coarse_ratio = 50.f;  // ... on [hi / coarse_ratio, hi]
     int stall_rows = 32768; // after two coarsenings in a row that kept more than half of the rows, a
                             // next level of at most this many rows is the coarsest (0: off)
+    int fine_tma = 0;       // 1: the fine level's cycle kernels stream the matrix through shared
+                            // memory with TMA bulk copies (with half_fine; amg.cu k_fine_tma)
+    int fine_tma_stages = 4;  // ... in a ring of 2 or 4 stages
     int tail_rows = 0;      // levels (below the fine one) from which every level has at most this
                             // many rows run in one cluster launch (0: every level on its own)
 };
@@ -118,6 +121,10 @@ public:
     int64_t coarse_rows() const { return n_levels_ ? lv_[n_levels_ - 1].A.n : 0; }
     // the first level of the coarse tail run as one cluster launch (0: none) and its CTAs
     int tail_level() const { return tail_phases_ > 0 ? tail_level_ : 0; }
+    // the fine level's kernels stream the matrix with TMA; a stage wait that timed out (read
+    // back and cleared: the cycle's results are then not usable)
+    bool fine_tma() const { return fine_tma_; }
+    bool fine_tma_failed(cudaStream_t s);
     int tail_cluster() const { return tail_cluster_; }
     int kernels_per_apply() const;
     const float *fine_weights() const { return w0_used_; }  // null when the transfers are unweighted
@@ -207,6 +214,18 @@ private:
     DBuf<double> pw_part_, pw_sums_;  // its per-block partial norms and the two norms per level
     DBuf<float> w0_;                // sqrt(diag S) per fine row
     DBuf<uint16_t> fine_half_;      // FP16 bits of the fine matrix's values (half_fine)
+    // the fine level's TMA-staged cycle kernels (k_fine_tma): ready, stage size, grid, the
+    // widest tile read at setup and the stage-wait error flag
+    bool fine_tma_ = false;
+    int fine_stages_ = 4;
+    int32_t fine_stage_slots_ = 0;
+    int fine_tma_grid_ = 0;
+    DBuf<unsigned int> tile_max_;
+    DBuf<int32_t> tma_err_;
+    cudaError_t prepare_fine_tma(unsigned int widest, cudaStream_t s);
+    template <int MODE>
+    void launch_fine(const int32_t *n_done, int32_t n_inst, const float *b, const float *invd, const float *x_in,
+                     float *x_out, float *d, float c0, float c1, float c2, cudaStream_t s) const;
     // the coarse tail: levels tail_level_ .. coarsest of the cycle from level 0 as one cluster
     // launch running a list of phases (amg.cu, k_tail)
     cudaError_t build_tail(cudaStream_t s);

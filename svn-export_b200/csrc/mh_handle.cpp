@@ -1045,6 +1045,8 @@ mh::AmgOptions amg_options() {
     env_i("MH_AMG_TAIL", o.tail_rows, 0, 1 << 22);
     env_i("MH_AMG_LEVELS", o.max_levels, 2, 20);
     env_i("MH_AMG_CDEG", o.coarse_degree, 1, 64);
+    env_i("MH_AMG_TMA", o.fine_tma, 0, 1);
+    env_i("MH_AMG_TMA_STAGES", o.fine_tma_stages, 2, 4);
     env_i("MH_AMG_STALL", o.stall_rows, 0, 1 << 24);
     if (const char *e = getenv("MH_AMG_CRATIO")) {
         const float x = (float)atof(e);
@@ -1493,6 +1495,10 @@ int solve_impl(mh_handle *h, const mh_solve_opts *opts_in, mh_solve_stats *stats
             return MH_ERR_INVALID;
     }
     if (rc) return rc;
+    if ((o.method == MH_SOLVER_AMG || o.method == MH_SOLVER_FCG_LEARNED) && h->amg.fine_tma_failed(h->stream)) {
+        h->err = "multigrid: a fine-level shared-memory stage did not complete (bounded wait timed out)";
+        return MH_ERR_CUDA;
+    }
     if (res.status == MH_OK && res.fell_back) res.status = MH_FELL_BACK;
     CK(cudaEventRecord(h->ev[3], h->stream));
     CK(mh::launch_backsub(h->ed, h->as, h->sys, h->sol, h->topo.n_sides(), h->mesh.n_el, h->topo.n_edges(),
