@@ -383,16 +383,21 @@ typedef struct mh_tune_result {
     int32_t rows_per_thread;    /* R of the Krylov kernels (mh_autotune)                  */
     int32_t sell_rows_per_warp; /* rows one warp's SELL-32 tile covers: 32 R              */
     int32_t k1_group;           /* elements per K1 block (one per thread): 64, 128 or 256 */
-    int32_t reserved_i;
+    int32_t amg_fine_passes;    /* multigrid pairing passes from the fine level: 2 or 3
+                                   (0: not tuned, MH_AMG_PASSES set)                       */
     double  us_per_iter_fp32;   /* FP32 CG iteration at R                                  */
     double  us_per_iter_fp64;   /* FP64 CG iteration at R                                  */
     double  us_assembly;        /* K1 + gather at k1_group (median of three)               */
-    double  reserved[3];
+    double  ms_amg_solve;       /* complete MH_SOLVER_AMG solve (setup included), host clock,
+                                   at amg_fine_passes                                       */
+    double  reserved[2];
 } mh_tune_result;
 
-/* mh_autotune, then the element group of the assembly's K1 kernel: the matrix and rhs are
- * assembled again (same values) three times per group size and the fastest median is kept
- * for every later assembly. */
+/* mh_autotune, then the element group of the assembly's K1 kernel (the matrix and rhs are
+ * assembled again, same values, three times per group size; the fastest median is kept for
+ * every later assembly), then the multigrid's pairing passes from the fine level (2 or 3: two
+ * complete MH_SOLVER_AMG solves of the assembled system each, hierarchy rebuilt; the faster is
+ * kept for the handle's later multigrid solves).  The solves overwrite the solution. */
 int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out);
 
 /* ---- unsteady MH (DarcyFlowMH_Unsteady, darcy_flow_mh.cc:1601-1675) ----------------- */

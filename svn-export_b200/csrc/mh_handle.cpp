@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -84,6 +85,7 @@ struct mh_handle {
     int loop_iters[2] = {0, 0};
     int32_t *d_loop = nullptr;  // {bodies run, body cap} of the device-side loop
     int k1_group = 128;         // elements per K1 block (mh_autotune_ex)
+    int amg_fine_passes = 0;    // pairing passes from the fine level chosen by mh_autotune_ex (0: default)
     bool host_loop = false;     // the current solve polls from the host instead (mh_solve_opts)
     std::vector<cudaEvent_t> prof_ev[2];
     int32_t *h_done = nullptr;
@@ -1059,6 +1061,14 @@ mh::AmgOptions amg_options() {
     return o;
 }
 
+// the options with what mh_autotune_ex chose for this handle
+mh::AmgOptions amg_options_for(const mh_handle *h) {
+    mh::AmgOptions o = amg_options();
+    if (h->amg_fine_passes > 0) o.pair_passes = h->amg_fine_passes;
+    return o;
+}
+
+
 // The multigrid preconditioner for the current matrix, with the fine level's smoother weights
 // of the method: the network's (learned method), the caller's (mh_smoother_weights_set), or
 // none.  The hierarchy is rebuilt when the matrix changed (ms_setup: its device time, else 0);
@@ -1096,7 +1106,7 @@ int prepare_multigrid(mh_handle *h, Pc kind, double &ms_setup) {
         h->amg_epoch += 1;
         h->amg_matrix_epoch = h->matrix_epoch;
         CK(cudaEventRecord(h->ev[6], h->stream));
-        cudaError_t e = h->amg.setup(h->sys, amg_options(), h->stream);
+        cudaError_t e = h->amg.setup(h->sys, amg_options_for(h), h->stream);
         CK(cudaEventRecord(h->ev[7], h->stream));
         CK(cudaEventSynchronize(h->ev[7]));
         float ms = 0.f;
@@ -1248,8 +1258,8 @@ int ensure_train(mh_handle *h, int n_pairs) {
 // Multigrid options of training: the cycle without the energy-optimal coarse scaling (so that
 // it is linear in the residual and its adjoint exact) and with FP32 fine values (those of the
 // adjoint's products)
-mh::AmgOptions training_amg_options() {
-    mh::AmgOptions o = amg_options();
+mh::AmgOptions training_amg_options(const mh_handle *h) {
+    mh::AmgOptions o = amg_options_for(h);
     o.kcycle = 0;
     o.half_fine = 0;
     return o;
@@ -1389,7 +1399,7 @@ int training_setup(mh_handle *h) {
         if ((rc = apply_launch_shape(h, 1, t))) return rc;
     }
     h->amg.set_fine_weights(h->sn_w);
-    cudaError_t e = h->amg.setup(h->sys, training_amg_options(), h->stream);
+    cudaError_t e = h->amg.setup(h->sys, training_amg_options(h), h->stream);
     h->amg_epoch += 1;
     h->amg_matrix_epoch = -1;  // the next solve builds the solver's hierarchy again
     h->amg_training = true;
@@ -2498,6 +2508,42 @@ int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out) {
     out->k1_group = best_g;
     out->us_assembly = best;
     out->sell_rows_per_warp = 32 * R;
+    // the multigrid's pairing passes from the fine level (aggregates of up to 4 or 8 fine rows):
+    // which one converges faster depends on the system (hub-dominated fractured systems gain
+    // from the larger aggregates, smooth ones lose), so each is timed on this system: two
+    // complete solves to 1e-10 with the hierarchy rebuilt for each, the faster of the two kept
+    // unless MH_AMG_PASSES fixes the count
+    if (!getenv("MH_AMG_PASSES")) {
+        double best_ms = 1e300;
+        int best_p = 2;
+        for (int p : {2, 3}) {
+            h->amg_fine_passes = p;
+            double t_min = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {
+                mh_solve_opts so;
+                mh_solve_opts_default(&so);
+                so.method = MH_SOLVER_AMG;
+                so.r_tol = 1e-10;
+                mh_solve_stats st;
+                std::memset(&st, 0, sizeof(st));
+                h->amg_matrix_epoch = -1;  // the setup is part of what is timed
+                const auto t0 = std::chrono::steady_clock::now();
+                rc = solve_impl(h, &so, &st, false);
+                const double ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                if (rc < 0) return rc;
+                if (st.status == MH_OK || st.status == MH_FELL_BACK) t_min = std::min(t_min, ms);
+            }
+            if (t_min < best_ms) {
+                best_ms = t_min;
+                best_p = p;
+            }
+        }
+        h->amg_fine_passes = best_p;
+        h->amg_matrix_epoch = -1;  // the next solve builds the hierarchy with the choice
+        out->amg_fine_passes = best_p;
+        out->ms_amg_solve = best_ms < 1e299 ? best_ms : 0.0;
+    }
     return MH_OK;
 }
 

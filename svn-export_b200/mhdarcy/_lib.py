@@ -98,8 +98,8 @@ class SolveStats(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("rows_per_thread", C.c_int32), ("sell_rows_per_warp", C.c_int32), ("k1_group", C.c_int32),
-                ("reserved_i", C.c_int32), ("us_per_iter_fp32", C.c_double), ("us_per_iter_fp64", C.c_double),
-                ("us_assembly", C.c_double), ("reserved", C.c_double * 3)]
+                ("amg_fine_passes", C.c_int32), ("us_per_iter_fp32", C.c_double), ("us_per_iter_fp64", C.c_double),
+                ("us_assembly", C.c_double), ("ms_amg_solve", C.c_double), ("reserved", C.c_double * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}

@@ -93,6 +93,9 @@ def test_autotune_keeps_results(gpu):
         assert tune["rows_per_thread"] in (1, 2, 4) and tune["us_per_iter_fp32"] > 0
         assert tune["sell_rows_per_warp"] == 32 * tune["rows_per_thread"]
         assert tune["k1_group"] in (64, 128, 256) and tune["us_assembly"] > 0
+        assert tune["amg_fine_passes"] in (2, 3) and tune["ms_amg_solve"] > 0
+        st = s.solve(method=_lib.MH_SOLVER_AMG, r_tol=1e-10)
+        assert st["status"] == 0
         # the assembly with the chosen element group gives the same system bit for bit
         s.assemble()
         rp1, col1, val1, rhs1 = s.schur_system()
