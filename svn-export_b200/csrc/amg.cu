@@ -846,15 +846,17 @@ __global__ void k_dense_gemv(Gate gate, const float *__restrict__ inv, int64_t n
 // instead of one dependent load chain per slot; coarse rows (longer, irregular) loop.
 // the fine level's row: slots loaded 8 at a time, values from FP32 or their FP16 copy
 template <bool HALF>
+// The slots are a stream read once per pass: loaded evict-first (ld.global.cs) so that they
+// do not push the gathered vector out of L2.
 __device__ __forceinline__ float fine_dot(const MatView &A, int64_t base, int w, int ln, const float *__restrict__ x) {
-    auto value = [&](int64_t slot) { return HALF ? __half2float(A.hval[slot]) : __ldg(A.val + slot); };
+    auto value = [&](int64_t slot) { return HALF ? __half2float(__ldcs(A.hval + slot)) : __ldcs(A.val + slot); };
     constexpr int kB = 8;
     int32_t c[kB];
     float v[kB];
 #pragma unroll
     for (int k = 0; k < kB; ++k) {
         const int64_t slot = base + (int64_t)k * kS + ln;
-        c[k] = k < w ? __ldg(A.col + slot) : 0;
+        c[k] = k < w ? __ldcs(A.col + slot) : 0;
         v[k] = k < w ? value(slot) : 0.f;
     }
     float g[kB];
@@ -865,7 +867,7 @@ __device__ __forceinline__ float fine_dot(const MatView &A, int64_t base, int w,
     for (int k = 0; k < kB; ++k) y += v[k] * g[k];
     for (int j = kB; j < w; ++j) {
         const int64_t slot = base + (int64_t)j * kS + ln;
-        y += value(slot) * x[__ldg(A.col + slot)];
+        y += value(slot) * x[__ldcs(A.col + slot)];
     }
     return y;
 }
