@@ -748,6 +748,8 @@ def run_ours(a, rank, world):
         "data": "synthetic: seeded fractured Kuhn cube, log-normal conductivity (no public dataset)",
         "config": workload_config(a.config, N, Z, sz.mh_size, ne),
         "method": best, "instances_per_step": per_step,
+        "method_note": ("value is the fastest converged method's (%s); every method's figure, the learned "
+                        "one's (fcg) included, is under methods and speedup_vs_pcg64" % best),
         "parallelism": ("batch sharded over ranks" if a.config == 3 else "replicas") if world > 1 else "single GPU",
         "autotune": tune,
         "e2e": {"value": round(world * per_step * a.steps / (ms_e2e / 1e3), 4), "unit": "solves/s",
