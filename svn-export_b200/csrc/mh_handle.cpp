@@ -87,6 +87,7 @@ struct mh_handle {
     int k1_group = 128;         // elements per K1 block (mh_autotune_ex)
     int amg_fine_passes = 0;    // pairing passes from the fine level chosen by mh_autotune_ex (0: default)
     bool host_loop = false;     // the current solve polls from the host instead (mh_solve_opts)
+    bool loop_unavailable = false;  // the device-side loop could not be built: poll from the host
     std::vector<cudaEvent_t> prof_ev[2];
     int32_t *h_done = nullptr;
     cudaEvent_t ev[8] = {};
@@ -584,7 +585,11 @@ int run_krylov_loop(mh_handle *h, int prec, int ipg, int max_it) {
 // from the in-graph events.
 int run_krylov(mh_handle *h, int prec, int ipg, int max_it, bool prof) {
     ipg = std::max(1, ipg);  // an empty graph would never make progress
-    if (!prof && !h->host_loop) return run_krylov_loop(h, prec, ipg, max_it);
+    if (!prof && !h->host_loop && !h->loop_unavailable) {
+        const int rc = run_krylov_loop(h, prec, ipg, max_it);
+        if (rc != MH_ERR_CUDA || h->loop_graph[prec == 64 ? 0 : 1]) return rc;
+        h->loop_unavailable = true;  // the loop graph itself failed: the host-polled form
+    }
     const int gi = prec == 64 ? 0 : 1, pi = prof ? 1 : 0;
     int rc = capture_iterations(h, prec, ipg, prof);
     if (rc) return rc;
@@ -909,7 +914,7 @@ void drop_fcg_graph(mh_handle *h) {
 int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, int max_it, bool prof) {
     ipg = std::max(1, ipg);  // an empty graph would never make progress
     prof = prof && (kind == Pc::Amg || kind == Pc::Nn);
-    const bool loop = !prof && !h->host_loop;
+    const bool loop = !prof && !h->host_loop && !h->loop_unavailable;
     const FcgKey key{(int)kind, ipg, degree, lo, hi, h->amg_epoch, prof, loop};
     if (prof) {
         const int steps = h->amg.fine_steps();
@@ -937,7 +942,10 @@ int run_fcg(mh_handle *h, Pc kind, int degree, double lo, double hi, int ipg, in
                     return b;
                 },
                 &g);
-            if (rc) return rc;
+            if (rc) {  // the loop graph itself failed: the host-polled form from now on
+                h->loop_unavailable = true;
+                return run_fcg(h, kind, degree, lo, hi, ipg, max_it, prof);
+            }
         } else {
             CK(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < ipg && e == cudaSuccess; ++k)
