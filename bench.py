@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--pcg-accuracy", action="store_true", help="also time pcg64 at r_tol 1e-12 in the error block")
     ap.add_argument("--extra-config", default="2,3",
                     help="comma list of further workloads timed with fewer steps, reported under `extra` (0: none)")
+    ap.add_argument("--extra-unsteady", type=int, default=100, metavar="K",
+                    help="also time the cfg4 unsteady protocol for K steps under extra.cfg4_unsteady (0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-precond", choices=["jacobi", "ilu0", "ilu3"], default="jacobi",
                     help="preconditioner of the CPU path's CG: Jacobi (threaded throughout; the faster CPU solve on "
@@ -231,6 +233,10 @@ def roofline(stats_list, N, Z, peaks):
 
 # ---------------------------------------------------------------- unsteady --------------
 def run_unsteady(a, rank, world):
+    print(json.dumps(unsteady_line(a)), flush=True)
+
+
+def unsteady_line(a):
     """K steps of the unsteady MH system (mh_unsteady_step: right-hand side from the previous
     pressures, solve, back-substitution) with the boundary pressure on x = 0 following
     1 + 0.5 sin(2 pi t); each method starts from zero pressure.  The matrix is the same in every
@@ -320,7 +326,7 @@ def run_unsteady(a, rank, world):
             "config": {"workload": "cfg%d: %s, dt %g, %d steps" % (a.config, WORKLOADS[a.config], dt, a.unsteady),
                        "window": "steps %d-%d (the learned method trains after step %d)" % (k0 + 1, a.unsteady, k0)},
             "method": best, "methods": out}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------- accuracy --------------
@@ -769,6 +775,13 @@ def run_ours(a, rank, world):
     extra = [c for c in extra if c != a.config]
     if extra and world == 1:
         out["extra"] = {"cfg%d" % c: run_extra_config(a, c, ["pcg64", "amg"], barrier) for c in extra}
+    if a.extra_unsteady > 0 and world == 1:
+        # the unsteady protocol of cfg4 (train the learned method after step 20, compare steps
+        # 21..K), as in --config 4 --unsteady K
+        from types import SimpleNamespace
+        u = SimpleNamespace(**vars(a))
+        u.config, u.unsteady, u.warmup, u.methods = 4, a.extra_unsteady, 3, "pcg64,amg,fcg"
+        out.setdefault("extra", {})["cfg4_unsteady"] = unsteady_line(u)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
