@@ -382,7 +382,8 @@ int mh_autotune(mh_handle *h, int32_t iterations, int32_t *rows_per_thread, doub
 typedef struct mh_tune_result {
     int32_t rows_per_thread;    /* R of the Krylov kernels (mh_autotune)                  */
     int32_t sell_rows_per_warp; /* rows one warp's SELL-32 tile covers: 32 R              */
-    int32_t k1_group;           /* elements per K1 block (one per thread): 64, 128 or 256 */
+    int32_t k1_group;           /* elements per K1 block (one per thread): 64, 128 or 256;
+                                   0 for a general system (mh_csr_create: no assembly)      */
     int32_t amg_fine_passes;    /* multigrid pairing passes from the fine level: 2 or 3
                                    (0: not tuned, MH_AMG_PASSES set)                       */
     double  us_per_iter_fp32;   /* FP32 CG iteration at R                                  */

@@ -2495,6 +2495,7 @@ int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out) {
     double best = 1e300;
     int best_g = h->k1_group;
     for (int G : {64, 128, 256}) {
+        if (h->general) break;  // a general CSR system has no element assembly
         float t[3];
         for (float &tk : t) {
             CK(cudaEventRecord(h->ev[0], h->stream));
@@ -2513,8 +2514,8 @@ int mh_autotune_ex(mh_handle *h, int32_t iterations, mh_tune_result *out) {
         }
     }
     h->k1_group = best_g;
-    out->k1_group = best_g;
-    out->us_assembly = best;
+    out->k1_group = h->general ? 0 : best_g;
+    out->us_assembly = h->general ? 0.0 : best;
     out->sell_rows_per_warp = 32 * R;
     // the multigrid's pairing passes from the fine level (aggregates of up to 4 or 8 fine rows):
     // which one converges faster depends on the system (hub-dominated fractured systems gain
