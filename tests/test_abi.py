@@ -62,3 +62,41 @@ def test_invalid_arguments():
     assert _lib.lib.mh_create(None, C.byref(h)) == _lib.MH_ERR_INVALID
     h2 = C.c_void_p()
     assert _lib.lib.mh_cube_mesh_create(0, 0, None, None, 0, None, None, None, C.byref(h2)) == _lib.MH_ERR_INVALID
+
+
+STRUCTS = {  # C type in include/mh_darcy.h -> ctypes mirror in mhdarcy/_lib.py
+    "mh_mesh_desc": "MeshDesc", "mh_mortar_desc": "MortarDesc", "mh_gmsh_info": "GmshInfo",
+    "mh_sizes": "Sizes", "mh_coeffs": "Coeffs", "mh_bc": "BC", "mh_solve_opts": "SolveOpts",
+    "mh_solve_stats": "SolveStats", "mh_tune_result": "TuneResult", "mh_learn_opts": "LearnOpts",
+    "mh_learn_stats": "LearnStats",
+}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every public struct has the same size and field offsets in the header (compiled with
+    gcc) and in the ctypes mirror the Python bindings pass to the library."""
+    import ctypes
+    import shutil
+    import subprocess
+    from mhdarcy import _lib
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mh_darcy.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        py = getattr(_lib, pyname)
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for cname, pyname in STRUCTS.items():
+        py = getattr(_lib, pyname)
+        assert int(out["%s size" % cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(out["%s.%s" % (cname, f)]) == getattr(py, f).offset, (cname, f)
