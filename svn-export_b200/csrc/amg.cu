@@ -1234,11 +1234,13 @@ __global__ void __launch_bounds__(256) k_coarse_dots(Gate gate, MatView A, const
 // warp waits for its slots from DRAM before it can issue its gathers, and the kernel runs at
 // load latency (about 0.6 of the copy bandwidth).  Here a CTA streams tiles of 8 slices
 // (256 rows) through a ring of NST shared-memory stages with 1D bulk copies (cp.async.bulk,
-// completion counted on an mbarrier), so the DRAM stream runs NST - 1 tiles ahead of the warps, which read their slots from shared memory and only wait on the
-// gathers.  The row arithmetic and its summation order are those of k_sm_first_step, k_sm_step<1>
-// and k_residual<1> (bit-identical results).  Every wait is bounded: a stage that does not
-// complete in kFineSpin polls sets *err, and the CTA waits (bounded again) for its copies in
-// flight before it returns.
+// completion counted on an mbarrier), so the DRAM stream runs NST - 1 tiles ahead of the warps,
+// which read their slots from shared memory and only wait on the gathers.  The row arithmetic
+// and its summation order are those of k_sm_first_step, k_sm_step<1> and k_residual<1>
+// (bit-identical results).  Measured, it is no faster: the gathers, not the slots, set the
+// latency, and the stages halve the threads per SM (fine_tma, off by default).  Every wait is
+// bounded: a stage that does not complete in kFineSpin polls sets *err, and the CTA waits
+// (bounded again) for its copies in flight before it returns.
 constexpr int kFineTileSlices = 8;
 constexpr int kFineSpin = 1 << 22;
 
@@ -1416,7 +1418,8 @@ __global__ void k_fine_tile_max(const int64_t *__restrict__ off, int64_t n_slice
 // summation order (rows in 32-row slices with G warps each, the 256-thread groups of the long
 // rows and of the scaling's partial sums), so the tail gives the same bits as the separate
 // launches.  Vectors written by one phase are read by later ones through L2 (ld.global.cg);
-// the matrices through the read-only path.
+// the matrices through the read-only path.  Measured, a phase costs more than the launch it
+// saves (the chain of dependent L2 loads stays), so the tail is off by default (tail_rows).
 constexpr int kTailThreads = 1024, kTailWarps = kTailThreads / 32;
 constexpr int kTailGroups = kTailThreads / 256;  // 256-thread groups per CTA
 
